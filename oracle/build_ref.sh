@@ -1,0 +1,25 @@
+#!/usr/bin/env bash
+# Builds the reference's own mechanism kernels into oracle/_ref/libref_<mech>.so
+# (test infrastructure: used by tests, tests/golden/make_golden.py and the CPU
+# baseline only).  Reads the reference sources where they lie; copies nothing.
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+set -euo pipefail
+HERE="$(cd "$(dirname "$0")" && pwd)"
+REF="${1:-/root/reference}"
+OUT="$HERE/_ref"
+mkdir -p "$OUT"
+if [ ! -d "$REF/Mechanisms" ]; then
+  echo "build_ref: no reference tree at $REF; keeping prebuilt $OUT" >&2
+  exit 0
+fi
+for mech in LiDryer drm19 dodecane_lu heptane_lu_88sk; do
+  src="$REF/Mechanisms/$mech/mechanism.H"
+  lib="$OUT/libref_${mech}.so"
+  if [ -f "$lib" ] && [ "$lib" -nt "$src" ] && [ "$lib" -nt "$HERE/ref_wrap.cpp" ]; then
+    continue
+  fi
+  g++ -std=c++17 -O3 -march=x86-64-v3 -fPIC -shared -fvisibility=hidden \
+      -I"$HERE/amrex_stub" -I"$REF/Mechanisms/$mech" \
+      "$HERE/ref_wrap.cpp" -o "$lib.tmp"
+  mv "$lib.tmp" "$lib"
+done

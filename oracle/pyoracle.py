@@ -1,0 +1,396 @@
+"""ORACLE / TEST INFRASTRUCTURE ONLY: ctypes access to the CPU checker.
+
+Two libraries are wrapped:
+
+* ``oracle/liboracle.so`` -- the table-driven C restatement of the
+  reference's chemistry (mech_eval.c, reactor.c);
+* ``oracle/_ref/libref_<mech>.so`` -- the reference's own generated
+  ``mechanism.H`` kernels compiled on the host (ref_wrap.cpp).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg
+import this module, always as the checker.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+_LP = C.POINTER(C.c_long)
+_lib = None
+_ref = {}
+
+
+def _p(a):
+    return a.ctypes.data_as(_DP)
+
+
+def build():
+    subprocess.run(["bash", os.path.join(HERE, "build_oracle.sh")], check=True)
+    subprocess.run(["bash", os.path.join(HERE, "build_ref.sh")], check=True)
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("rtol", C.c_double),
+        ("atol", C.c_double),
+        ("max_order", C.c_int),
+        ("max_steps", C.c_long),
+        ("max_nls_iters", C.c_int),
+        ("max_err_fails", C.c_int),
+        ("jac_eval_freq", C.c_int),
+        ("use_ref_kernels", C.c_int),
+        ("rk64_nsubsteps_guess", C.c_int),
+        ("rk64_nsubsteps_min", C.c_int),
+        ("rk64_nsubsteps_max", C.c_int),
+        ("typ_vals", _DP),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("nsteps", C.c_long),
+        ("nfe", C.c_long),
+        ("nje", C.c_long),
+        ("nsetups", C.c_long),
+        ("nni", C.c_long),
+        ("ncfn", C.c_long),
+        ("netf", C.c_long),
+        ("status", C.c_int),
+        ("last_order", C.c_int),
+        ("last_h", C.c_double),
+    ]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            subprocess.run(["bash", os.path.join(HERE, "build_oracle.sh")], check=True)
+        L = C.CDLL(path)
+        L.ppo_mech.restype = C.c_void_p
+        L.ppo_mech.argtypes = [C.c_char_p]
+        L.ppo_nsp.argtypes = [C.c_char_p]
+        for fn in ("ppo_cv_R", "ppo_cp_R", "ppo_dcvpRdT", "ppo_species_internal_energy",
+                   "ppo_species_enthalpy", "ppo_gibbs", "ppo_ckums", "ppo_ckhms"):
+            getattr(L, fn).argtypes = [C.c_void_p, C.c_double, _DP]
+        for fn in ("ppo_ckubms", "ppo_ckhbms", "ppo_ckcvbs", "ppo_ckcpbs"):
+            getattr(L, fn).argtypes = [C.c_void_p, C.c_double, _DP]
+            getattr(L, fn).restype = C.c_double
+        L.ppo_ckrhoy.argtypes = [C.c_void_p, C.c_double, C.c_double, _DP]
+        L.ppo_ckrhoy.restype = C.c_double
+        L.ppo_get_t_given_ey.argtypes = [C.c_void_p, C.c_double, _DP, _DP]
+        L.ppo_get_t_given_hy.argtypes = [C.c_void_p, C.c_double, _DP, _DP]
+        L.ppo_production_rate.argtypes = [C.c_void_p, _DP, _DP, C.c_double]
+        L.ppo_ckwc.argtypes = [C.c_void_p, C.c_double, _DP, _DP]
+        L.ppo_ajacobian.argtypes = [C.c_void_p, _DP, _DP, C.c_double, C.c_int]
+        L.ppo_dwdot.argtypes = [C.c_void_p, _DP, _DP, C.c_double, C.c_int]
+        L.ppo_reactor_rhs.argtypes = [C.c_void_p, C.c_int, C.c_double, _DP, _DP, C.c_double,
+                                      C.c_double, _DP]
+        L.ppo_reactor_rhs.restype = C.c_double
+        L.ppo_reactor_jac.argtypes = [C.c_void_p, C.c_int, _DP, _DP]
+        L.ppo_default_options.argtypes = [C.POINTER(Options)]
+        L.ppo_bdf_cell.argtypes = [C.c_void_p, C.c_int, C.POINTER(Options), _DP, _DP, C.c_double,
+                                   C.c_double, C.c_double, C.POINTER(Stats)]
+        L.ppo_rk64_cell.argtypes = [C.c_void_p, C.c_int, C.POINTER(Options), _DP, _DP, C.c_double,
+                                    C.c_double, C.c_double]
+        L.ppo_react_flat.argtypes = [C.c_char_p, C.c_int, C.POINTER(Options), C.c_int, _DP, _DP,
+                                     _DP, _DP, C.c_double, C.c_int, C.c_int, _LP, _IP]
+        L.ppo_load_ref.argtypes = [C.c_char_p, C.c_char_p]
+        _lib = L
+    return _lib
+
+
+def ref_path(mech):
+    return os.path.join(HERE, "_ref", f"libref_{mech}.so")
+
+
+def have_ref(mech):
+    return os.path.exists(ref_path(mech))
+
+
+class Mech:
+    """Table-driven oracle for one mechanism."""
+
+    def __init__(self, name):
+        self.name = name
+        self.L = lib()
+        self.M = self.L.ppo_mech(name.encode())
+        if not self.M:
+            raise KeyError(name)
+        self.nsp = self.L.ppo_nsp(name.encode())
+
+    def _vecT(self, fn, T):
+        out = np.zeros(self.nsp)
+        getattr(self.L, fn)(self.M, float(T), _p(out))
+        return out
+
+    def gibbs(self, T):
+        return self._vecT("ppo_gibbs", T)
+
+    def cv_R(self, T):
+        return self._vecT("ppo_cv_R", T)
+
+    def cp_R(self, T):
+        return self._vecT("ppo_cp_R", T)
+
+    def species_internal_energy(self, T):
+        return self._vecT("ppo_species_internal_energy", T)
+
+    def species_enthalpy(self, T):
+        return self._vecT("ppo_species_enthalpy", T)
+
+    def ckums(self, T):
+        return self._vecT("ppo_ckums", T)
+
+    def ckhms(self, T):
+        return self._vecT("ppo_ckhms", T)
+
+    def ckubms(self, T, y):
+        y = np.ascontiguousarray(y, float)
+        return self.L.ppo_ckubms(self.M, float(T), _p(y))
+
+    def ckhbms(self, T, y):
+        y = np.ascontiguousarray(y, float)
+        return self.L.ppo_ckhbms(self.M, float(T), _p(y))
+
+    def ckcvbs(self, T, y):
+        y = np.ascontiguousarray(y, float)
+        return self.L.ppo_ckcvbs(self.M, float(T), _p(y))
+
+    def ckcpbs(self, T, y):
+        y = np.ascontiguousarray(y, float)
+        return self.L.ppo_ckcpbs(self.M, float(T), _p(y))
+
+    def ckrhoy(self, P, T, y):
+        y = np.ascontiguousarray(y, float)
+        return self.L.ppo_ckrhoy(self.M, float(P), float(T), _p(y))
+
+    def t_given_ey(self, e, y, T0):
+        y = np.ascontiguousarray(y, float)
+        t = np.array([T0], float)
+        ierr = self.L.ppo_get_t_given_ey(self.M, float(e), _p(y), _p(t))
+        return t[0], ierr
+
+    def t_given_hy(self, h, y, T0):
+        y = np.ascontiguousarray(y, float)
+        t = np.array([T0], float)
+        ierr = self.L.ppo_get_t_given_hy(self.M, float(h), _p(y), _p(t))
+        return t[0], ierr
+
+    def production_rate(self, sc, T):
+        sc = np.ascontiguousarray(sc, float)
+        w = np.zeros(self.nsp)
+        self.L.ppo_production_rate(self.M, _p(w), _p(sc), float(T))
+        return w
+
+    def ajacobian(self, sc, T, consP):
+        sc = np.ascontiguousarray(sc, float)
+        J = np.zeros((self.nsp + 1) ** 2)
+        self.L.ppo_ajacobian(self.M, _p(J), _p(sc), float(T), int(consP))
+        return J
+
+    def reactor_rhs(self, reactor_type, t, y, rhoe, rhoesrc, src):
+        y = np.ascontiguousarray(y, float)
+        src = np.ascontiguousarray(src, float)
+        f = np.zeros(self.nsp + 1)
+        T = self.L.ppo_reactor_rhs(self.M, reactor_type, float(t), _p(y), _p(f), float(rhoe),
+                                   float(rhoesrc), _p(src))
+        return f, T
+
+    def reactor_jac(self, reactor_type, y):
+        y = np.ascontiguousarray(y, float)
+        J = np.zeros((self.nsp + 1) ** 2)
+        self.L.ppo_reactor_jac(self.M, reactor_type, _p(y), _p(J))
+        return J.reshape(self.nsp + 1, self.nsp + 1)  # [col][row]
+
+
+def options(**kw):
+    o = Options()
+    lib().ppo_default_options(C.byref(o))
+    typ = kw.pop("typ_vals", None)
+    for k, v in kw.items():
+        setattr(o, k, v)
+    if typ is not None:
+        arr = np.ascontiguousarray(typ, float)
+        o._typ = arr
+        o.typ_vals = _p(arr)
+    return o
+
+
+def bdf_cell(mech, reactor_type, y, src, rhoe, rhoesrc, dt, **kw):
+    M = Mech(mech)
+    o = options(**kw)
+    if o.use_ref_kernels:
+        load_ref(mech)
+    y = np.array(y, float)
+    src = np.ascontiguousarray(src, float)
+    st = Stats()
+    flag = M.L.ppo_bdf_cell(M.M, reactor_type, C.byref(o), _p(y), _p(src), float(rhoe),
+                            float(rhoesrc), float(dt), C.byref(st))
+    return y, flag, st
+
+
+def rk64_cell(mech, reactor_type, y, src, rhoe, rhoesrc, dt, **kw):
+    M = Mech(mech)
+    o = options(**kw)
+    if o.use_ref_kernels:
+        load_ref(mech)
+    y = np.array(y, float)
+    src = np.ascontiguousarray(src, float)
+    n = M.L.ppo_rk64_cell(M.M, reactor_type, C.byref(o), _p(y), _p(src), float(rhoe),
+                          float(rhoesrc), float(dt))
+    return y, n
+
+
+def react_flat(mech, reactor_type, rY, rYsrc, rX, rX_src, dt, method=0, nthreads=0, **kw):
+    """Per-cell CPU integration of YCOrder arrays (modified in place)."""
+    o = options(**kw)
+    if o.use_ref_kernels:
+        load_ref(mech)
+    ncells = rX.shape[0]
+    nfe = np.zeros(ncells, dtype=np.int64)
+    st = np.zeros(ncells, dtype=np.int32)
+    flag = lib().ppo_react_flat(mech.encode(), reactor_type, C.byref(o), method, _p(rY), _p(rYsrc),
+                                _p(rX), _p(rX_src), float(dt), ncells, nthreads,
+                                nfe.ctypes.data_as(_LP), st.ctypes.data_as(_IP))
+    return flag, nfe, st
+
+
+def load_ref(mech):
+    rc = lib().ppo_load_ref(mech.encode(), ref_path(mech).encode())
+    if rc != 0:
+        raise RuntimeError(f"cannot load reference kernels for {mech}: {rc}")
+
+
+class Ref:
+    """The reference's own compiled mechanism kernels (oracle/_ref)."""
+
+    def __init__(self, mech):
+        if mech in _ref:
+            self.L = _ref[mech]
+        else:
+            path = ref_path(mech)
+            if not os.path.exists(path):
+                raise FileNotFoundError(path)
+            L = C.CDLL(path)
+            for fn in ("ref_productionRate",):
+                getattr(L, fn).argtypes = [_DP, _DP, C.c_double]
+            L.ref_CKWC.argtypes = [C.c_double, _DP, _DP]
+            L.ref_aJacobian.argtypes = [_DP, _DP, C.c_double, C.c_int]
+            L.ref_DWDOT.argtypes = [_DP, _DP, C.c_double, C.c_int]
+            for fn in ("ref_gibbs", "ref_speciesInternalEnergy", "ref_speciesEnthalpy", "ref_cv_R",
+                       "ref_cp_R", "ref_dcvpRdT", "ref_CKUMS", "ref_CKHMS"):
+                getattr(L, fn).argtypes = [_DP, C.c_double] if fn not in ("ref_CKUMS", "ref_CKHMS") \
+                    else [C.c_double, _DP]
+            for fn in ("ref_CKUBMS", "ref_CKHBMS", "ref_CKCVBS", "ref_CKCPBS"):
+                getattr(L, fn).argtypes = [C.c_double, _DP]
+                getattr(L, fn).restype = C.c_double
+            L.ref_CKRHOY.argtypes = [C.c_double, C.c_double, _DP]
+            L.ref_CKRHOY.restype = C.c_double
+            L.ref_GET_T_GIVEN_EY.argtypes = [C.c_double, _DP, _DP]
+            L.ref_GET_T_GIVEN_HY.argtypes = [C.c_double, _DP, _DP]
+            L.ref_reactor_rhs.argtypes = [C.c_int, C.c_double, _DP, _DP, C.c_double, C.c_double, _DP]
+            L.ref_reactor_rhs.restype = C.c_double
+            L.ref_reactor_jac.argtypes = [C.c_int, _DP, _DP]
+            L.ref_mw.argtypes = [_DP]
+            L.ref_imw.argtypes = [_DP]
+            _ref[mech] = L
+            self.L = L
+        self.nsp = self.L.ref_nsp()
+
+    def mw(self):
+        a = np.zeros(self.nsp)
+        self.L.ref_mw(_p(a))
+        return a
+
+    def imw(self):
+        a = np.zeros(self.nsp)
+        self.L.ref_imw(_p(a))
+        return a
+
+    def production_rate(self, sc, T):
+        sc = np.ascontiguousarray(sc, float)
+        w = np.zeros(self.nsp)
+        self.L.ref_productionRate(_p(w), _p(sc), float(T))
+        return w
+
+    def ajacobian(self, sc, T, consP):
+        sc = np.ascontiguousarray(sc, float)
+        J = np.zeros((self.nsp + 1) ** 2)
+        self.L.ref_aJacobian(_p(J), _p(sc), float(T), int(consP))
+        return J
+
+    def vecT(self, fn, T):
+        out = np.zeros(self.nsp)
+        getattr(self.L, fn)(_p(out), float(T))
+        return out
+
+    def gibbs(self, T):
+        return self.vecT("ref_gibbs", T)
+
+    def species_internal_energy(self, T):
+        return self.vecT("ref_speciesInternalEnergy", T)
+
+    def species_enthalpy(self, T):
+        return self.vecT("ref_speciesEnthalpy", T)
+
+    def cv_R(self, T):
+        return self.vecT("ref_cv_R", T)
+
+    def cp_R(self, T):
+        return self.vecT("ref_cp_R", T)
+
+    def ckums(self, T):
+        out = np.zeros(self.nsp)
+        self.L.ref_CKUMS(float(T), _p(out))
+        return out
+
+    def ckhms(self, T):
+        out = np.zeros(self.nsp)
+        self.L.ref_CKHMS(float(T), _p(out))
+        return out
+
+    def ckubms(self, T, y):
+        return self.L.ref_CKUBMS(float(T), _p(np.ascontiguousarray(y, float)))
+
+    def ckhbms(self, T, y):
+        return self.L.ref_CKHBMS(float(T), _p(np.ascontiguousarray(y, float)))
+
+    def ckcvbs(self, T, y):
+        return self.L.ref_CKCVBS(float(T), _p(np.ascontiguousarray(y, float)))
+
+    def ckcpbs(self, T, y):
+        return self.L.ref_CKCPBS(float(T), _p(np.ascontiguousarray(y, float)))
+
+    def ckrhoy(self, P, T, y):
+        return self.L.ref_CKRHOY(float(P), float(T), _p(np.ascontiguousarray(y, float)))
+
+    def t_given_ey(self, e, y, T0):
+        t = np.array([T0], float)
+        ierr = self.L.ref_GET_T_GIVEN_EY(float(e), _p(np.ascontiguousarray(y, float)), _p(t))
+        return t[0], ierr
+
+    def t_given_hy(self, h, y, T0):
+        t = np.array([T0], float)
+        ierr = self.L.ref_GET_T_GIVEN_HY(float(h), _p(np.ascontiguousarray(y, float)), _p(t))
+        return t[0], ierr
+
+    def reactor_rhs(self, reactor_type, t, y, rhoe, rhoesrc, src):
+        y = np.ascontiguousarray(y, float)
+        f = np.zeros(self.nsp + 1)
+        T = self.L.ref_reactor_rhs(reactor_type, float(t), _p(y), _p(f), float(rhoe),
+                                   float(rhoesrc), _p(np.ascontiguousarray(src, float)))
+        return f, T
+
+    def reactor_jac(self, reactor_type, y):
+        J = np.zeros((self.nsp + 1) ** 2)
+        self.L.ref_reactor_jac(reactor_type, _p(np.ascontiguousarray(y, float)), _p(J))
+        return J.reshape(self.nsp + 1, self.nsp + 1)
