@@ -1,0 +1,171 @@
+/*
+ * pelephysics_b200 -- C ABI of the B200 stiff-chemistry engine.
+ *
+ * The entry points mirror the reference's reactor interface
+ * (Source/Reactions/ReactorBase.H:13-106): a reactor is created by name
+ * (Source/Factory.H:72-81), initialised with a reactor type and a cell count
+ * (ReactorBase::init, ReactorBase.H:19), and advanced over a time step either
+ * on flat per-cell arrays (ReactorBase::react, ReactorBase.H:42-54) or on a
+ * box of Array4 views (ReactorBase::react, ReactorBase.H:25-40).  Plain
+ * pointers and sizes only; no CUDA or C++ types cross the boundary (streams
+ * are passed as void*, the value of a cudaStream_t).
+ *
+ * Every call returns 0 on success or a negative PPB_E* code; ppb_last_error()
+ * gives a message.  No call aborts the process or traps the GPU.
+ */
+#ifndef PELEPHYSICS_B200_H
+#define PELEPHYSICS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PPB_E_ARG (-1)      /* invalid argument */
+#define PPB_E_CUDA (-2)     /* CUDA runtime error */
+#define PPB_E_MECH (-3)     /* unknown mechanism */
+#define PPB_E_STATE (-4)    /* call out of order (e.g. react before init) */
+#define PPB_E_INTEGRATE (1) /* at least one cell failed to integrate (flat path of
+                               ReactorCvode.cpp:1639-1641 returns 1 too); per-cell
+                               flags via ppb_get_cell_status */
+
+/* reactor types (Source/Reactions/ReactorTypes.H:10-11) */
+#define PPB_REACTOR_E 1 /* internal energy / cv */
+#define PPB_REACTOR_H 2 /* enthalpy / cp */
+
+/* integration engine */
+#define PPB_ENGINE_PLAIN 0 /* one thread per cell, FP64 */
+#define PPB_ENGINE_TUNED 1 /* one warp per cell, persistent work queue */
+
+typedef struct ppb_reactor ppb_reactor;
+
+/* Options.  The first block carries the reference's ParmParse keys with the
+ * reference defaults (ReactorCvode.cpp:18-35, ReactorCvode.H:187-197,
+ * ReactorCvode.cpp:480-497, ReactorRK64.cpp:12-18); the second block is
+ * engine tuning. */
+typedef struct ppb_options {
+  double rtol;              /* ode.rtol, 1e-6 */
+  double atol;              /* ode.atol, 1e-10 */
+  int max_order;            /* cvode.max_order, 2 */
+  int max_steps;            /* CVodeSetMaxNumSteps, 10000 */
+  int max_nls_iters;        /* ode.max_nls_iters, 3 */
+  int max_err_fails;        /* CVodeSetMaxErrTestFails, 100 */
+  int jac_eval_freq;        /* CVodeSetJacEvalFrequency, 100 */
+  int clean_init_massfrac;  /* ode.clean_init_massfrac, 0 */
+  int rk64_nsubsteps_guess; /* ode.rk64_nsubsteps_guess, 10 */
+  int rk64_nsubsteps_min;   /* ode.rk64_nsubsteps_min, 5 */
+  int rk64_nsubsteps_max;   /* ode.rk64_nsubsteps_max, 500 */
+  int verbose;              /* ode.verbose, 0 */
+  int engine;               /* PPB_ENGINE_TUNED */
+  int lu_fp32;              /* factor I - gamma J in FP32 + FP64 refinement, 0 */
+  int refine_sweeps;        /* refinement sweeps with lu_fp32, 1 */
+  int warps_per_block;      /* tuned engine block size in warps, 0 = auto */
+  int use_graph;            /* replay react() as a captured CUDA graph, 1 */
+} ppb_options;
+
+/* An amrex::Array4<Real>-compatible view: element (i,j,k,n) lives at
+ * p[(i-lo[0]) + (j-lo[1])*jstride + (k-lo[2])*kstride + n*nstride]. */
+typedef struct ppb_array4 {
+  double* p;
+  long jstride, kstride, nstride;
+  int lo[3], hi[3]; /* inclusive bounds of the allocation */
+  int ncomp;
+} ppb_array4;
+
+typedef struct ppb_array4i {
+  int* p;
+  long jstride, kstride, nstride;
+  int lo[3], hi[3];
+  int ncomp;
+} ppb_array4i;
+
+/* Fill an options struct with the reference defaults. */
+void ppb_default_options(ppb_options* opt);
+
+/* Last error message of the calling thread. */
+const char* ppb_last_error(void);
+
+/* Mechanisms compiled into the library: returns the number of species and
+ * reactions of `mechanism`, or PPB_E_MECH. */
+int ppb_mechanism_info(const char* mechanism, int* nspecies, int* nreactions);
+/* Name of species k of `mechanism` (NULL when out of range). */
+const char* ppb_species_name(const char* mechanism, int k);
+
+/* Molecular weights (g/mol) of the species of `mechanism` (mechanism.H
+ * get_mw), written to the HOST array mw[N]. */
+int ppb_molecular_weights(const char* mechanism, double* mw);
+
+/* ReactorBase::create (Factory.H:72-81).  integrator is "ReactorCvode"
+ * (BDF, the ReactorCvode drop-in) or "ReactorRK64" (explicit RK64). */
+int ppb_create(const char* mechanism, const char* integrator, ppb_reactor** out);
+/* ReactorBase::init(reactor_type, ncells) (ReactorBase.H:19) with options. */
+int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* opt);
+/* ReactorBase::set_typ_vals_ode (ReactorBase.H:88, ReactorBase.cpp:6-31):
+ * N+1 typical values; atol becomes typ_vals[i] * atol. */
+int ppb_set_typ_vals(ppb_reactor* r, const double* typ_vals, int n);
+/* ReactorBase::close (ReactorBase.H:21) and destruction. */
+int ppb_close(ppb_reactor* r);
+void ppb_destroy(ppb_reactor* r);
+
+/* ReactorBase::react on flat YCOrder HOST arrays (ReactorBase.H:42-54;
+ * ReactorCvode.cpp:1491-1689, ReactorRK64.cpp:22-164):
+ *   rY[ncells*(N+1)]  rhoY_k then T per cell (in/out)
+ *   rYsrc[ncells*N]   species sources (in)
+ *   rX[ncells]        rho*e or rho*h (in/out: rX += dt*rX_src)
+ *   rX_src[ncells]    energy source (in)
+ * dt_react and time are in/out as in the reference (time += dt_react).
+ * Returns the number of right-hand-side evaluations summed over cells (BDF)
+ * or the average number of RK steps (RK64) as a non-negative value in *cost,
+ * and 0 / PPB_E_INTEGRATE / an error code as the return value. */
+int ppb_react_flat(ppb_reactor* r, double* rY, double* rYsrc, double* rX, double* rX_src, double* dt_react,
+                   double* time, int ncells, void* stream, long* cost);
+
+/* Same on DEVICE arrays in the same YCOrder layout. */
+int ppb_react_flat_device(ppb_reactor* r, double* rY, double* rYsrc, double* rX, double* rX_src,
+                          double* dt_react, double* time, int ncells, void* stream, long* cost);
+
+/* Same on DEVICE arrays already in species-major (SoA) layout with leading
+ * dimension ld >= ncells: y[i*ld + c] for i <= N, src[i*ld + c] for i < N. */
+int ppb_react_soa_device(ppb_reactor* r, double* y, const double* src, double* rX, const double* rX_src, int ld,
+                         double* dt_react, double* time, int ncells, void* stream, long* cost);
+
+/* ReactorBase::react on a box of DEVICE Array4 views (ReactorBase.H:25-40;
+ * ReactorCvode.cpp:1267-1489 with box_flatten/box_unflatten of
+ * ReactorUtils.H:160-291): lo/hi are the box bounds (inclusive); rY has N
+ * components, T, rEner, rEner_src and FC one; cells with mask == -1 are
+ * skipped and get FC = 0. */
+int ppb_react_box(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 rY, ppb_array4 rYsrc, ppb_array4 T,
+                  ppb_array4 rEner, ppb_array4 rEner_src, ppb_array4 FC, ppb_array4i mask, double* dt_react,
+                  double* time, void* stream);
+
+/* Per-cell integrator flag (0 ok, 1 skipped by mask, <0 CVODE-style failure
+ * code) and cost (RHS evaluations or RK steps) of the last react call. */
+int ppb_get_cell_status(ppb_reactor* r, int* status, int* cost, int ncells);
+
+/* Pointwise mechanism kernels on DEVICE arrays, one cell per row, for
+ * parity checks; team = 1 (thread per cell) or 32 (warp per cell).
+ * mechanism.H productionRate (SI: mol/m^3 in, mol/m^3/s out):
+ *   sc[ncells*N], T[ncells] -> wdot[ncells*N] */
+int ppb_production_rate(const char* mechanism, const double* sc, const double* T, double* wdot, int ncells, int team,
+                        void* stream);
+/* mechanism.H aJacobian (SI), J[ncells*(N+1)^2] with
+ * J[k*(N+1)+m] = d wdot_m / d sc_k */
+int ppb_ajacobian(const char* mechanism, const double* sc, const double* T, int consP, double* J, int ncells,
+                  int team, void* stream);
+/* mechanism.H GET_T_GIVEN_EY (eh = 0) / GET_T_GIVEN_HY (eh = 1): e[ncells],
+ * Y[ncells*N], T[ncells] in (initial guess) / out. */
+int ppb_t_from_energy(const char* mechanism, int eh, const double* e, const double* Y, double* T, int ncells,
+                      int team, void* stream);
+/* ReactorUtils.H fKernelSpec: y[ncells*(N+1)] YCOrder, rhoe/rhoesrc[ncells],
+ * src[ncells*N] -> ydot[ncells*(N+1)] at time t since the start of react. */
+int ppb_reactor_rhs(const char* mechanism, int reactor_type, double t, const double* y, const double* rhoe,
+                    const double* rhoesrc, const double* src, double* ydot, int ncells, int team, void* stream);
+
+/* Fuego::PYT2RE (Source/Eos/Fuego.H:313-327) on DEVICE arrays: rho from
+ * CKRHOY(P, T, Y) and e = CKUBMS (eh = 0) or h = CKHBMS (eh = 1), erg/g. */
+int ppb_pyt2re(const char* mechanism, int eh, const double* P, const double* T, const double* Y, double* rho,
+               double* e, int ncells, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

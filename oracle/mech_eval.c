@@ -21,6 +21,18 @@ const PPBMechTables* ppo_mech(const char* name)
   return 0;
 }
 
+const char* ppo_species_name(const char* name, int k)
+{
+  const PPBMechTables* M = ppo_mech(name);
+  return (M && k >= 0 && k < M->nsp) ? M->species[k] : 0;
+}
+
+void ppo_mw(const char* name, double* mw)
+{
+  const PPBMechTables* M = ppo_mech(name);
+  for (int k = 0; M && k < M->nsp; k++) mw[k] = M->mw[k];
+}
+
 int ppo_nsp(const char* name)
 {
   const PPBMechTables* M = ppo_mech(name);
@@ -241,8 +253,12 @@ static inline double refc_pow(int p, double refC, double refCinv)
   return r;
 }
 
-// production.py:991-1435 (productionRate, SI units)
-void ppo_production_rate(const PPBMechTables* M, double* wdot, const double* sc, double T)
+// production.py:991-1435 (productionRate, SI units).  When absterm is not
+// NULL it also receives, per species, sum over reactions of
+// |nu| (|q_f| + |q_r|): the magnitude against which the rounding error of
+// the (cancelling) sum wdot is measured.
+static void production_rate_impl(const PPBMechTables* M, double* wdot, const double* sc,
+                                 double T, double* absterm)
 {
   const int N = M->nsp;
   const double invT = 1.0 / T;
@@ -310,6 +326,7 @@ void ppo_production_rate(const PPBMechTables* M, double* wdot, const double* sc,
     for (int j = 0; j < M->rx_wup_n[r]; j++) {
       const int s = M->rx_wup_sp[r * PPB_MAXW + j];
       const double c = M->rx_wup_c[r * PPB_MAXW + j];
+      if (absterm) absterm[s] += fabs(c) * (fabs(qf) + fabs(qr));
       if (c == -1.0) {
         wdot[s] -= qdot;
       } else if (c == 1.0) {
@@ -321,6 +338,18 @@ void ppo_production_rate(const PPBMechTables* M, double* wdot, const double* sc,
       }
     }
   }
+}
+
+void ppo_production_rate(const PPBMechTables* M, double* wdot, const double* sc, double T)
+{
+  production_rate_impl(M, wdot, sc, T, 0);
+}
+
+void ppo_production_rate_abs(const PPBMechTables* M, double* absterm, const double* sc, double T)
+{
+  double w[128];
+  for (int i = 0; i < M->nsp; i++) absterm[i] = 0.0;
+  production_rate_impl(M, w, sc, T, absterm);
 }
 
 // mechanism.H CKWC (LiDryer :2606-2622)

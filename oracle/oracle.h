@@ -18,6 +18,8 @@ extern "C" {
 
 const PPBMechTables* ppo_mech(const char* name);
 int ppo_nsp(const char* name);
+const char* ppo_species_name(const char* name, int k);
+void ppo_mw(const char* name, double* mw);
 
 // thermo, per species (mechanism.H cv_R / cp_R / dcvpRdT /
 // speciesInternalEnergy / speciesEnthalpy / gibbs)
@@ -40,6 +42,8 @@ int ppo_get_t_given_ey(const PPBMechTables* M, double e, const double* y, double
 int ppo_get_t_given_hy(const PPBMechTables* M, double h, const double* y, double* T);
 // rates and Jacobian (mechanism.H productionRate / aJacobian / DWDOT / CKWC)
 void ppo_production_rate(const PPBMechTables* M, double* wdot, const double* sc, double T);
+// per species sum |nu| (|q_f| + |q_r|): the scale of wdot's rounding error
+void ppo_production_rate_abs(const PPBMechTables* M, double* absterm, const double* sc, double T);
 void ppo_ckwc(const PPBMechTables* M, double T, const double* C, double* wdot);
 void ppo_ajacobian(const PPBMechTables* M, double* J, const double* sc, double T, int consP);
 void ppo_dwdot(const PPBMechTables* M, double* J, const double* sc, double T, int consP);

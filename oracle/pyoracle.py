@@ -89,6 +89,7 @@ def lib():
         L.ppo_get_t_given_ey.argtypes = [C.c_void_p, C.c_double, _DP, _DP]
         L.ppo_get_t_given_hy.argtypes = [C.c_void_p, C.c_double, _DP, _DP]
         L.ppo_production_rate.argtypes = [C.c_void_p, _DP, _DP, C.c_double]
+        L.ppo_production_rate_abs.argtypes = [C.c_void_p, _DP, _DP, C.c_double]
         L.ppo_ckwc.argtypes = [C.c_void_p, C.c_double, _DP, _DP]
         L.ppo_ajacobian.argtypes = [C.c_void_p, _DP, _DP, C.c_double, C.c_int]
         L.ppo_dwdot.argtypes = [C.c_void_p, _DP, _DP, C.c_double, C.c_int]
@@ -104,6 +105,9 @@ def lib():
         L.ppo_react_flat.argtypes = [C.c_char_p, C.c_int, C.POINTER(Options), C.c_int, _DP, _DP,
                                      _DP, _DP, C.c_double, C.c_int, C.c_int, _LP, _IP]
         L.ppo_load_ref.argtypes = [C.c_char_p, C.c_char_p]
+        L.ppo_species_name.argtypes = [C.c_char_p, C.c_int]
+        L.ppo_species_name.restype = C.c_char_p
+        L.ppo_mw.argtypes = [C.c_char_p, _DP]
         _lib = L
     return _lib
 
@@ -126,6 +130,14 @@ class Mech:
         if not self.M:
             raise KeyError(name)
         self.nsp = self.L.ppo_nsp(name.encode())
+
+    def species(self):
+        return [self.L.ppo_species_name(self.name.encode(), k).decode() for k in range(self.nsp)]
+
+    def mw(self):
+        a = np.zeros(self.nsp)
+        self.L.ppo_mw(self.name.encode(), _p(a))
+        return a
 
     def _vecT(self, fn, T):
         out = np.zeros(self.nsp)
@@ -189,6 +201,12 @@ class Mech:
         sc = np.ascontiguousarray(sc, float)
         w = np.zeros(self.nsp)
         self.L.ppo_production_rate(self.M, _p(w), _p(sc), float(T))
+        return w
+
+    def production_rate_abs(self, sc, T):
+        sc = np.ascontiguousarray(sc, float)
+        w = np.zeros(self.nsp)
+        self.L.ppo_production_rate_abs(self.M, _p(w), _p(sc), float(T))
         return w
 
     def ajacobian(self, sc, T, consP):

@@ -1,0 +1,91 @@
+"""Build the engine's shared library for sm_100a: pelephysics_b200/libppb200.so.
+
+The kernels are compiled once per species count of the shipped mechanisms
+(ppb_engine_ns.cu with -DPPB_NS=<N>), in parallel, then linked with the
+common kernels and the C-ABI layer.  Objects are rebuilt only when a source
+or header is newer.  Usage: ``python -m pelephysics_b200.build [-j N]``.
+"""
+
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libppb200.so")
+NVCC = os.environ.get("NVCC", "nvcc")
+SPECIES_COUNTS = (9, 21, 53, 88)
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-diag-suppress", "177,550"]
+
+
+def _headers():
+    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(
+        os.path.join(CSRC, "mech", "*.h")
+    ) + [os.path.join(os.path.dirname(HERE), "include", "pelephysics_b200.h")]
+
+
+def _units():
+    units = [
+        ("ppb_engine.o", "ppb_engine.cu", []),
+        ("ppb_abi.o", "ppb_abi.cu", []),
+    ]
+    for ns in SPECIES_COUNTS:
+        units.append((f"ppb_engine_ns{ns}.o", "ppb_engine_ns.cu", [f"-DPPB_NS={ns}"]))
+    return units
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _compile(unit, extra_flags):
+    obj, src, defs = unit
+    out = os.path.join(OBJ, obj)
+    srcp = os.path.join(CSRC, src)
+    if not _stale(out, [srcp] + _headers()):
+        return None
+    cmd = [NVCC] + ARCH + FLAGS + extra_flags + defs + ["-c", srcp, "-o", out + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {obj}:\n{r.stdout}\n{r.stderr}")
+    os.replace(out + ".tmp", out)
+    return obj
+
+
+def build(jobs: int | None = None, verbose: bool = False, extra_flags=()) -> str:
+    """Compile (incrementally) and link the engine; returns the library path."""
+    os.makedirs(OBJ, exist_ok=True)
+    units = _units()
+    jobs = jobs or min(len(units), os.cpu_count() or 4)
+    with ThreadPoolExecutor(max_workers=jobs) as ex:
+        done = list(ex.map(lambda u: _compile(u, list(extra_flags)), units))
+    objs = [os.path.join(OBJ, u[0]) for u in units]
+    if any(done) or _stale(LIB, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB + ".tmp"] + objs + ["-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+        os.replace(LIB + ".tmp", LIB)
+    if verbose:
+        print("built", LIB, "recompiled:", [d for d in done if d])
+    return LIB
+
+
+if __name__ == "__main__":
+    j = None
+    if "-j" in sys.argv:
+        j = int(sys.argv[sys.argv.index("-j") + 1])
+    try:
+        build(j, verbose=True)
+    except RuntimeError as e:
+        print(e, file=sys.stderr)
+        sys.exit(1)

@@ -1,0 +1,639 @@
+// C ABI of the B200 chemistry engine (include/pelephysics_b200.h).
+//
+// A ppb_reactor plays the role of the reference's ReactorCvode / ReactorRK64
+// object (Source/Reactions/ReactorCvode.{H,cpp}, ReactorRK64.{H,cpp}): it is
+// created by name, initialised once, and then advances batches of cells.
+// Device scratch is owned by the reactor and grown on demand; the device
+// paths can be replayed as a captured CUDA graph.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pelephysics_b200.h"
+#include "ppb_bdf.cuh"
+#include "ppb_engine.h"
+
+using namespace ppb;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg)
+{
+  g_err = msg;
+  return code;
+}
+
+static int cuda_fail(int e, const char* where)
+{
+  if (e == 0) return 0;
+  return fail(PPB_E_CUDA, std::string(where) + ": " + cudaGetErrorString((cudaError_t)e));
+}
+
+#define PPB_CUDA(call, where)                                                                                      \
+  do {                                                                                                             \
+    int _e = (int)(call);                                                                                          \
+    if (_e) return cuda_fail(_e, where);                                                                           \
+  } while (0)
+
+// One device copy of each mechanism per device, shared by all reactors.
+static std::mutex g_mech_mu;
+static std::vector<DeviceMechanism*> g_mechs;
+
+static int device_mechanism(const PPBMechTables* t, DeviceMechanism** out)
+{
+  int dev = 0;
+  PPB_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_mech_mu);
+  for (auto* m : g_mechs) {
+    if (m->host == t && m->device == dev) {
+      *out = m;
+      return 0;
+    }
+  }
+  auto* m = new DeviceMechanism();
+  int e = upload_mechanism(t, m);
+  if (e) {
+    delete m;
+    return cuda_fail(e, "upload_mechanism");
+  }
+  g_mechs.push_back(m);
+  *out = m;
+  return 0;
+}
+
+struct GraphKey {
+  const void* p[6];
+  int ncells, ld;
+  double dt;
+  cudaStream_t st;
+  bool operator==(const GraphKey& o) const
+  {
+    return memcmp(p, o.p, sizeof(p)) == 0 && ncells == o.ncells && ld == o.ld && dt == o.dt && st == o.st;
+  }
+};
+
+struct ppb_reactor {
+  std::string mech;
+  int method = METHOD_BDF;
+  const PPBMechTables* t = nullptr;
+  DeviceMechanism* dm = nullptr;
+  int reactor_type = 0;
+  bool inited = false;
+  ppb_options opt{};
+  std::vector<double> typ_vals;
+  // device scratch
+  size_t cap = 0;
+  double *aos = nullptr, *aos_src = nullptr, *soa = nullptr, *soa_src = nullptr, *rhoe = nullptr, *rhoesrc = nullptr;
+  double* atolv = nullptr;
+  int *status = nullptr, *nfe = nullptr, *queue = nullptr, *mask = nullptr;
+  int last_ncells = 0;
+  // graph cache for the device paths; capture runs on a private stream (the
+  // legacy default stream cannot be captured) and the graph is launched on
+  // the caller's stream
+  cudaGraphExec_t gexec = nullptr;
+  GraphKey gkey{};
+  cudaStream_t cap_stream = nullptr;
+};
+
+static void free_scratch(ppb_reactor* r)
+{
+  cudaFree(r->aos);
+  cudaFree(r->aos_src);
+  cudaFree(r->soa);
+  cudaFree(r->soa_src);
+  cudaFree(r->rhoe);
+  cudaFree(r->rhoesrc);
+  cudaFree(r->status);
+  cudaFree(r->nfe);
+  cudaFree(r->queue);
+  cudaFree(r->mask);
+  r->aos = r->aos_src = r->soa = r->soa_src = r->rhoe = r->rhoesrc = nullptr;
+  r->status = r->nfe = r->queue = r->mask = nullptr;
+  r->cap = 0;
+  if (r->gexec) cudaGraphExecDestroy(r->gexec);
+  r->gexec = nullptr;
+}
+
+static int ensure_scratch(ppb_reactor* r, int ncells)
+{
+  if ((size_t)ncells <= r->cap && r->queue) return 0;
+  free_scratch(r);
+  const size_t n = r->t->nsp + 1, c = (size_t)ncells;
+  PPB_CUDA(cudaMalloc(&r->aos, n * c * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->aos_src, n * c * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->soa, n * c * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->soa_src, n * c * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->rhoe, c * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->rhoesrc, c * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->status, c * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->nfe, c * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->mask, c * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->queue, 16), "cudaMalloc");
+  r->cap = c;
+  return 0;
+}
+
+static Options engine_options(const ppb_reactor* r)
+{
+  Options o{};
+  o.rtol = r->opt.rtol;
+  o.atol = r->opt.atol;
+  o.max_order = r->opt.max_order;
+  o.max_steps = r->opt.max_steps;
+  o.max_nls_iters = r->opt.max_nls_iters;
+  o.max_err_fails = r->opt.max_err_fails;
+  o.jac_eval_freq = r->opt.jac_eval_freq;
+  o.reactor_type = r->reactor_type;
+  o.lu_fp32 = r->opt.lu_fp32;
+  o.refine_sweeps = r->opt.refine_sweeps;
+  o.rk_guess = r->opt.rk64_nsubsteps_guess;
+  o.rk_min = r->opt.rk64_nsubsteps_min;
+  o.rk_max = r->opt.rk64_nsubsteps_max;
+  o.use_typ_vals = r->typ_vals.empty() ? 0 : 1;
+  return o;
+}
+
+static LaunchConfig launch_config(const ppb_reactor* r)
+{
+  LaunchConfig lc;
+  lc.engine = r->opt.engine;
+  lc.lu_fp32 = r->opt.lu_fp32;
+  lc.warps_per_block = r->opt.warps_per_block;
+  if (lc.warps_per_block <= 0) {
+    // largest block (<= 8 warps) whose shared-memory workspace still fits
+    const size_t cb = team_cell_bytes(r->t, r->opt.lu_fp32);
+    int w = 8;
+    while (w > 1 && cb * w > 200 * 1024) w--;
+    lc.warps_per_block = w;
+  }
+  lc.persistent = 1;
+  return lc;
+}
+
+// Capture body() on the reactor's private stream into r->gexec.
+template <typename F>
+static int capture(ppb_reactor* r, const GraphKey& key, F body)
+{
+  if (r->gexec && r->gkey == key) return 0;
+  if (r->gexec) cudaGraphExecDestroy(r->gexec);
+  r->gexec = nullptr;
+  if (!r->cap_stream) PPB_CUDA(cudaStreamCreateWithFlags(&r->cap_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  cudaGraph_t g;
+  PPB_CUDA(cudaStreamBeginCapture(r->cap_stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  int be = body(r->cap_stream);
+  cudaError_t ce = cudaStreamEndCapture(r->cap_stream, &g);
+  if (be) return be;
+  PPB_CUDA(ce, "cudaStreamEndCapture");
+  cudaError_t ie = cudaGraphInstantiate(&r->gexec, g, 0);
+  cudaGraphDestroy(g);
+  PPB_CUDA(ie, "cudaGraphInstantiate");
+  r->gkey = key;
+  return 0;
+}
+
+extern "C" {
+
+void ppb_default_options(ppb_options* o)
+{
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->rtol = 1e-6;
+  o->atol = 1e-10;
+  o->max_order = 2;
+  o->max_steps = 10000;
+  o->max_nls_iters = 3;
+  o->max_err_fails = 100;
+  o->jac_eval_freq = 100;
+  o->clean_init_massfrac = 0;
+  o->rk64_nsubsteps_guess = 10;
+  o->rk64_nsubsteps_min = 5;
+  o->rk64_nsubsteps_max = 500;
+  o->verbose = 0;
+  o->engine = PPB_ENGINE_TUNED;
+  o->lu_fp32 = 0;
+  o->refine_sweeps = 1;
+  o->warps_per_block = 0;
+  o->use_graph = 1;
+}
+
+const char* ppb_last_error(void) { return g_err.c_str(); }
+
+int ppb_mechanism_info(const char* mechanism, int* nspecies, int* nreactions)
+{
+  const PPBMechTables* t = mechanism ? find_mechanism(mechanism) : nullptr;
+  if (!t) return fail(PPB_E_MECH, std::string("unknown mechanism ") + (mechanism ? mechanism : "(null)"));
+  if (nspecies) *nspecies = t->nsp;
+  if (nreactions) *nreactions = t->nrxn;
+  return 0;
+}
+
+const char* ppb_species_name(const char* mechanism, int k)
+{
+  const PPBMechTables* t = mechanism ? find_mechanism(mechanism) : nullptr;
+  if (!t || k < 0 || k >= t->nsp) return nullptr;
+  return t->species[k];
+}
+
+int ppb_molecular_weights(const char* mechanism, double* mw)
+{
+  const PPBMechTables* t = mechanism ? find_mechanism(mechanism) : nullptr;
+  if (!t) return fail(PPB_E_MECH, std::string("unknown mechanism ") + (mechanism ? mechanism : "(null)"));
+  if (!mw) return fail(PPB_E_ARG, "ppb_molecular_weights: null output");
+  for (int k = 0; k < t->nsp; k++) mw[k] = t->mw[k];
+  return 0;
+}
+
+int ppb_create(const char* mechanism, const char* integrator, ppb_reactor** out)
+{
+  if (!out) return fail(PPB_E_ARG, "ppb_create: null output");
+  *out = nullptr;
+  const PPBMechTables* t = mechanism ? find_mechanism(mechanism) : nullptr;
+  if (!t) return fail(PPB_E_MECH, std::string("unknown mechanism ") + (mechanism ? mechanism : "(null)"));
+  int method;
+  if (!integrator || !strcmp(integrator, "ReactorCvode") || !strcmp(integrator, "ReactorB200")) {
+    method = METHOD_BDF;
+  } else if (!strcmp(integrator, "ReactorRK64") || !strcmp(integrator, "ReactorB200RK")) {
+    method = METHOD_RK64;
+  } else {
+    return fail(PPB_E_ARG, std::string("unknown integrator ") + integrator);
+  }
+  auto* r = new ppb_reactor();
+  r->mech = mechanism;
+  r->method = method;
+  r->t = t;
+  ppb_default_options(&r->opt);
+  *out = r;
+  return 0;
+}
+
+int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* opt)
+{
+  if (!r) return fail(PPB_E_ARG, "ppb_init: null reactor");
+  // ReactorTypes::check_reactor_type (ReactorTypes.H:12-18)
+  if (reactor_type != PPB_REACTOR_E && reactor_type != PPB_REACTOR_H)
+    return fail(PPB_E_ARG, "Wrong reactor type. Choose between 1 (e) or 2 (h).");
+  if (opt) r->opt = *opt;
+  if (r->opt.max_order < 1 || r->opt.max_order > 5) return fail(PPB_E_ARG, "max_order must be in 1..5");
+  if (r->opt.max_nls_iters < 1 || r->opt.max_steps < 1 || r->opt.rtol < 0 || r->opt.atol < 0)
+    return fail(PPB_E_ARG, "invalid integrator options");
+  if (r->opt.engine != PPB_ENGINE_PLAIN && r->opt.engine != PPB_ENGINE_TUNED)
+    return fail(PPB_E_ARG, "engine must be PPB_ENGINE_PLAIN or PPB_ENGINE_TUNED");
+  if (r->opt.engine == PPB_ENGINE_PLAIN && r->opt.lu_fp32)
+    return fail(PPB_E_ARG, "the plain engine is FP64 only");
+  r->reactor_type = reactor_type;
+  int e = device_mechanism(r->t, &r->dm);
+  if (e) return e;
+  if (ncells > 0) {
+    e = ensure_scratch(r, ncells);
+    if (e) return e;
+  }
+  r->inited = true;
+  return 0;
+}
+
+int ppb_set_typ_vals(ppb_reactor* r, const double* typ_vals, int n)
+{
+  if (!r || !typ_vals) return fail(PPB_E_ARG, "ppb_set_typ_vals: null argument");
+  if (n != r->t->nsp + 1) return fail(PPB_E_ARG, "ppb_set_typ_vals: expected N+1 values");
+  r->typ_vals.assign(typ_vals, typ_vals + n);
+  if (!r->atolv) PPB_CUDA(cudaMalloc(&r->atolv, n * 8), "cudaMalloc");
+  std::vector<double> at(n);
+  for (int i = 0; i < n; i++) at[i] = typ_vals[i] * r->opt.atol;
+  PPB_CUDA(cudaMemcpy(r->atolv, at.data(), n * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+  if (r->gexec) {
+    cudaGraphExecDestroy(r->gexec);
+    r->gexec = nullptr;
+  }
+  return 0;
+}
+
+int ppb_close(ppb_reactor* r)
+{
+  if (!r) return fail(PPB_E_ARG, "ppb_close: null reactor");
+  free_scratch(r);
+  if (r->cap_stream) cudaStreamDestroy(r->cap_stream);
+  r->cap_stream = nullptr;
+  cudaFree(r->atolv);
+  r->atolv = nullptr;
+  r->inited = false;
+  return 0;
+}
+
+void ppb_destroy(ppb_reactor* r)
+{
+  if (!r) return;
+  ppb_close(r);
+  delete r;
+}
+
+// Integrate a species-major batch already on the device (the core call).
+static int run_batch(ppb_reactor* r, Batch b, double dt, cudaStream_t st)
+{
+  b.atolv = r->atolv;
+  b.status = r->status;
+  b.nfe = r->nfe;
+  const Options o = engine_options(r);
+  const LaunchConfig lc = launch_config(r);
+  int e = launch_react(*r->dm, o, r->method, lc, b, dt, r->queue, st);
+  return cuda_fail(e, "launch_react");
+}
+
+static int finish(ppb_reactor* r, int ncells, cudaStream_t st, long* cost)
+{
+  r->last_ncells = ncells;
+  std::vector<int> stat(ncells), nfe(ncells);
+  PPB_CUDA(cudaMemcpyAsync(stat.data(), r->status, ncells * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  PPB_CUDA(cudaMemcpyAsync(nfe.data(), r->nfe, ncells * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  PPB_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  long tot = 0;
+  int bad = 0;
+  for (int c = 0; c < ncells; c++) {
+    tot += nfe[c];
+    if (stat[c] < 0) bad++;
+  }
+  if (cost) *cost = (r->method == METHOD_RK64) ? (ncells ? tot / ncells : 0) : tot;
+  if (bad) return fail(PPB_E_INTEGRATE, std::to_string(bad) + " cell(s) failed to integrate");
+  return 0;
+}
+
+int ppb_react_flat(ppb_reactor* r, double* rY, double* rYsrc, double* rX, double* rX_src, double* dt_react,
+                   double* time, int ncells, void* stream, long* cost)
+{
+  if (!r || !r->inited) return fail(PPB_E_STATE, "react before init");
+  if (ncells < 0 || !dt_react || !time || (ncells > 0 && (!rY || !rYsrc || !rX || !rX_src)))
+    return fail(PPB_E_ARG, "ppb_react_flat: invalid arguments");
+  if (ncells == 0) {
+    if (cost) *cost = 0;
+    *time += *dt_react;
+    return 0;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  int e = ensure_scratch(r, ncells);
+  if (e) return e;
+  const int N = r->t->nsp, n = N + 1;
+  PPB_CUDA(cudaMemcpyAsync(r->aos, rY, (size_t)ncells * n * 8, cudaMemcpyHostToDevice, st), "H2D rY");
+  PPB_CUDA(cudaMemcpyAsync(r->aos_src, rYsrc, (size_t)ncells * N * 8, cudaMemcpyHostToDevice, st), "H2D rYsrc");
+  PPB_CUDA(cudaMemcpyAsync(r->rhoe, rX, (size_t)ncells * 8, cudaMemcpyHostToDevice, st), "H2D rX");
+  PPB_CUDA(cudaMemcpyAsync(r->rhoesrc, rX_src, (size_t)ncells * 8, cudaMemcpyHostToDevice, st), "H2D rX_src");
+  PPB_CUDA(launch_aos_to_soa(r->aos, n, r->soa, ncells, n, ncells, st), "aos_to_soa");
+  PPB_CUDA(launch_aos_to_soa(r->aos_src, N, r->soa_src, ncells, N, ncells, st), "aos_to_soa");
+  Batch b{};
+  b.y = r->soa;
+  b.src = r->soa_src;
+  b.rhoe = r->rhoe;
+  b.rhoesrc = r->rhoesrc;
+  b.mask = nullptr;
+  b.ncells = ncells;
+  b.ld = ncells;
+  e = run_batch(r, b, *dt_react, st);
+  if (e) return e;
+  PPB_CUDA(launch_soa_to_aos(r->soa, ncells, n, r->aos, n, ncells, st), "soa_to_aos");
+  PPB_CUDA(cudaMemcpyAsync(rY, r->aos, (size_t)ncells * n * 8, cudaMemcpyDeviceToHost, st), "D2H rY");
+  e = finish(r, ncells, st, cost);
+  // ReactorCvode.cpp:1652-1655: rX += dt * rX_src on the host arrays
+  for (int i = 0; i < ncells; i++) rX[i] = rX[i] + *dt_react * rX_src[i];
+  *time += *dt_react;
+  return e;
+}
+
+// Device YCOrder path, optionally replayed as a CUDA graph.
+int ppb_react_flat_device(ppb_reactor* r, double* rY, double* rYsrc, double* rX, double* rX_src,
+                          double* dt_react, double* time, int ncells, void* stream, long* cost)
+{
+  if (!r || !r->inited) return fail(PPB_E_STATE, "react before init");
+  if (ncells < 0 || !dt_react || !time || (ncells > 0 && (!rY || !rYsrc || !rX || !rX_src)))
+    return fail(PPB_E_ARG, "ppb_react_flat_device: invalid arguments");
+  if (ncells == 0) {
+    if (cost) *cost = 0;
+    *time += *dt_react;
+    return 0;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  int e = ensure_scratch(r, ncells);
+  if (e) return e;
+  const int N = r->t->nsp, n = N + 1;
+  const double dt = *dt_react;
+  GraphKey key{{rY, rYsrc, rX, rX_src, nullptr, nullptr}, ncells, ncells, dt, st};
+  auto body = [&](cudaStream_t s) -> int {
+    int ee = launch_aos_to_soa(rY, n, r->soa, ncells, n, ncells, s);
+    if (!ee) ee = launch_aos_to_soa(rYsrc, N, r->soa_src, ncells, N, ncells, s);
+    if (ee) return cuda_fail(ee, "aos_to_soa");
+    Batch b{};
+    b.y = r->soa;
+    b.src = r->soa_src;
+    b.rhoe = rX;
+    b.rhoesrc = rX_src;
+    b.ncells = ncells;
+    b.ld = ncells;
+    ee = run_batch(r, b, dt, s);
+    if (ee) return ee;
+    ee = launch_soa_to_aos(r->soa, ncells, n, rY, n, ncells, s);
+    if (!ee) ee = launch_energy_update(rX, rX_src, dt, ncells, s);
+    if (ee) return cuda_fail(ee, "soa_to_aos");
+    return 0;
+  };
+  if (r->opt.use_graph) {
+    e = capture(r, key, body);
+    if (e) return e;
+    PPB_CUDA(cudaGraphLaunch(r->gexec, st), "cudaGraphLaunch");
+  } else {
+    e = body(st);
+    if (e) return e;
+  }
+  e = finish(r, ncells, st, cost);
+  *time += dt;
+  return e;
+}
+
+int ppb_react_soa_device(ppb_reactor* r, double* y, const double* src, double* rX, const double* rX_src, int ld,
+                         double* dt_react, double* time, int ncells, void* stream, long* cost)
+{
+  if (!r || !r->inited) return fail(PPB_E_STATE, "react before init");
+  if (ncells < 0 || ld < ncells || !dt_react || !time || (ncells > 0 && (!y || !src || !rX || !rX_src)))
+    return fail(PPB_E_ARG, "ppb_react_soa_device: invalid arguments");
+  if (ncells == 0) {
+    if (cost) *cost = 0;
+    *time += *dt_react;
+    return 0;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  int e = ensure_scratch(r, ncells);
+  if (e) return e;
+  const double dt = *dt_react;
+  GraphKey key{{y, src, rX, rX_src, (void*)1, nullptr}, ncells, ld, dt, st};
+  Batch b{};
+  b.y = y;
+  b.src = const_cast<double*>(src);
+  b.rhoe = rX;
+  b.rhoesrc = rX_src;
+  b.ncells = ncells;
+  b.ld = ld;
+  auto body = [&](cudaStream_t s) -> int {
+    int ee = run_batch(r, b, dt, s);
+    if (!ee) ee = cuda_fail(launch_energy_update(rX, rX_src, dt, ncells, s), "energy_update");
+    return ee;
+  };
+  if (r->opt.use_graph) {
+    e = capture(r, key, body);
+    if (e) return e;
+    PPB_CUDA(cudaGraphLaunch(r->gexec, st), "cudaGraphLaunch");
+  } else {
+    e = body(st);
+    if (e) return e;
+  }
+  e = finish(r, ncells, st, cost);
+  *time += dt;
+  return e;
+}
+
+static BoxView view(const ppb_array4& a)
+{
+  BoxView v;
+  v.p = a.p;
+  v.jstride = a.jstride;
+  v.kstride = a.kstride;
+  v.nstride = a.nstride;
+  for (int d = 0; d < 3; d++) v.lo[d] = a.lo[d];
+  return v;
+}
+
+static bool covers(const ppb_array4& a, const int lo[3], const int hi[3], int ncomp)
+{
+  if (!a.p || a.ncomp < ncomp) return false;
+  for (int d = 0; d < 3; d++)
+    if (lo[d] < a.lo[d] || hi[d] > a.hi[d]) return false;
+  return true;
+}
+
+int ppb_react_box(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 rY, ppb_array4 rYsrc, ppb_array4 T,
+                  ppb_array4 rEner, ppb_array4 rEner_src, ppb_array4 FC, ppb_array4i mask, double* dt_react,
+                  double* time, void* stream)
+{
+  if (!r || !r->inited) return fail(PPB_E_STATE, "react before init");
+  if (!lo || !hi || !dt_react || !time) return fail(PPB_E_ARG, "ppb_react_box: null argument");
+  const int N = r->t->nsp;
+  long ncl = 1;
+  for (int d = 0; d < 3; d++) {
+    if (hi[d] < lo[d]) return fail(PPB_E_ARG, "ppb_react_box: empty box");
+    ncl *= (hi[d] - lo[d] + 1);
+  }
+  if (ncl > (1L << 30)) return fail(PPB_E_ARG, "ppb_react_box: box too large");
+  if (!covers(rY, lo, hi, N) || !covers(rYsrc, lo, hi, N) || !covers(T, lo, hi, 1) || !covers(rEner, lo, hi, 1) ||
+      !covers(rEner_src, lo, hi, 1) || !covers(FC, lo, hi, 1))
+    return fail(PPB_E_ARG, "ppb_react_box: an Array4 does not cover the box");
+  if (mask.p) {
+    for (int d = 0; d < 3; d++)
+      if (lo[d] < mask.lo[d] || hi[d] > mask.hi[d]) return fail(PPB_E_ARG, "ppb_react_box: mask does not cover the box");
+  }
+  const int ncells = (int)ncl;
+  cudaStream_t st = (cudaStream_t)stream;
+  int e = ensure_scratch(r, ncells);
+  if (e) return e;
+  BoxArgs a{};
+  for (int d = 0; d < 3; d++) {
+    a.lo[d] = lo[d];
+    a.hi[d] = hi[d];
+  }
+  a.rY = view(rY);
+  a.rYsrc = view(rYsrc);
+  a.T = view(T);
+  a.rE = view(rEner);
+  a.rEs = view(rEner_src);
+  a.FC = view(FC);
+  a.mask.p = mask.p;
+  a.mask.jstride = mask.jstride;
+  a.mask.kstride = mask.kstride;
+  a.mask.nstride = mask.nstride;
+  for (int d = 0; d < 3; d++) a.mask.lo[d] = mask.lo[d];
+  Batch b{};
+  b.y = r->soa;
+  b.src = r->soa_src;
+  b.rhoe = r->rhoe;
+  b.rhoesrc = r->rhoesrc;
+  b.mask = r->mask;
+  b.ncells = ncells;
+  b.ld = ncells;
+  b.nfe = r->nfe;
+  PPB_CUDA(launch_box_flatten(*r->dm, r->reactor_type, r->opt.clean_init_massfrac, a, b, st), "box_flatten");
+  e = run_batch(r, b, *dt_react, st);
+  if (e) return e;
+  PPB_CUDA(launch_box_unflatten(*r->dm, r->reactor_type, r->opt.clean_init_massfrac, a, b, *dt_react, st),
+           "box_unflatten");
+  e = finish(r, ncells, st, nullptr);
+  *time += *dt_react;
+  return e;
+}
+
+int ppb_get_cell_status(ppb_reactor* r, int* status, int* cost, int ncells)
+{
+  if (!r || ncells < 0 || ncells > r->last_ncells) return fail(PPB_E_ARG, "ppb_get_cell_status: bad arguments");
+  if (status) PPB_CUDA(cudaMemcpy(status, r->status, (size_t)ncells * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  if (cost) PPB_CUDA(cudaMemcpy(cost, r->nfe, (size_t)ncells * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  return 0;
+}
+
+static int point_mech(const char* mechanism, DeviceMechanism** dm)
+{
+  const PPBMechTables* t = mechanism ? find_mechanism(mechanism) : nullptr;
+  if (!t) return fail(PPB_E_MECH, std::string("unknown mechanism ") + (mechanism ? mechanism : "(null)"));
+  return device_mechanism(t, dm);
+}
+
+int ppb_production_rate(const char* mechanism, const double* sc, const double* T, double* wdot, int ncells, int team,
+                        void* stream)
+{
+  DeviceMechanism* dm;
+  int e = point_mech(mechanism, &dm);
+  if (e) return e;
+  if (ncells < 0 || (team != 1 && team != 32)) return fail(PPB_E_ARG, "ppb_production_rate: bad arguments");
+  return cuda_fail(launch_production_rate(*dm, sc, T, wdot, ncells, team, (cudaStream_t)stream), "production_rate");
+}
+
+int ppb_ajacobian(const char* mechanism, const double* sc, const double* T, int consP, double* J, int ncells,
+                  int team, void* stream)
+{
+  DeviceMechanism* dm;
+  int e = point_mech(mechanism, &dm);
+  if (e) return e;
+  if (ncells < 0 || (team != 1 && team != 32)) return fail(PPB_E_ARG, "ppb_ajacobian: bad arguments");
+  return cuda_fail(launch_ajacobian(*dm, sc, T, consP, J, ncells, team, (cudaStream_t)stream), "ajacobian");
+}
+
+int ppb_t_from_energy(const char* mechanism, int eh, const double* e_in, const double* Y, double* T, int ncells,
+                      int team, void* stream)
+{
+  DeviceMechanism* dm;
+  int e = point_mech(mechanism, &dm);
+  if (e) return e;
+  if (ncells < 0 || (team != 1 && team != 32)) return fail(PPB_E_ARG, "ppb_t_from_energy: bad arguments");
+  return cuda_fail(launch_t_from_energy(*dm, eh, e_in, Y, T, ncells, team, (cudaStream_t)stream), "t_from_energy");
+}
+
+int ppb_reactor_rhs(const char* mechanism, int reactor_type, double t, const double* y, const double* rhoe,
+                    const double* rhoesrc, const double* src, double* ydot, int ncells, int team, void* stream)
+{
+  DeviceMechanism* dm;
+  int e = point_mech(mechanism, &dm);
+  if (e) return e;
+  if (ncells < 0 || (team != 1 && team != 32) || (reactor_type != 1 && reactor_type != 2))
+    return fail(PPB_E_ARG, "ppb_reactor_rhs: bad arguments");
+  return cuda_fail(launch_reactor_rhs(*dm, reactor_type, t, y, rhoe, rhoesrc, src, ydot, ncells, team,
+                                      (cudaStream_t)stream),
+                   "reactor_rhs");
+}
+
+int ppb_pyt2re(const char* mechanism, int eh, const double* P, const double* T, const double* Y, double* rho,
+               double* e_out, int ncells, void* stream)
+{
+  DeviceMechanism* dm;
+  int e = point_mech(mechanism, &dm);
+  if (e) return e;
+  if (ncells < 0 || (eh != 0 && eh != 1)) return fail(PPB_E_ARG, "ppb_pyt2re: bad arguments");
+  return cuda_fail(launch_pyt2re(*dm, eh, P, T, Y, rho, e_out, ncells, (cudaStream_t)stream), "pyt2re");
+}
+
+} // extern "C"

@@ -1,0 +1,852 @@
+// Per-cell reactor model and stiff integrators for the B200 engine.
+//
+//  * reactor_rhs  : the reference's fKernelSpec (Source/Reactions/
+//                   ReactorUtils.H:358-415) over the Fuego EOS wrappers
+//  * reactor_jac  : the CPU dense analytical Jacobian callback
+//                   (Source/Reactions/ReactorCvodeJacobian.cpp:86-152)
+//  * bdf_cell     : variable-order (1..5) BDF in Nordsieck form with
+//                   fixed-leading-coefficient coefficients, WRMS local error
+//                   test, step/order selection and a modified Newton on
+//                   I - gamma J: the CVODE algorithm with the options the
+//                   reference sets (ReactorCvode.cpp:230-503)
+//  * rk64_cell    : ReactorRK64.cpp:73-144
+//
+// One team of TEAM lanes integrates one cell; every lane holds the scalar
+// integrator state, vectors are lane-strided over team-shared memory.
+#pragma once
+#include "ppb_mech.cuh"
+
+namespace ppb {
+
+enum { ST_OK = 0, ST_TOO_MUCH_WORK = -1, ST_ERR_FAILURE = -3, ST_CONV_FAILURE = -4,
+       ST_LSETUP_FAIL = -6, ST_TOO_CLOSE = -27, ST_SKIPPED = 1 };
+
+struct Options {
+  double rtol, atol;
+  int max_order, max_steps, max_nls_iters, max_err_fails, jac_eval_freq;
+  int reactor_type;      // 1: e / cv, 2: h / cp
+  int lu_fp32;           // factor I - gamma J in FP32 and refine in FP64
+  int refine_sweeps;     // iterative-refinement sweeps when lu_fp32
+  int rk_guess, rk_min, rk_max;
+  int use_typ_vals;
+};
+
+// Team-shared per-cell workspace.  LT is the LU storage type.
+template <typename LT>
+struct Work {
+  double* zn[6];
+  double *ewt, *acor, *y, *tempv, *ftemp, *delta;
+  double *J, *src, *atolv;
+  LT* A;
+  int* piv;
+  // rate scratch
+  double *Y, *sc, *g, *qd, *wdot, *ei, *h1, *h2, *h3;
+};
+
+template <int TEAM>
+__device__ double reactor_rhs(
+  const Team<TEAM>& tm, const DevMech& M, int rtype, double t, const double* y, double* ydot, double rhoe,
+  double rhoesrc, const double* src, double* Y, double* sc, double* g, double* qd, double* wdot, double* ei)
+{
+  const int N = M.nsp;
+  double a = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) a += y[s];
+  const double rho = tm.sum(a);
+  const double rinv = 1.0 / rho;
+  for (int s = tm.lane; s < N; s += TEAM) Y[s] = y[s] * rinv;
+  tm.sync();
+  const double nrg = (rhoe + rhoesrc * t) * rinv;
+  double T = y[N];
+  const int EH = (rtype == 2);
+  t_from_energy(tm, M, EH, nrg, Y, T);
+  const double cv = mix_c(tm, M, EH, T, Y);
+  const double invT = 1.0 / T;
+  const double RT = RU * T;
+  for (int s = tm.lane; s < N; s += TEAM) {
+    const double im = __ldg(M.imw + s);
+    ei[s] = (EH ? h_RT(M, s, T, invT) : u_RT(M, s, T, invT)) * (RT * im);
+    sc[s] = (rho * Y[s] * im) * 1.0e6;
+  }
+  tm.sync();
+  RateScratch rs{sc, g, qd};
+  production_rate(tm, M, wdot, sc, T, rs);
+  double acc = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) {
+    const double cd = wdot[s] * 1.0e-6 * __ldg(M.mw + s) + src[s];
+    ydot[s] = cd;
+    acc += cd * ei[s];
+  }
+  const double esrc = rhoesrc - tm.sum(acc);
+  if (tm.lane == 0) ydot[N] = esrc * (rinv / cv);
+  tm.sync();
+  return T;
+}
+
+// Reactor Jacobian, column-major n x n: J[i*n + k] = d f_k / d y_i.
+template <int TEAM, int PER>
+__device__ void reactor_jac(
+  const Team<TEAM>& tm, const DevMech& M, int rtype, const double* y, double* J, double* sc, double* g,
+  double* wdot, double* h1, double* h2, double* h3, double* h4)
+{
+  const int N = M.nsp, n = N + 1;
+  double a = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) a += y[s];
+  const double rho = tm.sum(a);
+  const double temp = y[N];
+  for (int s = tm.lane; s < N; s += TEAM) {
+    const double Ys = y[s] / rho;
+    sc[s] = 1.e6 * (rho * Ys * __ldg(M.imw + s));
+  }
+  tm.sync();
+  RateScratch rs{sc, g, nullptr};
+  ajacobian<TEAM, PER>(tm, M, J, sc, temp, rtype == 2 ? 1 : 0, rs, wdot, h1, h2, h3, h4);
+  // DWDOT unit rescaling followed by the cJac mw/imw scaling, column by column
+  for (int i = tm.lane; i < n; i += TEAM) {
+    double* col = J + i * n;
+    if (i < N) {
+      const double imi = __ldg(M.imw + i);
+      for (int k = 0; k < N; k++) col[k] = col[k] * __ldg(M.mw + k) * imi;
+      col[N] = (col[N] * 1.e6) * imi;
+    } else {
+      for (int k = 0; k < N; k++) col[k] = (col[k] * 1.e-6) * __ldg(M.mw + k);
+      col[N] = 0.0;
+    }
+  }
+  tm.sync();
+}
+
+// ---------------------------------------------------------------- dense LU
+// Partial-pivoting LU of a column-major n x n matrix (first maximum wins, as
+// the SUNDIALS dense GETRF).  Returns 0 or k+1 for a zero pivot.
+template <int TEAM, typename LT>
+__device__ int lu_factor(const Team<TEAM>& tm, LT* A, int n, int* piv)
+{
+  for (int k = 0; k < n; k++) {
+    LT* colk = A + k * n;
+    double best = -1.0;
+    int bi = n;
+    for (int i = k + tm.lane; i < n; i += TEAM) {
+      const double v = fabs((double)colk[i]);
+      if (v > best) {
+        best = v;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int o = TEAM / 2; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(tm.mask, best, o, TEAM);
+      const int oi = __shfl_xor_sync(tm.mask, bi, o, TEAM);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    const int l = bi;
+    // a zero column is singular; an all-NaN column selects no row (bi == n)
+    if (!(best > 0.0) || l >= n) {
+      tm.sync();
+      return k + 1;
+    }
+    if (tm.lane == 0) piv[k] = l;
+    if (l != k) {
+      for (int j = tm.lane; j < n; j += TEAM) {
+        const LT t = A[j * n + l];
+        A[j * n + l] = A[j * n + k];
+        A[j * n + k] = t;
+      }
+    }
+    tm.sync();
+    const LT mult = (LT)1.0 / colk[k];
+    for (int i = k + 1 + tm.lane; i < n; i += TEAM) colk[i] *= mult;
+    tm.sync();
+    for (int i = k + 1 + tm.lane; i < n; i += TEAM) {
+      const LT lik = colk[i];
+      for (int j = k + 1; j < n; j++) {
+        const LT akj = A[j * n + k];
+        if (akj != (LT)0) A[j * n + i] -= akj * lik;
+      }
+    }
+    tm.sync();
+  }
+  return 0;
+}
+
+// Solve (LU) x = b in place (b team-shared, double).
+template <int TEAM, typename LT>
+__device__ void lu_solve(const Team<TEAM>& tm, const LT* A, int n, const int* piv, double* b)
+{
+  if (tm.lane == 0) {
+    for (int k = 0; k < n; k++) {
+      const int pk = piv[k];
+      if (pk != k) {
+        const double t = b[k];
+        b[k] = b[pk];
+        b[pk] = t;
+      }
+    }
+  }
+  tm.sync();
+  for (int k = 0; k < n - 1; k++) {
+    const double bk = b[k];
+    const LT* colk = A + k * n;
+    for (int i = k + 1 + tm.lane; i < n; i += TEAM) b[i] -= (double)colk[i] * bk;
+    tm.sync();
+  }
+  for (int k = n - 1; k > 0; k--) {
+    const LT* colk = A + k * n;
+    const double bk = b[k] / (double)colk[k];
+    tm.sync();
+    if (tm.lane == k % TEAM) b[k] = bk;
+    for (int i = tm.lane; i < k; i += TEAM) b[i] -= (double)colk[i] * bk;
+    tm.sync();
+  }
+  if (tm.lane == 0) b[0] /= (double)A[0];
+  tm.sync();
+}
+
+// ---------------------------------------------------------------- BDF
+struct BdfScalars {
+  double tau[7], tq[6], l[6];
+  double h, hprime, hscale, eta, etamax, tn, rl1, gamma, gammap, gamrat, crate, delp, acnrm, saved_tq5, hu;
+  double gamma_lu; // gamma of the factored matrix I - gamma J
+  int q, qprime, qwait, L, qmax, indx_acor, jcur;
+  int nst, nstlp, nstlj, nfe, nje, nsetups, nni, ncfn, netf;
+};
+
+struct CellIn {
+  double rhoe, rhoesrc;
+};
+
+template <int NS, int TEAM, typename LT>
+struct Bdf {
+  static constexpr int n = NS + 1;
+  static constexpr int PER = (NS + TEAM - 1) / TEAM;
+  const Team<TEAM>& tm;
+  const DevMech& M;
+  const Options& o;
+  Work<LT>& w;
+  CellIn cin;
+  BdfScalars s;
+
+  __device__ Bdf(const Team<TEAM>& t, const DevMech& m, const Options& op, Work<LT>& wk, CellIn ci)
+    : tm(t), M(m), o(op), w(wk), cin(ci)
+  {
+  }
+
+  __device__ double wrms(const double* v) const
+  {
+    double a = 0.0;
+    for (int i = tm.lane; i < n; i += TEAM) {
+      const double x = v[i] * w.ewt[i];
+      a += x * x;
+    }
+    return sqrt(tm.sum(a) / n);
+  }
+
+  __device__ void set_ewt(const double* y)
+  {
+    for (int i = tm.lane; i < n; i += TEAM) {
+      const double at = o.use_typ_vals ? w.atolv[i] : o.atol;
+      w.ewt[i] = 1.0 / (o.rtol * fabs(y[i]) + at);
+    }
+    tm.sync();
+  }
+
+  __device__ void f(double t, const double* y, double* fy)
+  {
+    reactor_rhs<TEAM>(tm, M, o.reactor_type, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
+                      w.ei);
+    s.nfe++;
+  }
+
+  __device__ void jac()
+  {
+    reactor_jac<TEAM, PER>(tm, M, o.reactor_type, w.y, w.J, w.sc, w.g, w.wdot, w.Y, w.ei, w.h1, w.h2);
+  }
+
+  __device__ int hin(double tout)
+  {
+    const double tdiff = tout - s.tn;
+    if (tdiff == 0.0) return ST_TOO_CLOSE;
+    const double tdist = fabs(tdiff);
+    const double tround = 2.220446049250313e-16 * fmax(fabs(s.tn), fabs(tout));
+    if (tdist < 2.0 * tround) return ST_TOO_CLOSE;
+    const double hlb = 100.0 * tround;
+    double hub_inv = 0.0;
+    for (int i = tm.lane; i < n; i += TEAM) {
+      const double t1 = 0.1 * fabs(w.zn[0][i]) + 1.0 / w.ewt[i];
+      hub_inv = fmax(hub_inv, fabs(w.zn[1][i]) / t1);
+    }
+    hub_inv = tm.max(hub_inv);
+    double hub = 0.1 * tdist;
+    if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
+    double hg = sqrt(hlb * hub);
+    if (hub < hlb) {
+      s.h = hg;
+      return ST_OK;
+    }
+    double hnew = hg;
+    for (int count1 = 1; count1 <= 4; count1++) {
+      for (int i = tm.lane; i < n; i += TEAM) w.y[i] = hg * w.zn[1][i] + w.zn[0][i];
+      tm.sync();
+      f(s.tn + hg, w.y, w.tempv);
+      for (int i = tm.lane; i < n; i += TEAM) w.tempv[i] = (w.tempv[i] - w.zn[1][i]) * (1.0 / hg);
+      tm.sync();
+      const double yddnrm = wrms(w.tempv);
+      hnew = (yddnrm * hub * hub > 2.0) ? sqrt(2.0 / yddnrm) : sqrt(hg * hub);
+      if (count1 == 4) break;
+      const double hrat = hnew / hg;
+      if (hrat > 0.5 && hrat < 2.0) break;
+      if (count1 > 1 && hrat > 2.0) {
+        hnew = hg;
+        break;
+      }
+      hg = hnew;
+    }
+    double h0 = 0.5 * hnew;
+    if (h0 < hlb) h0 = hlb;
+    if (h0 > hub) h0 = hub;
+    s.h = h0;
+    return ST_OK;
+  }
+
+  __device__ void rescale()
+  {
+    double factor = s.eta;
+    for (int j = 1; j <= s.q; j++) {
+      for (int i = tm.lane; i < n; i += TEAM) w.zn[j][i] *= factor;
+      factor *= s.eta;
+    }
+    tm.sync();
+    s.h = s.hscale * s.eta;
+    s.hscale = s.h;
+  }
+
+  __device__ void predict()
+  {
+    s.tn += s.h;
+    for (int i = tm.lane; i < n; i += TEAM) {
+      for (int k = 1; k <= s.q; k++)
+        for (int j = s.q; j >= k; j--) w.zn[j - 1][i] += w.zn[j][i];
+    }
+    tm.sync();
+  }
+
+  __device__ void restore(double saved_t)
+  {
+    s.tn = saved_t;
+    for (int i = tm.lane; i < n; i += TEAM) {
+      for (int k = 1; k <= s.q; k++)
+        for (int j = s.q; j >= k; j--) w.zn[j - 1][i] -= w.zn[j][i];
+    }
+    tm.sync();
+  }
+
+  __device__ void set_bdf()
+  {
+    double alpha0, alpha0_hat, xi_inv, xistar_inv, hsum;
+    const int q = s.q;
+    s.l[0] = s.l[1] = xi_inv = xistar_inv = 1.0;
+    for (int i = 2; i <= q; i++) s.l[i] = 0.0;
+    alpha0 = alpha0_hat = -1.0;
+    hsum = s.h;
+    if (q > 1) {
+      for (int j = 2; j < q; j++) {
+        hsum += s.tau[j - 1];
+        xi_inv = s.h / hsum;
+        alpha0 -= 1.0 / j;
+        for (int i = j; i >= 1; i--) s.l[i] += s.l[i - 1] * xi_inv;
+      }
+      alpha0 -= 1.0 / q;
+      xistar_inv = -s.l[1] - alpha0;
+      hsum += s.tau[q - 1];
+      xi_inv = s.h / hsum;
+      alpha0_hat = -s.l[1] - xi_inv;
+      for (int i = q; i >= 1; i--) s.l[i] += s.l[i - 1] * xistar_inv;
+    }
+    const double A1 = 1.0 - alpha0_hat + alpha0;
+    const double A2 = 1.0 + q * A1;
+    s.tq[2] = fabs(A1 / (alpha0 * A2));
+    s.tq[5] = fabs(A2 * xistar_inv / (s.l[q] * xi_inv));
+    if (s.qwait == 1) {
+      if (q > 1) {
+        const double C = xistar_inv / s.l[q];
+        const double A3 = alpha0 + 1.0 / q;
+        const double A4 = alpha0_hat + xi_inv;
+        const double Cpinv = (1.0 - A4 + A3) / A3;
+        s.tq[1] = fabs(C * Cpinv);
+      } else {
+        s.tq[1] = 1.0;
+      }
+      hsum += s.tau[q];
+      xi_inv = s.h / hsum;
+      const double A5 = alpha0 - (1.0 / (q + 1));
+      const double A6 = alpha0_hat - xi_inv;
+      const double Cppinv = (1.0 - A6 + A5) / A2;
+      s.tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
+    }
+    s.tq[4] = 0.1 / s.tq[2];
+  }
+
+  __device__ void set()
+  {
+    set_bdf();
+    s.rl1 = 1.0 / s.l[1];
+    s.gamma = s.h * s.rl1;
+    if (s.nst == 0) s.gammap = s.gamma;
+    s.gamrat = (s.nst > 0) ? s.gamma / s.gammap : 1.0;
+  }
+
+  // cvLsSetup: (re)use J, form I - gamma J, factor
+  __device__ int ls_setup(int convfail)
+  {
+    const double dgamma = fabs((s.gamma / s.gammap) - 1.0);
+    const bool jbad = (s.nst == 0) || (s.nst >= s.nstlj + o.jac_eval_freq) || ((convfail == 1) && (dgamma < 0.2)) ||
+                      (convfail == 2);
+    if (!jbad) {
+      s.jcur = 0;
+    } else {
+      s.nje++;
+      s.nstlj = s.nst;
+      s.jcur = 1;
+      jac();
+    }
+    s.gamma_lu = s.gamma;
+    for (int i = tm.lane; i < n; i += TEAM) {
+      for (int j = 0; j < n; j++) {
+        double v = -s.gamma * w.J[j * n + i];
+        if (i == j) v += 1.0;
+        w.A[j * n + i] = (LT)v;
+      }
+    }
+    tm.sync();
+    return lu_factor<TEAM, LT>(tm, w.A, n, w.piv) ? 1 : 0;
+  }
+
+  // x := (I - gamma J)^{-1} b, with FP64 iterative refinement when the
+  // factor is FP32.  b and x are w.delta; w.tempv is scratch.
+  __device__ void ls_solve()
+  {
+    if (sizeof(LT) == sizeof(double) || o.refine_sweeps <= 0) {
+      lu_solve<TEAM, LT>(tm, w.A, n, w.piv, w.delta);
+      return;
+    }
+    // keep b in ftemp-sized scratch: w.h3 (length >= n)
+    double* b = w.h3;
+    for (int i = tm.lane; i < n; i += TEAM) b[i] = w.delta[i];
+    tm.sync();
+    lu_solve<TEAM, LT>(tm, w.A, n, w.piv, w.delta);
+    for (int sweep = 0; sweep < o.refine_sweeps; sweep++) {
+      // r = b - (I - gamma_lu J) x in FP64, against the matrix that was
+      // factored (CVODE corrects a stale gamma afterwards, in nls)
+      for (int i = tm.lane; i < n; i += TEAM) {
+        double ax = w.delta[i];
+        double jx = 0.0;
+        for (int j = 0; j < n; j++) jx += w.J[j * n + i] * w.delta[j];
+        ax -= s.gamma_lu * jx;
+        w.tempv[i] = b[i] - ax;
+      }
+      tm.sync();
+      lu_solve<TEAM, LT>(tm, w.A, n, w.piv, w.tempv);
+      for (int i = tm.lane; i < n; i += TEAM) w.delta[i] += w.tempv[i];
+      tm.sync();
+    }
+  }
+
+  __device__ void nls_residual()
+  {
+    for (int i = tm.lane; i < n; i += TEAM) w.y[i] = w.zn[0][i] + w.acor[i];
+    tm.sync();
+    f(s.tn, w.y, w.ftemp);
+    for (int i = tm.lane; i < n; i += TEAM) {
+      const double r = s.rl1 * w.zn[1][i] + w.acor[i];
+      w.delta[i] = -s.gamma * w.ftemp[i] + r;
+    }
+    tm.sync();
+  }
+
+  __device__ int nls(int nflag)
+  {
+    const int convfail = ((nflag == 0) || (nflag == 2)) ? 0 : 2;
+    bool callSetup = (nflag == 1) || (nflag == 2) || (s.nst == 0) || (s.nst >= s.nstlp + 20) ||
+                     (fabs(s.gamrat - 1.0) > 0.3);
+    for (int i = tm.lane; i < n; i += TEAM) w.acor[i] = 0.0;
+    tm.sync();
+    bool jbad = false;
+    int retval = 0;
+    for (;;) {
+      nls_residual();
+      if (callSetup) {
+        const int ier = ls_setup(jbad ? 1 : convfail);
+        s.nsetups++;
+        s.gamrat = 1.0;
+        s.gammap = s.gamma;
+        s.crate = 1.0;
+        s.nstlp = s.nst;
+        if (ier) return -1;
+      }
+      int m = 0;
+      for (;;) {
+        s.nni++;
+        for (int i = tm.lane; i < n; i += TEAM) w.delta[i] = -w.delta[i];
+        tm.sync();
+        ls_solve();
+        if (s.gamrat != 1.0) {
+          const double sc = 2.0 / (1.0 + s.gamrat);
+          for (int i = tm.lane; i < n; i += TEAM) w.delta[i] *= sc;
+        }
+        for (int i = tm.lane; i < n; i += TEAM) w.acor[i] += w.delta[i];
+        tm.sync();
+        const double del = wrms(w.delta);
+        if (m > 0) s.crate = fmax(0.3 * s.crate, del / s.delp);
+        const double dcon = del * fmin(1.0, s.crate) / s.tq[4];
+        if (dcon <= 1.0) {
+          s.acnrm = (m == 0) ? del : wrms(w.acor);
+          s.jcur = 0;
+          return 0;
+        }
+        if ((m >= 1) && (del > 2.0 * s.delp)) {
+          retval = 1;
+          break;
+        }
+        s.delp = del;
+        m++;
+        if (m >= o.max_nls_iters) {
+          retval = 1;
+          break;
+        }
+        nls_residual();
+      }
+      if (retval > 0 && !s.jcur) {
+        callSetup = true;
+        jbad = true;
+        for (int i = tm.lane; i < n; i += TEAM) w.acor[i] = 0.0;
+        tm.sync();
+        continue;
+      }
+      break;
+    }
+    return retval;
+  }
+
+  __device__ void increase_bdf()
+  {
+    double alpha0, alpha1, prod, xi, xiold, hsum, A1;
+    for (int i = 0; i <= s.qmax; i++) s.l[i] = 0.0;
+    s.l[2] = alpha1 = prod = xiold = 1.0;
+    alpha0 = -1.0;
+    hsum = s.hscale;
+    if (s.q > 1) {
+      for (int j = 1; j < s.q; j++) {
+        hsum += s.tau[j + 1];
+        xi = hsum / s.hscale;
+        prod *= xi;
+        alpha0 -= 1.0 / (j + 1);
+        alpha1 += 1.0 / xi;
+        for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xiold + s.l[i - 1];
+        xiold = xi;
+      }
+    }
+    A1 = (-alpha0 - alpha1) / prod;
+    for (int i = tm.lane; i < n; i += TEAM) {
+      const double zL = A1 * w.zn[s.indx_acor][i];
+      w.zn[s.L][i] = zL;
+      for (int j = 2; j <= s.q; j++) w.zn[j][i] += s.l[j] * zL;
+    }
+    tm.sync();
+  }
+
+  __device__ void decrease_bdf()
+  {
+    double hsum, xi;
+    for (int i = 0; i <= s.qmax; i++) s.l[i] = 0.0;
+    s.l[2] = 1.0;
+    hsum = 0.0;
+    for (int j = 1; j <= s.q - 2; j++) {
+      hsum += s.tau[j];
+      xi = hsum / s.hscale;
+      for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xi + s.l[i - 1];
+    }
+    for (int i = tm.lane; i < n; i += TEAM)
+      for (int j = 2; j < s.q; j++) w.zn[j][i] -= s.l[j] * w.zn[s.q][i];
+    tm.sync();
+  }
+
+  __device__ void adjust_order(int deltaq)
+  {
+    if ((s.q == 2) && (deltaq != 1)) return;
+    if (deltaq == 1) increase_bdf();
+    else if (deltaq == -1) decrease_bdf();
+  }
+
+  __device__ int handle_nflag(int& nflag, double saved_t, int& ncf)
+  {
+    if (nflag == 0) return 2; // DO_ERROR_TEST
+    s.ncfn++;
+    restore(saved_t);
+    if (nflag < 0) return ST_LSETUP_FAIL;
+    ncf++;
+    s.etamax = 1.0;
+    if (ncf == 10) return ST_CONV_FAILURE;
+    s.eta = 0.25;
+    nflag = 1;
+    rescale();
+    return 3; // PREDICT_AGAIN
+  }
+
+  __device__ int do_error_test(int& nflag, double saved_t, int& nef, double& dsm)
+  {
+    dsm = s.acnrm * s.tq[2];
+    if (dsm <= 1.0) return ST_OK;
+    nef++;
+    s.netf++;
+    nflag = 2;
+    restore(saved_t);
+    if (nef == o.max_err_fails) return ST_ERR_FAILURE;
+    s.etamax = 1.0;
+    if (nef <= 3) {
+      s.eta = 1.0 / (pow(6.0 * dsm, 1.0 / s.L) + 1.0e-6);
+      s.eta = fmax(0.1, s.eta);
+      if (nef >= 2) s.eta = fmin(s.eta, 0.2);
+      rescale();
+      return 5; // TRY_AGAIN
+    }
+    if (s.q > 1) {
+      s.eta = 0.1;
+      adjust_order(-1);
+      s.L = s.q;
+      s.q--;
+      s.qwait = s.L;
+      rescale();
+      return 5;
+    }
+    s.eta = 0.1;
+    s.h *= s.eta;
+    s.hscale = s.h;
+    s.qwait = 10;
+    f(s.tn, w.zn[0], w.tempv);
+    for (int i = tm.lane; i < n; i += TEAM) w.zn[1][i] = s.h * w.tempv[i];
+    tm.sync();
+    return 5;
+  }
+
+  __device__ void complete_step()
+  {
+    s.nst++;
+    s.hu = s.h;
+    for (int i = s.q; i >= 2; i--) s.tau[i] = s.tau[i - 1];
+    if ((s.q == 1) && (s.nst > 1)) s.tau[2] = s.tau[1];
+    s.tau[1] = s.h;
+    const bool save = ((s.qwait - 1) == 1) && (s.q != s.qmax);
+    for (int i = tm.lane; i < n; i += TEAM) {
+      const double a = w.acor[i];
+      for (int j = 0; j <= s.q; j++) w.zn[j][i] += s.l[j] * a;
+      if (save) w.zn[s.qmax][i] = a;
+    }
+    tm.sync();
+    s.qwait--;
+    if (save) {
+      s.saved_tq5 = s.tq[5];
+      s.indx_acor = s.qmax;
+    }
+  }
+
+  __device__ void set_eta()
+  {
+    if ((s.eta > 0.0) && (s.eta < 1.5)) {
+      s.eta = 1.0;
+      s.hprime = s.h;
+    } else {
+      s.eta = fmin(s.eta, s.etamax);
+      s.hprime = s.h * s.eta;
+    }
+  }
+
+  __device__ void prepare_next_step(double dsm)
+  {
+    if (s.etamax == 1.0) {
+      s.qwait = s.qwait > 2 ? s.qwait : 2;
+      s.qprime = s.q;
+      s.hprime = s.h;
+      s.eta = 1.0;
+      return;
+    }
+    const double etaq = 1.0 / (pow(6.0 * dsm, 1.0 / s.L) + 1.0e-6);
+    if (s.qwait != 0) {
+      s.eta = etaq;
+      s.qprime = s.q;
+      set_eta();
+      return;
+    }
+    s.qwait = 2;
+    double etaqm1 = 0.0;
+    if (s.q > 1) {
+      const double ddn = wrms(w.zn[s.q]) * s.tq[1];
+      etaqm1 = 1.0 / (pow(6.0 * ddn, 1.0 / s.q) + 1.0e-6);
+    }
+    double etaqp1 = 0.0;
+    if (s.q != s.qmax && s.saved_tq5 != 0.0) {
+      const double cquot = (s.tq[5] / s.saved_tq5) * pow(s.h / s.tau[2], (double)s.L);
+      for (int i = tm.lane; i < n; i += TEAM) w.tempv[i] = -cquot * w.zn[s.qmax][i] + w.acor[i];
+      tm.sync();
+      const double dup = wrms(w.tempv) * s.tq[3];
+      etaqp1 = 1.0 / (pow(10.0 * dup, 1.0 / (s.L + 1)) + 1.0e-6);
+    }
+    const double etam = fmax(etaqm1, fmax(etaq, etaqp1));
+    if ((etam > 0.0) && (etam < 1.5)) {
+      s.eta = 1.0;
+      s.qprime = s.q;
+    } else if (etam == etaq) {
+      s.eta = etaq;
+      s.qprime = s.q;
+    } else if (etam == etaqm1) {
+      s.eta = etaqm1;
+      s.qprime = s.q - 1;
+    } else {
+      s.eta = etaqp1;
+      s.qprime = s.q + 1;
+      for (int i = tm.lane; i < n; i += TEAM) w.zn[s.qmax][i] = w.acor[i];
+      tm.sync();
+    }
+    set_eta();
+  }
+
+  __device__ void adjust_params()
+  {
+    if (s.qprime != s.q) {
+      adjust_order(s.qprime - s.q);
+      s.q = s.qprime;
+      s.L = s.q + 1;
+      s.qwait = s.L;
+    }
+    rescale();
+  }
+
+  __device__ int step()
+  {
+    const double saved_t = s.tn;
+    int ncf = 0, nef = 0, nflag = 0;
+    double dsm = 0.0;
+    if ((s.nst > 0) && (s.hprime != s.h)) adjust_params();
+    for (;;) {
+      predict();
+      set();
+      nflag = nls(nflag);
+      const int kflag = handle_nflag(nflag, saved_t, ncf);
+      if (kflag == 3) continue;
+      if (kflag != 2) return kflag;
+      const int eflag = do_error_test(nflag, saved_t, nef, dsm);
+      if (eflag == 5) continue;
+      if (eflag != ST_OK) return eflag;
+      break;
+    }
+    complete_step();
+    prepare_next_step(dsm);
+    s.etamax = 10.0;
+    return ST_OK;
+  }
+
+  // Integrate w.zn[0] (initial y, team-shared) over [0, tout]; result in w.y.
+  __device__ int run(double tout)
+  {
+    s = BdfScalars{};
+    s.qmax = o.max_order;
+    s.q = 1;
+    s.L = 2;
+    s.qwait = 2;
+    s.etamax = 10000.0;
+    s.tn = 0.0;
+    set_ewt(w.zn[0]);
+    f(s.tn, w.zn[0], w.zn[1]);
+    int flag = hin(tout);
+    if (flag == ST_OK) {
+      s.hscale = s.h;
+      s.hprime = s.h;
+      for (int i = tm.lane; i < n; i += TEAM) w.zn[1][i] *= s.h;
+      tm.sync();
+      int nstloc = 0;
+      for (;;) {
+        if (s.nst > 0) set_ewt(w.zn[0]);
+        if (nstloc >= o.max_steps) {
+          flag = ST_TOO_MUCH_WORK;
+          break;
+        }
+        flag = step();
+        if (flag != ST_OK) break;
+        nstloc++;
+        if ((s.tn - tout) * s.h >= 0.0) {
+          const double sfac = (tout - s.tn) / s.h;
+          for (int i = tm.lane; i < n; i += TEAM) {
+            double v = w.zn[s.q][i];
+            for (int j = s.q - 1; j >= 0; j--) v = w.zn[j][i] + sfac * v;
+            w.y[i] = v;
+          }
+          tm.sync();
+          break;
+        }
+      }
+    }
+    if (flag != ST_OK) {
+      for (int i = tm.lane; i < n; i += TEAM) w.y[i] = w.zn[0][i];
+      tm.sync();
+    }
+    return flag;
+  }
+};
+
+// ReactorRK64.cpp:73-144 for one cell (team).  y (team-shared) in/out;
+// returns the number of RK steps.
+template <int TEAM, typename LT>
+__device__ int rk64_cell(const Team<TEAM>& tm, const DevMech& M, const Options& o, Work<LT>& w, CellIn cin,
+                         double dt)
+{
+  const double alpha[6] = {0.218150805229859, 0.256702469801519, 0.527402592007520,
+                           0.0484864267224467, 1.24517071533530, 0.412366034843237};
+  const double beta[6] = {-0.113554138044166, -0.215118587818400, -0.0510152146250577,
+                          -1.07992686223881, -0.248664241213447, 0.0};
+  const double err[6] = {-0.0554699315064507, 0.158481845574980, -0.0905918835751907,
+                         -0.219084567203338, 0.164022338959433, 0.0426421977505659};
+  const int neq = M.nsp + 1;
+  double* soln = w.y;
+  double* carry = w.zn[0];
+  double* error = w.zn[1];
+  double* ydot = w.ftemp;
+  for (int i = tm.lane; i < neq; i += TEAM) carry[i] = soln[i];
+  tm.sync();
+  double t = 0.0;
+  double dt_rk = dt / (double)o.rk_guess;
+  const double dt_rk_min = dt / (double)o.rk_max;
+  const double dt_rk_max = dt / (double)o.rk_min;
+  int nsteps = 0;
+  // the reference loop has no step cap; dt_rk >= dt / rk_max bounds it except
+  // for round-off tails, which the cap below ends
+  const int cap = 4 * o.rk_max + 1000;
+  while (t < dt && nsteps < cap) {
+    for (int i = tm.lane; i < neq; i += TEAM) error[i] = 0.0;
+    tm.sync();
+    for (int st = 0; st < 6; st++) {
+      reactor_rhs<TEAM>(tm, M, o.reactor_type, t, soln, ydot, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd,
+                        w.wdot, w.ei);
+      for (int i = tm.lane; i < neq; i += TEAM) {
+        error[i] += err[st] * dt_rk * ydot[i];
+        soln[i] = carry[i] + alpha[st] * dt_rk * ydot[i];
+        carry[i] = soln[i] + beta[st] * dt_rk * ydot[i];
+      }
+      tm.sync();
+    }
+    t += dt_rk;
+    nsteps++;
+    double me = 1e-50;
+    for (int i = tm.lane; i < neq; i += TEAM) me = fabs(error[i]) > me ? fabs(error[i]) : me;
+    me = tm.max(me);
+    if (me < o.atol) {
+      dt_rk = fmin(dt_rk_max, dt_rk * (1.0 * pow((o.atol / me), 0.25)));
+    } else {
+      dt_rk = fmax(dt_rk_min, dt_rk * (1.0 * pow((o.atol / me), 0.2)));
+    }
+    dt_rk = fmin(dt_rk, dt - t);
+  }
+  return nsteps;
+}
+
+} // namespace ppb

@@ -1,0 +1,512 @@
+// CUDA kernels of the B200 chemistry engine (sm_100a) and their launchers.
+//
+// Two integration engines share one device implementation (ppb_bdf.cuh):
+//  * plain: one thread per cell, FP64 everywhere, per-cell arrays in
+//    thread-local memory, one launch over all cells -- the straightforward
+//    GPU mapping of the reference's per-cell loop;
+//  * tuned: one warp per cell, per-cell arrays in shared memory, a persistent
+//    grid sized to the resident capacity of the GPU whose warps pull cells
+//    from a device work queue, optional FP32 factorisation of I - gamma J
+//    with FP64 iterative refinement.
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "ppb_work.cuh"
+#include "ppb_engine.h"
+#include "mech/mech_LiDryer.h"
+#include "mech/mech_drm19.h"
+#include "mech/mech_dodecane_lu.h"
+#include "mech/mech_heptane_lu_88sk.h"
+
+namespace ppb {
+
+const PPBMechTables* find_mechanism(const char* name)
+{
+  if (!strcmp(name, "LiDryer")) return &ppbm_LiDryer;
+  if (!strcmp(name, "drm19")) return &ppbm_drm19;
+  if (!strcmp(name, "dodecane_lu")) return &ppbm_dodecane_lu;
+  if (!strcmp(name, "heptane_lu_88sk")) return &ppbm_heptane_lu_88sk;
+  return nullptr;
+}
+
+// ------------------------------------------------------------ upload
+namespace {
+struct Packer {
+  std::vector<char> buf;
+  template <typename T>
+  size_t add(const T* p, size_t n)
+  {
+    size_t off = (buf.size() + 15) & ~size_t(15);
+    buf.resize(off + n * sizeof(T) + 16);
+    if (n) memcpy(buf.data() + off, p, n * sizeof(T));
+    return off;
+  }
+};
+} // namespace
+
+int upload_mechanism(const PPBMechTables* t, DeviceMechanism* out)
+{
+  const int N = t->nsp, R = t->nrxn;
+  // species-major gather lists of the productionRate updates
+  std::vector<int> wg_off(N + 1, 0), wg_rx;
+  std::vector<double> wg_c;
+  for (int s = 0; s < N; s++) {
+    wg_off[s] = (int)wg_rx.size();
+    for (int r = 0; r < R; r++) {
+      for (int j = 0; j < t->rx_wup_n[r]; j++) {
+        if (t->rx_wup_sp[r * PPB_MAXW + j] == s) {
+          wg_rx.push_back(r);
+          wg_c.push_back(t->rx_wup_c[r * PPB_MAXW + j]);
+        }
+      }
+    }
+  }
+  wg_off[N] = (int)wg_rx.size();
+  Packer pk;
+  struct Rec {
+    size_t off;
+    const void** dst;
+  };
+  DevMech dm{};
+  dm.nsp = N;
+  dm.nrxn = R;
+  std::vector<std::pair<size_t, const void**>> recs;
+#define PPB_ADD(field, ptr, count) recs.push_back({pk.add(ptr, count), (const void**)&dm.field})
+  PPB_ADD(mw, t->mw, N);
+  PPB_ADD(imw, t->imw, N);
+  PPB_ADD(tmid, t->tmid, N);
+  PPB_ADD(th_cv, t->th_cv, N * 10);
+  PPB_ADD(th_cp, t->th_cp, N * 10);
+  PPB_ADD(th_dcp, t->th_dcp, N * 8);
+  PPB_ADD(th_u, t->th_u, N * 12);
+  PPB_ADD(th_h, t->th_h, N * 12);
+  PPB_ADD(th_g, t->th_g, N * 14);
+  PPB_ADD(rx_kind, t->rx_kind, R);
+  PPB_ADD(rx_rev, t->rx_rev, R);
+  PPB_ADD(rx_kcpow, t->rx_kcpow, R);
+  PPB_ADD(rx_A, t->rx_A, R);
+  PPB_ADD(rx_beta, t->rx_beta, R);
+  PPB_ADD(rx_EaR, t->rx_EaR, R);
+  PPB_ADD(rx_sum_nuk, t->rx_sum_nuk, R);
+  PPB_ADD(fps_n, t->rx_fps_n, R);
+  PPB_ADD(fps_sp, t->rx_fps_sp, R * PPB_MAXPS);
+  PPB_ADD(fps_c, t->rx_fps_c, R * PPB_MAXPS);
+  PPB_ADD(rps_n, t->rx_rps_n, R);
+  PPB_ADD(rps_sp, t->rx_rps_sp, R * PPB_MAXPS);
+  PPB_ADD(rps_c, t->rx_rps_c, R * PPB_MAXPS);
+  PPB_ADD(kc_n, t->rx_kc_n, R);
+  PPB_ADD(kc_sp, t->rx_kc_sp, R * PPB_MAXKC);
+  PPB_ADD(kc_c, t->rx_kc_c, R * PPB_MAXKC);
+  PPB_ADD(wup_n, t->rx_wup_n, R);
+  PPB_ADD(wup_sp, t->rx_wup_sp, R * PPB_MAXW);
+  PPB_ADD(wup_c, t->rx_wup_c, R * PPB_MAXW);
+  PPB_ADD(jn_n, t->rx_jn_n, R);
+  PPB_ADD(jn_sp, t->rx_jn_sp, R * PPB_MAXJN);
+  PPB_ADD(jn_c, t->rx_jn_c, R * PPB_MAXJN);
+  PPB_ADD(hr_n, t->rx_hr_n, R);
+  PPB_ADD(hr_sp, t->rx_hr_sp, R * PPB_MAXPS);
+  PPB_ADD(hr_c, t->rx_hr_c, R * PPB_MAXPS);
+  PPB_ADD(hp_n, t->rx_hp_n, R);
+  PPB_ADD(hp_sp, t->rx_hp_sp, R * PPB_MAXPS);
+  PPB_ADD(hp_c, t->rx_hp_c, R * PPB_MAXPS);
+  PPB_ADD(eff_off, t->eff_off, R + 1);
+  PPB_ADD(eff_sp, t->eff_sp, t->eff_off[R]);
+  PPB_ADD(eff_e, t->eff_e, t->eff_off[R]);
+  PPB_ADD(eff_m1, t->eff_m1, t->eff_off[R]);
+  PPB_ADD(fo_d, t->fo_d, R * PPB_NFOD);
+  PPB_ADD(fo_i, t->fo_i, R * PPB_NFOI);
+  PPB_ADD(wg_off, wg_off.data(), N + 1);
+  PPB_ADD(wg_rx, wg_rx.data(), wg_rx.size());
+  PPB_ADD(wg_c, wg_c.data(), wg_c.size());
+#undef PPB_ADD
+  void* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, pk.buf.size());
+  if (e != cudaSuccess) return (int)e;
+  e = cudaMemcpy(d, pk.buf.data(), pk.buf.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return (int)e;
+  }
+  for (auto& r : recs) *r.second = (const char*)d + r.first;
+  out->host = t;
+  cudaGetDevice(&out->device);
+  out->blob = d;
+  out->dm = new DevMech(dm);
+  return 0;
+}
+
+void free_mechanism(DeviceMechanism* m)
+{
+  if (m->blob) cudaFree(m->blob);
+  delete m->dm;
+  m->blob = nullptr;
+  m->dm = nullptr;
+}
+
+size_t team_cell_bytes(const PPBMechTables* t, int lu_fp32)
+{
+  return lu_fp32 ? team_bytes<float>(t->nsp, t->nrxn) : team_bytes<double>(t->nsp, t->nrxn);
+}
+
+#define PPB_DECL(NS)                                                                                              \
+  int launch_react_##NS(const DeviceMechanism&, const Options&, int, const LaunchConfig&, Batch, double, int*,      \
+                        cudaStream_t);                                                                             \
+  int launch_ajacobian_##NS(const DevMech&, const double*, const double*, int, double*, int, int, cudaStream_t);
+PPB_DECL(9)
+PPB_DECL(21)
+PPB_DECL(53)
+PPB_DECL(88)
+
+int launch_react(const DeviceMechanism& m, const Options& o, int method, const LaunchConfig& lc, Batch b,
+                 double dt, int* queue, cudaStream_t st)
+{
+  switch (m.host->nsp) {
+  case 9:
+    return launch_react_9(m, o, method, lc, b, dt, queue, st);
+  case 21:
+    return launch_react_21(m, o, method, lc, b, dt, queue, st);
+  case 53:
+    return launch_react_53(m, o, method, lc, b, dt, queue, st);
+  case 88:
+    return launch_react_88(m, o, method, lc, b, dt, queue, st);
+  default:
+    return (int)cudaErrorNotSupported;
+  }
+}
+
+// ------------------------------------------------------------ layout
+// Tiled transpose through shared memory: AoS rows of nc_aos doubles per cell
+// (first ncomp used) <-> species-major planes of leading dimension ld.
+__global__ void k_aos_to_soa(const double* __restrict__ aos, int nc_aos, double* __restrict__ soa, int ld,
+                             int ncomp, int ncells)
+{
+  __shared__ double tile[32][33];
+  const int c0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int c = c0 + r, i = i0 + threadIdx.x;
+    if (c < ncells && i < ncomp) tile[r][threadIdx.x] = aos[(size_t)c * nc_aos + i];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, c = c0 + threadIdx.x;
+    if (c < ncells && i < ncomp) soa[(size_t)i * ld + c] = tile[threadIdx.x][r];
+  }
+}
+
+__global__ void k_soa_to_aos(const double* __restrict__ soa, int ld, int ncomp, double* __restrict__ aos, int nc_aos,
+                             int ncells)
+{
+  __shared__ double tile[32][33];
+  const int c0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, c = c0 + threadIdx.x;
+    if (c < ncells && i < ncomp) tile[threadIdx.x][r] = soa[(size_t)i * ld + c];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int c = c0 + r, i = i0 + threadIdx.x;
+    if (c < ncells && i < ncomp) aos[(size_t)c * nc_aos + i] = tile[r][threadIdx.x];
+  }
+}
+
+int launch_aos_to_soa(const double* aos, int nc_aos, double* soa, int ld, int ncomp, int ncells, cudaStream_t st)
+{
+  if (ncells <= 0 || ncomp <= 0) return 0;
+  dim3 grid((ncells + 31) / 32, (ncomp + 31) / 32), block(32, 8);
+  k_aos_to_soa<<<grid, block, 0, st>>>(aos, nc_aos, soa, ld, ncomp, ncells);
+  return (int)cudaGetLastError();
+}
+
+int launch_soa_to_aos(const double* soa, int ld, int ncomp, double* aos, int nc_aos, int ncells, cudaStream_t st)
+{
+  if (ncells <= 0 || ncomp <= 0) return 0;
+  dim3 grid((ncells + 31) / 32, (ncomp + 31) / 32), block(32, 8);
+  k_soa_to_aos<<<grid, block, 0, st>>>(soa, ld, ncomp, aos, nc_aos, ncells);
+  return (int)cudaGetLastError();
+}
+
+// ------------------------------------------------------------ pointwise
+
+template <int TEAM>
+__global__ void k_production_rate(DevMech M, const double* sc, const double* T, double* wdot, int ncells)
+{
+  extern __shared__ __align__(16) double psm[];
+  Team<TEAM> tm;
+  const int N = M.nsp;
+  const int per_block = blockDim.x / TEAM;
+  const int slot = threadIdx.x / TEAM;
+  const int c = blockIdx.x * per_block + slot;
+  double local[8 * 96];
+  double* base = (TEAM == 1) ? local : psm + (size_t)slot * point_doubles(N, M.nrxn, false);
+  if (TEAM == 1 && c >= ncells) return;
+  const int cc = c < ncells ? c : ncells - 1;
+  double* s_sc = base;
+  double* s_g = base + (N + 1);
+  double* s_w = base + 2 * (N + 1);
+  double* s_qd = base + 8 * (N + 1);
+  for (int s = tm.lane; s < N; s += TEAM) s_sc[s] = sc[(size_t)cc * N + s];
+  tm.sync();
+  RateScratch rs{s_sc, s_g, s_qd};
+  production_rate<TEAM>(tm, M, s_w, s_sc, T[cc], rs);
+  if (c < ncells)
+    for (int s = tm.lane; s < N; s += TEAM) wdot[(size_t)c * N + s] = s_w[s];
+}
+
+template <int TEAM>
+__global__ void k_t_from_energy(DevMech M, int eh, const double* e, const double* Y, double* T, int ncells)
+{
+  Team<TEAM> tm;
+  const int per_block = blockDim.x / TEAM;
+  const int c = blockIdx.x * per_block + threadIdx.x / TEAM;
+  if (TEAM == 1 && c >= ncells) return;
+  const int cc = c < ncells ? c : ncells - 1;
+  double t = T[cc];
+  t_from_energy<TEAM>(tm, M, eh, e[cc], Y + (size_t)cc * M.nsp, t);
+  if (c < ncells && tm.lane == 0) T[c] = t;
+}
+
+template <int TEAM>
+__global__ void k_reactor_rhs(DevMech M, int rtype, double t, const double* y, const double* rhoe,
+                              const double* rhoesrc, const double* src, double* ydot, int ncells)
+{
+  extern __shared__ __align__(16) double psm[];
+  Team<TEAM> tm;
+  const int N = M.nsp, n = N + 1;
+  const int per_block = blockDim.x / TEAM;
+  const int slot = threadIdx.x / TEAM;
+  const int c = blockIdx.x * per_block + slot;
+  double local[10 * 96];
+  if (TEAM == 1 && c >= ncells) return;
+  const int cc = c < ncells ? c : ncells - 1;
+  double* base = (TEAM == 1) ? local : psm + (size_t)slot * (10 * (size_t)n + M.nrxn);
+  double* s_y = base;
+  double* s_f = base + n;
+  double* s_src = base + 2 * n;
+  double* Yb = base + 3 * n;
+  double* scb = base + 4 * n;
+  double* gb = base + 5 * n;
+  double* wb = base + 6 * n;
+  double* eb = base + 7 * n;
+  double* qd = base + 10 * n;
+  for (int i = tm.lane; i < n; i += TEAM) {
+    s_y[i] = y[(size_t)cc * n + i];
+    s_src[i] = (i < N) ? src[(size_t)cc * N + i] : 0.0;
+  }
+  tm.sync();
+  reactor_rhs<TEAM>(tm, M, rtype, t, s_y, s_f, rhoe[cc], rhoesrc[cc], s_src, Yb, scb, gb, qd, wb, eb);
+  if (c < ncells)
+    for (int i = tm.lane; i < n; i += TEAM) ydot[(size_t)c * n + i] = s_f[i];
+}
+
+int launch_production_rate(const DeviceMechanism& m, const double* sc, const double* T, double* wdot, int ncells,
+                           int team, cudaStream_t st)
+{
+  const DevMech& M = *m.dm;
+  if (ncells <= 0) return 0;
+  if (team == 1) {
+    k_production_rate<1><<<(ncells + 63) / 64, 64, 0, st>>>(M, sc, T, wdot, ncells);
+  } else {
+    const int cells_per_block = 4;
+    const size_t shm = point_doubles(M.nsp, M.nrxn, false) * 8 * cells_per_block;
+    cudaFuncSetAttribute((const void*)k_production_rate<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    k_production_rate<32><<<(ncells + cells_per_block - 1) / cells_per_block, 32 * cells_per_block, shm, st>>>(
+      M, sc, T, wdot, ncells);
+  }
+  return (int)cudaGetLastError();
+}
+
+int launch_ajacobian(const DeviceMechanism& m, const double* sc, const double* T, int consP, double* J, int ncells,
+                     int team, cudaStream_t st)
+{
+  if (ncells <= 0) return 0;
+  const DevMech& M = *m.dm;
+  switch (M.nsp) {
+  case 9:
+    return launch_ajacobian_9(M, sc, T, consP, J, ncells, team, st);
+  case 21:
+    return launch_ajacobian_21(M, sc, T, consP, J, ncells, team, st);
+  case 53:
+    return launch_ajacobian_53(M, sc, T, consP, J, ncells, team, st);
+  case 88:
+    return launch_ajacobian_88(M, sc, T, consP, J, ncells, team, st);
+  default:
+    return (int)cudaErrorNotSupported;
+  }
+}
+
+int launch_t_from_energy(const DeviceMechanism& m, int eh, const double* e, const double* Y, double* T, int ncells,
+                         int team, cudaStream_t st)
+{
+  if (ncells <= 0) return 0;
+  const DevMech& M = *m.dm;
+  if (team == 1) {
+    k_t_from_energy<1><<<(ncells + 63) / 64, 64, 0, st>>>(M, eh, e, Y, T, ncells);
+  } else {
+    k_t_from_energy<32><<<(ncells + 3) / 4, 128, 0, st>>>(M, eh, e, Y, T, ncells);
+  }
+  return (int)cudaGetLastError();
+}
+
+int launch_reactor_rhs(const DeviceMechanism& m, int reactor_type, double t, const double* y, const double* rhoe,
+                       const double* rhoesrc, const double* src, double* ydot, int ncells, int team,
+                       cudaStream_t st)
+{
+  if (ncells <= 0) return 0;
+  const DevMech& M = *m.dm;
+  if (team == 1) {
+    k_reactor_rhs<1><<<(ncells + 63) / 64, 64, 0, st>>>(M, reactor_type, t, y, rhoe, rhoesrc, src, ydot, ncells);
+  } else {
+    const int cells_per_block = 4;
+    const size_t shm = (10 * (size_t)(M.nsp + 1) + M.nrxn) * 8 * cells_per_block;
+    cudaFuncSetAttribute((const void*)k_reactor_rhs<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    k_reactor_rhs<32><<<(ncells + cells_per_block - 1) / cells_per_block, 32 * cells_per_block, shm, st>>>(
+      M, reactor_type, t, y, rhoe, rhoesrc, src, ydot, ncells);
+  }
+  return (int)cudaGetLastError();
+}
+
+// ------------------------------------------------------------ box path
+// ReactorUtils.H:160-220 (box_flatten) for one cell per thread: Array4 views
+// -> species-major batch, T recomputed from the energy with the stored T as
+// the Newton start.
+__device__ inline long a4(const BoxView& v, int i, int j, int k, int n)
+{
+  return (long)(i - v.lo[0]) + (long)(j - v.lo[1]) * v.jstride + (long)(k - v.lo[2]) * v.kstride + (long)n * v.nstride;
+}
+
+__device__ inline long a4i(const BoxViewI& v, int i, int j, int k, int n)
+{
+  return (long)(i - v.lo[0]) + (long)(j - v.lo[1]) * v.jstride + (long)(k - v.lo[2]) * v.kstride + (long)n * v.nstride;
+}
+
+__global__ void k_box_flatten(DevMech M, int rtype, int clean, BoxArgs a, Batch b)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= b.ncells) return;
+  const int lx = a.hi[0] - a.lo[0] + 1, ly = a.hi[1] - a.lo[1] + 1;
+  const int i = a.lo[0] + c % lx, j = a.lo[1] + (c / lx) % ly, k = a.lo[2] + c / (lx * ly);
+  const int N = M.nsp;
+  int* mk = const_cast<int*>(b.mask);
+  mk[c] = a.mask.p ? a.mask.p[a4i(a.mask, i, j, k, 0)] : 1;
+  double Y[96];
+  double rho_old = 0.0, rho = 0.0;
+  if (clean)
+    for (int n = 0; n < N; n++) rho_old += a.rY.p[a4(a.rY, i, j, k, n)];
+  for (int n = 0; n < N; n++) {
+    const double v = a.rY.p[a4(a.rY, i, j, k, n)];
+    const double rYn = clean ? fmin(fmax(0.0, v), rho_old) : v;
+    b.y[(size_t)n * b.ld + c] = rYn;
+    b.src[(size_t)n * b.ld + c] = a.rYsrc.p[a4(a.rYsrc, i, j, k, n)];
+    rho += rYn;
+    Y[n] = rYn;
+  }
+  const double rinv = 1.0 / rho;
+  for (int n = 0; n < N; n++) Y[n] *= rinv;
+  double T = a.T.p[a4(a.T, i, j, k, 0)];
+  const double rE = a.rE.p[a4(a.rE, i, j, k, 0)];
+  const_cast<double*>(b.rhoe)[c] = rE;
+  const_cast<double*>(b.rhoesrc)[c] = a.rEs.p[a4(a.rEs, i, j, k, 0)];
+  Team<1> tm;
+  t_from_energy<1>(tm, M, rtype == 2, rE * rinv, Y, T);
+  b.y[(size_t)N * b.ld + c] = T;
+}
+
+// ReactorUtils.H:222-291 (box_unflatten): batch -> Array4 views, energy
+// advanced by dt * source, T from the new energy, FC = cost (0 if masked).
+__global__ void k_box_unflatten(DevMech M, int rtype, int clean, BoxArgs a, Batch b, double dt)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= b.ncells) return;
+  const int lx = a.hi[0] - a.lo[0] + 1, ly = a.hi[1] - a.lo[1] + 1;
+  const int i = a.lo[0] + c % lx, j = a.lo[1] + (c / lx) % ly, k = a.lo[2] + c / (lx * ly);
+  const int N = M.nsp;
+  if (b.mask[c] == -1) {
+    a.FC.p[a4(a.FC, i, j, k, 0)] = 0.0;
+    return;
+  }
+  double Y[96];
+  double rho_old = 0.0, rho_oc = 0.0, rho = 0.0;
+  if (clean) {
+    for (int n = 0; n < N; n++) rho_old += a.rY.p[a4(a.rY, i, j, k, n)];
+    for (int n = 0; n < N; n++) {
+      Y[n] = fmin(fmax(0.0, a.rY.p[a4(a.rY, i, j, k, n)]), rho_old);
+      rho_oc += Y[n];
+    }
+  }
+  for (int n = 0; n < N; n++) {
+    const long idx = a4(a.rY, i, j, k, n);
+    const double yv = b.y[(size_t)n * b.ld + c];
+    const double rYn = clean ? a.rY.p[idx] + (yv - Y[n]) * rho_old / rho_oc : yv;
+    a.rY.p[idx] = rYn;
+    rho += rYn;
+    Y[n] = rYn;
+  }
+  const double rinv = 1.0 / rho;
+  for (int n = 0; n < N; n++) Y[n] *= rinv;
+  double T = b.y[(size_t)N * b.ld + c];
+  const long ie = a4(a.rE, i, j, k, 0);
+  const double rE = b.rhoe[c] + dt * a.rEs.p[a4(a.rEs, i, j, k, 0)];
+  a.rE.p[ie] = rE;
+  Team<1> tm;
+  t_from_energy<1>(tm, M, rtype == 2, rE * rinv, Y, T);
+  a.T.p[a4(a.T, i, j, k, 0)] = T;
+  a.FC.p[a4(a.FC, i, j, k, 0)] = (double)(b.nfe ? b.nfe[c] : 0);
+}
+
+int launch_box_flatten(const DeviceMechanism& m, int rtype, int clean, const BoxArgs& a, Batch b, cudaStream_t st)
+{
+  if (b.ncells <= 0) return 0;
+  k_box_flatten<<<(b.ncells + 127) / 128, 128, 0, st>>>(*m.dm, rtype, clean, a, b);
+  return (int)cudaGetLastError();
+}
+
+int launch_box_unflatten(const DeviceMechanism& m, int rtype, int clean, const BoxArgs& a, Batch b, double dt,
+                         cudaStream_t st)
+{
+  if (b.ncells <= 0) return 0;
+  k_box_unflatten<<<(b.ncells + 127) / 128, 128, 0, st>>>(*m.dm, rtype, clean, a, b, dt);
+  return (int)cudaGetLastError();
+}
+
+// rX += dt * rX_src on device arrays (the flat path's energy update,
+// ReactorCvode.cpp:1652-1655)
+__global__ void k_energy_update(double* rX, const double* rXs, double dt, int n)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n) rX[c] = rX[c] + dt * rXs[c];
+}
+
+int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells, cudaStream_t st)
+{
+  if (ncells <= 0) return 0;
+  k_energy_update<<<(ncells + 255) / 256, 256, 0, st>>>(rX, rX_src, dt, ncells);
+  return (int)cudaGetLastError();
+}
+
+// Fuego::PYT2RE / PYT2RH (Source/Eos/Fuego.H:313-327): density from P, T, Y
+// (CKRHOY) and the mass-specific internal energy (eh = 0) or enthalpy
+// (eh = 1) at T.
+__global__ void k_pyt2re(DevMech M, int eh, const double* P, const double* T, const double* Y, double* rho, double* e,
+                         int ncells)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const double* y = Y + (size_t)c * M.nsp;
+  const double t = T[c];
+  double yow = 0.0;
+  for (int s = 0; s < M.nsp; s++) yow += y[s] * __ldg(M.imw + s);
+  rho[c] = P[c] / (RU * t * yow);
+  Team<1> tm;
+  e[c] = mix_e<1>(tm, M, eh, t, y);
+}
+
+int launch_pyt2re(const DeviceMechanism& m, int eh, const double* P, const double* T, const double* Y, double* rho,
+                  double* e, int ncells, cudaStream_t st)
+{
+  if (ncells <= 0) return 0;
+  k_pyt2re<<<(ncells + 127) / 128, 128, 0, st>>>(*m.dm, eh, P, T, Y, rho, e, ncells);
+  return (int)cudaGetLastError();
+}
+
+} // namespace ppb

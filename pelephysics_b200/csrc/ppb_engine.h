@@ -1,0 +1,96 @@
+// Host-side interface between the C-ABI layer and the CUDA kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "mech/mech_tables.h"
+
+namespace ppb {
+struct DevMech;
+struct Options;
+
+// A mechanism uploaded to one device.
+struct DeviceMechanism {
+  const PPBMechTables* host = nullptr;
+  int device = -1;
+  void* blob = nullptr; // one device allocation holding every table
+  DevMech* dm = nullptr; // host copy of the device pointer struct
+};
+
+int upload_mechanism(const PPBMechTables* t, DeviceMechanism* out);
+void free_mechanism(DeviceMechanism* m);
+const PPBMechTables* find_mechanism(const char* name);
+
+// Device-resident batch of cells, species-major (SoA): y[i * ld + c] for
+// i < N+1, src[i * ld + c] for i < N, ld >= ncells.
+struct Batch {
+  double* y;
+  double* src;
+  const double* rhoe;
+  const double* rhoesrc;
+  const double* atolv; // N+1 absolute tolerances or nullptr
+  const int* mask;     // per cell, -1 skips the cell; nullptr: all cells
+  int* status;         // per cell integrator flag (may be nullptr)
+  int* nfe;            // per cell RHS evaluations / RK steps (may be nullptr)
+  int ncells;
+  int ld;
+};
+
+enum Engine { ENGINE_PLAIN = 0, ENGINE_TUNED = 1 };
+enum Method { METHOD_BDF = 0, METHOD_RK64 = 1 };
+
+struct LaunchConfig {
+  int engine = ENGINE_TUNED;
+  int warps_per_block = 4;
+  int lu_fp32 = 0;
+  int persistent = 1; // work queue
+};
+
+// Integrate every cell of the batch over dt.  queue is a device int used by
+// the persistent kernel (reset inside the call).  Returns a cudaError_t.
+int launch_react(const DeviceMechanism& m, const Options& o, int method, const LaunchConfig& lc, Batch b,
+                 double dt, int* queue, cudaStream_t st);
+
+// Layout conversion kernels (HBM-bound): YCOrder AoS <-> species-major SoA.
+int launch_aos_to_soa(const double* aos, int nc_aos, double* soa, int ld, int ncomp, int ncells, cudaStream_t st);
+int launch_soa_to_aos(const double* soa, int ld, int ncomp, double* aos, int nc_aos, int ncells, cudaStream_t st);
+
+// Pointwise kernels (AoS per cell), team = 1 or 32.
+int launch_production_rate(const DeviceMechanism& m, const double* sc, const double* T, double* wdot, int ncells,
+                           int team, cudaStream_t st);
+int launch_ajacobian(const DeviceMechanism& m, const double* sc, const double* T, int consP, double* J, int ncells,
+                     int team, cudaStream_t st);
+int launch_t_from_energy(const DeviceMechanism& m, int eh, const double* e, const double* Y, double* T, int ncells,
+                         int team, cudaStream_t st);
+int launch_reactor_rhs(const DeviceMechanism& m, int reactor_type, double t, const double* y, const double* rhoe,
+                       const double* rhoesrc, const double* src, double* ydot, int ncells, int team,
+                       cudaStream_t st);
+
+// Array4-style views (device memory) of one box.
+struct BoxView {
+  double* p;
+  long jstride, kstride, nstride;
+  int lo[3];
+};
+struct BoxViewI {
+  int* p;
+  long jstride, kstride, nstride;
+  int lo[3];
+};
+struct BoxArgs {
+  int lo[3], hi[3]; // box (inclusive)
+  BoxView rY, rYsrc, T, rE, rEs, FC;
+  BoxViewI mask;    // p == nullptr: every cell active
+};
+// box_flatten / box_unflatten; the batch's mask array receives the Array4
+// mask values and must be writable device memory.
+int launch_box_flatten(const DeviceMechanism& m, int rtype, int clean, const BoxArgs& a, Batch b, cudaStream_t st);
+int launch_box_unflatten(const DeviceMechanism& m, int rtype, int clean, const BoxArgs& a, Batch b, double dt,
+                         cudaStream_t st);
+
+int launch_pyt2re(const DeviceMechanism& m, int eh, const double* P, const double* T, const double* Y, double* rho,
+                  double* e, int ncells, cudaStream_t st);
+int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells, cudaStream_t st);
+
+// Bytes of shared memory one team-integrated cell needs.
+size_t team_cell_bytes(const PPBMechTables* t, int lu_fp32);
+} // namespace ppb

@@ -1,0 +1,219 @@
+// Kernels of the B200 chemistry engine instantiated for one species count
+// (compiled once per mechanism size with -DPPB_NS=<N>).
+#include "ppb_engine.h"
+#include "ppb_work.cuh"
+
+#ifndef PPB_NS
+#error "compile with -DPPB_NS=<number of species>"
+#endif
+
+namespace ppb {
+
+// ------------------------------------------------------------ react kernels
+template <int NS, int TEAM, typename LT>
+__device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options& o, int method, Work<LT>& w,
+                          const Batch& b, int c, double dt)
+{
+  const int n = NS + 1;
+  if (b.mask && b.mask[c] == -1) {
+    if (tm.lane == 0) {
+      if (b.status) b.status[c] = ST_SKIPPED;
+      if (b.nfe) b.nfe[c] = 0;
+    }
+    return;
+  }
+  for (int i = tm.lane; i < n; i += TEAM) {
+    const double v = b.y[(size_t)i * b.ld + c];
+    w.zn[0][i] = v;
+    w.y[i] = v;
+    w.src[i] = (i < NS) ? b.src[(size_t)i * b.ld + c] : 0.0;
+    if (o.use_typ_vals) w.atolv[i] = b.atolv[i];
+  }
+  tm.sync();
+  const CellIn cin{b.rhoe[c], b.rhoesrc[c]};
+  int flag, cost;
+  if (method == METHOD_BDF) {
+    Bdf<NS, TEAM, LT> bdf(tm, M, o, w, cin);
+    flag = bdf.run(dt);
+    cost = bdf.s.nfe;
+  } else {
+    cost = rk64_cell<TEAM, LT>(tm, M, o, w, cin, dt);
+    flag = ST_OK;
+  }
+  for (int i = tm.lane; i < n; i += TEAM) b.y[(size_t)i * b.ld + c] = w.y[i];
+  if (tm.lane == 0) {
+    if (b.status) b.status[c] = flag;
+    if (b.nfe) b.nfe[c] = cost;
+  }
+  tm.sync();
+}
+
+// plain: one thread per cell, FP64, per-cell arrays in thread-local memory
+template <int NS>
+__global__ void __launch_bounds__(128) k_react_plain(DevMech M, Options o, int method, Batch b, double dt)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= b.ncells) return;
+  constexpr int n = NS + 1;
+  double buf[n * n + 22 * n];
+  double A[n * n];
+  int piv[n];
+  Work<double> w;
+  {
+    double* p = buf;
+    for (int j = 0; j < 6; j++) {
+      w.zn[j] = p;
+      p += n;
+    }
+    w.ewt = p; p += n;
+    w.acor = p; p += n;
+    w.y = p; p += n;
+    w.tempv = p; p += n;
+    w.ftemp = p; p += n;
+    w.delta = p; p += n;
+    w.J = p; p += n * n;
+    w.src = p; p += n;
+    w.atolv = p; p += n;
+    w.Y = p; p += n;
+    w.sc = p; p += n;
+    w.g = p; p += n;
+    w.wdot = p; p += n;
+    w.ei = p; p += n;
+    w.h1 = p; p += n;
+    w.h2 = p; p += n;
+    w.h3 = p; p += n;
+    w.qd = nullptr;
+    w.A = A;
+    w.piv = piv;
+  }
+  Team<1> tm;
+  react_one<NS, 1, double>(tm, M, o, method, w, b, c, dt);
+}
+
+// tuned: one warp per cell, shared-memory workspace, persistent work queue
+template <int NS, typename LT>
+__global__ void __launch_bounds__(256) k_react_team(DevMech M, Options o, int method, Batch b, double dt,
+                                                    int* queue, size_t cell_bytes, int persistent)
+{
+  extern __shared__ __align__(16) char smem[];
+  Team<32> tm;
+  const int warp = threadIdx.x / 32;
+  Work<LT> w;
+  carve<LT>(w, smem + (size_t)warp * cell_bytes, M.nsp, M.nrxn);
+  const int wpb = blockDim.x / 32;
+  if (persistent) {
+    for (;;) {
+      int c = 0;
+      if (tm.lane == 0) c = atomicAdd(queue, 1);
+      c = __shfl_sync(0xffffffffu, c, 0);
+      if (c >= b.ncells) break;
+      react_one<NS, 32, LT>(tm, M, o, method, w, b, c, dt);
+    }
+  } else {
+    const int c = blockIdx.x * wpb + warp;
+    if (c < b.ncells) react_one<NS, 32, LT>(tm, M, o, method, w, b, c, dt);
+  }
+}
+
+template <int NS>
+static int launch_react_ns(const DeviceMechanism& m, const Options& o, int method, const LaunchConfig& lc,
+                           Batch b, double dt, int* queue, cudaStream_t st)
+{
+  const DevMech& M = *m.dm;
+  if (b.ncells <= 0) return 0;
+  if (lc.engine == ENGINE_PLAIN) {
+    const int threads = 128;
+    const int blocks = (b.ncells + threads - 1) / threads;
+    k_react_plain<NS><<<blocks, threads, 0, st>>>(M, o, method, b, dt);
+    return (int)cudaGetLastError();
+  }
+  const int wpb = lc.warps_per_block > 0 ? lc.warps_per_block : 4;
+  const size_t cb = lc.lu_fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
+  const size_t shm = cb * wpb;
+  auto kern = lc.lu_fp32 ? (void (*)(DevMech, Options, int, Batch, double, int*, size_t, int))k_react_team<NS, float>
+                         : (void (*)(DevMech, Options, int, Batch, double, int*, size_t, int))k_react_team<NS, double>;
+  cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  if (e != cudaSuccess) return (int)e;
+  int blocks;
+  if (lc.persistent) {
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)kern, wpb * 32, shm);
+    if (e != cudaSuccess) return (int)e;
+    if (per_sm < 1) return (int)cudaErrorInvalidConfiguration;
+    blocks = nsm * per_sm;
+    const int need = (b.ncells + wpb - 1) / wpb;
+    if (blocks > need) blocks = need;
+    e = cudaMemsetAsync(queue, 0, sizeof(int), st);
+    if (e != cudaSuccess) return (int)e;
+  } else {
+    blocks = (b.ncells + wpb - 1) / wpb;
+  }
+  kern<<<blocks, wpb * 32, shm, st>>>(M, o, method, b, dt, queue, cb, lc.persistent);
+  return (int)cudaGetLastError();
+}
+
+template <int TEAM, int PER>
+__global__ void k_ajacobian(DevMech M, const double* sc, const double* T, int consP, double* J, int ncells)
+{
+  extern __shared__ __align__(16) double psm[];
+  Team<TEAM> tm;
+  const int N = M.nsp, n = N + 1;
+  const int per_block = blockDim.x / TEAM;
+  const int slot = threadIdx.x / TEAM;
+  const int c = blockIdx.x * per_block + slot;
+  if (TEAM == 1 && c >= ncells) return;
+  const int cc = c < ncells ? c : ncells - 1;
+  double local[8 * 96];
+  double* base = (TEAM == 1) ? local : psm + (size_t)slot * point_doubles(N, M.nrxn, true);
+  double* s_sc = base;
+  double* s_g = base + n;
+  double* s_w = base + 2 * n;
+  double* h1 = base + 3 * n;
+  double* h2 = base + 4 * n;
+  double* h3 = base + 5 * n;
+  double* h4 = base + 6 * n;
+  // serial: accumulate straight into the output; team: into shared memory
+  double* s_J = (TEAM == 1) ? J + (size_t)cc * n * n : base + 8 * n + M.nrxn;
+  for (int s = tm.lane; s < N; s += TEAM) s_sc[s] = sc[(size_t)cc * N + s];
+  tm.sync();
+  RateScratch rs{s_sc, s_g, nullptr};
+  ajacobian<TEAM, PER>(tm, M, s_J, s_sc, T[cc], consP, rs, s_w, h1, h2, h3, h4);
+  if (TEAM > 1 && c < ncells)
+    for (int i = tm.lane; i < n * n; i += TEAM) J[(size_t)c * n * n + i] = s_J[i];
+}
+
+template <int NS>
+static int launch_ajac_ns(const DevMech& M, const double* sc, const double* T, int consP, double* J, int ncells,
+                          int team, cudaStream_t st)
+{
+  if (team == 1) {
+    const int threads = 64;
+    k_ajacobian<1, NS><<<(ncells + threads - 1) / threads, threads, 0, st>>>(M, sc, T, consP, J, ncells);
+  } else {
+    const int cells_per_block = 2;
+    const size_t shm = point_doubles(M.nsp, M.nrxn, true) * 8 * cells_per_block;
+    auto k = k_ajacobian<32, (NS + 31) / 32>;
+    cudaError_t e = cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    if (e != cudaSuccess) return (int)e;
+    k<<<(ncells + cells_per_block - 1) / cells_per_block, 32 * cells_per_block, shm, st>>>(M, sc, T, consP, J,
+                                                                                          ncells);
+  }
+  return (int)cudaGetLastError();
+}
+
+
+#define PPB_CAT2(a, b) a##b
+#define PPB_CAT(a, b) PPB_CAT2(a, b)
+int PPB_CAT(launch_react_, PPB_NS)(const DeviceMechanism& m, const Options& o, int method, const LaunchConfig& lc,
+                                   Batch b, double dt, int* queue, cudaStream_t st)
+{
+  return launch_react_ns<PPB_NS>(m, o, method, lc, b, dt, queue, st);
+}
+int PPB_CAT(launch_ajacobian_, PPB_NS)(const DevMech& M, const double* sc, const double* T, int consP, double* J,
+                                       int ncells, int team, cudaStream_t st)
+{
+  return launch_ajac_ns<PPB_NS>(M, sc, T, consP, J, ncells, team, st);
+}
+} // namespace ppb

@@ -1,0 +1,680 @@
+// Device-side mechanism arithmetic for the B200 chemistry engine.
+//
+// Every function here evaluates the same formulas as the reference's
+// CEPTR-generated Mechanisms/<mech>/mechanism.H (productionRate, aJacobian,
+// NASA-7 thermo, GET_T_GIVEN_EY/HY) from data tables instead of straight-line
+// code, so one compiled kernel serves every mechanism of a given species
+// count.  The functions are written for a "team" of TEAM lanes that share one
+// cell: TEAM == 1 is one thread per cell (the plain path), TEAM == 32 is one
+// warp per cell (the tuned path).  Per-cell vectors live in memory shared by
+// the team (shared memory for TEAM > 1, thread-local memory for TEAM == 1);
+// lane l owns entries l, l+TEAM, ...  Team reductions use xor-butterflies so
+// every lane ends with a bitwise-identical scalar, which keeps the control
+// flow of the integrator uniform across the team.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "mech/mech_tables.h"
+
+namespace ppb {
+
+constexpr double RU = 8.31446261815324e7; // erg/(mol K), PhysicsConstants.H:11
+
+// Device copy of PPBMechTables (same layout) plus the species-major gather
+// lists used to sum reaction rates into species rates without atomics.
+struct DevMech {
+  int nsp, nrxn;
+  const double *mw, *imw, *tmid;
+  const double *th_cv, *th_cp, *th_dcp, *th_u, *th_h, *th_g;
+  const int *rx_kind, *rx_rev, *rx_kcpow;
+  const double *rx_A, *rx_beta, *rx_EaR, *rx_sum_nuk;
+  const int *fps_n, *fps_sp;
+  const double* fps_c;
+  const int *rps_n, *rps_sp;
+  const double* rps_c;
+  const int *kc_n, *kc_sp;
+  const double* kc_c;
+  const int *wup_n, *wup_sp;
+  const double* wup_c;
+  const int *jn_n, *jn_sp;
+  const double* jn_c;
+  const int *hr_n, *hr_sp;
+  const double* hr_c;
+  const int *hp_n, *hp_sp;
+  const double* hp_c;
+  const int *eff_off, *eff_sp;
+  const double *eff_e, *eff_m1;
+  const double* fo_d;
+  const int* fo_i;
+  // species-major gather of the productionRate updates: for species s,
+  // entries g in [wg_off[s], wg_off[s+1]) add wg_c[g] * qdot[wg_rx[g]]
+  const int *wg_off, *wg_rx;
+  const double* wg_c;
+};
+
+template <int TEAM>
+struct Team {
+  int lane;
+  unsigned mask;
+  __device__ __forceinline__ Team()
+  {
+    lane = (TEAM == 1) ? 0 : (int)(threadIdx.x % TEAM);
+    if (TEAM == 32) {
+      mask = 0xffffffffu;
+    } else if (TEAM == 1) {
+      mask = 1u << (threadIdx.x % 32);
+    } else {
+      mask = ((1u << (TEAM & 31)) - 1u) << ((threadIdx.x % 32) / TEAM * TEAM);
+    }
+  }
+  __device__ __forceinline__ void sync() const
+  {
+    if (TEAM > 1) __syncwarp(mask);
+  }
+  __device__ __forceinline__ double sum(double x) const
+  {
+#pragma unroll
+    for (int o = TEAM / 2; o > 0; o >>= 1) x += __shfl_xor_sync(mask, x, o, TEAM);
+    return x;
+  }
+  __device__ __forceinline__ double max(double x) const
+  {
+#pragma unroll
+    for (int o = TEAM / 2; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(mask, x, o, TEAM));
+    return x;
+  }
+  __device__ __forceinline__ int imax(int x) const
+  {
+#pragma unroll
+    for (int o = TEAM / 2; o > 0; o >>= 1) x = ::max(x, __shfl_xor_sync(mask, x, o, TEAM));
+    return x;
+  }
+  // broadcast from team lane src
+  __device__ __forceinline__ double bcast(double x, int src) const
+  {
+    return (TEAM == 1) ? x : __shfl_sync(mask, x, src, TEAM);
+  }
+};
+
+__device__ __forceinline__ int nasa_range(const DevMech& M, int s, double T)
+{
+  const double tm = __ldg(M.tmid + s);
+  return (tm >= 0.0 && T < tm) ? 0 : 1;
+}
+
+// mechanism.H cv_R (thermo.py:516-526)
+__device__ __forceinline__ double cv_R(const DevMech& M, int s, double T)
+{
+  const double* c = M.th_cv + (2 * s + nasa_range(M, s, T)) * 5;
+  const double T2 = T * T, T3 = T * T * T, T4 = T * T * T * T;
+  return __ldg(c) + __ldg(c + 1) * T + __ldg(c + 2) * T2 + __ldg(c + 3) * T3 + __ldg(c + 4) * T4;
+}
+// mechanism.H cp_R (thermo.py:549-559)
+__device__ __forceinline__ double cp_R(const DevMech& M, int s, double T)
+{
+  const double* c = M.th_cp + (2 * s + nasa_range(M, s, T)) * 5;
+  const double T2 = T * T, T3 = T * T * T, T4 = T * T * T * T;
+  return __ldg(c) + __ldg(c + 1) * T + __ldg(c + 2) * T2 + __ldg(c + 3) * T3 + __ldg(c + 4) * T4;
+}
+// mechanism.H dcvpRdT (thermo.py:561-570)
+__device__ __forceinline__ double dcvpRdT(const DevMech& M, int s, double T)
+{
+  const double* c = M.th_dcp + (2 * s + nasa_range(M, s, T)) * 4;
+  const double T2 = T * T, T3 = T * T * T;
+  return __ldg(c) + __ldg(c + 1) * T + __ldg(c + 2) * T2 + __ldg(c + 3) * T3;
+}
+// mechanism.H speciesInternalEnergy, e/RT (thermo.py:625-646)
+__device__ __forceinline__ double u_RT(const DevMech& M, int s, double T, double invT)
+{
+  const double* c = M.th_u + (2 * s + nasa_range(M, s, T)) * 6;
+  const double T2 = T * T, T3 = T * T * T, T4 = T * T * T * T;
+  return __ldg(c) + __ldg(c + 1) * T + __ldg(c + 2) * T2 + __ldg(c + 3) * T3 + __ldg(c + 4) * T4 +
+         __ldg(c + 5) * invT;
+}
+// mechanism.H speciesEnthalpy, h/RT (thermo.py:649-669)
+__device__ __forceinline__ double h_RT(const DevMech& M, int s, double T, double invT)
+{
+  const double* c = M.th_h + (2 * s + nasa_range(M, s, T)) * 6;
+  const double T2 = T * T, T3 = T * T * T, T4 = T * T * T * T;
+  return __ldg(c) + __ldg(c + 1) * T + __ldg(c + 2) * T2 + __ldg(c + 3) * T3 + __ldg(c + 4) * T4 +
+         __ldg(c + 5) * invT;
+}
+// mechanism.H gibbs, g/RT (thermo.py:572-595)
+__device__ __forceinline__ double g_RT(const DevMech& M, int s, double T, double invT, double logT)
+{
+  const double* c = M.th_g + (2 * s + nasa_range(M, s, T)) * 7;
+  const double T2 = T * T, T3 = T * T * T, T4 = T * T * T * T;
+  return __ldg(c) * invT + __ldg(c + 1) + __ldg(c + 2) * logT + __ldg(c + 3) * T + __ldg(c + 4) * T2 +
+         __ldg(c + 5) * T3 + __ldg(c + 6) * T4;
+}
+
+// Mixture energy (EH=0: CKUBMS, erg/g) or enthalpy (EH=1: CKHBMS) and the
+// matching heat capacity (CKCVBS / CKCPBS) of mass fractions Y (team-shared).
+template <int TEAM>
+__device__ __forceinline__ void mix_e_c(
+  const Team<TEAM>& tm, const DevMech& M, int EH, double T, const double* Y, double& e, double& c)
+{
+  const double invT = 1.0 / T;
+  double se = 0.0, sc = 0.0;
+  for (int s = tm.lane; s < M.nsp; s += TEAM) {
+    const double im = __ldg(M.imw + s);
+    const double ys = Y[s];
+    se += ys * (EH ? h_RT(M, s, T, invT) : u_RT(M, s, T, invT)) * im;
+    sc += ys * (EH ? cp_R(M, s, T) : cv_R(M, s, T)) * im;
+  }
+  se = tm.sum(se);
+  sc = tm.sum(sc);
+  const double RT = RU * T;
+  e = se * RT;
+  c = sc * RU;
+}
+
+template <int TEAM>
+__device__ __forceinline__ double mix_e(const Team<TEAM>& tm, const DevMech& M, int EH, double T, const double* Y)
+{
+  const double invT = 1.0 / T;
+  double se = 0.0;
+  for (int s = tm.lane; s < M.nsp; s += TEAM) {
+    se += Y[s] * (EH ? h_RT(M, s, T, invT) : u_RT(M, s, T, invT)) * __ldg(M.imw + s);
+  }
+  se = tm.sum(se);
+  return se * (RU * T);
+}
+
+template <int TEAM>
+__device__ __forceinline__ double mix_c(const Team<TEAM>& tm, const DevMech& M, int EH, double T, const double* Y)
+{
+  double sc = 0.0;
+  for (int s = tm.lane; s < M.nsp; s += TEAM) {
+    sc += Y[s] * (EH ? cp_R(M, s, T) : cv_R(M, s, T)) * __ldg(M.imw + s);
+  }
+  sc = tm.sum(sc);
+  return sc * RU;
+}
+
+// mechanism.H GET_T_GIVEN_EY / GET_T_GIVEN_HY: Newton from the supplied T,
+// |step| <= 100 K, stop at |dT| < 1e-6 K, <= 200 iterations, linear
+// extrapolation outside [90, 4000] K (returns 1 there).
+template <int TEAM>
+__device__ int t_from_energy(const Team<TEAM>& tm, const DevMech& M, int EH, double e, const double* Y, double& t)
+{
+  const double tmin = 90, tmax = 4000;
+  const double emin = mix_e(tm, M, EH, tmin, Y);
+  const double emax = mix_e(tm, M, EH, tmax, Y);
+  if (e < emin) {
+    t = tmin - (emin - e) / mix_c(tm, M, EH, tmin, Y);
+    return 1;
+  }
+  if (e > emax) {
+    t = tmax - (emax - e) / mix_c(tm, M, EH, tmax, Y);
+    return 1;
+  }
+  double t1 = t;
+  if (t1 < tmin || t1 > tmax) t1 = tmin + (tmax - tmin) / (emax - emin) * (e - emin);
+  for (int i = 0; i < 200; ++i) {
+    double e1, cv;
+    mix_e_c(tm, M, EH, t1, Y, e1, cv);
+    double dt = (e - e1) / cv;
+    if (dt > 100.) {
+      dt = 100.;
+    } else if (dt < -100.) {
+      dt = -100.;
+    } else if (fabs(dt) < 1.e-6) {
+      break;
+    }
+    t1 += dt;
+  }
+  t = t1;
+  return 0;
+}
+
+__device__ __forceinline__ double phase_space(const int* sp, const double* c, int n, const double* sc)
+{
+  double p = 1.0;
+  for (int j = 0; j < n; j++) {
+    const double x = sc[__ldg(sp + j)];
+    const int o = (int)__ldg(c + j);
+    double t = x;
+    for (int q = 1; q < o; q++) t *= x;
+    p *= t;
+  }
+  return p;
+}
+
+__device__ __forceinline__ double refc_pow(int p, double refC, double refCinv)
+{
+  double r = 1.0;
+  for (int q = 0; q < p; q++) r *= refCinv;
+  for (int q = 0; q < -p; q++) r *= refC;
+  return r;
+}
+
+// Net rate of progress of reaction r as the reference's productionRate
+// computes it (production.py:991-1435); optionally returns q_f and q_r.
+__device__ __forceinline__ double rxn_qdot(
+  const DevMech& M, int r, double T, double invT, double logT, double refC, double refCinv, double mixture,
+  const double* sc, const double* g, double* qf_out = nullptr, double* qr_out = nullptr)
+{
+  const int kind = __ldg(M.rx_kind + r);
+  const double k_f = __ldg(M.rx_A + r) * exp(__ldg(M.rx_beta + r) * logT - __ldg(M.rx_EaR + r) * invT);
+  double Corr = 1.0;
+  const bool corr = (kind == PPB_RX_THIRD || kind == PPB_RX_TROE || kind == PPB_RX_LINDEMANN);
+  if (corr) {
+    Corr = mixture;
+    const int e1 = __ldg(M.eff_off + r + 1);
+    for (int e = __ldg(M.eff_off + r); e < e1; e++) {
+      const double m1 = __ldg(M.eff_m1 + e);
+      if (m1 != 0.0) Corr += m1 * sc[__ldg(M.eff_sp + e)];
+    }
+  }
+  if (kind == PPB_RX_TROE || kind == PPB_RX_LINDEMANN) {
+    const double* fd = M.fo_d + r * PPB_NFOD;
+    const int* fi = M.fo_i + r * PPB_NFOI;
+    const double redP =
+      Corr / k_f * __ldg(fd + PPB_FO_P0) * exp(__ldg(fd + PPB_FO_BETA0) * logT - __ldg(fd + PPB_FO_EAR0) * invT);
+    const double F = redP / (1.0 + redP);
+    if (kind == PPB_RX_TROE) {
+      const double logPred = log10(redP);
+      double fc = 0.0;
+      if (__ldg(fi + PPB_FOI_P1)) fc = __ldg(fd + PPB_FO_OMA) * exp(-T * __ldg(fd + PPB_FO_IT3));
+      if (__ldg(fi + PPB_FOI_P2)) fc += __ldg(fd + PPB_FO_A) * exp(-T * __ldg(fd + PPB_FO_IT1));
+      if (__ldg(fi + PPB_FOI_NTROE) == 4) fc += exp(-__ldg(fd + PPB_FO_T2) * invT);
+      const double logFcent = log10(fc);
+      const double troe_c = -0.4 - 0.67 * logFcent;
+      const double troe_n = 0.75 - 1.27 * logFcent;
+      const double troe = (troe_c + logPred) / (troe_n - 0.14 * (troe_c + logPred));
+      const double F_troe = exp(M_LN10 * logFcent / (1.0 + troe * troe));
+      Corr = F * F_troe;
+    } else {
+      Corr = F;
+    }
+  }
+  const double phf = phase_space(M.fps_sp + r * PPB_MAXPS, M.fps_c + r * PPB_MAXPS, __ldg(M.fps_n + r), sc);
+  const double qf = corr ? Corr * k_f * phf : k_f * phf;
+  double qr = 0.0;
+  if (__ldg(M.rx_rev + r)) {
+    double arg = 0.0;
+    const int nk = __ldg(M.kc_n + r);
+    for (int j = 0; j < nk; j++) arg += __ldg(M.kc_c + r * PPB_MAXKC + j) * g[__ldg(M.kc_sp + r * PPB_MAXKC + j)];
+    const double phr = phase_space(M.rps_sp + r * PPB_MAXPS, M.rps_c + r * PPB_MAXPS, __ldg(M.rps_n + r), sc);
+    qr = (corr ? Corr * k_f : k_f) * exp(-arg) * refc_pow(__ldg(M.rx_kcpow + r), refC, refCinv) * phr;
+  }
+  if (qf_out) *qf_out = qf;
+  if (qr_out) *qr_out = qr;
+  return qf - qr;
+}
+
+// Per-cell scratch for the rate evaluation (team-shared).
+struct RateScratch {
+  double* sc;  // [nsp] SI concentrations
+  double* g;   // [nsp] g/RT
+  double* qd;  // [nrxn] net rates (TEAM > 1)
+};
+
+// productionRate (SI): wdot[s] for s owned by the lane (team-shared wdot).
+template <int TEAM>
+__device__ void production_rate(
+  const Team<TEAM>& tm, const DevMech& M, double* wdot, const double* sc_in, double T, RateScratch& rs)
+{
+  const double invT = 1.0 / T;
+  const double logT = log(T);
+  const double refC = 101325 / 8.31446 * invT;
+  const double refCinv = 1 / refC;
+  double mix = 0.0;
+  for (int s = tm.lane; s < M.nsp; s += TEAM) {
+    mix += sc_in[s];
+    rs.g[s] = g_RT(M, s, T, invT, logT);
+  }
+  const double mixture = tm.sum(mix);
+  tm.sync();
+  if (TEAM == 1) {
+    for (int s = 0; s < M.nsp; s++) wdot[s] = 0.0;
+    for (int r = 0; r < M.nrxn; r++) {
+      const double qdot = rxn_qdot(M, r, T, invT, logT, refC, refCinv, mixture, sc_in, rs.g);
+      const int nw = __ldg(M.wup_n + r);
+      for (int j = 0; j < nw; j++) {
+        const int s = __ldg(M.wup_sp + r * PPB_MAXW + j);
+        const double c = __ldg(M.wup_c + r * PPB_MAXW + j);
+        if (c == -1.0) {
+          wdot[s] -= qdot;
+        } else if (c == 1.0) {
+          wdot[s] += qdot;
+        } else if (c < 0) {
+          wdot[s] -= (-c) * qdot;
+        } else {
+          wdot[s] += c * qdot;
+        }
+      }
+    }
+  } else {
+    for (int r = tm.lane; r < M.nrxn; r += TEAM) {
+      rs.qd[r] = rxn_qdot(M, r, T, invT, logT, refC, refCinv, mixture, sc_in, rs.g);
+    }
+    tm.sync();
+    for (int s = tm.lane; s < M.nsp; s += TEAM) {
+      double w = 0.0;
+      const int g1 = __ldg(M.wg_off + s + 1);
+      for (int gi = __ldg(M.wg_off + s); gi < g1; gi++) w += __ldg(M.wg_c + gi) * rs.qd[__ldg(M.wg_rx + gi)];
+      wdot[s] = w;
+    }
+  }
+  tm.sync();
+}
+
+__device__ __forceinline__ bool has_sp(const int* sp, int n, int k)
+{
+  for (int j = 0; j < n; j++)
+    if (__ldg(sp + j) == k) return true;
+  return false;
+}
+
+__device__ __forceinline__ double dphase(const int* sp, const double* c, int n, const double* sc, int k)
+{
+  double p = 1.0;
+  for (int j = 0; j < n; j++) {
+    const double x = sc[__ldg(sp + j)];
+    const int o = (int)__ldg(c + j);
+    if (__ldg(sp + j) == k) {
+      if (o > 1) {
+        p *= (double)o;
+        for (int q = 1; q < o; q++) p *= x;
+      }
+    } else {
+      double t = x;
+      for (int q = 1; q < o; q++) t *= x;
+      p *= t;
+    }
+  }
+  return p;
+}
+
+// The reference's analytical Jacobian (jacobian.py:12-283, :546-1305), SI,
+// column-major J[k*(N+1)+m] = d wdot_m / d sc_k with the temperature row and
+// column.  Reactions are visited in order by the whole team; lane l owns
+// columns k = l, l+TEAM, ...  The consP == 0 branch reproduces the generated
+// code exactly, including its use of dqdc[k] values left over from an
+// earlier reaction when a species has zero third-body efficiency and no rate
+// term (the generated code never assigns dqdc[k] then but still reads it).
+// wdot/hrt/crt/dcrt/ehrt are team-shared scratch of length nsp.
+template <int TEAM, int PER>
+__device__ void ajacobian(
+  const Team<TEAM>& tm, const DevMech& M, double* J, const double* sc, double T, int consP, RateScratch& rs,
+  double* wdot, double* hrt, double* crt, double* dcrt, double* ehrt)
+{
+  const int N = M.nsp, n = N + 1;
+  for (int i = tm.lane; i < n * n; i += TEAM) J[i] = 0.0;
+  const double invT = 1.0 / T;
+  const double invT2 = invT * invT;
+  const double logT = log(T);
+  const double refC = 101325 / 8.31446 / T;
+  const double refCinv = 1.0 / refC;
+  double mix = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) {
+    mix += sc[s];
+    rs.g[s] = g_RT(M, s, T, invT, logT);
+    hrt[s] = h_RT(M, s, T, invT);
+    wdot[s] = 0.0;
+  }
+  const double mixture = tm.sum(mix);
+  tm.sync();
+  const double ln10 = log(10.0);
+  const double log10e = 1.0 / log(10.0);
+  double dq[PER]; // dqdc of the lane's species, carried across reactions
+#pragma unroll
+  for (int p = 0; p < PER; p++) dq[p] = 0.0;
+  for (int r = 0; r < M.nrxn; r++) {
+    const int kind = __ldg(M.rx_kind + r);
+    const bool falloff = (kind == PPB_RX_TROE || kind == PPB_RX_LINDEMANN);
+    const bool has_alpha = (kind == PPB_RX_THIRD) || falloff;
+    const bool rev = __ldg(M.rx_rev + r) != 0;
+    const int* fsp = M.fps_sp + r * PPB_MAXPS;
+    const double* fc = M.fps_c + r * PPB_MAXPS;
+    const int fn = __ldg(M.fps_n + r);
+    const int* rsp = M.rps_sp + r * PPB_MAXPS;
+    const double* rc = M.rps_c + r * PPB_MAXPS;
+    const int rn = __ldg(M.rps_n + r);
+    const int e0 = __ldg(M.eff_off + r), e1 = __ldg(M.eff_off + r + 1);
+    double alpha = 0.0;
+    if (has_alpha) {
+      alpha = mixture;
+      for (int e = e0; e < e1; e++) {
+        const double em1 = __ldg(M.eff_e + e) - 1.0;
+        if (em1 != 0.0) alpha += em1 * sc[__ldg(M.eff_sp + e)];
+      }
+    }
+    const double phi_f = phase_space(fsp, fc, fn, sc);
+    double k_f = __ldg(M.rx_A + r) * exp(__ldg(M.rx_beta + r) * logT - __ldg(M.rx_EaR + r) * invT);
+    const double dlnkfdT = __ldg(M.rx_beta + r) * invT + __ldg(M.rx_EaR + r) * invT2;
+    double Pr = 0.0, fPr = 0.0, F = 1.0, dlogFdlogPr = 0.0, dlogFdT = 0.0, dlogfPrdT = 0.0;
+    if (falloff) {
+      const double* fd = M.fo_d + r * PPB_NFOD;
+      const int* fi = M.fo_i + r * PPB_NFOI;
+      const double k_0 =
+        __ldg(fd + PPB_FO_K0) * exp(__ldg(fd + PPB_FO_BETA0) * logT - __ldg(fd + PPB_FO_EAR0) * invT);
+      Pr = __ldg(fd + PPB_FO_PRDIM) * alpha / k_f * k_0;
+      fPr = Pr / (1.0 + Pr);
+      const double dlnk0dT = __ldg(fd + PPB_FO_BETA0) * invT + __ldg(fd + PPB_FO_EAR0) * invT2;
+      const double dlogPrdT = log10e * (dlnk0dT - dlnkfdT);
+      dlogfPrdT = dlogPrdT / (1.0 + Pr);
+      if (kind == PPB_RX_TROE) {
+        const double a = __ldg(fd + PPB_FO_A), T3 = __ldg(fd + PPB_FO_T3);
+        const double T1 = __ldg(fd + PPB_FO_T1), T2 = __ldg(fd + PPB_FO_T2);
+        const double logPr = log10(Pr);
+        const double Fcent1 = __ldg(fi + PPB_FOI_J1) ? (1. - a) * exp(-T / T3) : 0.;
+        const double Fcent2 = __ldg(fi + PPB_FOI_J2) ? a * exp(-T / T1) : 0.;
+        const double Fcent3 = (__ldg(fi + PPB_FOI_NTROE) == 4) ? exp(-T2 * invT) : 0.;
+        const double Fcent = Fcent1 + Fcent2 + Fcent3;
+        const double logFcent = log10(Fcent);
+        const double troe_c = -.4 - .67 * logFcent;
+        const double troe_n = .75 - 1.27 * logFcent;
+        const double troePr_den = 1.0 / (troe_n - .14 * (troe_c + logPr));
+        const double troePr = (troe_c + logPr) * troePr_den;
+        const double troe = 1.0 / (1.0 + troePr * troePr);
+        F = exp(M_LN10 * logFcent * troe);
+        double s = 0.0;
+        if (__ldg(fi + PPB_FOI_J1)) s += -Fcent1 / T3;
+        if (__ldg(fi + PPB_FOI_J2)) s += -Fcent2 / T1;
+        if (__ldg(fi + PPB_FOI_J3)) s += Fcent3 * T2 * invT2;
+        const double dlogFcentdT = log10e / Fcent * (s);
+        const double dlogFdcn_fac = 2.0 * logFcent * troe * troe * troePr * troePr_den;
+        const double dlogFdc = -troe_n * dlogFdcn_fac * troePr_den;
+        const double dlogFdn = dlogFdcn_fac * troePr;
+        dlogFdlogPr = dlogFdc;
+        dlogFdT = dlogFcentdT * (troe - 0.67 * dlogFdc - 1.27 * dlogFdn) + dlogFdlogPr * dlogPrdT;
+      }
+    }
+    double q, q_nocor = 0.0, Corr = 1.0, dqdT, k_r = 0.0;
+    if (!rev) {
+      if (!has_alpha) {
+        q = k_f * phi_f;
+      } else {
+        q_nocor = k_f * phi_f;
+        if (falloff) {
+          Corr = fPr * F;
+          q = Corr * q_nocor;
+        } else {
+          q = alpha * q_nocor;
+        }
+      }
+      if (falloff) {
+        dqdT = Corr * dlnkfdT * k_f * phi_f + ln10 * (dlogfPrdT + dlogFdT) * q;
+      } else if (has_alpha) {
+        dqdT = alpha * dlnkfdT * k_f * phi_f;
+      } else {
+        dqdT = dlnkfdT * k_f * phi_f;
+      }
+    } else {
+      const double phi_r = phase_space(rsp, rc, rn, sc);
+      double arg = 0.0;
+      const int nk = __ldg(M.kc_n + r);
+      for (int j = 0; j < nk; j++) arg += __ldg(M.kc_c + r * PPB_MAXKC + j) * rs.g[__ldg(M.kc_sp + r * PPB_MAXKC + j)];
+      const double Kc = refc_pow(-__ldg(M.rx_kcpow + r), refC, refCinv) * exp(arg);
+      k_r = k_f / Kc;
+      double hsum_r = 0.0, hsum_p = 0.0;
+      const int nhr = __ldg(M.hr_n + r), nhp = __ldg(M.hp_n + r);
+      for (int j = 0; j < nhr; j++) {
+        const double c = __ldg(M.hr_c + r * PPB_MAXPS + j);
+        const double h = hrt[__ldg(M.hr_sp + r * PPB_MAXPS + j)];
+        hsum_r += (c == 1.0) ? h : c * h;
+      }
+      for (int j = 0; j < nhp; j++) {
+        const double c = __ldg(M.hp_c + r * PPB_MAXPS + j);
+        const double h = hrt[__ldg(M.hp_sp + r * PPB_MAXPS + j)];
+        hsum_p += (c == 1.0) ? h : c * h;
+      }
+      const double snk = __ldg(M.rx_sum_nuk + r);
+      double inner = -(hsum_r) + (hsum_p);
+      if (snk > 0) {
+        inner -= snk;
+      } else if (snk < 0) {
+        inner += -snk;
+      }
+      const double dlnKcdT = invT * (inner);
+      const double dkrdT = (dlnkfdT - dlnKcdT) * k_r;
+      if (!has_alpha) {
+        q = k_f * phi_f - k_r * phi_r;
+      } else {
+        q_nocor = k_f * phi_f - k_r * phi_r;
+        if (falloff) {
+          Corr = fPr * F;
+          q = Corr * q_nocor;
+        } else {
+          q = alpha * q_nocor;
+        }
+      }
+      if (falloff) {
+        dqdT = Corr * (dlnkfdT * k_f * phi_f - dkrdT * phi_r) + ln10 * (dlogfPrdT + dlogFdT) * q;
+      } else if (has_alpha) {
+        dqdT = alpha * (dlnkfdT * k_f * phi_f - dkrdT * phi_r);
+      } else {
+        dqdT = (dlnkfdT * k_f * phi_f - dkrdT * phi_r);
+      }
+    }
+    const int jnn = __ldg(M.jn_n + r);
+    const int* jsp = M.jn_sp + r * PPB_MAXJN;
+    const double* jc = M.jn_c + r * PPB_MAXJN;
+    // wdot (owned species only) and the d/dT row
+    for (int j = 0; j < jnn; j++) {
+      const int s = __ldg(jsp + j);
+      const double nu = __ldg(jc + j);
+      if (s % TEAM == tm.lane) {
+        if (nu == 1) {
+          wdot[s] += q;
+        } else if (nu == -1) {
+          wdot[s] -= q;
+        } else if (nu > 0) {
+          wdot[s] += nu * q;
+        } else if (nu < 0) {
+          wdot[s] -= (-nu) * q;
+        }
+        if (nu != 0) J[N * n + s] += nu * dqdT;
+      }
+    }
+    if (falloff) {
+      k_f *= Corr;
+      if (rev) k_r *= Corr;
+    } else if (has_alpha) {
+      k_f *= alpha;
+      if (rev) k_r *= alpha;
+    }
+    const double dcdc_fac = falloff ? q / alpha * (1.0 / (Pr + 1.0) + dlogFdlogPr) : 0.0;
+    const int* hrs = M.hr_sp + r * PPB_MAXPS;
+    const int hrn = __ldg(M.hr_n + r);
+    const int* hps = M.hp_sp + r * PPB_MAXPS;
+    const int hpn = __ldg(M.hp_n + r);
+    const double fac = falloff ? dcdc_fac : q_nocor;
+#pragma unroll
+    for (int p = 0; p < PER; p++) {
+      const int k = tm.lane + p * TEAM;
+      if (k >= N) break;
+      const bool inr = has_sp(hrs, hrn, k);
+      const bool inp = rev && has_sp(hps, hpn, k);
+      double d = 0.0;
+      bool apply = false;
+      if (has_alpha) {
+        int ei = -1;
+        for (int e = e0; e < e1; e++) {
+          if (__ldg(M.eff_sp + e) == k) {
+            ei = e;
+            break;
+          }
+        }
+        if (consP == 1) {
+          if (ei >= 0) {
+            d = (__ldg(M.eff_e + ei) - 1) * fac;
+            apply = true;
+          }
+          if (inr) {
+            d += k_f * dphase(fsp, fc, fn, sc, k);
+            apply = true;
+          }
+          if (inp) {
+            d -= k_r * dphase(rsp, rc, rn, sc, k);
+            apply = true;
+          }
+        } else {
+          const double e = (ei >= 0) ? __ldg(M.eff_e + ei) : 1.0;
+          if (!(e == 0.0 && !inr && !inp)) {
+            if (e == 0.0) {
+              d = 0.0;
+              if (inr) d = k_f * dphase(fsp, fc, fn, sc, k);
+              if (inp) d = (inr ? d : 0.0) - k_r * dphase(rsp, rc, rn, sc, k);
+            } else {
+              d = (e == 1.0) ? fac : e * fac;
+              if (inr) d += k_f * dphase(fsp, fc, fn, sc, k);
+              if (inp) d -= k_r * dphase(rsp, rc, rn, sc, k);
+            }
+            dq[p] = d;
+          }
+          d = dq[p];
+          apply = true;
+        }
+      } else {
+        if (inr) d += k_f * dphase(fsp, fc, fn, sc, k);
+        if (inp) d -= k_r * dphase(rsp, rc, rn, sc, k);
+        apply = inr || inp;
+      }
+      if (apply) {
+        for (int j = 0; j < jnn; j++) {
+          const double nu = __ldg(jc + j);
+          if (nu != 0) J[k * n + __ldg(jsp + j)] += nu * d;
+        }
+      }
+    }
+  }
+  tm.sync();
+  // temperature row and column (jacobian.py:203-281)
+  double a_cmix = 0.0, a_ehmix = 0.0, a_dcmix = 0.0, a_dehmix = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) {
+    const double cr = consP ? cp_R(M, s, T) : cv_R(M, s, T);
+    const double dc = dcvpRdT(M, s, T);
+    const double eh = consP ? hrt[s] : u_RT(M, s, T, invT);
+    crt[s] = cr;
+    dcrt[s] = dc;
+    ehrt[s] = eh;
+    a_cmix += cr * sc[s];
+    a_dcmix += dc * sc[s];
+    a_ehmix += eh * wdot[s];
+    a_dehmix += invT * (cr - eh) * wdot[s] + eh * J[N * n + s];
+  }
+  const double cmix = tm.sum(a_cmix);
+  const double dcmixdT = tm.sum(a_dcmix);
+  const double ehmix = tm.sum(a_ehmix);
+  const double dehmixdT = tm.sum(a_dehmix);
+  tm.sync();
+  const double cmixinv = 1.0 / cmix;
+  const double tmp1 = ehmix * cmixinv;
+  const double tmp3 = cmixinv * T;
+  const double tmp2 = tmp1 * tmp3;
+  for (int k = tm.lane; k < N; k += TEAM) {
+    double dehmixdc = 0.0;
+    for (int m = 0; m < N; ++m) dehmixdc += ehrt[m] * J[k * n + m];
+    J[k * n + N] = tmp2 * crt[k] - tmp3 * dehmixdc;
+  }
+  if (tm.lane == 0) J[N * n + N] = -tmp1 + tmp2 * dcmixdT - tmp3 * dehmixdT;
+  tm.sync();
+}
+
+} // namespace ppb

@@ -1,0 +1,172 @@
+"""Python mirror of the reference's reactor interface over the C ABI.
+
+``Reactor`` follows ``pele::physics::reactions::ReactorBase``
+(Source/Reactions/ReactorBase.H:13-106): ``Reactor.create(name)`` as
+``ReactorBase::create`` (Source/Factory.H:72-81), ``init(reactor_type,
+ncells)``, ``react(...)`` on flat per-cell arrays or on a box, ``close()``.
+The reference's ParmParse keys (``ode.rtol``, ``cvode.max_order``, ...) are
+accepted as keyword options of ``init``.  Host arrays are numpy; device
+arrays are torch CUDA tensors (torch is used for device memory only).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+_KEYS = {
+    # ParmParse key -> ppb_options field
+    "ode.rtol": "rtol",
+    "ode.atol": "atol",
+    "cvode.max_order": "max_order",
+    "ode.max_nls_iters": "max_nls_iters",
+    "ode.clean_init_massfrac": "clean_init_massfrac",
+    "ode.rk64_nsubsteps_guess": "rk64_nsubsteps_guess",
+    "ode.rk64_nsubsteps_min": "rk64_nsubsteps_min",
+    "ode.rk64_nsubsteps_max": "rk64_nsubsteps_max",
+    "ode.verbose": "verbose",
+}
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return getattr(stream, "cuda_stream", stream)
+
+
+class Reactor:
+    """A chemistry reactor on the GPU ("ReactorCvode" or "ReactorRK64")."""
+
+    def __init__(self, mechanism: str, integrator: str = "ReactorCvode"):
+        self.mechanism = mechanism
+        self.integrator = integrator
+        self.nsp, self.nrxn = _lib.mechanism_info(mechanism)
+        h = C.c_void_p()
+        check(lib().ppb_create(mechanism.encode(), integrator.encode(), C.byref(h)))
+        self._h = h
+        self.reactor_type = None
+
+    @classmethod
+    def create(cls, identifier: str, mechanism: str):
+        return cls(mechanism, identifier)
+
+    def init(self, reactor_type: int, ncells: int = 0, **opts):
+        o = _lib.default_options()
+        for k, v in opts.items():
+            setattr(o, _KEYS.get(k, k), v)
+        check(lib().ppb_init(self._h, int(reactor_type), int(ncells), C.byref(o)))
+        self.reactor_type = reactor_type
+        self.options = o
+        return 0
+
+    def set_typ_vals_ode(self, vals):
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        check(lib().ppb_set_typ_vals(self._h, v.ctypes.data_as(C.POINTER(C.c_double)), v.size))
+
+    def react(self, rY, rYsrc, rX, rX_src, dt_react, time=0.0, ncells=None, stream=None, raise_on_fail=True):
+        """Flat YCOrder react; numpy (host) or torch CUDA (device) arrays.
+
+        Returns (cost, dt_react, time, code) with the reference's return
+        conventions (cost = summed RHS evaluations for BDF, average RK steps
+        for RK64).
+        """
+        if ncells is None:
+            ncells = rX.shape[0]
+        dt = C.c_double(dt_react)
+        t = C.c_double(time)
+        cost = C.c_long(0)
+        fn = lib().ppb_react_flat if isinstance(rY, np.ndarray) else lib().ppb_react_flat_device
+        for a in (rY, rYsrc, rX, rX_src):
+            if isinstance(a, np.ndarray):
+                assert a.dtype == np.float64 and a.flags.c_contiguous
+        code = fn(self._h, _ptr(rY), _ptr(rYsrc), _ptr(rX), _ptr(rX_src), C.byref(dt), C.byref(t), int(ncells),
+                  _stream(stream), C.byref(cost))
+        if raise_on_fail or code < 0:
+            check(code)
+        return cost.value, dt.value, t.value, code
+
+    def react_soa(self, y, src, rX, rX_src, dt_react, time=0.0, ld=None, ncells=None, stream=None,
+                  raise_on_fail=True):
+        """Species-major device arrays y[(N+1), ld], src[N, ld]."""
+        if ncells is None:
+            ncells = rX.shape[0]
+        if ld is None:
+            ld = y.shape[-1]
+        dt = C.c_double(dt_react)
+        t = C.c_double(time)
+        cost = C.c_long(0)
+        code = lib().ppb_react_soa_device(self._h, _ptr(y), _ptr(src), _ptr(rX), _ptr(rX_src), int(ld), C.byref(dt),
+                                         C.byref(t), int(ncells), _stream(stream), C.byref(cost))
+        if raise_on_fail or code < 0:
+            check(code)
+        return cost.value, dt.value, t.value, code
+
+    def react_box(self, lo, hi, rY, rYsrc, T, rEner, rEner_src, FC, mask=None, dt_react=0.0, time=0.0,
+                  stream=None, raise_on_fail=True):
+        """Box react on torch CUDA tensors shaped [ncomp, nz, ny, nx] that
+        cover exactly the box lo..hi (inclusive)."""
+        lo3 = (C.c_int * 3)(*lo)
+        hi3 = (C.c_int * 3)(*hi)
+
+        def a4(t, cls=_lib.Array4):
+            v = cls()
+            v.p = t.data_ptr()
+            nc, nz, ny, nx = t.shape
+            v.jstride, v.kstride, v.nstride = nx, nx * ny, nx * ny * nz
+            v.lo[:] = list(lo)
+            v.hi[:] = list(hi)
+            v.ncomp = nc
+            return v
+
+        m = _lib.Array4i()
+        if mask is not None:
+            m = a4(mask, _lib.Array4i)
+        dt = C.c_double(dt_react)
+        t = C.c_double(time)
+        code = lib().ppb_react_box(self._h, lo3, hi3, a4(rY), a4(rYsrc), a4(T), a4(rEner), a4(rEner_src), a4(FC), m,
+                                   C.byref(dt), C.byref(t), _stream(stream))
+        if raise_on_fail or code < 0:
+            check(code)
+        return dt.value, t.value, code
+
+    def cell_status(self, ncells):
+        st = np.zeros(ncells, np.int32)
+        cost = np.zeros(ncells, np.int32)
+        check(lib().ppb_get_cell_status(self._h, st.ctypes.data_as(C.POINTER(C.c_int)),
+                                        cost.ctypes.data_as(C.POINTER(C.c_int)), int(ncells)))
+        return st, cost
+
+    def close(self):
+        if self._h:
+            lib().ppb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pyt2re(mechanism, P, T, Y, eh=0, stream=None):
+    """Device EOS: (rho, e or h) from P, T, Y (torch CUDA float64 tensors)."""
+    import torch
+
+    n = T.shape[0]
+    rho = torch.empty_like(T)
+    e = torch.empty_like(T)
+    check(lib().ppb_pyt2re(mechanism.encode(), int(eh), _ptr(P), _ptr(T), _ptr(Y), _ptr(rho), _ptr(e), int(n),
+                           _stream(stream)))
+    return rho, e

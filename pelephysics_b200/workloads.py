@@ -1,0 +1,178 @@
+"""Seeded synthetic reacting fields with the shapes of the benchmark configs.
+
+The reference has no public input fields for this path (its drivers build
+cells from an initial condition or a plotfile, Testing/Exec/ReactEval/
+main.cpp:204-387), so the benchmark cases are generated here from a fixed
+recipe:
+
+* ``premix_cells``: per-cell T = T0 + dT U(0,1) then phi = phi0 + dphi U(0,1)
+  (numpy default_rng(seed), drawn in that order), fuel/O2/N2 mole fractions
+  with 3.76 N2 per O2 at pressure P (1 atm by default), density and energy
+  from the ideal gas (CKRHOY, CKUBMS/CKHBMS) -- the LiDryer 16^3 case uses it
+  directly;
+* ``fourier_field``: a [0,1]-normalised sum of random 3-D Fourier modes
+  (integer wave vectors in [1,4]^3, phases U(0, 2 pi), unit amplitudes);
+* ``drm19_field``: drm19 at 64^3: T = 1100 + 1100 s(x) with s the 8-mode
+  field of seed 1, phi = 0.6 + 0.8 U, P = 1 atm; cells with s > 0.7 are
+  burnt: they take the composition of a premixed cell of the same phi that
+  was integrated for 1 ms at constant volume from 1700 K (a pool of 256 phi
+  values integrated once on the GPU), at the cell's own T.
+
+Mass fractions are YCOrder per cell; energies are rho*e (reactor type 1) or
+rho*h (type 2).  Density and energy come from the engine's device EOS.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+
+P_ATM = 1013250.0  # dyn/cm^2
+
+# fuel species and O2 per unit fuel for the shipped mechanisms
+FUELS = {
+    "LiDryer": ("H2", 0.5),
+    "drm19": ("CH4", 2.0),
+    "dodecane_lu": ("NC12H26", 18.5),
+    "heptane_lu_88sk": ("nc7h16", 11.0),
+}
+
+
+def mole_fractions(mech, phi, species):
+    """Fuel/O2/N2 premix: X_fuel = phi X_O2 / nu_O2, X_N2 = 3.76 X_O2."""
+    fuel, nu = FUELS[mech]
+    low = [s.lower() for s in species]
+    i_f, i_o, i_n = low.index(fuel.lower()), low.index("o2"), low.index("n2")
+    phi = np.asarray(phi, float)
+    xo = 1.0 / (1.0 + 3.76 + phi / nu)
+    X = np.zeros(phi.shape + (len(species),))
+    X[..., i_o] = xo
+    X[..., i_n] = 3.76 * xo
+    X[..., i_f] = phi / nu * xo
+    return X
+
+
+def mass_fractions(X, mw):
+    Y = X * mw
+    return Y / Y.sum(axis=-1, keepdims=True)
+
+
+def fourier_field(shape, nmodes, seed):
+    rng = np.random.default_rng(seed)
+    k = rng.integers(1, 5, size=(nmodes, 3))
+    ph = rng.uniform(0.0, 2 * np.pi, size=nmodes)
+    nz, ny, nx = shape
+    z, y, x = np.meshgrid(np.arange(nz) / nz, np.arange(ny) / ny, np.arange(nx) / nx, indexing="ij")
+    s = np.zeros(shape)
+    for m in range(nmodes):
+        s += np.cos(2 * np.pi * (k[m, 0] * x + k[m, 1] * y + k[m, 2] * z) + ph[m])
+    s -= s.min()
+    return s / s.max()
+
+
+def _device_state(mech, T, Y, P, reactor_type, device):
+    """rho, rho*e (or rho*h) on the device from T, Y at pressure P."""
+    import torch
+
+    from .reactor import pyt2re
+
+    n = T.shape[0]
+    Td = torch.as_tensor(T, dtype=torch.float64, device=device)
+    Yd = torch.as_tensor(np.ascontiguousarray(Y), dtype=torch.float64, device=device)
+    Pd = torch.full((n,), float(P), dtype=torch.float64, device=device)
+    rho, e = pyt2re(mech, Pd, Td, Yd, eh=1 if reactor_type == 2 else 0)
+    torch.cuda.synchronize()
+    return rho.cpu().numpy(), (rho * e).cpu().numpy()
+
+
+class Cells:
+    """Flat YCOrder batch: rY [n, N+1] (rhoY then T), rYsrc [n, N], rX, rX_src."""
+
+    def __init__(self, mech, rY, rYsrc, rX, rX_src, reactor_type, dt, meta=None):
+        self.mech = mech
+        self.rY = np.ascontiguousarray(rY)
+        self.rYsrc = np.ascontiguousarray(rYsrc)
+        self.rX = np.ascontiguousarray(rX)
+        self.rX_src = np.ascontiguousarray(rX_src)
+        self.reactor_type = reactor_type
+        self.dt = dt
+        self.meta = meta or {}
+
+    @property
+    def ncells(self):
+        return self.rX.shape[0]
+
+    def copy(self):
+        return Cells(self.mech, self.rY.copy(), self.rYsrc.copy(), self.rX.copy(), self.rX_src.copy(),
+                     self.reactor_type, self.dt, dict(self.meta))
+
+
+def premix_cells(mech, ncells, seed, T0, dT, phi0, dphi, P=P_ATM, reactor_type=1, dt=1e-4, device="cuda"):
+    species = _lib.species_names(mech)
+    mw = _lib.molecular_weights(mech)
+    rng = np.random.default_rng(seed)
+    T = T0 + dT * rng.uniform(size=ncells)
+    phi = phi0 + dphi * rng.uniform(size=ncells)
+    Y = mass_fractions(mole_fractions(mech, phi, species), mw)
+    rho, rhoE = _device_state(mech, T, Y, P, reactor_type, device)
+    N = len(species)
+    rY = np.zeros((ncells, N + 1))
+    rY[:, :N] = rho[:, None] * Y
+    rY[:, N] = T
+    return Cells(mech, rY, np.zeros((ncells, N)), rhoE, np.zeros(ncells), reactor_type, dt,
+                 {"T": T, "phi": phi, "P": P})
+
+
+def lidryer_16(device="cuda"):
+    """LiDryer, 16^3 cells, T 1000-1400 K, phi 0.5-2, 1 atm, dt 1e-4 s (seed 0)."""
+    return premix_cells("LiDryer", 16 ** 3, 0, 1000.0, 400.0, 0.5, 1.5, reactor_type=1, dt=1e-4, device=device)
+
+
+def burnt_pool(mech, phis, reactor, device="cuda", t_burn=1e-3, T_start=1700.0):
+    """Compositions after integrating premixed cells for t_burn at constant
+    volume from T_start (one cell per phi), with the given GPU reactor."""
+    species = _lib.species_names(mech)
+    mw = _lib.molecular_weights(mech)
+    n = len(phis)
+    T = np.full(n, T_start)
+    Y = mass_fractions(mole_fractions(mech, phis, species), mw)
+    rho, rhoE = _device_state(mech, T, Y, P_ATM, 1, device)
+    N = len(species)
+    rY = np.zeros((n, N + 1))
+    rY[:, :N] = rho[:, None] * Y
+    rY[:, N] = T
+    reactor.react(rY, np.zeros((n, N)), rhoE.copy(), np.zeros(n), t_burn, raise_on_fail=False)
+    Yb = np.clip(rY[:, :N], 0.0, None)
+    return Yb / Yb.sum(axis=1, keepdims=True)
+
+
+def drm19_field(n=64, device="cuda", seed=1, pool_reactor=None, burnt_threshold=0.7):
+    """drm19 on an n^3 box: the 64^3 case of the benchmark (see module doc)."""
+    mech = "drm19"
+    species = _lib.species_names(mech)
+    mw = _lib.molecular_weights(mech)
+    N = len(species)
+    s = fourier_field((n, n, n), 8, seed).reshape(-1)
+    ncells = s.size
+    rng = np.random.default_rng(seed)
+    T = 1100.0 + 1100.0 * s
+    phi = 0.6 + 0.8 * rng.uniform(size=ncells)
+    Y = mass_fractions(mole_fractions(mech, phi, species), mw)
+    burnt = s > burnt_threshold
+    if burnt.any():
+        if pool_reactor is None:
+            from .reactor import Reactor
+
+            pool_reactor = Reactor(mech)
+            pool_reactor.init(1, 256, rtol=1e-8, atol=1e-10, max_order=5)
+        pool_phi = np.linspace(0.6, 1.4, 256)
+        pool = burnt_pool(mech, pool_phi, pool_reactor, device=device)
+        idx = np.clip(np.rint((phi[burnt] - 0.6) / 0.8 * 255).astype(int), 0, 255)
+        Y[burnt] = pool[idx]
+    rho, rhoE = _device_state(mech, T, Y, P_ATM, 1, device)
+    rY = np.zeros((ncells, N + 1))
+    rY[:, :N] = rho[:, None] * Y
+    rY[:, N] = T
+    return Cells(mech, rY, np.zeros((ncells, N)), rhoE, np.zeros(ncells), 1, 1e-5,
+                 {"T": T, "phi": phi, "burnt": burnt, "s": s})

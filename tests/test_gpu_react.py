@@ -1,0 +1,221 @@
+"""GPU integration parity: the engine's react() paths through the C ABI
+against the CPU oracle on the same seeded cells.
+
+Bar (from the engine's accuracy contract, at rtol = atol = 1e-10):
+integrated T within 1e-6 relative and mass fractions within 1e-8 absolute
+of the FP64 oracle, for the plain engine, the tuned engine and the tuned
+engine with the FP32 factor + FP64 refinement."""
+
+import numpy as np
+import pytest
+
+from pelephysics_b200 import _lib
+from pelephysics_b200.reactor import Reactor
+from tests.helpers import premix_oracle
+
+pytestmark = pytest.mark.gpu
+
+ENGINES = [
+    dict(engine=0),
+    dict(engine=1),
+    dict(engine=1, lu_fp32=1, refine_sweeps=1),
+]
+
+
+def oracle_react(oracle, mech, rtype, rY, src, rX, rXs, dt, method=0, **kw):
+    y = rY.copy()
+    x = rX.copy()
+    flag, nfe, st = oracle.react_flat(mech, rtype, y, np.ascontiguousarray(src), x, rXs, dt, method=method, **kw)
+    return y, x, flag, nfe, st
+
+
+def compare(y, ref, T_rtol=1e-6, Y_atol=1e-8):
+    N = ref.shape[1] - 1
+    Tg, Tr = y[:, N], ref[:, N]
+    assert np.all(np.isfinite(y))
+    dT = np.abs(Tg - Tr) / Tr
+    Yg = y[:, :N] / y[:, :N].sum(axis=1, keepdims=True)
+    Yr = ref[:, :N] / ref[:, :N].sum(axis=1, keepdims=True)
+    dY = np.abs(Yg - Yr)
+    assert dT.max() <= T_rtol, f"max rel T error {dT.max():.3e}"
+    assert dY.max() <= Y_atol, f"max abs Y error {dY.max():.3e}"
+    return dT.max(), dY.max()
+
+
+@pytest.mark.parametrize("eng", ENGINES, ids=["plain", "tuned", "tuned_fp32"])
+def test_lidryer_bdf(cuda, oracle, eng):
+    mech, rtype, dt = "LiDryer", 1, 1e-4
+    rY, src, rX, rXs = premix_oracle(oracle, mech, 48, 0, 1000.0, 400.0, 0.5, 1.5)
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5)
+    ref, xref, flag, nfe, _ = oracle_react(oracle, mech, rtype, rY, src, rX, rXs, dt, **opts)
+    assert flag == 0
+    r = Reactor(mech)
+    r.init(rtype, 48, **opts, **eng)
+    y = rY.copy()
+    x = rX.copy()
+    cost, dtr, t, code = r.react(y, src.copy(), x, rXs.copy(), dt, 0.0)
+    assert code == 0 and t == dt
+    compare(y, ref)
+    np.testing.assert_allclose(x, xref, rtol=0, atol=0)
+    st, c = r.cell_status(48)
+    assert np.all(st == 0)
+    assert cost == c.sum() > 0
+
+
+@pytest.mark.parametrize("eng", ENGINES, ids=["plain", "tuned", "tuned_fp32"])
+def test_drm19_bdf(cuda, oracle, eng):
+    mech, rtype, dt = "drm19", 1, 1e-5
+    rY, src, rX, rXs = premix_oracle(oracle, mech, 32, 1, 1100.0, 1100.0, 0.6, 0.8)
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5)
+    ref, _, flag, _, _ = oracle_react(oracle, mech, rtype, rY, src, rX, rXs, dt, **opts)
+    assert flag == 0
+    r = Reactor(mech)
+    r.init(rtype, 32, **opts, **eng)
+    y = rY.copy()
+    r.react(y, src.copy(), rX.copy(), rXs.copy(), dt)
+    compare(y, ref)
+
+
+@pytest.mark.parametrize("eng", ENGINES[:2], ids=["plain", "tuned"])
+def test_enthalpy_reactor_with_sources(cuda, oracle, eng):
+    """Reactor type 2 with nonzero species and energy sources, default
+    (reference) max order 2."""
+    mech, rtype, dt = "LiDryer", 2, 2e-5
+    rY, src, rX, rXs = premix_oracle(oracle, mech, 16, 7, 1100.0, 300.0, 0.5, 1.0, reactor_type=2)
+    rng = np.random.default_rng(8)
+    src = rng.normal(0.0, 1e-3, src.shape) * rY[:, :-1] / dt
+    src -= (rY[:, :-1] / rY[:, :-1].sum(axis=1, keepdims=True)) * src.sum(axis=1, keepdims=True)
+    rXs = rng.normal(0.0, 1e-3, 16) * np.abs(rX) / dt
+    opts = dict(rtol=1e-10, atol=1e-10)
+    ref, xref, flag, _, _ = oracle_react(oracle, mech, rtype, rY, src, rX, rXs, dt, **opts)
+    assert flag == 0
+    r = Reactor(mech)
+    r.init(rtype, 16, **opts, **eng)
+    y = rY.copy()
+    x = rX.copy()
+    r.react(y, src.copy(), x, rXs.copy(), dt)
+    compare(y, ref)
+    np.testing.assert_allclose(x, xref, rtol=1e-15)
+
+
+@pytest.mark.parametrize("eng", ENGINES[:2], ids=["plain", "tuned"])
+def test_rk64(cuda, oracle, eng):
+    mech, rtype, dt = "LiDryer", 1, 2e-6
+    rY, src, rX, rXs = premix_oracle(oracle, mech, 16, 2, 1000.0, 400.0, 0.5, 1.5)
+    ref, _, _, steps, _ = oracle_react(oracle, mech, rtype, rY, src, rX, rXs, dt, method=1, atol=1e-10)
+    r = Reactor(mech, "ReactorRK64")
+    r.init(rtype, 16, atol=1e-10, **eng)
+    y = rY.copy()
+    cost, _, _, _ = r.react(y, src.copy(), rX.copy(), rXs.copy(), dt)
+    compare(y, ref, T_rtol=1e-9, Y_atol=1e-11)
+    _, c = r.cell_status(16)
+    assert cost == int(c.sum() / 16)
+    assert np.abs(c - steps).max() <= 1
+
+
+def test_device_paths_match_host_path(cuda, oracle):
+    """YCOrder device path (captured as a CUDA graph and replayed) and the
+    species-major device path give the host path's numbers exactly."""
+    torch = cuda
+    mech, rtype, dt = "drm19", 1, 1e-5
+    rY, src, rX, rXs = premix_oracle(oracle, mech, 40, 4, 1200.0, 900.0, 0.6, 0.8)
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5)
+    r = Reactor(mech)
+    r.init(rtype, 40, **opts)
+    yh = rY.copy()
+    xh = rX.copy()
+    r.react(yh, src.copy(), xh, rXs.copy(), dt)
+    for rep in range(2):  # second call replays the cached graph
+        yd = torch.as_tensor(rY, device="cuda").contiguous()
+        xd = torch.as_tensor(rX, device="cuda")
+        sd = torch.as_tensor(src, device="cuda")
+        xsd = torch.as_tensor(rXs, device="cuda")
+        r.react(yd, sd, xd, xsd, dt)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(yd.cpu().numpy(), yh)
+        np.testing.assert_array_equal(xd.cpu().numpy(), xh)
+    ys = torch.as_tensor(rY.T.copy(), device="cuda")
+    xs = torch.as_tensor(rX, device="cuda")
+    ss = torch.as_tensor(src.T.copy(), device="cuda")
+    xss = torch.as_tensor(rXs, device="cuda")
+    r.react_soa(ys, ss, xs, xss, dt)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(ys.cpu().numpy().T, yh)
+
+
+def test_box_path_mask_and_clean_massfrac(cuda, oracle):
+    """react(Box, Array4...) with a mask and ode.clean_init_massfrac:
+    box_flatten / box_unflatten semantics (ReactorUtils.H:160-291)."""
+    torch = cuda
+    mech, rtype, dt = "LiDryer", 1, 5e-5
+    nx, ny, nz = 4, 3, 2
+    n = nx * ny * nz
+    rY, src, rX, rXs = premix_oracle(oracle, mech, n, 9, 1000.0, 400.0, 0.5, 1.5)
+    N = rY.shape[1] - 1
+    M = oracle.Mech(mech)
+    rY[3, 4] = -1e-12  # a slightly negative species density to clip
+    mask = np.ones(n, np.int32)
+    mask[[2, 5]] = -1
+    Tstore = rY[:, N] + 30.0  # stored T differs; flatten recomputes it from energy
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5, clean_init_massfrac=1)
+    r = Reactor(mech)
+    r.init(rtype, n, **opts)
+
+    def box(a, nc):
+        return torch.as_tensor(np.ascontiguousarray(a.T.reshape(nc, nz, ny, nx)), device="cuda")
+
+    bY = box(rY[:, :N], N)
+    bS = box(src, N)
+    bT = box(Tstore[:, None], 1)
+    bE = box(rX[:, None], 1)
+    bEs = box(rXs[:, None], 1)
+    bFC = torch.zeros((1, nz, ny, nx), dtype=torch.float64, device="cuda")
+    bM = torch.as_tensor(mask.reshape(1, nz, ny, nx), device="cuda")
+    r.react_box((0, 0, 0), (nx - 1, ny - 1, nz - 1), bY, bS, bT, bE, bEs, bFC, bM, dt_react=dt)
+    torch.cuda.synchronize()
+    outY = bY.cpu().numpy().reshape(N, n).T
+    outT = bT.cpu().numpy().reshape(n)
+    outFC = bFC.cpu().numpy().reshape(n)
+    for c in range(n):
+        if mask[c] == -1:
+            np.testing.assert_array_equal(outY[c], rY[c, :N])
+            assert outFC[c] == 0.0
+            continue
+        rho_old = rY[c, :N].sum()
+        clip = np.minimum(np.maximum(0.0, rY[c, :N]), rho_old)
+        rho = clip.sum()
+        T0, _ = M.t_given_ey(rX[c] / rho, clip / rho, Tstore[c])
+        y, flag, st = oracle.bdf_cell(mech, rtype, np.r_[clip, T0], src[c], rX[c], rXs[c], dt, rtol=1e-10,
+                                      atol=1e-10, max_order=5)
+        assert flag == 0
+        newY = rY[c, :N] + (y[:N] - clip) * rho_old / clip.sum()
+        # the integration contract: mass fractions within 1e-8 absolute
+        np.testing.assert_allclose(outY[c] / rho_old, newY / rho_old, rtol=0, atol=1e-8)
+        rE = rX[c] + dt * rXs[c]
+        Tn, _ = M.t_given_ey(rE / newY.sum(), newY / newY.sum(), y[N])
+        assert abs(outT[c] - Tn) <= 1e-6 * Tn
+        assert outFC[c] > 0
+
+
+def test_too_much_work_reported_per_cell(cuda, oracle):
+    """A step cap the cells cannot meet yields the CVODE TOO_MUCH_WORK flag
+    per cell and PPB_E_INTEGRATE from react, with the state left finite."""
+    mech = "LiDryer"
+    rY, src, rX, rXs = premix_oracle(oracle, mech, 8, 0, 1200.0, 100.0, 1.0, 0.0)
+    for eng in (0, 1):
+        r = Reactor(mech)
+        r.init(1, 8, rtol=1e-10, atol=1e-10, max_steps=3, engine=eng)
+        y = rY.copy()
+        cost, _, _, code = r.react(y, src.copy(), rX.copy(), rXs.copy(), 1e-4, raise_on_fail=False)
+        assert code == _lib.PPB_E_INTEGRATE
+        st, _ = r.cell_status(8)
+        assert np.all(st == -1)
+        assert np.all(np.isfinite(y))
+
+
+def test_empty_batch(cuda):
+    r = Reactor("LiDryer")
+    r.init(1, 0)
+    e = np.zeros((0, 10))
+    cost, dt, t, code = r.react(e, np.zeros((0, 9)), np.zeros(0), np.zeros(0), 1e-5, 1.0, ncells=0)
+    assert code == 0 and cost == 0 and abs(t - (1.0 + 1e-5)) < 1e-15
