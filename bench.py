@@ -1,0 +1,427 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 chemistry engine: drm19 on a 64^3 field.
+
+One step = one react() call advancing every cell of the field by dt = 1e-5 s
+(constant-volume reactor, BDF orders <= 5, rtol = atol = 1e-10) -- the
+drm19 64^3 workload (262144 cells: T = 1100 + 1100 s(x) from an 8-mode
+seed-1 Fourier field, phi = 0.6 + 0.8 U, 1 atm, burnt cells at the
+composition of a 1 ms pre-integration).  Metric: cells advanced per second
+of device time (cells/s per dt), for the tuned engine (warp per cell,
+persistent work queue, CUDA graph).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank integrates its own 64^3 field (weak scaling; the
+cells are independent, so there is no data-path collective); the time is the
+max over ranks.  --impl reference times the reference's CPU chemistry on the
+host cores (the CVODE-algorithm BDF of oracle/ over the reference's own
+compiled mechanism kernels) on a bounded sample of the same cells.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MECH = "drm19"
+DT = 1e-5
+OPTS = dict(rtol=1e-10, atol=1e-10, max_order=5)
+METRIC = "cells/s per dt (drm19 64^3, tuned engine)"
+# FP64 floating-point operations of one reactor RHS and one reactor Jacobian
+# evaluation for drm19 (dadd + dmul + 2 dfma, exp/log included), counted with
+# ncu on single-cell launches of the pointwise kernels; see
+# profiles/drm19_flops_per_evaluation.md for the command and raw counts.
+FLOPS_RHS = {"drm19": None}
+FLOPS_JAC = {"drm19": None}
+CPU_SAMPLE = 8192  # cells of the field integrated by the CPU baseline
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def oracle_eos(po, mech):
+    M = po.Mech(mech)
+
+    def eos(T, Y, P, rtype):
+        rho = np.array([M.ckrhoy(P, t, y) for t, y in zip(T, Y)])
+        e = np.array([(M.ckubms if rtype == 1 else M.ckhbms)(t, y) for t, y in zip(T, Y)])
+        return rho, rho * e
+
+    return eos, M.species(), M.mw()
+
+
+def cpu_sample_index(ncells, n):
+    return np.sort(np.random.default_rng(7).permutation(ncells)[:n])
+
+
+def run_cpu(po, cells, idx, nthreads=0):
+    """The oracle (reference kernels) on cells[idx]; returns (seconds, rY)."""
+    po.load_ref(MECH)
+    rY = cells.rY[idx].copy()
+    rX = cells.rX[idx].copy()
+    src = np.ascontiguousarray(cells.rYsrc[idx])
+    rXs = cells.rX_src[idx].copy()
+    t0 = time.perf_counter()
+    flag, nfe, st = po.react_flat(MECH, 1, rY, src, rX, rXs, DT, use_ref_kernels=1, nthreads=nthreads, **OPTS)
+    return time.perf_counter() - t0, rY, flag
+
+
+def reference_arm(args):
+    ws, rank, _ = dist_info()
+    if rank != 0:
+        return 0
+    from oracle import pyoracle as po
+    from pelephysics_b200 import workloads as wl
+
+    eos, species, mw = oracle_eos(po, MECH)
+    cells = wl.drm19_field(64, eos=eos, species=species, mw=mw)
+    idx = cpu_sample_index(cells.ncells, CPU_SAMPLE)
+    cores = os.cpu_count()
+    for _ in range(args.warmup):
+        run_cpu(po, cells, idx[:1024])
+    times = []
+    for _ in range(args.steps):
+        dt, _, flag = run_cpu(po, cells, idx)
+        times.append(dt)
+    tot = sum(times)
+    value = len(idx) * args.steps / tot
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "cells/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "drm19 64^3 field, dt 1e-5 s, BDF q<=5, rtol=atol=1e-10",
+                   "sample_cells_per_step": int(len(idx))},
+        "cpu_baseline": {"value": value, "unit": "cells/s", "cores": cores, "kind": "reference",
+                         "sample": f"{len(idx)} seeded cells of the 64^3 field per step; CVODE-algorithm BDF "
+                                   "(oracle/reactor.c) over the reference's own compiled drm19 mechanism "
+                                   "kernels (oracle/_ref), OpenMP over all host threads; SUNDIALS is absent so "
+                                   "ReactorCvode itself cannot be built"},
+        "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_flops(stats, n):
+    """FP64 work of the CVODE algorithm from per-cell counters: RHS and
+    Jacobian evaluations, (2/3) n^3 + n^2 per factorisation of I - gamma J,
+    2 n^2 per Newton solve."""
+    fr, fj = FLOPS_RHS.get(MECH), FLOPS_JAC.get(MECH)
+    if fr is None or fj is None:
+        return None
+    nfe, nje, nset, nni = (stats[:, i].astype(np.float64).sum() for i in (1, 2, 3, 4))
+    return nfe * fr + nje * fj + nset * (2.0 / 3.0 * n ** 3 + n * n) + nni * 2.0 * n * n
+
+
+def our_arm(args):
+    import torch
+
+    ws, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        pg = dist
+
+    from pelephysics_b200 import workloads as wl
+    from pelephysics_b200.reactor import Reactor, probe_fp64_peak
+
+    cells = wl.drm19_field(args.edge, device=dev)
+    n = cells.ncells
+    N = cells.rY.shape[1] - 1
+    # device-resident species-major state and a pristine copy
+    y0 = torch.as_tensor(cells.rY.T.copy(), device=dev)
+    s0 = torch.as_tensor(cells.rYsrc.T.copy(), device=dev)
+    x0 = torch.as_tensor(cells.rX, device=dev)
+    xs = torch.as_tensor(cells.rX_src, device=dev)
+    y = y0.clone()
+    x = x0.clone()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    r = Reactor(MECH)
+    r.init(1, n, engine=1, **OPTS)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        y.copy_(y0)
+        x.copy_(x0)
+        r.react_soa(y, s0, x, xs, DT, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()  # evict L2 between timed steps (outside the events)
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    t_dev = sum(ms) / 1e3
+    if pg:
+        tt = torch.tensor([t_dev], device=dev, dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_dev = float(tt.item())
+    value = n * ws * args.steps / t_dev
+    y_gpu = y.cpu().numpy().T.copy()
+    stats = r.cell_stats(n)
+    status, _ = r.cell_status(n)
+
+    # end to end through the public flat API on pinned host buffers
+    hy = torch.empty((n, N + 1), dtype=torch.float64).pin_memory().numpy()
+    hs = torch.empty((n, N), dtype=torch.float64).pin_memory().numpy()
+    hx = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    hxs = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    hs[:] = cells.rYsrc
+    hxs[:] = cells.rX_src
+    re2e = Reactor(MECH)
+    re2e.init(1, n, engine=1, **OPTS)
+    hy[:] = cells.rY
+    hx[:] = cells.rX
+    re2e.react(hy, hs, hx, hxs, DT)  # warm
+    e2e_t = 0.0
+    for k in range(args.steps):
+        hy[:] = cells.rY
+        hx[:] = cells.rX
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        re2e.react(hy, hs, hx, hxs, DT)
+        e2e_t += time.perf_counter() - t0
+    if pg:
+        tt = torch.tensor([e2e_t], device=dev, dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+    e2e = n * ws * args.steps / e2e_t
+    h2d = n * (N + 1) * 8 + n * N * 8 + 2 * n * 8
+    d2h = n * (N + 1) * 8 + 2 * n * 4
+    re2e.close()
+
+    out = {}
+    if rank == 0:
+        # plain engine on a strided sub-field (the full field takes tens of s)
+        sub = np.arange(0, n, 8)
+        rp = Reactor(MECH)
+        rp.init(1, sub.size, engine=0, **OPTS)
+        yp = torch.as_tensor(cells.rY[sub], device=dev).contiguous()
+        xp = torch.as_tensor(cells.rX[sub], device=dev)
+        sp = torch.as_tensor(cells.rYsrc[sub], device=dev).contiguous()
+        xsp = torch.as_tensor(cells.rX_src[sub], device=dev)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        rp.react(yp, sp, xp, xsp, DT)
+        b.record()
+        torch.cuda.synchronize()
+        plain_value = sub.size / (a.elapsed_time(b) / 1e3)
+        y_plain = yp.cpu().numpy()
+        dT_plain = float(np.max(np.abs(y_plain[:, N] - y_gpu[sub, N]) / y_gpu[sub, N]))
+        rp.close()
+        peak = probe_fp64_peak()
+        flops = algorithmic_flops(stats, N + 1)
+        out.update(plain_value=plain_value, dT_plain=dT_plain, fp64_peak_gflops=peak, flops=flops)
+
+    cpu = None
+    acc = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        from oracle import pyoracle as po
+
+        idx = cpu_sample_index(n, CPU_SAMPLE)
+        secs, y_cpu, flag = run_cpu(po, cells, idx)
+        cpu = {"value": len(idx) / secs, "unit": "cells/s", "cores": os.cpu_count(), "kind": "reference",
+               "sample": f"{len(idx)} seeded cells of the same 64^3 field, one react; CVODE-algorithm BDF "
+                         "(oracle/reactor.c) over the reference's own compiled drm19 kernels (oracle/_ref), "
+                         "OpenMP over all host threads (ReactorCvode needs the absent SUNDIALS)"}
+        g = y_gpu[idx]
+        dT = np.abs(g[:, N] - y_cpu[:, N]) / y_cpu[:, N]
+        Yg = g[:, :N] / g[:, :N].sum(1, keepdims=True)
+        Yc = y_cpu[:, :N] / y_cpu[:, :N].sum(1, keepdims=True)
+        acc = {"cells": int(len(idx)), "max_rel_T": float(dT.max()), "max_abs_Y": float(np.abs(Yg - Yc).max())}
+
+    if rank == 0:
+        t_step = t_dev / args.steps
+        roof = None
+        if out.get("flops") is not None:
+            achieved = out["flops"] / t_step / 1e12
+            peak_t = out["fp64_peak_gflops"] / 1e3
+            roof = {"bound": "fp64", "achieved": achieved, "peak": peak_t, "unit": "TFLOP/s",
+                    "frac": achieved / peak_t, "traffic": None,
+                    "peak_source": "measured FP64 FMA probe on this GPU (ppb_probe_fp64_peak)"}
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "cells/s",
+            "n_gpus": ws,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "drm19 64^3 field (262144 cells/GPU), dt 1e-5 s, constant-volume, BDF q<=5, "
+                                   "rtol=atol=1e-10", "cells_per_gpu": n, "l2": "flushed between timed steps",
+                       "engine": "tuned: warp per cell, persistent work queue, CUDA graph, FP64 LU"},
+            "e2e": {"value": e2e, "unit": "cells/s", "h2d_bytes_per_step": h2d * ws, "d2h_bytes_per_step": d2h * ws},
+            "gpu_launches": 2 * args.steps,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "tuned_vs_plain": {"plain_value": out["plain_value"], "ratio": value / ws / out["plain_value"],
+                               "plain_sample": "every 8th cell, one react", "max_rel_T_tuned_vs_plain": out["dT_plain"]},
+            "accuracy_vs_fp64_oracle": acc,
+            "cell_failures": int(np.sum(status < 0)),
+            "wall_s": wall,
+        }
+        print(json.dumps(line), flush=True)
+    r.close()
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def flops_probe():
+    """One drm19 cell: reactor RHS and reactor Jacobian pointwise kernels,
+    thread per cell (run under ncu to count FP64 operations)."""
+    import torch
+
+    from pelephysics_b200 import _lib, workloads as wl
+
+    cells = wl.premix_cells(MECH, 1, 3, 1500.0, 0.0, 1.0, 0.0, dt=DT)
+    N = cells.rY.shape[1] - 1
+    y = torch.as_tensor(cells.rY, device="cuda")
+    x = torch.as_tensor(cells.rX, device="cuda")
+    xs = torch.as_tensor(cells.rX_src, device="cuda")
+    s = torch.as_tensor(cells.rYsrc, device="cuda")
+    f = torch.zeros_like(y)
+    _lib.check(_lib.lib().ppb_reactor_rhs(MECH.encode(), 1, 0.0, y.data_ptr(), x.data_ptr(), xs.data_ptr(),
+                                          s.data_ptr(), f.data_ptr(), 1, 1, None))
+    rho = y[:, :N].sum()
+    sc = (y[:, :N] / torch.as_tensor(_lib.molecular_weights(MECH), device="cuda")) * 1e6
+    J = torch.zeros(((N + 1) ** 2,), dtype=torch.float64, device="cuda")
+    T = y[:, N].contiguous()
+    _lib.check(_lib.lib().ppb_ajacobian(MECH.encode(), sc.contiguous().data_ptr(), T.data_ptr(), 0, J.data_ptr(), 1,
+                                        1, None))
+    torch.cuda.synchronize()
+    print("flops probe done", float(rho))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--edge", type=int, default=64, help="field edge (profiling runs use a smaller box)")
+    ap.add_argument("--flops-probe", action="store_true",
+                    help="launch one single-cell RHS and one Jacobian evaluation (for an ncu FP64 op count)")
+    args = ap.parse_args()
+    if args.flops_probe:
+        return flops_probe()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

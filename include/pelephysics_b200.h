@@ -141,6 +141,18 @@ int ppb_react_box(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 r
  * code) and cost (RHS evaluations or RK steps) of the last react call. */
 int ppb_get_cell_status(ppb_reactor* r, int* status, int* cost, int ncells);
 
+/* Per-cell integrator counters of the last react call, 7 ints per cell:
+ * steps, RHS evaluations, Jacobian evaluations, matrix factorisations,
+ * Newton iterations, error-test failures, convergence failures (the
+ * statistics ReactorCvode::print_final_stats reports, ReactorCvode.cpp:
+ * 1838-1901, kept per cell).  RK64: steps, 6*steps, then zeros. */
+int ppb_get_cell_stats(ppb_reactor* r, int* stats, int ncells);
+
+/* Measured FP64 FMA throughput of the current device in GFLOP/s (a short
+ * probe kernel); the denominator of the engine's compute roofline.  No
+ * counterpart in the reference. */
+int ppb_probe_fp64_peak(double* gflops, void* stream);
+
 /* Pointwise mechanism kernels on DEVICE arrays, one cell per row, for
  * parity checks; team = 1 (thread per cell) or 32 (warp per cell).
  * mechanism.H productionRate (SI: mol/m^3 in, mol/m^3/s out):

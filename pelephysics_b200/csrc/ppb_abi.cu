@@ -89,7 +89,7 @@ struct ppb_reactor {
   size_t cap = 0;
   double *aos = nullptr, *aos_src = nullptr, *soa = nullptr, *soa_src = nullptr, *rhoe = nullptr, *rhoesrc = nullptr;
   double* atolv = nullptr;
-  int *status = nullptr, *nfe = nullptr, *queue = nullptr, *mask = nullptr;
+  int *status = nullptr, *nfe = nullptr, *queue = nullptr, *mask = nullptr, *stats = nullptr;
   int last_ncells = 0;
   // graph cache for the device paths; capture runs on a private stream (the
   // legacy default stream cannot be captured) and the graph is launched on
@@ -111,6 +111,8 @@ static void free_scratch(ppb_reactor* r)
   cudaFree(r->nfe);
   cudaFree(r->queue);
   cudaFree(r->mask);
+  cudaFree(r->stats);
+  r->stats = nullptr;
   r->aos = r->aos_src = r->soa = r->soa_src = r->rhoe = r->rhoesrc = nullptr;
   r->status = r->nfe = r->queue = r->mask = nullptr;
   r->cap = 0;
@@ -132,6 +134,7 @@ static int ensure_scratch(ppb_reactor* r, int ncells)
   PPB_CUDA(cudaMalloc(&r->status, c * 4), "cudaMalloc");
   PPB_CUDA(cudaMalloc(&r->nfe, c * 4), "cudaMalloc");
   PPB_CUDA(cudaMalloc(&r->mask, c * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->stats, c * 7 * 4), "cudaMalloc");
   PPB_CUDA(cudaMalloc(&r->queue, 16), "cudaMalloc");
   r->cap = c;
   return 0;
@@ -336,6 +339,7 @@ static int run_batch(ppb_reactor* r, Batch b, double dt, cudaStream_t st)
   b.atolv = r->atolv;
   b.status = r->status;
   b.nfe = r->nfe;
+  b.stats = r->stats;
   const Options o = engine_options(r);
   const LaunchConfig lc = launch_config(r);
   int e = launch_react(*r->dm, o, r->method, lc, b, dt, r->queue, st);
@@ -574,6 +578,19 @@ int ppb_get_cell_status(ppb_reactor* r, int* status, int* cost, int ncells)
   if (status) PPB_CUDA(cudaMemcpy(status, r->status, (size_t)ncells * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
   if (cost) PPB_CUDA(cudaMemcpy(cost, r->nfe, (size_t)ncells * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
   return 0;
+}
+
+int ppb_get_cell_stats(ppb_reactor* r, int* stats, int ncells)
+{
+  if (!r || !stats || ncells < 0 || ncells > r->last_ncells) return fail(PPB_E_ARG, "ppb_get_cell_stats: bad arguments");
+  PPB_CUDA(cudaMemcpy(stats, r->stats, (size_t)ncells * 7 * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  return 0;
+}
+
+int ppb_probe_fp64_peak(double* gflops, void* stream)
+{
+  if (!gflops) return fail(PPB_E_ARG, "ppb_probe_fp64_peak: null output");
+  return cuda_fail(probe_fp64_peak(gflops, (cudaStream_t)stream), "probe_fp64_peak");
 }
 
 static int point_mech(const char* mechanism, DeviceMechanism** dm)

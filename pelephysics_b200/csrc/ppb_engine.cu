@@ -509,4 +509,51 @@ int launch_pyt2re(const DeviceMechanism& m, int eh, const double* P, const doubl
   return (int)cudaGetLastError();
 }
 
+// Peak FP64 FMA throughput of the device: every thread runs 8 independent
+// FMA chains; 2 flops per FMA.
+__global__ void k_fp64_probe(double* out, int iters)
+{
+  double a[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) a[j] = threadIdx.x * 1e-9 + j;
+  const double m = 0.999999999, c = 1e-9;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) a[j] = fma(a[j], m, c);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; j++) s += a[j];
+  if (s == 12345.678) out[0] = s; // never true; keeps the chains live
+}
+
+int probe_fp64_peak(double* gflops, cudaStream_t st)
+{
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  double* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, 8);
+  if (e != cudaSuccess) return (int)e;
+  const int threads = 256, blocks = nsm * 8, iters = 4096;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  k_fp64_probe<<<blocks, threads, 0, st>>>(d, iters); // warm-up
+  cudaEventRecord(a, st);
+  const int reps = 5;
+  for (int r = 0; r < reps; r++) k_fp64_probe<<<blocks, threads, 0, st>>>(d, iters);
+  cudaEventRecord(b, st);
+  e = cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(d);
+  if (e != cudaSuccess) return (int)e;
+  const double flops = 2.0 * 8.0 * iters * (double)threads * blocks * reps;
+  *gflops = flops / (ms * 1e-3) / 1e9;
+  return (int)cudaGetLastError();
+}
+
 } // namespace ppb

@@ -31,6 +31,7 @@ struct Batch {
   const int* mask;     // per cell, -1 skips the cell; nullptr: all cells
   int* status;         // per cell integrator flag (may be nullptr)
   int* nfe;            // per cell RHS evaluations / RK steps (may be nullptr)
+  int* stats;          // per cell [nsteps, nfe, nje, nsetups, nni, netf, ncfn] (may be nullptr)
   int ncells;
   int ld;
 };
@@ -89,6 +90,8 @@ int launch_box_unflatten(const DeviceMechanism& m, int rtype, int clean, const B
 
 int launch_pyt2re(const DeviceMechanism& m, int eh, const double* P, const double* T, const double* Y, double* rho,
                   double* e, int ncells, cudaStream_t st);
+// FP64 FMA throughput probe: returns GFLOP/s measured with CUDA events.
+int probe_fp64_peak(double* gflops, cudaStream_t st);
 int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells, cudaStream_t st);
 
 // Bytes of shared memory one team-integrated cell needs.

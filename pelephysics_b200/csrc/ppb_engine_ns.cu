@@ -36,9 +36,25 @@ __device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options&
     Bdf<NS, TEAM, LT> bdf(tm, M, o, w, cin);
     flag = bdf.run(dt);
     cost = bdf.s.nfe;
+    if (b.stats && tm.lane == 0) {
+      int* st = b.stats + (size_t)c * 7;
+      st[0] = bdf.s.nst;
+      st[1] = bdf.s.nfe;
+      st[2] = bdf.s.nje;
+      st[3] = bdf.s.nsetups;
+      st[4] = bdf.s.nni;
+      st[5] = bdf.s.netf;
+      st[6] = bdf.s.ncfn;
+    }
   } else {
     cost = rk64_cell<TEAM, LT>(tm, M, o, w, cin, dt);
     flag = ST_OK;
+    if (b.stats && tm.lane == 0) {
+      int* st = b.stats + (size_t)c * 7;
+      st[0] = cost;
+      st[1] = 6 * cost;
+      for (int q = 2; q < 7; q++) st[q] = 0;
+    }
   }
   for (int i = tm.lane; i < n; i += TEAM) b.y[(size_t)i * b.ld + c] = w.y[i];
   if (tm.lane == 0) {

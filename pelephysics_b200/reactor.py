@@ -148,6 +148,12 @@ class Reactor:
                                         cost.ctypes.data_as(C.POINTER(C.c_int)), int(ncells)))
         return st, cost
 
+    def cell_stats(self, ncells):
+        """[ncells, 7]: steps, nfe, nje, nsetups, nni, netf, ncfn."""
+        st = np.zeros((ncells, 7), np.int32)
+        check(lib().ppb_get_cell_stats(self._h, st.ctypes.data_as(C.POINTER(C.c_int)), int(ncells)))
+        return st
+
     def close(self):
         if self._h:
             lib().ppb_destroy(self._h)
@@ -158,6 +164,13 @@ class Reactor:
             self.close()
         except Exception:
             pass
+
+
+def probe_fp64_peak():
+    """Measured FP64 FMA throughput of the current GPU, GFLOP/s."""
+    g = C.c_double()
+    check(lib().ppb_probe_fp64_peak(C.byref(g), None))
+    return g.value
 
 
 def pyt2re(mechanism, P, T, Y, eh=0, stream=None):

@@ -14,15 +14,20 @@ recipe:
   (integer wave vectors in [1,4]^3, phases U(0, 2 pi), unit amplitudes);
 * ``drm19_field``: drm19 at 64^3: T = 1100 + 1100 s(x) with s the 8-mode
   field of seed 1, phi = 0.6 + 0.8 U, P = 1 atm; cells with s > 0.7 are
-  burnt: they take the composition of a premixed cell of the same phi that
-  was integrated for 1 ms at constant volume from 1700 K (a pool of 256 phi
-  values integrated once on the GPU), at the cell's own T.
+  burnt: they take the composition of a premixed cell of the nearest phi
+  that was integrated for 1 ms at constant volume from 1700 K (the 256-entry
+  pool data/drm19_burnt_pool.npz, made by data/make_burnt_pool.py), at the
+  cell's own T.
 
 Mass fractions are YCOrder per cell; energies are rho*e (reactor type 1) or
-rho*h (type 2).  Density and energy come from the engine's device EOS.
+rho*h (type 2).  Density and energy come from an EOS callable
+``eos(T, Y, P, reactor_type) -> (rho, rho*e)``; the default is the engine's
+device EOS (Fuego PYT2RE on the GPU).
 """
 
 from __future__ import annotations
+
+import os
 
 import numpy as np
 
@@ -108,14 +113,20 @@ class Cells:
                      self.reactor_type, self.dt, dict(self.meta))
 
 
-def premix_cells(mech, ncells, seed, T0, dT, phi0, dphi, P=P_ATM, reactor_type=1, dt=1e-4, device="cuda"):
-    species = _lib.species_names(mech)
-    mw = _lib.molecular_weights(mech)
+def device_eos(mech, device="cuda"):
+    return lambda T, Y, P, rtype: _device_state(mech, T, Y, P, rtype, device)
+
+
+def premix_cells(mech, ncells, seed, T0, dT, phi0, dphi, P=P_ATM, reactor_type=1, dt=1e-4, device="cuda",
+                 eos=None, species=None, mw=None):
+    species = species or _lib.species_names(mech)
+    mw = _lib.molecular_weights(mech) if mw is None else mw
+    eos = eos or device_eos(mech, device)
     rng = np.random.default_rng(seed)
     T = T0 + dT * rng.uniform(size=ncells)
     phi = phi0 + dphi * rng.uniform(size=ncells)
     Y = mass_fractions(mole_fractions(mech, phi, species), mw)
-    rho, rhoE = _device_state(mech, T, Y, P, reactor_type, device)
+    rho, rhoE = eos(T, Y, P, reactor_type)
     N = len(species)
     rY = np.zeros((ncells, N + 1))
     rY[:, :N] = rho[:, None] * Y
@@ -129,29 +140,18 @@ def lidryer_16(device="cuda"):
     return premix_cells("LiDryer", 16 ** 3, 0, 1000.0, 400.0, 0.5, 1.5, reactor_type=1, dt=1e-4, device=device)
 
 
-def burnt_pool(mech, phis, reactor, device="cuda", t_burn=1e-3, T_start=1700.0):
-    """Compositions after integrating premixed cells for t_burn at constant
-    volume from T_start (one cell per phi), with the given GPU reactor."""
-    species = _lib.species_names(mech)
-    mw = _lib.molecular_weights(mech)
-    n = len(phis)
-    T = np.full(n, T_start)
-    Y = mass_fractions(mole_fractions(mech, phis, species), mw)
-    rho, rhoE = _device_state(mech, T, Y, P_ATM, 1, device)
-    N = len(species)
-    rY = np.zeros((n, N + 1))
-    rY[:, :N] = rho[:, None] * Y
-    rY[:, N] = T
-    reactor.react(rY, np.zeros((n, N)), rhoE.copy(), np.zeros(n), t_burn, raise_on_fail=False)
-    Yb = np.clip(rY[:, :N], 0.0, None)
-    return Yb / Yb.sum(axis=1, keepdims=True)
+def burnt_pool():
+    """(phi, Y) of the committed burnt-composition pool for drm19."""
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "drm19_burnt_pool.npz"))
+    return d["phi"], d["Y"]
 
 
-def drm19_field(n=64, device="cuda", seed=1, pool_reactor=None, burnt_threshold=0.7):
+def drm19_field(n=64, device="cuda", seed=1, burnt_threshold=0.7, eos=None, species=None, mw=None):
     """drm19 on an n^3 box: the 64^3 case of the benchmark (see module doc)."""
     mech = "drm19"
-    species = _lib.species_names(mech)
-    mw = _lib.molecular_weights(mech)
+    species = species or _lib.species_names(mech)
+    mw = _lib.molecular_weights(mech) if mw is None else mw
+    eos = eos or device_eos(mech, device)
     N = len(species)
     s = fourier_field((n, n, n), 8, seed).reshape(-1)
     ncells = s.size
@@ -161,16 +161,11 @@ def drm19_field(n=64, device="cuda", seed=1, pool_reactor=None, burnt_threshold=
     Y = mass_fractions(mole_fractions(mech, phi, species), mw)
     burnt = s > burnt_threshold
     if burnt.any():
-        if pool_reactor is None:
-            from .reactor import Reactor
-
-            pool_reactor = Reactor(mech)
-            pool_reactor.init(1, 256, rtol=1e-8, atol=1e-10, max_order=5)
-        pool_phi = np.linspace(0.6, 1.4, 256)
-        pool = burnt_pool(mech, pool_phi, pool_reactor, device=device)
-        idx = np.clip(np.rint((phi[burnt] - 0.6) / 0.8 * 255).astype(int), 0, 255)
-        Y[burnt] = pool[idx]
-    rho, rhoE = _device_state(mech, T, Y, P_ATM, 1, device)
+        pphi, pY = burnt_pool()
+        idx = np.clip(np.rint((phi[burnt] - pphi[0]) / (pphi[-1] - pphi[0]) * (len(pphi) - 1)).astype(int), 0,
+                      len(pphi) - 1)
+        Y[burnt] = pY[idx]
+    rho, rhoE = eos(T, Y, P_ATM, 1)
     rY = np.zeros((ncells, N + 1))
     rY[:, :N] = rho[:, None] * Y
     rY[:, N] = T
