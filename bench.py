@@ -41,8 +41,8 @@ METRIC = "cells/s per dt (drm19 64^3, tuned engine)"
 # evaluation for drm19 (dadd + dmul + 2 dfma, exp/log included), counted with
 # ncu on single-cell launches of the pointwise kernels; see
 # profiles/drm19_flops_per_evaluation.md for the command and raw counts.
-FLOPS_RHS = {"drm19": None}
-FLOPS_JAC = {"drm19": None}
+FLOPS_RHS = {"drm19": 12023.0}
+FLOPS_JAC = {"drm19": 22943.0}
 CPU_SAMPLE = 8192  # cells of the field integrated by the CPU baseline
 
 
@@ -369,6 +369,8 @@ def our_arm(args):
                                "plain_sample": "every 8th cell, one react", "max_rel_T_tuned_vs_plain": out["dT_plain"]},
             "accuracy_vs_fp64_oracle": acc,
             "cell_failures": int(np.sum(status < 0)),
+            "per_cell_mean": dict(zip(["steps", "rhs", "jac", "lu", "newton", "err_fail", "conv_fail"],
+                                      [round(float(v), 3) for v in stats.mean(axis=0)])),
             "wall_s": wall,
         }
         print(json.dumps(line), flush=True)

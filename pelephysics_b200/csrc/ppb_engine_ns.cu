@@ -10,9 +10,9 @@
 namespace ppb {
 
 // ------------------------------------------------------------ react kernels
-template <int NS, int TEAM, typename LT>
-__device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options& o, int method, Work<LT>& w,
-                          const Batch& b, int c, double dt)
+template <int NS, int TEAM, typename LT, int METHOD>
+__device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options& o, Work<LT>& w, const Batch& b,
+                          int c, double dt)
 {
   const int n = NS + 1;
   if (b.mask && b.mask[c] == -1) {
@@ -32,7 +32,7 @@ __device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options&
   tm.sync();
   const CellIn cin{b.rhoe[c], b.rhoesrc[c]};
   int flag, cost;
-  if (method == METHOD_BDF) {
+  if (METHOD == METHOD_BDF) {
     Bdf<NS, TEAM, LT> bdf(tm, M, o, w, cin);
     flag = bdf.run(dt);
     cost = bdf.s.nfe;
@@ -65,8 +65,8 @@ __device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options&
 }
 
 // plain: one thread per cell, FP64, per-cell arrays in thread-local memory
-template <int NS>
-__global__ void __launch_bounds__(128) k_react_plain(DevMech M, Options o, int method, Batch b, double dt)
+template <int NS, int METHOD>
+__global__ void __launch_bounds__(128) k_react_plain(DevMech M, Options o, Batch b, double dt)
 {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= b.ncells) return;
@@ -103,13 +103,13 @@ __global__ void __launch_bounds__(128) k_react_plain(DevMech M, Options o, int m
     w.piv = piv;
   }
   Team<1> tm;
-  react_one<NS, 1, double>(tm, M, o, method, w, b, c, dt);
+  react_one<NS, 1, double, METHOD>(tm, M, o, w, b, c, dt);
 }
 
 // tuned: one warp per cell, shared-memory workspace, persistent work queue
-template <int NS, typename LT>
-__global__ void __launch_bounds__(256) k_react_team(DevMech M, Options o, int method, Batch b, double dt,
-                                                    int* queue, size_t cell_bytes, int persistent)
+template <int NS, typename LT, int METHOD>
+__global__ void __launch_bounds__(256) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
+                                                    size_t cell_bytes, int persistent)
 {
   extern __shared__ __align__(16) char smem[];
   Team<32> tm;
@@ -123,11 +123,11 @@ __global__ void __launch_bounds__(256) k_react_team(DevMech M, Options o, int me
       if (tm.lane == 0) c = atomicAdd(queue, 1);
       c = __shfl_sync(0xffffffffu, c, 0);
       if (c >= b.ncells) break;
-      react_one<NS, 32, LT>(tm, M, o, method, w, b, c, dt);
+      react_one<NS, 32, LT, METHOD>(tm, M, o, w, b, c, dt);
     }
   } else {
     const int c = blockIdx.x * wpb + warp;
-    if (c < b.ncells) react_one<NS, 32, LT>(tm, M, o, method, w, b, c, dt);
+    if (c < b.ncells) react_one<NS, 32, LT, METHOD>(tm, M, o, w, b, c, dt);
   }
 }
 
@@ -140,14 +140,20 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
   if (lc.engine == ENGINE_PLAIN) {
     const int threads = 128;
     const int blocks = (b.ncells + threads - 1) / threads;
-    k_react_plain<NS><<<blocks, threads, 0, st>>>(M, o, method, b, dt);
+    if (method == METHOD_BDF)
+      k_react_plain<NS, METHOD_BDF><<<blocks, threads, 0, st>>>(M, o, b, dt);
+    else
+      k_react_plain<NS, METHOD_RK64><<<blocks, threads, 0, st>>>(M, o, b, dt);
     return (int)cudaGetLastError();
   }
   const int wpb = lc.warps_per_block > 0 ? lc.warps_per_block : 4;
-  const size_t cb = lc.lu_fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
+  const bool fp32 = lc.lu_fp32 && method == METHOD_BDF;
+  const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
   const size_t shm = cb * wpb;
-  auto kern = lc.lu_fp32 ? (void (*)(DevMech, Options, int, Batch, double, int*, size_t, int))k_react_team<NS, float>
-                         : (void (*)(DevMech, Options, int, Batch, double, int*, size_t, int))k_react_team<NS, double>;
+  typedef void (*KT)(DevMech, Options, Batch, double, int*, size_t, int);
+  KT kern = (method == METHOD_RK64) ? (KT)k_react_team<NS, double, METHOD_RK64>
+            : fp32                  ? (KT)k_react_team<NS, float, METHOD_BDF>
+                                    : (KT)k_react_team<NS, double, METHOD_BDF>;
   cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   if (e != cudaSuccess) return (int)e;
   int blocks;
@@ -166,7 +172,7 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
   } else {
     blocks = (b.ncells + wpb - 1) / wpb;
   }
-  kern<<<blocks, wpb * 32, shm, st>>>(M, o, method, b, dt, queue, cb, lc.persistent);
+  kern<<<blocks, wpb * 32, shm, st>>>(M, o, b, dt, queue, cb, lc.persistent);
   return (int)cudaGetLastError();
 }
 
