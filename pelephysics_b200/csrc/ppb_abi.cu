@@ -19,13 +19,19 @@
 
 using namespace ppb;
 
-static thread_local std::string g_err;
+// last error message of the calling thread (fixed storage, so that setting
+// it never allocates)
+static thread_local char g_err[512];
 
 static int fail(int code, const std::string& msg)
 {
-  g_err = msg;
+  snprintf(g_err, sizeof(g_err), "%s", msg.c_str());
   return code;
 }
+
+namespace ppb {
+void set_error(const char* msg) { snprintf(g_err, sizeof(g_err), "%s", msg); }
+} // namespace ppb
 
 static int cuda_fail(int e, const char* where)
 {
@@ -223,7 +229,7 @@ void ppb_default_options(ppb_options* o)
   o->use_graph = 1;
 }
 
-const char* ppb_last_error(void) { return g_err.c_str(); }
+const char* ppb_last_error(void) { return g_err; }
 
 int ppb_mechanism_info(const char* mechanism, int* nspecies, int* nreactions)
 {

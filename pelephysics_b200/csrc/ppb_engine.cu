@@ -8,6 +8,7 @@
 //    grid sized to the resident capacity of the GPU whose warps pull cells
 //    from a device work queue, optional FP32 factorisation of I - gamma J
 //    with FP64 iterative refinement.
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -32,47 +33,55 @@ const PPBMechTables* find_mechanism(const char* name)
 
 // ------------------------------------------------------------ upload
 namespace {
+// Packs every table into one byte image with 16-byte aligned sections and
+// records each section's offset in a DevMech whose pointers are offsets.
 struct Packer {
-  std::vector<char> buf;
+  char* buf;     // destination image (nullptr: size only)
+  size_t cap;    // capacity of buf
+  size_t used = 0;
+  bool overflow = false;
   template <typename T>
   size_t add(const T* p, size_t n)
   {
-    size_t off = (buf.size() + 15) & ~size_t(15);
-    buf.resize(off + n * sizeof(T) + 16);
-    if (n) memcpy(buf.data() + off, p, n * sizeof(T));
+    size_t off = (used + 15) & ~size_t(15);
+    const size_t end = off + n * sizeof(T);
+    if (buf && end <= cap) {
+      if (n) memcpy(buf + off, p, n * sizeof(T));
+    } else if (buf) {
+      overflow = true;
+    }
+    used = end;
     return off;
   }
+  // write n values at byte offset off (no alignment)
+  template <typename T>
+  void put(size_t off, const T* p, size_t n)
+  {
+    if (!buf) return;
+    if (off + n * sizeof(T) > cap) {
+      overflow = true;
+      return;
+    }
+    memcpy(buf + off, p, n * sizeof(T));
+  }
 };
+
+template <typename T>
+void set_off(const T*& field, size_t off)
+{
+  field = reinterpret_cast<const T*>(off);
+}
 } // namespace
 
-int upload_mechanism(const PPBMechTables* t, DeviceMechanism* out)
+// Species-major gather lists (species -> (reaction, coefficient)) of the
+// productionRate updates, built into the image after the tables.
+static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
 {
   const int N = t->nsp, R = t->nrxn;
-  // species-major gather lists of the productionRate updates
-  std::vector<int> wg_off(N + 1, 0), wg_rx;
-  std::vector<double> wg_c;
-  for (int s = 0; s < N; s++) {
-    wg_off[s] = (int)wg_rx.size();
-    for (int r = 0; r < R; r++) {
-      for (int j = 0; j < t->rx_wup_n[r]; j++) {
-        if (t->rx_wup_sp[r * PPB_MAXW + j] == s) {
-          wg_rx.push_back(r);
-          wg_c.push_back(t->rx_wup_c[r * PPB_MAXW + j]);
-        }
-      }
-    }
-  }
-  wg_off[N] = (int)wg_rx.size();
-  Packer pk;
-  struct Rec {
-    size_t off;
-    const void** dst;
-  };
-  DevMech dm{};
+  dm = DevMech{};
   dm.nsp = N;
   dm.nrxn = R;
-  std::vector<std::pair<size_t, const void**>> recs;
-#define PPB_ADD(field, ptr, count) recs.push_back({pk.add(ptr, count), (const void**)&dm.field})
+#define PPB_ADD(field, ptr, count) set_off(dm.field, pk.add(ptr, count))
   PPB_ADD(mw, t->mw, N);
   PPB_ADD(imw, t->imw, N);
   PPB_ADD(tmid, t->tmid, N);
@@ -116,19 +125,78 @@ int upload_mechanism(const PPBMechTables* t, DeviceMechanism* out)
   PPB_ADD(eff_m1, t->eff_m1, t->eff_off[R]);
   PPB_ADD(fo_d, t->fo_d, R * PPB_NFOD);
   PPB_ADD(fo_i, t->fo_i, R * PPB_NFOI);
-  PPB_ADD(wg_off, wg_off.data(), N + 1);
-  PPB_ADD(wg_rx, wg_rx.data(), wg_rx.size());
-  PPB_ADD(wg_c, wg_c.data(), wg_c.size());
 #undef PPB_ADD
+  // gather lists, written entry by entry at exact offsets (no temporary
+  // containers, so packing itself allocates nothing)
+  int total = 0;
+  for (int r = 0; r < R; r++) total += t->rx_wup_n[r];
+  const size_t off_goff = (pk.used + 15) & ~size_t(15);
+  const size_t off_grx = (off_goff + (N + 1) * sizeof(int) + 15) & ~size_t(15);
+  const size_t off_gc = (off_grx + total * sizeof(int) + 15) & ~size_t(15);
+  int k = 0;
+  for (int s = 0; s < N; s++) {
+    pk.put(off_goff + s * sizeof(int), &k, 1);
+    for (int r = 0; r < R; r++) {
+      for (int j = 0; j < t->rx_wup_n[r]; j++) {
+        if (t->rx_wup_sp[r * PPB_MAXW + j] != s) continue;
+        pk.put(off_grx + k * sizeof(int), &r, 1);
+        pk.put(off_gc + k * sizeof(double), &t->rx_wup_c[r * PPB_MAXW + j], 1);
+        k++;
+      }
+    }
+  }
+  pk.put(off_goff + N * sizeof(int), &k, 1);
+  pk.used = off_gc + total * sizeof(double);
+  set_off(dm.wg_off, off_goff);
+  set_off(dm.wg_rx, off_grx);
+  set_off(dm.wg_c, off_gc);
+  return pk.used;
+}
+
+size_t packed_mechanism_bytes(const PPBMechTables* t)
+{
+  Packer pk{nullptr, 0};
+  DevMech dm;
+  return pack_all(t, pk, dm);
+}
+
+// Image of the tables in host memory `buf` (capacity cap) and the device
+// pointer struct for the image placed at device address `dev_base`.
+int pack_mechanism(const PPBMechTables* t, char* buf, size_t cap, const void* dev_base, DevMech* out)
+{
+  Packer pk{buf, cap};
+  DevMech dm;
+  pack_all(t, pk, dm);
+  if (pk.overflow) return -1;
+  const char* b = (const char*)dev_base;
+  // every pointer member of DevMech follows the two ints
+  const size_t first = offsetof(DevMech, mw);
+  const size_t count = (sizeof(DevMech) - first) / sizeof(void*);
+  for (size_t i = 0; i < count; i++) {
+    const void** slot = (const void**)((char*)&dm + first + i * sizeof(void*));
+    *slot = b + (size_t)(*slot);
+  }
+  *out = dm;
+  return 0;
+}
+
+int upload_mechanism(const PPBMechTables* t, DeviceMechanism* out)
+{
+  const size_t bytes = packed_mechanism_bytes(t);
+  std::vector<char> img(bytes);
   void* d = nullptr;
-  cudaError_t e = cudaMalloc(&d, pk.buf.size());
+  cudaError_t e = cudaMalloc(&d, bytes);
   if (e != cudaSuccess) return (int)e;
-  e = cudaMemcpy(d, pk.buf.data(), pk.buf.size(), cudaMemcpyHostToDevice);
+  DevMech dm;
+  if (pack_mechanism(t, img.data(), bytes, d, &dm)) {
+    cudaFree(d);
+    return (int)cudaErrorInvalidValue;
+  }
+  e = cudaMemcpy(d, img.data(), bytes, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cudaFree(d);
     return (int)e;
   }
-  for (auto& r : recs) *r.second = (const char*)d + r.first;
   out->host = t;
   cudaGetDevice(&out->device);
   out->blob = d;

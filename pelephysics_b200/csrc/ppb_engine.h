@@ -17,6 +17,10 @@ struct DeviceMechanism {
 };
 
 int upload_mechanism(const PPBMechTables* t, DeviceMechanism* out);
+// Table image for caller-owned device memory: size, and packing into a host
+// buffer with device pointers relocated to dev_base.
+size_t packed_mechanism_bytes(const PPBMechTables* t);
+int pack_mechanism(const PPBMechTables* t, char* buf, size_t cap, const void* dev_base, DevMech* out);
 void free_mechanism(DeviceMechanism* m);
 const PPBMechTables* find_mechanism(const char* name);
 
@@ -93,6 +97,10 @@ int launch_pyt2re(const DeviceMechanism& m, int eh, const double* P, const doubl
 // FP64 FMA throughput probe: returns GFLOP/s measured with CUDA events.
 int probe_fp64_peak(double* gflops, cudaStream_t st);
 int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells, cudaStream_t st);
+
+// Store the message ppb_last_error() returns for the calling thread (no
+// allocation).
+void set_error(const char* msg);
 
 // Bytes of shared memory one team-integrated cell needs.
 size_t team_cell_bytes(const PPBMechTables* t, int lu_fp32);
