@@ -177,6 +177,29 @@ int ppb_reactor_rhs(const char* mechanism, int reactor_type, double t, const dou
 int ppb_pyt2re(const char* mechanism, int eh, const double* P, const double* T, const double* Y, double* rho,
                double* e, int ncells, void* stream);
 
+/* Allocation-free flat react on DEVICE YCOrder arrays (no counterpart in the
+ * reference).  For callers that must not have a library allocate GPU memory,
+ * e.g. applications whose device memory is owned by an arena allocator
+ * (AMReX-based codes hand every device buffer out of the AMReX Arena).  It
+ * runs the tuned engine out of one static device array of 32 MiB per GPU
+ * holding the mechanism tables and the per-call scratch, and calls no
+ * cudaMalloc/cudaFree.  Limits: at most
+ * floor((30 MiB - 1 KiB) / (8 (2N+1) + 12)) cells per call (drm19: 88,360;
+ * heptane_lu_88sk: 22,028); larger calls return PPB_E_ARG.  The first call on
+ * a device (and the first use of each further mechanism there) does a
+ * synchronous set-up -- resolving the array's address and copying the
+ * mechanism tables -- and should come before any stream capture.  Every call
+ * on a device shares the array and keeps the last call's contents; calls
+ * that overlap on the GPU race and must not be issued.  integrator is
+ * "ReactorCvode" or "ReactorRK64"; opt may be NULL (reference defaults); the
+ * arrays are as in ppb_react_flat and rX += dt_react * rX_src.  When nfailed
+ * is not NULL the call waits for the stream and stores the number of cells
+ * that failed (returning PPB_E_INTEGRATE if any); with nfailed == NULL it
+ * returns once the work is queued. */
+int ppb_react_flat_device_noalloc(const char* mechanism, const char* integrator, int reactor_type,
+                                  const ppb_options* opt, double* rY, double* rYsrc, double* rX, double* rX_src,
+                                  double dt_react, int ncells, void* stream, int* nfailed);
+
 #ifdef __cplusplus
 }
 #endif

@@ -104,6 +104,8 @@ def lib():
     L.ppb_reactor_rhs.argtypes = [C.c_char_p, C.c_int, C.c_double, dp, dp, dp, dp, dp, C.c_int, C.c_int, vp]
     L.ppb_get_cell_stats.argtypes = [vp, ip, C.c_int]
     L.ppb_probe_fp64_peak.argtypes = [dpp, vp]
+    L.ppb_react_flat_device_noalloc.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(Options), dp, dp, dp, dp,
+                                                C.c_double, C.c_int, vp, ip]
     L.ppb_molecular_weights.argtypes = [C.c_char_p, dpp]
     L.ppb_pyt2re.argtypes = [C.c_char_p, C.c_int, dp, dp, dp, dp, dp, C.c_int, vp]
     _lib = L
