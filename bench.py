@@ -407,6 +407,48 @@ def flops_probe():
     return 0
 
 
+def kernel_probe(ncells=16384, reps=5):
+    """Device time of the pointwise reactor RHS and Jacobian kernels on the
+    drm19 field's first ncells cells, thread-per-cell and warp-per-cell."""
+    import torch
+
+    from pelephysics_b200 import _lib, workloads as wl
+
+    cells = wl.drm19_field(64)
+    N = cells.rY.shape[1] - 1
+    n = min(ncells, cells.ncells)
+    y = torch.as_tensor(cells.rY[:n], device="cuda").contiguous()
+    x = torch.as_tensor(cells.rX[:n], device="cuda")
+    xs = torch.as_tensor(cells.rX_src[:n], device="cuda")
+    s = torch.as_tensor(cells.rYsrc[:n], device="cuda").contiguous()
+    f = torch.zeros_like(y)
+    mw = torch.as_tensor(_lib.molecular_weights(MECH), device="cuda")
+    sc = (y[:, :N] / mw * 1e6).contiguous()
+    T = y[:, N].contiguous()
+    J = torch.zeros((n, (N + 1) ** 2), dtype=torch.float64, device="cuda")
+    L = _lib.lib()
+    out = {}
+    for team in (1, 32):
+        for name, fn in (("rhs", lambda: L.ppb_reactor_rhs(MECH.encode(), 1, 0.0, y.data_ptr(), x.data_ptr(),
+                                                               xs.data_ptr(), s.data_ptr(), f.data_ptr(), n, team, None)),
+                         ("jac", lambda: L.ppb_ajacobian(MECH.encode(), sc.data_ptr(), T.data_ptr(), 0, J.data_ptr(),
+                                                             n, team, None)),
+                         ("rates", lambda: L.ppb_production_rate(MECH.encode(), sc.data_ptr(), T.data_ptr(),
+                                                                 f.data_ptr(), n, team, None))):
+            _lib.check(fn())
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                fn()
+            b.record()
+            torch.cuda.synchronize()
+            us = a.elapsed_time(b) * 1e3 / reps
+            out[f"{name}_team{team}"] = {"us_per_launch": round(us, 2), "ns_per_cell": round(us * 1e3 / n, 3)}
+    print(json.dumps({"kernel_probe": out, "cells": n}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -415,11 +457,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--edge", type=int, default=64, help="field edge (profiling runs use a smaller box)")
+    ap.add_argument("--kernel-probe", action="store_true",
+                    help="time the pointwise RHS / Jacobian / rate kernels on the field's cells")
     ap.add_argument("--flops-probe", action="store_true",
                     help="launch one single-cell RHS and one Jacobian evaluation (for an ncu FP64 op count)")
     args = ap.parse_args()
     if args.flops_probe:
         return flops_probe()
+    if args.kernel_probe:
+        return kernel_probe()
     if args.impl == "reference":
         return reference_arm(args)
     return our_arm(args)
