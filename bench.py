@@ -449,6 +449,45 @@ def kernel_probe(ncells=16384, reps=5):
     return 0
 
 
+def phase_probe(edge=64, engine=1, lu_fp32=0):
+    """Per-phase cycle totals of one react() of the field (needs the profiling
+    build: PPB_LIB=pelephysics_b200/libppb200_phase.so)."""
+    import ctypes as C
+
+    import torch
+
+    from pelephysics_b200 import _lib, workloads as wl
+    from pelephysics_b200.reactor import Reactor
+
+    L = _lib.lib()
+    if not hasattr(L, "ppb_phase_cycles"):
+        raise SystemExit("phase probe needs PPB_LIB=pelephysics_b200/libppb200_phase.so")
+    cells = wl.drm19_field(edge)
+    n = cells.ncells
+    r = Reactor(MECH)
+    r.init(1, n, engine=engine, lu_fp32=lu_fp32, use_graph=0, **OPTS)
+    buf = (C.c_ulonglong * 7)()
+    y = torch.as_tensor(cells.rY.T.copy(), device="cuda")
+    s_ = torch.as_tensor(cells.rYsrc.T.copy(), device="cuda")
+    x = torch.as_tensor(cells.rX, device="cuda")
+    xs = torch.as_tensor(cells.rX_src, device="cuda")
+    r.react_soa(y.clone(), s_, x.clone(), xs, DT)
+    torch.cuda.synchronize()
+    L.ppb_phase_cycles(buf, 1)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    r.react_soa(y, s_, x, xs, DT)
+    b.record()
+    torch.cuda.synchronize()
+    L.ppb_phase_cycles(buf, 1)
+    names = ["rhs", "jac", "lu", "solve", "newton", "step", "total"]
+    tot = buf[6]
+    res = {k: {"cycles_per_cell": buf[i] / n, "frac_of_total": buf[i] / tot} for i, k in enumerate(names)}
+    print(json.dumps({"phase_probe": res, "cells": n, "ms": a.elapsed_time(b),
+                      "per_cell_mean": r.cell_stats(n).mean(axis=0).round(3).tolist()}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -457,6 +496,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--edge", type=int, default=64, help="field edge (profiling runs use a smaller box)")
+    ap.add_argument("--phase-probe", action="store_true",
+                    help="per-phase cycle counters of one react (profiling build, PPB_LIB)")
     ap.add_argument("--kernel-probe", action="store_true",
                     help="time the pointwise RHS / Jacobian / rate kernels on the field's cells")
     ap.add_argument("--flops-probe", action="store_true",
@@ -466,6 +507,8 @@ def main():
         return flops_probe()
     if args.kernel_probe:
         return kernel_probe()
+    if args.phase_probe:
+        return phase_probe(args.edge)
     if args.impl == "reference":
         return reference_arm(args)
     return our_arm(args)

@@ -11,7 +11,9 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libppb200.so")
+# PPB_LIB selects another build of the engine (e.g. the profiling variant
+# libppb200_phase.so with per-phase cycle counters)
+LIB_PATH = os.environ.get("PPB_LIB", os.path.join(HERE, "libppb200.so"))
 HEADER = os.path.join(os.path.dirname(HERE), "include", "pelephysics_b200.h")
 
 PPB_E_ARG, PPB_E_CUDA, PPB_E_MECH, PPB_E_STATE, PPB_E_INTEGRATE = -1, -2, -3, -4, 1

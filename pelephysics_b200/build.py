@@ -18,6 +18,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libppb200.so")
+# profiling variant: per-phase cycle counters in the BDF kernels
+PHASE_OBJ = os.path.join(HERE, "_build_phase")
+PHASE_LIB = os.path.join(HERE, "libppb200_phase.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 SPECIES_COUNTS = (9, 21, 53, 88)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -48,9 +51,9 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def _compile(unit, extra_flags):
+def _compile(unit, extra_flags, objdir=OBJ):
     obj, src, defs = unit
-    out = os.path.join(OBJ, obj)
+    out = os.path.join(objdir, obj)
     srcp = os.path.join(CSRC, src)
     if not _stale(out, [srcp] + _headers()):
         return None
@@ -62,23 +65,25 @@ def _compile(unit, extra_flags):
     return obj
 
 
-def build(jobs: int | None = None, verbose: bool = False, extra_flags=()) -> str:
+def build(jobs: int | None = None, verbose: bool = False, extra_flags=(), phase_timers: bool = False) -> str:
     """Compile (incrementally) and link the engine; returns the library path."""
-    os.makedirs(OBJ, exist_ok=True)
+    objdir, lib = (PHASE_OBJ, PHASE_LIB) if phase_timers else (OBJ, LIB)
+    flags = list(extra_flags) + (["-DPPB_PHASE_TIMERS"] if phase_timers else [])
+    os.makedirs(objdir, exist_ok=True)
     units = _units()
     jobs = jobs or min(len(units), os.cpu_count() or 4)
     with ThreadPoolExecutor(max_workers=jobs) as ex:
-        done = list(ex.map(lambda u: _compile(u, list(extra_flags)), units))
-    objs = [os.path.join(OBJ, u[0]) for u in units]
-    if any(done) or _stale(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB + ".tmp"] + objs + ["-lcudart"]
+        done = list(ex.map(lambda u: _compile(u, flags, objdir), units))
+    objs = [os.path.join(objdir, u[0]) for u in units]
+    if any(done) or _stale(lib, objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", lib + ".tmp"] + objs + ["-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-        os.replace(LIB + ".tmp", LIB)
+        os.replace(lib + ".tmp", lib)
     if verbose:
-        print("built", LIB, "recompiled:", [d for d in done if d])
-    return LIB
+        print("built", lib, "recompiled:", [d for d in done if d])
+    return lib
 
 
 if __name__ == "__main__":
@@ -86,7 +91,7 @@ if __name__ == "__main__":
     if "-j" in sys.argv:
         j = int(sys.argv[sys.argv.index("-j") + 1])
     try:
-        build(j, verbose=True)
+        build(j, verbose=True, phase_timers="--phase-timers" in sys.argv)
     except RuntimeError as e:
         print(e, file=sys.stderr)
         sys.exit(1)

@@ -659,4 +659,9 @@ int ppb_pyt2re(const char* mechanism, int eh, const double* P, const double* T, 
   return cuda_fail(launch_pyt2re(*dm, eh, P, T, Y, rho, e_out, ncells, (cudaStream_t)stream), "pyt2re");
 }
 
+#ifdef PPB_PHASE_TIMERS
+// Profiling builds only: per-phase cycle totals of the BDF kernels.
+int ppb_phase_cycles(unsigned long long* out, int reset) { return cuda_fail(phase_cycles(out, reset), "phase"); }
+#endif
+
 } // extern "C"

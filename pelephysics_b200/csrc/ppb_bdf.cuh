@@ -18,6 +18,19 @@
 
 namespace ppb {
 
+// Optional per-phase cycle counters (compile with -DPPB_PHASE_TIMERS): each
+// team accumulates clock64() deltas per phase and adds them to
+// g_phase_cycles at the end of a cell.  Off in the shipped library.
+enum Phase { PH_RHS = 0, PH_JAC, PH_LU, PH_SOLVE, PH_NEWTON, PH_STEP, PH_TOTAL, PH_COUNT };
+#ifdef PPB_PHASE_TIMERS
+static __device__ unsigned long long g_phase_cycles[PH_COUNT]; // one copy per translation unit
+#define PPB_TIC(ph) const long long _tic_##ph = clock64()
+#define PPB_TOC(ph) s.phase[ph] += clock64() - _tic_##ph
+#else
+#define PPB_TIC(ph)
+#define PPB_TOC(ph)
+#endif
+
 enum { ST_OK = 0, ST_TOO_MUCH_WORK = -1, ST_ERR_FAILURE = -3, ST_CONV_FAILURE = -4,
        ST_LSETUP_FAIL = -6, ST_TOO_CLOSE = -27, ST_SKIPPED = 1 };
 
@@ -67,6 +80,7 @@ __device__ double reactor_rhs(
     ei[s] = (EH ? h_RT(M, s, T, invT) : u_RT(M, s, T, invT)) * (RT * im);
     sc[s] = (rho * Y[s] * im) * 1.0e6;
   }
+  if (tm.lane == 0) sc[N] = 1.0; // padding slot of the packed reaction records
   tm.sync();
   RateScratch rs{sc, g, qd};
   production_rate(tm, M, wdot, sc, T, rs);
@@ -86,7 +100,7 @@ __device__ double reactor_rhs(
 template <int TEAM, int PER>
 __device__ void reactor_jac(
   const Team<TEAM>& tm, const DevMech& M, int rtype, const double* y, double* J, double* sc, double* g,
-  double* wdot, double* h1, double* h2, double* h3, double* h4)
+  double* wdot, double* h1, double* h2, double* h3, double* h4, double* qd = nullptr, double* jx = nullptr)
 {
   const int N = M.nsp, n = N + 1;
   double a = 0.0;
@@ -97,8 +111,9 @@ __device__ void reactor_jac(
     const double Ys = y[s] / rho;
     sc[s] = 1.e6 * (rho * Ys * __ldg(M.imw + s));
   }
+  if (tm.lane == 0) sc[N] = 1.0; // padding slot of the packed reaction records
   tm.sync();
-  RateScratch rs{sc, g, nullptr};
+  RateScratch rs{sc, g, qd, jx};
   ajacobian<TEAM, PER>(tm, M, J, sc, temp, rtype == 2 ? 1 : 0, rs, wdot, h1, h2, h3, h4);
   // DWDOT unit rescaling followed by the cJac mw/imw scaling, column by column
   for (int i = tm.lane; i < n; i += TEAM) {
@@ -211,6 +226,9 @@ struct BdfScalars {
   double gamma_lu; // gamma of the factored matrix I - gamma J
   int q, qprime, qwait, L, qmax, indx_acor, jcur;
   int nst, nstlp, nstlj, nfe, nje, nsetups, nni, ncfn, netf;
+#ifdef PPB_PHASE_TIMERS
+  long long phase[PH_COUNT];
+#endif
 };
 
 struct CellIn {
@@ -254,14 +272,21 @@ struct Bdf {
 
   __device__ void f(double t, const double* y, double* fy)
   {
+    PPB_TIC(PH_RHS);
     reactor_rhs<TEAM>(tm, M, o.reactor_type, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
                       w.ei);
     s.nfe++;
+    PPB_TOC(PH_RHS);
   }
 
   __device__ void jac()
   {
-    reactor_jac<TEAM, PER>(tm, M, o.reactor_type, w.y, w.J, w.sc, w.g, w.wdot, w.Y, w.ei, w.h1, w.h2);
+    PPB_TIC(PH_JAC);
+    // the Newton matrix region is free while the Jacobian is formed: it holds
+    // the per-reaction factors of the warp-cooperative evaluation
+    reactor_jac<TEAM, PER>(tm, M, o.reactor_type, w.y, w.J, w.sc, w.g, w.wdot, w.Y, w.ei, w.h1, w.h2,
+                           TEAM > 1 ? w.qd : nullptr, TEAM > 1 ? reinterpret_cast<double*>(w.A) : nullptr);
+    PPB_TOC(PH_JAC);
   }
 
   __device__ int hin(double tout)
@@ -412,6 +437,7 @@ struct Bdf {
       jac();
     }
     s.gamma_lu = s.gamma;
+    PPB_TIC(PH_LU);
     for (int i = tm.lane; i < n; i += TEAM) {
       for (int j = 0; j < n; j++) {
         double v = -s.gamma * w.J[j * n + i];
@@ -420,12 +446,21 @@ struct Bdf {
       }
     }
     tm.sync();
-    return lu_factor<TEAM, LT>(tm, w.A, n, w.piv) ? 1 : 0;
+    const int ier = lu_factor<TEAM, LT>(tm, w.A, n, w.piv) ? 1 : 0;
+    PPB_TOC(PH_LU);
+    return ier;
   }
 
   // x := (I - gamma J)^{-1} b, with FP64 iterative refinement when the
   // factor is FP32.  b and x are w.delta; w.tempv is scratch.
   __device__ void ls_solve()
+  {
+    PPB_TIC(PH_SOLVE);
+    ls_solve_impl();
+    PPB_TOC(PH_SOLVE);
+  }
+
+  __device__ void ls_solve_impl()
   {
     if (sizeof(LT) == sizeof(double) || o.refine_sweeps <= 0) {
       lu_solve<TEAM, LT>(tm, w.A, n, w.piv, w.delta);
@@ -466,6 +501,14 @@ struct Bdf {
   }
 
   __device__ int nls(int nflag)
+  {
+    PPB_TIC(PH_NEWTON);
+    const int r = nls_impl(nflag);
+    PPB_TOC(PH_NEWTON);
+    return r;
+  }
+
+  __device__ int nls_impl(int nflag)
   {
     const int convfail = ((nflag == 0) || (nflag == 2)) ? 0 : 2;
     bool callSetup = (nflag == 1) || (nflag == 2) || (s.nst == 0) || (s.nst >= s.nstlp + 20) ||
@@ -724,6 +767,14 @@ struct Bdf {
 
   __device__ int step()
   {
+    PPB_TIC(PH_STEP);
+    const int r = step_impl();
+    PPB_TOC(PH_STEP);
+    return r;
+  }
+
+  __device__ int step_impl()
+  {
     const double saved_t = s.tn;
     int ncf = 0, nef = 0, nflag = 0;
     double dsm = 0.0;
@@ -750,6 +801,7 @@ struct Bdf {
   __device__ int run(double tout)
   {
     s = BdfScalars{};
+    PPB_TIC(PH_TOTAL);
     s.qmax = o.max_order;
     s.q = 1;
     s.L = 2;
@@ -790,6 +842,11 @@ struct Bdf {
       for (int i = tm.lane; i < n; i += TEAM) w.y[i] = w.zn[0][i];
       tm.sync();
     }
+    PPB_TOC(PH_TOTAL);
+#ifdef PPB_PHASE_TIMERS
+    if (tm.lane == 0)
+      for (int q = 0; q < PH_COUNT; q++) atomicAdd(&g_phase_cycles[q], (unsigned long long)s.phase[q]);
+#endif
     return flag;
   }
 };

@@ -147,6 +147,157 @@ static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
   }
   pk.put(off_goff + N * sizeof(int), &k, 1);
   pk.used = off_gc + total * sizeof(double);
+  // aJacobian net-stoichiometry gather (species -> (reaction, nu)), reaction order
+  int jtotal = 0;
+  for (int r = 0; r < R; r++)
+    for (int j = 0; j < t->rx_jn_n[r]; j++) jtotal += (t->rx_jn_c[r * PPB_MAXJN + j] != 0.0);
+  const size_t off_joff = (pk.used + 15) & ~size_t(15);
+  const size_t off_jrx = (off_joff + (N + 1) * sizeof(int) + 15) & ~size_t(15);
+  const size_t off_jc = (off_jrx + jtotal * sizeof(int) + 15) & ~size_t(15);
+  k = 0;
+  for (int sp = 0; sp < N; sp++) {
+    pk.put(off_joff + sp * sizeof(int), &k, 1);
+    for (int r = 0; r < R; r++) {
+      for (int j = 0; j < t->rx_jn_n[r]; j++) {
+        if (t->rx_jn_sp[r * PPB_MAXJN + j] != sp || t->rx_jn_c[r * PPB_MAXJN + j] == 0.0) continue;
+        pk.put(off_jrx + k * sizeof(int), &r, 1);
+        pk.put(off_jc + k * sizeof(double), &t->rx_jn_c[r * PPB_MAXJN + j], 1);
+        k++;
+      }
+    }
+  }
+  pk.put(off_joff + N * sizeof(int), &k, 1);
+  pk.used = off_jc + jtotal * sizeof(double);
+  set_off(dm.jg_off, off_joff);
+  set_off(dm.jg_rx, off_jrx);
+  set_off(dm.jg_c, off_jc);
+  // packed reaction records, fall-off records and efficiency masks
+  const size_t off_rxp = (pk.used + 15) & ~size_t(15);
+  int nfo = 0;
+  for (int r = 0; r < R; r++)
+    if (t->rx_kind[r] == PPB_RX_TROE || t->rx_kind[r] == PPB_RX_LINDEMANN) nfo++;
+  int nalpha = 0;
+  for (int r = 0; r < R; r++)
+    if (t->rx_kind[r] == PPB_RX_THIRD || t->rx_kind[r] == PPB_RX_TROE || t->rx_kind[r] == PPB_RX_LINDEMANN)
+      nalpha++;
+  const size_t off_fop = off_rxp + (size_t)R * sizeof(RxPack);
+  const size_t off_msk = off_fop + (size_t)nfo * sizeof(FoPack);
+  const size_t off_effd = off_msk + (size_t)R * 4 * sizeof(unsigned);
+  int fo = 0, aslot = 0;
+  for (int r = 0; r < R; r++) {
+    RxPack p;
+    memset(&p, 0, sizeof(p));
+    p.A = t->rx_A[r];
+    p.beta = t->rx_beta[r];
+    p.EaR = t->rx_EaR[r];
+    for (int j = 0; j < 4; j++) p.fsp[j] = (unsigned char)N;
+    for (int j = 0; j < 8; j++) p.rsp[j] = (unsigned char)N;
+    for (int j = 0; j < 6; j++) {
+      p.kcs[j] = (unsigned char)N;
+      p.jns[j] = (unsigned char)N;
+    }
+    int nf = 0, nr = 0;
+    for (int j = 0; j < t->rx_fps_n[r]; j++)
+      for (int q = 0; q < (int)t->rx_fps_c[r * PPB_MAXPS + j]; q++)
+        if (nf < 4) p.fsp[nf++] = (unsigned char)t->rx_fps_sp[r * PPB_MAXPS + j];
+        else pk.overflow = true;
+    for (int j = 0; j < t->rx_rps_n[r]; j++)
+      for (int q = 0; q < (int)t->rx_rps_c[r * PPB_MAXPS + j]; q++)
+        if (nr < 8) p.rsp[nr++] = (unsigned char)t->rx_rps_sp[r * PPB_MAXPS + j];
+        else pk.overflow = true;
+    p.nf = (unsigned char)nf;
+    p.nr = (unsigned char)nr;
+    // the enthalpy-sum lists of the Jacobian must be the phase-space lists
+    // (true without non-stoichiometric orders): the packed Jacobian reads
+    // both from the slots
+    {
+      int cnt = 0;
+      for (int j = 0; j < t->rx_hr_n[r]; j++) {
+        const int sp = t->rx_hr_sp[r * PPB_MAXPS + j];
+        int o = 0;
+        for (int q = 0; q < nf; q++) o += (p.fsp[q] == sp);
+        if ((double)o != t->rx_hr_c[r * PPB_MAXPS + j]) pk.overflow = true;
+        cnt += o;
+      }
+      if (cnt != nf) pk.overflow = true;
+      if (t->rx_rev[r]) {
+        cnt = 0;
+        for (int j = 0; j < t->rx_hp_n[r]; j++) {
+          const int sp = t->rx_hp_sp[r * PPB_MAXPS + j];
+          int o = 0;
+          for (int q = 0; q < nr; q++) o += (p.rsp[q] == sp);
+          if ((double)o != t->rx_hp_c[r * PPB_MAXPS + j]) pk.overflow = true;
+          cnt += o;
+        }
+        if (cnt != nr) pk.overflow = true;
+      }
+    }
+    if (t->rx_kc_n[r] > 6 || t->rx_jn_n[r] > 6) pk.overflow = true;
+    for (int j = 0; j < t->rx_kc_n[r]; j++)
+      if ((double)(signed char)t->rx_kc_c[r * PPB_MAXKC + j] != t->rx_kc_c[r * PPB_MAXKC + j]) pk.overflow = true;
+    for (int j = 0; j < t->rx_jn_n[r]; j++)
+      if ((double)(signed char)t->rx_jn_c[r * PPB_MAXJN + j] != t->rx_jn_c[r * PPB_MAXJN + j]) pk.overflow = true;
+    for (int j = 0; j < t->rx_kc_n[r] && j < 6; j++) {
+      p.kcs[j] = (unsigned char)t->rx_kc_sp[r * PPB_MAXKC + j];
+      p.kcc[j] = (signed char)t->rx_kc_c[r * PPB_MAXKC + j];
+    }
+    for (int j = 0; j < t->rx_jn_n[r] && j < 6; j++) {
+      p.jns[j] = (unsigned char)t->rx_jn_sp[r * PPB_MAXJN + j];
+      p.jnc[j] = (signed char)t->rx_jn_c[r * PPB_MAXJN + j];
+    }
+    p.njn = (unsigned char)t->rx_jn_n[r];
+    p.kind = (unsigned char)t->rx_kind[r];
+    p.rev = (unsigned char)t->rx_rev[r];
+    p.kcpow = (signed char)t->rx_kcpow[r];
+    p.sum_nuk = (signed char)t->rx_sum_nuk[r];
+    p.eff0 = (unsigned short)t->eff_off[r];
+    p.effn = (unsigned short)(t->eff_off[r + 1] - t->eff_off[r]);
+    p.fo = 255;
+    if (t->rx_kind[r] == PPB_RX_TROE || t->rx_kind[r] == PPB_RX_LINDEMANN) {
+      const double* d = t->fo_d + r * PPB_NFOD;
+      const int* fi = t->fo_i + r * PPB_NFOI;
+      FoPack f;
+      memset(&f, 0, sizeof(f));
+      f.P0 = d[PPB_FO_P0];
+      f.k0 = d[PPB_FO_K0];
+      f.beta0 = d[PPB_FO_BETA0];
+      f.EaR0 = d[PPB_FO_EAR0];
+      f.prdim = d[PPB_FO_PRDIM];
+      f.a = d[PPB_FO_A];
+      f.T3 = d[PPB_FO_T3];
+      f.T1 = d[PPB_FO_T1];
+      f.T2 = d[PPB_FO_T2];
+      f.oma = d[PPB_FO_OMA];
+      f.iT3 = d[PPB_FO_IT3];
+      f.iT1 = d[PPB_FO_IT1];
+      f.ntroe = (unsigned char)fi[PPB_FOI_NTROE];
+      f.p1 = (unsigned char)fi[PPB_FOI_P1];
+      f.p2 = (unsigned char)fi[PPB_FOI_P2];
+      f.j1 = (unsigned char)fi[PPB_FOI_J1];
+      f.j2 = (unsigned char)fi[PPB_FOI_J2];
+      f.j3 = (unsigned char)fi[PPB_FOI_J3];
+      f.lindemann = (unsigned char)(t->rx_kind[r] == PPB_RX_LINDEMANN);
+      pk.put(off_fop + fo * sizeof(FoPack), &f, 1);
+      p.fo = (unsigned char)fo++;
+    }
+    if (t->rx_kind[r] == PPB_RX_THIRD || t->rx_kind[r] == PPB_RX_TROE || t->rx_kind[r] == PPB_RX_LINDEMANN) {
+      const double one = 1.0;
+      for (int q = 0; q < N; q++) pk.put(off_effd + ((size_t)aslot * N + q) * sizeof(double), &one, 1);
+      for (int e = t->eff_off[r]; e < t->eff_off[r + 1]; e++)
+        pk.put(off_effd + ((size_t)aslot * N + t->eff_sp[e]) * sizeof(double), &t->eff_e[e], 1);
+      p.aslot = (unsigned short)aslot++;
+    }
+    pk.put(off_rxp + r * sizeof(RxPack), &p, 1);
+    unsigned m[4] = {0, 0, 0, 0};
+    for (int e = t->eff_off[r]; e < t->eff_off[r + 1]; e++) m[t->eff_sp[e] >> 5] |= 1u << (t->eff_sp[e] & 31);
+    pk.put(off_msk + r * 4 * sizeof(unsigned), m, 4);
+  }
+  if (N > 127 || nfo > 254) pk.overflow = true;
+  pk.used = off_effd + (size_t)nalpha * N * sizeof(double);
+  set_off(dm.effd, off_effd);
+  set_off(dm.rxp, off_rxp);
+  set_off(dm.fop, off_fop);
+  set_off(dm.effmask, off_msk);
   set_off(dm.wg_off, off_goff);
   set_off(dm.wg_rx, off_grx);
   set_off(dm.wg_c, off_gc);
@@ -314,6 +465,7 @@ __global__ void k_production_rate(DevMech M, const double* sc, const double* T, 
   double* s_w = base + 2 * (N + 1);
   double* s_qd = base + 8 * (N + 1);
   for (int s = tm.lane; s < N; s += TEAM) s_sc[s] = sc[(size_t)cc * N + s];
+  if (tm.lane == 0) s_sc[N] = 1.0; // padding slot of the packed reaction records
   tm.sync();
   RateScratch rs{s_sc, s_g, s_qd};
   production_rate<TEAM>(tm, M, s_w, s_sc, T[cc], rs);
@@ -544,6 +696,26 @@ __global__ void k_energy_update(double* rX, const double* rXs, double dt, int n)
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c < n) rX[c] = rX[c] + dt * rXs[c];
 }
+
+#ifdef PPB_PHASE_TIMERS
+int phase_cycles_9(unsigned long long*, int);
+int phase_cycles_21(unsigned long long*, int);
+int phase_cycles_53(unsigned long long*, int);
+int phase_cycles_88(unsigned long long*, int);
+
+int phase_cycles(unsigned long long* out, int reset)
+{
+  for (int q = 0; q < PH_COUNT; q++) out[q] = 0;
+  int (*fns[4])(unsigned long long*, int) = {phase_cycles_9, phase_cycles_21, phase_cycles_53, phase_cycles_88};
+  for (auto fn : fns) {
+    unsigned long long part[PH_COUNT];
+    const int e = fn(part, reset);
+    if (e) return e;
+    for (int q = 0; q < PH_COUNT; q++) out[q] += part[q];
+  }
+  return 0;
+}
+#endif
 
 int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells, cudaStream_t st)
 {

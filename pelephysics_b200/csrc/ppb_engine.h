@@ -102,6 +102,10 @@ int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells
 // allocation).
 void set_error(const char* msg);
 
+#ifdef PPB_PHASE_TIMERS
+int phase_cycles(unsigned long long* out, int reset);
+#endif
+
 // Bytes of shared memory one team-integrated cell needs.
 size_t team_cell_bytes(const PPBMechTables* t, int lu_fp32);
 } // namespace ppb

@@ -197,10 +197,11 @@ __global__ void k_ajacobian(DevMech M, const double* sc, const double* T, int co
   double* h3 = base + 5 * n;
   double* h4 = base + 6 * n;
   // serial: accumulate straight into the output; team: into shared memory
-  double* s_J = (TEAM == 1) ? J + (size_t)cc * n * n : base + 8 * n + M.nrxn;
+  double* s_J = (TEAM == 1) ? J + (size_t)cc * n * n : base + 8 * n + 5 * M.nrxn;
   for (int s = tm.lane; s < N; s += TEAM) s_sc[s] = sc[(size_t)cc * N + s];
+  if (tm.lane == 0) s_sc[N] = 1.0; // padding slot of the packed reaction records
   tm.sync();
-  RateScratch rs{s_sc, s_g, nullptr};
+  RateScratch rs{s_sc, s_g, TEAM > 1 ? base + 8 * n : nullptr, TEAM > 1 ? base + 8 * n + M.nrxn : nullptr};
   ajacobian<TEAM, PER>(tm, M, s_J, s_sc, T[cc], consP, rs, s_w, h1, h2, h3, h4);
   if (TEAM > 1 && c < ncells)
     for (int i = tm.lane; i < n * n; i += TEAM) J[(size_t)c * n * n + i] = s_J[i];
@@ -238,4 +239,15 @@ int PPB_CAT(launch_ajacobian_, PPB_NS)(const DevMech& M, const double* sc, const
 {
   return launch_ajac_ns<PPB_NS>(M, sc, T, consP, J, ncells, team, st);
 }
+#ifdef PPB_PHASE_TIMERS
+int PPB_CAT(phase_cycles_, PPB_NS)(unsigned long long* out, int reset)
+{
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_phase_cycles, sizeof(unsigned long long) * PH_COUNT);
+  if (e == cudaSuccess && reset) {
+    unsigned long long z[PH_COUNT] = {};
+    e = cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z));
+  }
+  return (int)e;
+}
+#endif
 } // namespace ppb

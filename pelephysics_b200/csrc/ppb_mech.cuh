@@ -52,7 +52,43 @@ struct DevMech {
   // entries g in [wg_off[s], wg_off[s+1]) add wg_c[g] * qdot[wg_rx[g]]
   const int *wg_off, *wg_rx;
   const double* wg_c;
+  // packed per-reaction records (see RxPack) for the warp-cooperative paths
+  const struct RxPack* rxp;
+  const struct FoPack* fop;
+  const unsigned* effmask; // 4 words per reaction: species with a listed efficiency
+  const double* effd;      // [third-body reactions][nsp] efficiencies, 1 where unlisted
+  // species-major gather of the aJacobian net stoichiometry (jn lists)
+  const int *jg_off, *jg_rx;
+  const double* jg_c;
 };
+
+// One reaction in 80 bytes (5 x 16-byte loads).  Species lists are expanded
+// by order and padded with the index nsp, whose concentration slot holds 1.0
+// and whose g/RT and h/RT slots hold 0.
+struct alignas(16) RxPack {
+  double A, beta, EaR;     // SI pre-exponential, exponent, Ea/R
+  unsigned char fsp[4];    // forward phase space (reactants + explicit collider)
+  unsigned char rsp[8];    // reverse phase space
+  unsigned char kcs[6];    // Gibbs terms of the equilibrium exponent
+  signed char kcc[6];
+  unsigned char jns[6];    // aJacobian net stoichiometry
+  signed char jnc[6];
+  unsigned char kind, rev; // PPB_RX_*, reversible
+  signed char kcpow;       // power of 1/refC
+  signed char sum_nuk;     // (#products - #reactants) incl. collider
+  unsigned char fo;        // fall-off record, 255 = none
+  unsigned char nf, nr, njn;
+  unsigned short eff0, effn; // efficiency list
+  unsigned short aslot;      // row of the dense efficiency table (effd)
+  unsigned char pad[2];
+};
+static_assert(sizeof(RxPack) == 80, "RxPack is five 16-byte words");
+
+struct alignas(16) FoPack {
+  double P0, k0, beta0, EaR0, prdim, a, T3, T1, T2, oma, iT3, iT1;
+  unsigned char ntroe, p1, p2, j1, j2, j3, lindemann, pad[9];
+};
+static_assert(sizeof(FoPack) == 112, "FoPack is seven 16-byte words");
 
 template <int TEAM>
 struct Team {
@@ -306,11 +342,159 @@ __device__ __forceinline__ double rxn_qdot(
   return qf - qr;
 }
 
+__device__ __forceinline__ RxPack load_rx(const DevMech& M, int r)
+{
+  RxPack p;
+  const int4* src = reinterpret_cast<const int4*>(M.rxp + r);
+  int4* dst = reinterpret_cast<int4*>(&p);
+#pragma unroll
+  for (int i = 0; i < 5; i++) dst[i] = __ldg(src + i);
+  return p;
+}
+
+__device__ __forceinline__ FoPack load_fo(const DevMech& M, int f)
+{
+  FoPack p;
+  const int4* src = reinterpret_cast<const int4*>(M.fop + f);
+  int4* dst = reinterpret_cast<int4*>(&p);
+#pragma unroll
+  for (int i = 0; i < 7; i++) dst[i] = __ldg(src + i);
+  return p;
+}
+
+// Slot lists are sorted by species with repeats adjacent (a species of
+// order o fills o slots); the helpers walk them run by run so that each
+// product is formed exactly as from the (species, order) lists.
+
+// Phase space: product over runs of x^o, as phase_space() forms it.
+template <int K>
+__device__ __forceinline__ double slots_product(const unsigned char (&sp)[K], const double* sc)
+{
+  double p = 1.0;
+  int j = 0;
+#pragma unroll
+  for (int i = 0; i < K; i++) {
+    if (i != j) continue;
+    int c = 1;
+    while (j + c < K && sp[j + c] == sp[j]) c++;
+    const double x = sc[sp[j]];
+    double t = x;
+    for (int q = 1; q < c; q++) t *= x;
+    p *= t;
+    j += c;
+  }
+  return p;
+}
+
+// d(phase space)/d sc[k], as dphase() forms it (jacobian.py:1398-1515).
+template <int K>
+__device__ __forceinline__ double slots_dproduct(const unsigned char (&sp)[K], const double* sc, int k)
+{
+  double p = 1.0;
+  int j = 0;
+#pragma unroll
+  for (int i = 0; i < K; i++) {
+    if (i != j) continue;
+    int c = 1;
+    while (j + c < K && sp[j + c] == sp[j]) c++;
+    const double x = sc[sp[j]];
+    if (sp[j] == k) {
+      if (c > 1) {
+        p *= (double)c;
+        for (int q = 1; q < c; q++) p *= x;
+      }
+    } else {
+      double t = x;
+      for (int q = 1; q < c; q++) t *= x;
+      p *= t;
+    }
+    j += c;
+  }
+  return p;
+}
+
+// Sum over runs of o * h[species] (the enthalpy sums of dKc/dT).
+template <int K>
+__device__ __forceinline__ double slots_hsum(const unsigned char (&sp)[K], const double* h)
+{
+  double s = 0.0;
+  int j = 0;
+#pragma unroll
+  for (int i = 0; i < K; i++) {
+    if (i != j) continue;
+    int c = 1;
+    while (j + c < K && sp[j + c] == sp[j]) c++;
+    const double v = h[sp[j]];
+    s += (c == 1) ? v : (double)c * v;
+    j += c;
+  }
+  return s;
+}
+
+template <int K>
+__device__ __forceinline__ bool slots_has(const unsigned char (&sp)[K], int k)
+{
+  bool h = false;
+#pragma unroll
+  for (int j = 0; j < K; j++) h |= (sp[j] == k);
+  return h;
+}
+
+// Net rate of progress from a packed record (same formulas as rxn_qdot).
+__device__ __forceinline__ double rx_qdot_packed(
+  const DevMech& M, const RxPack& p, double T, double invT, double logT, double refC, double refCinv, double mixture,
+  const double* sc, const double* g)
+{
+  const int kind = p.kind;
+  const double k_f = p.A * exp(p.beta * logT - p.EaR * invT);
+  double Corr = 1.0;
+  const bool corr = (kind == PPB_RX_THIRD || kind == PPB_RX_TROE || kind == PPB_RX_LINDEMANN);
+  if (corr) {
+    Corr = mixture;
+    for (int e = p.eff0; e < p.eff0 + p.effn; e++) {
+      const double m1 = __ldg(M.eff_m1 + e);
+      if (m1 != 0.0) Corr += m1 * sc[__ldg(M.eff_sp + e)];
+    }
+  }
+  if (p.fo != 255) {
+    const FoPack f = load_fo(M, p.fo);
+    const double redP = Corr / k_f * f.P0 * exp(f.beta0 * logT - f.EaR0 * invT);
+    const double F = redP / (1.0 + redP);
+    if (!f.lindemann) {
+      const double logPred = log10(redP);
+      double fc = 0.0;
+      if (f.p1) fc = f.oma * exp(-T * f.iT3);
+      if (f.p2) fc += f.a * exp(-T * f.iT1);
+      if (f.ntroe == 4) fc += exp(-f.T2 * invT);
+      const double logFcent = log10(fc);
+      const double troe_c = -0.4 - 0.67 * logFcent;
+      const double troe_n = 0.75 - 1.27 * logFcent;
+      const double troe = (troe_c + logPred) / (troe_n - 0.14 * (troe_c + logPred));
+      const double F_troe = exp(M_LN10 * logFcent / (1.0 + troe * troe));
+      Corr = F * F_troe;
+    } else {
+      Corr = F;
+    }
+  }
+  const double phf = slots_product(p.fsp, sc);
+  const double qf = corr ? Corr * k_f * phf : k_f * phf;
+  double qr = 0.0;
+  if (p.rev) {
+    double arg = 0.0;
+#pragma unroll
+    for (int j = 0; j < 6; j++) arg += (double)p.kcc[j] * g[p.kcs[j]];
+    const double phr = slots_product(p.rsp, sc);
+    qr = (corr ? Corr * k_f : k_f) * exp(-arg) * refc_pow(p.kcpow, refC, refCinv) * phr;
+  }
+  return qf - qr;
+}
+
 // Per-cell scratch for the rate evaluation (team-shared).
 struct RateScratch {
-  double* sc;  // [nsp] SI concentrations
-  double* g;   // [nsp] g/RT
-  double* qd;  // [nrxn] net rates (TEAM > 1)
+  double* sc;           // [nsp + 1] SI concentrations (+ the padding slot)
+  double* g;            // [nsp + 1] g/RT (+ the padding slot)
+  double* qd;           // [nrxn] net rates (TEAM > 1)
+  double* jx = nullptr; // [4 nrxn] per-reaction Jacobian factors (TEAM > 1)
 };
 
 // productionRate (SI): wdot[s] for s owned by the lane (team-shared wdot).
@@ -349,8 +533,13 @@ __device__ void production_rate(
       }
     }
   } else {
+    // padding slots of the packed records: sc[nsp] = 1 (set by the caller),
+    // g[nsp] = 0
+    if (tm.lane == 0) rs.g[M.nsp] = 0.0;
+    tm.sync();
     for (int r = tm.lane; r < M.nrxn; r += TEAM) {
-      rs.qd[r] = rxn_qdot(M, r, T, invT, logT, refC, refCinv, mixture, sc_in, rs.g);
+      const RxPack p = load_rx(M, r);
+      rs.qd[r] = rx_qdot_packed(M, p, T, invT, logT, refC, refCinv, mixture, sc_in, rs.g);
     }
     tm.sync();
     for (int s = tm.lane; s < M.nsp; s += TEAM) {
@@ -390,6 +579,312 @@ __device__ __forceinline__ double dphase(const int* sp, const double* c, int n, 
   return p;
 }
 
+// Temperature row and column of the Jacobian (jacobian.py:203-281) from the
+// species columns, wdot and the d/dT row.
+template <int TEAM>
+__device__ void ajacobian_trow(
+  const Team<TEAM>& tm, const DevMech& M, double* J, const double* sc, double T, int consP, const double* wdot,
+  const double* hrt, double* crt, double* dcrt, double* ehrt)
+{
+  const int N = M.nsp, n = N + 1;
+  const double invT = 1.0 / T;
+  double a_cmix = 0.0, a_ehmix = 0.0, a_dcmix = 0.0, a_dehmix = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) {
+    const double cr = consP ? cp_R(M, s, T) : cv_R(M, s, T);
+    const double dc = dcvpRdT(M, s, T);
+    const double eh = consP ? hrt[s] : u_RT(M, s, T, invT);
+    crt[s] = cr;
+    dcrt[s] = dc;
+    ehrt[s] = eh;
+    a_cmix += cr * sc[s];
+    a_dcmix += dc * sc[s];
+    a_ehmix += eh * wdot[s];
+    a_dehmix += invT * (cr - eh) * wdot[s] + eh * J[N * n + s];
+  }
+  const double cmix = tm.sum(a_cmix);
+  const double dcmixdT = tm.sum(a_dcmix);
+  const double ehmix = tm.sum(a_ehmix);
+  const double dehmixdT = tm.sum(a_dehmix);
+  tm.sync();
+  const double cmixinv = 1.0 / cmix;
+  const double tmp1 = ehmix * cmixinv;
+  const double tmp3 = cmixinv * T;
+  const double tmp2 = tmp1 * tmp3;
+  for (int k = tm.lane; k < N; k += TEAM) {
+    double dehmixdc = 0.0;
+    for (int m = 0; m < N; ++m) dehmixdc += ehrt[m] * J[k * n + m];
+    J[k * n + N] = tmp2 * crt[k] - tmp3 * dehmixdc;
+  }
+  if (tm.lane == 0) J[N * n + N] = -tmp1 + tmp2 * dcmixdT - tmp3 * dehmixdT;
+  tm.sync();
+}
+
+// Per-reaction factors of the analytical Jacobian (jacobian.py:546-1305)
+// from a packed record: the net rate q, dq/dT, the forward and reverse rate
+// constants with the third-body / fall-off factor folded in, and the factor
+// that multiplies (efficiency - 1) in dq/dc.  Same formulas and operation
+// order as the reaction loop of ajacobian().
+struct RxJac {
+  double q, dqdT, kf, kr, fac;
+};
+
+__device__ __forceinline__ RxJac rx_jac_packed(
+  const DevMech& M, const RxPack& p, double T, double invT, double invT2, double logT, double refC, double refCinv,
+  double mixture, const double* sc, const double* g, const double* hrt)
+{
+  const double ln10 = log(10.0);
+  const double log10e = 1.0 / log(10.0);
+  const bool falloff = (p.fo != 255);
+  const bool has_alpha = (p.kind == PPB_RX_THIRD) || falloff;
+  const bool rev = p.rev != 0;
+  double alpha = 0.0;
+  if (has_alpha) {
+    alpha = mixture;
+    for (int e = p.eff0; e < p.eff0 + p.effn; e++) {
+      const double em1 = __ldg(M.eff_e + e) - 1.0;
+      if (em1 != 0.0) alpha += em1 * sc[__ldg(M.eff_sp + e)];
+    }
+  }
+  const double phi_f = slots_product(p.fsp, sc);
+  double k_f = p.A * exp(p.beta * logT - p.EaR * invT);
+  const double dlnkfdT = p.beta * invT + p.EaR * invT2;
+  double Pr = 0.0, fPr = 0.0, F = 1.0, dlogFdlogPr = 0.0, dlogFdT = 0.0, dlogfPrdT = 0.0;
+  if (falloff) {
+    const FoPack f = load_fo(M, p.fo);
+    const double k_0 = f.k0 * exp(f.beta0 * logT - f.EaR0 * invT);
+    Pr = f.prdim * alpha / k_f * k_0;
+    fPr = Pr / (1.0 + Pr);
+    const double dlnk0dT = f.beta0 * invT + f.EaR0 * invT2;
+    const double dlogPrdT = log10e * (dlnk0dT - dlnkfdT);
+    dlogfPrdT = dlogPrdT / (1.0 + Pr);
+    if (!f.lindemann) {
+      const double logPr = log10(Pr);
+      const double Fcent1 = f.j1 ? (1. - f.a) * exp(-T / f.T3) : 0.;
+      const double Fcent2 = f.j2 ? f.a * exp(-T / f.T1) : 0.;
+      const double Fcent3 = (f.ntroe == 4) ? exp(-f.T2 * invT) : 0.;
+      const double Fcent = Fcent1 + Fcent2 + Fcent3;
+      const double logFcent = log10(Fcent);
+      const double troe_c = -.4 - .67 * logFcent;
+      const double troe_n = .75 - 1.27 * logFcent;
+      const double troePr_den = 1.0 / (troe_n - .14 * (troe_c + logPr));
+      const double troePr = (troe_c + logPr) * troePr_den;
+      const double troe = 1.0 / (1.0 + troePr * troePr);
+      F = exp(M_LN10 * logFcent * troe);
+      double sm = 0.0;
+      if (f.j1) sm += -Fcent1 / f.T3;
+      if (f.j2) sm += -Fcent2 / f.T1;
+      if (f.j3) sm += Fcent3 * f.T2 * invT2;
+      const double dlogFcentdT = log10e / Fcent * (sm);
+      const double dlogFdcn_fac = 2.0 * logFcent * troe * troe * troePr * troePr_den;
+      const double dlogFdc = -troe_n * dlogFdcn_fac * troePr_den;
+      const double dlogFdn = dlogFdcn_fac * troePr;
+      dlogFdlogPr = dlogFdc;
+      dlogFdT = dlogFcentdT * (troe - 0.67 * dlogFdc - 1.27 * dlogFdn) + dlogFdlogPr * dlogPrdT;
+    }
+  }
+  double q, q_nocor = 0.0, Corr = 1.0, dqdT, k_r = 0.0;
+  if (!rev) {
+    if (!has_alpha) {
+      q = k_f * phi_f;
+    } else {
+      q_nocor = k_f * phi_f;
+      if (falloff) {
+        Corr = fPr * F;
+        q = Corr * q_nocor;
+      } else {
+        q = alpha * q_nocor;
+      }
+    }
+    if (falloff) {
+      dqdT = Corr * dlnkfdT * k_f * phi_f + ln10 * (dlogfPrdT + dlogFdT) * q;
+    } else if (has_alpha) {
+      dqdT = alpha * dlnkfdT * k_f * phi_f;
+    } else {
+      dqdT = dlnkfdT * k_f * phi_f;
+    }
+  } else {
+    const double phi_r = slots_product(p.rsp, sc);
+    double arg = 0.0;
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+      if (p.kcc[j]) arg += (double)p.kcc[j] * g[p.kcs[j]];
+    const double Kc = refc_pow(-p.kcpow, refC, refCinv) * exp(arg);
+    k_r = k_f / Kc;
+    const double hsum_r = slots_hsum(p.fsp, hrt);
+    const double hsum_p = slots_hsum(p.rsp, hrt);
+    const double snk = p.sum_nuk;
+    double inner = -(hsum_r) + (hsum_p);
+    if (snk > 0) {
+      inner -= snk;
+    } else if (snk < 0) {
+      inner += -snk;
+    }
+    const double dlnKcdT = invT * (inner);
+    const double dkrdT = (dlnkfdT - dlnKcdT) * k_r;
+    if (!has_alpha) {
+      q = k_f * phi_f - k_r * phi_r;
+    } else {
+      q_nocor = k_f * phi_f - k_r * phi_r;
+      if (falloff) {
+        Corr = fPr * F;
+        q = Corr * q_nocor;
+      } else {
+        q = alpha * q_nocor;
+      }
+    }
+    if (falloff) {
+      dqdT = Corr * (dlnkfdT * k_f * phi_f - dkrdT * phi_r) + ln10 * (dlogfPrdT + dlogFdT) * q;
+    } else if (has_alpha) {
+      dqdT = alpha * (dlnkfdT * k_f * phi_f - dkrdT * phi_r);
+    } else {
+      dqdT = (dlnkfdT * k_f * phi_f - dkrdT * phi_r);
+    }
+  }
+  if (falloff) {
+    k_f *= Corr;
+    if (rev) k_r *= Corr;
+  } else if (has_alpha) {
+    k_f *= alpha;
+    if (rev) k_r *= alpha;
+  }
+  RxJac o;
+  o.q = q;
+  o.dqdT = dqdT;
+  o.kf = k_f;
+  o.kr = k_r;
+  o.fac = falloff ? q / alpha * (1.0 / (Pr + 1.0) + dlogFdlogPr) : q_nocor;
+  return o;
+}
+
+// Warp-cooperative analytical Jacobian over the packed records, in three
+// passes: (1) lanes over reactions compute each reaction's factors (the
+// exp/log work) into jx and qd; (2) lanes over species gather wdot and the
+// d/dT row in reaction order; (3) the reactions are walked in order while
+// lane l updates columns l, l+TEAM, ... -- the same accumulation order into
+// each J entry as ajacobian(), including the reuse of a stale dq/dc value
+// for a zero-efficiency species without a rate term in the consP == 0 form.
+template <int TEAM, int PER>
+__device__ void ajacobian_packed(
+  const Team<TEAM>& tm, const DevMech& M, double* J, const double* sc, double T, int consP, RateScratch& rs,
+  double* wdot, double* hrt, double* crt, double* dcrt, double* ehrt)
+{
+  const int N = M.nsp, n = N + 1, R = M.nrxn;
+  for (int i = tm.lane; i < n * n; i += TEAM) J[i] = 0.0;
+  const double invT = 1.0 / T;
+  const double invT2 = invT * invT;
+  const double logT = log(T);
+  const double refC = 101325 / 8.31446 / T;
+  const double refCinv = 1.0 / refC;
+  double mix = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) {
+    mix += sc[s];
+    rs.g[s] = g_RT(M, s, T, invT, logT);
+    hrt[s] = h_RT(M, s, T, invT);
+  }
+  if (tm.lane == 0) {
+    rs.g[N] = 0.0;
+    hrt[N] = 0.0;
+  }
+  const double mixture = tm.sum(mix);
+  tm.sync();
+  // (1) per-reaction factors
+  double* jx = rs.jx;
+  for (int r = tm.lane; r < R; r += TEAM) {
+    const RxPack p = load_rx(M, r);
+    const RxJac f = rx_jac_packed(M, p, T, invT, invT2, logT, refC, refCinv, mixture, sc, rs.g, hrt);
+    rs.qd[r] = f.q;
+    jx[4 * r + 0] = f.kf;
+    jx[4 * r + 1] = f.kr;
+    jx[4 * r + 2] = f.fac;
+    jx[4 * r + 3] = f.dqdT;
+  }
+  tm.sync();
+  // (2) wdot and the d/dT row, reaction order per species
+  for (int s = tm.lane; s < N; s += TEAM) {
+    double w = 0.0, d = 0.0;
+    const int g1 = __ldg(M.jg_off + s + 1);
+    for (int gi = __ldg(M.jg_off + s); gi < g1; gi++) {
+      const int r = __ldg(M.jg_rx + gi);
+      const double nu = __ldg(M.jg_c + gi);
+      w += nu * rs.qd[r];
+      d += nu * jx[4 * r + 3];
+    }
+    wdot[s] = w;
+    J[N * n + s] = d;
+  }
+  // (3) species columns, reactions in order
+  double dq[PER];
+#pragma unroll
+  for (int q = 0; q < PER; q++) dq[q] = 0.0;
+  for (int r = 0; r < R; r++) {
+    const RxPack p = load_rx(M, r);
+    const bool falloff = (p.fo != 255);
+    const bool has_alpha = (p.kind == PPB_RX_THIRD) || falloff;
+    const bool rev = p.rev != 0;
+    const double k_f = jx[4 * r + 0];
+    const double k_r = jx[4 * r + 1];
+    const double fac = jx[4 * r + 2];
+    uint4 em = make_uint4(0u, 0u, 0u, 0u);
+    if (has_alpha) em = __ldg(reinterpret_cast<const uint4*>(M.effmask) + r);
+    const double* ed = M.effd + (size_t)p.aslot * N;
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+      const int k = tm.lane + q * TEAM;
+      if (k >= N) break;
+      const bool inr = slots_has(p.fsp, k);
+      const bool inp = rev && slots_has(p.rsp, k);
+      double d = 0.0;
+      bool apply = false;
+      if (has_alpha) {
+        const unsigned word = (k >> 5) == 0 ? em.x : (k >> 5) == 1 ? em.y : (k >> 5) == 2 ? em.z : em.w;
+        const bool listed = (word >> (k & 31)) & 1u;
+        if (consP == 1) {
+          if (listed) {
+            d = (__ldg(ed + k) - 1) * fac;
+            apply = true;
+          }
+          if (inr) {
+            d += k_f * slots_dproduct(p.fsp, sc, k);
+            apply = true;
+          }
+          if (inp) {
+            d -= k_r * slots_dproduct(p.rsp, sc, k);
+            apply = true;
+          }
+        } else {
+          const double e = listed ? __ldg(ed + k) : 1.0;
+          if (!(e == 0.0 && !inr && !inp)) {
+            if (e == 0.0) {
+              d = 0.0;
+              if (inr) d = k_f * slots_dproduct(p.fsp, sc, k);
+              if (inp) d = (inr ? d : 0.0) - k_r * slots_dproduct(p.rsp, sc, k);
+            } else {
+              d = (e == 1.0) ? fac : e * fac;
+              if (inr) d += k_f * slots_dproduct(p.fsp, sc, k);
+              if (inp) d -= k_r * slots_dproduct(p.rsp, sc, k);
+            }
+            dq[q] = d;
+          }
+          d = dq[q];
+          apply = true;
+        }
+      } else {
+        if (inr) d += k_f * slots_dproduct(p.fsp, sc, k);
+        if (inp) d -= k_r * slots_dproduct(p.rsp, sc, k);
+        apply = inr || inp;
+      }
+      if (apply) {
+        for (int j = 0; j < p.njn; j++) {
+          const double nu = (double)p.jnc[j];
+          if (nu != 0) J[k * n + p.jns[j]] += nu * d;
+        }
+      }
+    }
+  }
+  tm.sync();
+  ajacobian_trow<TEAM>(tm, M, J, sc, T, consP, wdot, hrt, crt, dcrt, ehrt);
+}
+
 // The reference's analytical Jacobian (jacobian.py:12-283, :546-1305), SI,
 // column-major J[k*(N+1)+m] = d wdot_m / d sc_k with the temperature row and
 // column.  Reactions are visited in order by the whole team; lane l owns
@@ -403,6 +898,12 @@ __device__ void ajacobian(
   const Team<TEAM>& tm, const DevMech& M, double* J, const double* sc, double T, int consP, RateScratch& rs,
   double* wdot, double* hrt, double* crt, double* dcrt, double* ehrt)
 {
+  if constexpr (TEAM > 1) {
+    if (rs.jx) {
+      ajacobian_packed<TEAM, PER>(tm, M, J, sc, T, consP, rs, wdot, hrt, crt, dcrt, ehrt);
+      return;
+    }
+  }
   const int N = M.nsp, n = N + 1;
   for (int i = tm.lane; i < n * n; i += TEAM) J[i] = 0.0;
   const double invT = 1.0 / T;
@@ -645,36 +1146,7 @@ __device__ void ajacobian(
     }
   }
   tm.sync();
-  // temperature row and column (jacobian.py:203-281)
-  double a_cmix = 0.0, a_ehmix = 0.0, a_dcmix = 0.0, a_dehmix = 0.0;
-  for (int s = tm.lane; s < N; s += TEAM) {
-    const double cr = consP ? cp_R(M, s, T) : cv_R(M, s, T);
-    const double dc = dcvpRdT(M, s, T);
-    const double eh = consP ? hrt[s] : u_RT(M, s, T, invT);
-    crt[s] = cr;
-    dcrt[s] = dc;
-    ehrt[s] = eh;
-    a_cmix += cr * sc[s];
-    a_dcmix += dc * sc[s];
-    a_ehmix += eh * wdot[s];
-    a_dehmix += invT * (cr - eh) * wdot[s] + eh * J[N * n + s];
-  }
-  const double cmix = tm.sum(a_cmix);
-  const double dcmixdT = tm.sum(a_dcmix);
-  const double ehmix = tm.sum(a_ehmix);
-  const double dehmixdT = tm.sum(a_dehmix);
-  tm.sync();
-  const double cmixinv = 1.0 / cmix;
-  const double tmp1 = ehmix * cmixinv;
-  const double tmp3 = cmixinv * T;
-  const double tmp2 = tmp1 * tmp3;
-  for (int k = tm.lane; k < N; k += TEAM) {
-    double dehmixdc = 0.0;
-    for (int m = 0; m < N; ++m) dehmixdc += ehrt[m] * J[k * n + m];
-    J[k * n + N] = tmp2 * crt[k] - tmp3 * dehmixdc;
-  }
-  if (tm.lane == 0) J[N * n + N] = -tmp1 + tmp2 * dcmixdT - tmp3 * dehmixdT;
-  tm.sync();
+  ajacobian_trow<TEAM>(tm, M, J, sc, T, consP, wdot, hrt, crt, dcrt, ehrt);
 }
 
 } // namespace ppb

@@ -4,12 +4,25 @@
 
 namespace ppb {
 // ------------------------------------------------------------ workspace
+// Newton-matrix region: the n x n factor, or the 4 doubles per reaction of
+// the warp-cooperative Jacobian evaluation, which uses it while the matrix is
+// not live, whichever is larger.
+template <typename LT>
+__host__ __device__ inline size_t a_region_bytes(int N, int R)
+{
+  const size_t n = N + 1;
+  size_t a = n * n * sizeof(LT);
+  const size_t jx = 32 * (size_t)R;
+  if (jx > a) a = jx;
+  return (a + 15) & ~size_t(15);
+}
+
 template <typename LT>
 __host__ __device__ inline size_t team_bytes(int N, int R)
 {
   const int n = N + 1;
   size_t d = (size_t)n * n + 22 * (size_t)n + (size_t)R;
-  size_t b = d * 8 + (size_t)n * n * sizeof(LT) + 4 * (size_t)n;
+  size_t b = d * 8 + a_region_bytes<LT>(N, R) + 4 * (size_t)n;
   return (b + 15) & ~size_t(15);
 }
 
@@ -42,15 +55,16 @@ __device__ inline void carve(Work<LT>& w, char* base, int N, int R)
   w.h3 = p; p += n;
   w.qd = p; p += R;
   w.A = (LT*)p;
-  w.piv = (int*)((char*)p + (size_t)n * n * sizeof(LT));
+  w.piv = (int*)((char*)p + a_region_bytes<LT>(N, R));
 }
 
 
 // team-shared scratch for the pointwise kernels: per cell
-//   sc[N], g[N], wdot[N], h[5][N], qd[R], J[(N+1)^2]
+//   sc[N+1], g[N+1], wdot[N+1], h[5][N+1], qd[R], then for the Jacobian
+//   jx[4R], J[(N+1)^2]
 __host__ __device__ inline size_t point_doubles(int N, int R, bool jac)
 {
   const int n = N + 1;
-  return (size_t)8 * n + R + (jac ? (size_t)n * n : 0);
+  return (size_t)8 * n + R + (jac ? 4 * (size_t)R + (size_t)n * n : 0);
 }
 } // namespace ppb
