@@ -314,6 +314,8 @@ def our_arm(args):
         y_plain = yp.cpu().numpy()
         dT_plain = float(np.max(np.abs(y_plain[:, N] - y_gpu[sub, N]) / y_gpu[sub, N]))
         rp.close()
+        if not args.no_adjoint:
+            out["adjoint"] = adjoint_measure(dev, args.adjoint_cells)
         peak = probe_fp64_peak()
         flops = algorithmic_flops(stats, N + 1)
         out.update(plain_value=plain_value, dT_plain=dT_plain, fp64_peak_gflops=peak, flops=flops)
@@ -368,6 +370,7 @@ def our_arm(args):
             "tuned_vs_plain": {"plain_value": out["plain_value"], "ratio": value / ws / out["plain_value"],
                                "plain_sample": "every 8th cell, one react", "max_rel_T_tuned_vs_plain": out["dT_plain"]},
             "accuracy_vs_fp64_oracle": acc,
+            "adjoint": out.get("adjoint"),
             "cell_failures": int(np.sum(status < 0)),
             "per_cell_mean": dict(zip(["steps", "rhs", "jac", "lu", "newton", "err_fail", "conv_fail"],
                                       [round(float(v), 3) for v in stats.mean(axis=0)])),
@@ -378,6 +381,61 @@ def our_arm(args):
     if pg:
         pg.destroy_process_group()
     return 0
+
+
+def adjoint_measure(dev, ncells):
+    """Adjoint workload: forward react() and the discrete adjoint of the loss
+    sum(w_T T + w_OH Y_OH) on drm19 h/c_p reactors over 5e-4 s; device time
+    of each (CUDA events) and their ratio."""
+    import torch
+
+    from pelephysics_b200 import adjoint as adj
+    from pelephysics_b200 import workloads as wl
+    from pelephysics_b200.reactor import Reactor
+
+    cells = wl.drm19_adjoint(ncells, device=dev)
+    n = cells.rY.shape[0]
+    t_end = cells.dt
+    ioh = [s.upper() for s in wl._lib.species_names(MECH)].index("OH")
+    g = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    y0, s, x0, xs = g(cells.rY), g(cells.rYsrc), g(cells.rX), g(cells.rX_src)
+    r = Reactor(MECH)
+    r.init(2, n, engine=1, **OPTS)
+    # warm-up on a few cells (allocations, graph capture)
+    yw, xw = y0[:256].clone(), x0[:256].clone()
+    r.react(yw, s[:256].contiguous(), xw, xs[:256].contiguous(), t_end)
+    r.adjoint(y0[:256].contiguous(), s[:256].contiguous(), x0[:256].contiguous(), xs[:256].contiguous(), t_end,
+              torch.zeros_like(y0[:256]))
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    y, x = y0.clone(), x0.clone()
+    a.record()
+    r.react(y, s, x, xs, t_end)
+    b.record()
+    torch.cuda.synchronize()
+    t_fwd = a.elapsed_time(b) / 1e3
+    fwd_stats = r.cell_stats(n)
+    w = g(cells.meta["w"])
+    L, lam = adj.loss_T_OH(y, ioh, w[0], w[1])
+    a.record()
+    y_adj, lam_y0, lam_e, grad = r.adjoint(y0, s, x0, xs, t_end, lam.contiguous())
+    b.record()
+    torch.cuda.synchronize()
+    t_adj = a.elapsed_time(b) / 1e3
+    st, _ = r.cell_status(n)
+    R = r.nrxn
+    gr = grad.cpu().numpy()
+    dT = float(((y_adj[:, -1] - y[:, -1]).abs() / y[:, -1]).max())
+    r.close()
+    return {"workload": f"drm19 {n} h/cp reactors, T 1100+500U, phi 0.5+1.5U, 1 atm, t_end 5e-4 s, "
+                        "rtol=atol=1e-10; L = sum(w_T T + w_OH Y_OH), w ~ N(0,1) seed 4",
+            "cells": n, "forward_ms": 1e3 * t_fwd, "adjoint_ms": 1e3 * t_adj, "ratio": t_adj / t_fwd,
+            "target_ratio": 5.0, "checkpoint_interval": 16, "loss": float(L),
+            "grad_norm": {"lnA": float(np.linalg.norm(gr[:R])), "beta": float(np.linalg.norm(gr[R:2 * R])),
+                          "EaR": float(np.linalg.norm(gr[2 * R:])),
+                          "y0": float(lam_y0.norm()), "rhoe": float(lam_e.norm())},
+            "failed_cells": int(np.sum(st < 0)), "max_rel_T_adjoint_forward_vs_react": dT,
+            "mean_steps": float(fwd_stats[:, 0].mean())}
 
 
 def flops_probe():
@@ -495,6 +553,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-workload measurement")
+    ap.add_argument("--adjoint-cells", type=int, default=65536)
     ap.add_argument("--edge", type=int, default=64, help="field edge (profiling runs use a smaller box)")
     ap.add_argument("--phase-probe", action="store_true",
                     help="per-phase cycle counters of one react (profiling build, PPB_LIB)")

@@ -60,6 +60,8 @@ typedef struct ppb_options {
   int refine_sweeps;        /* refinement sweeps with lu_fp32, 1 */
   int warps_per_block;      /* tuned engine block size in warps, 0 = auto */
   int use_graph;            /* replay react() as a captured CUDA graph, 1 */
+  int adjoint_checkpoint_interval; /* accepted BDF steps between adjoint checkpoints, 16 */
+  int adjoint_memory_mb;    /* device memory for adjoint checkpoints and tapes, 8192 */
 } ppb_options;
 
 /* An amrex::Array4<Real>-compatible view: element (i,j,k,n) lives at
@@ -199,6 +201,49 @@ int ppb_pyt2re(const char* mechanism, int eh, const double* P, const double* T, 
 int ppb_react_flat_device_noalloc(const char* mechanism, const char* integrator, int reactor_type,
                                   const ppb_options* opt, double* rY, double* rYsrc, double* rX, double* rX_src,
                                   double dt_react, int ncells, void* stream, int* nfailed);
+
+/* ---- Differentiation (no counterpart in the reference; the ReactorBase
+ * interface has no derivative entry points).
+ *
+ * Parameters are per reaction r: ln A_r, beta_r and Ea_r/R (K) of the
+ * forward rate constant k = A T^beta exp(-(Ea/R)/T) as the mechanism tables
+ * hold it (A in SI mol-m^3-s units; for fall-off reactions the high-pressure
+ * limit).  Gradient vectors are [3][R]: d/d ln A, d/d beta, d/d (Ea/R).
+ * dL/dEa in the mechanism's energy unit is dL/d(Ea/R) / R in that unit. */
+
+/* Arrhenius parameters of the reactor's mechanism (HOST arrays of R). */
+int ppb_get_arrhenius(ppb_reactor* r, double* A, double* beta, double* EaR);
+/* Replace them for this reactor (its react() and adjoint calls use a
+ * private copy of the mechanism tables from then on). */
+int ppb_set_arrhenius(ppb_reactor* r, const double* A, const double* beta, const double* EaR);
+
+/* Discrete adjoint of ppb_react_flat over dt_react for the BDF integrator
+ * ("ReactorCvode"), tuned engine, on DEVICE arrays (YCOrder, as
+ * ppb_react_flat_device; rX is not updated).  Given lam_y = dL/dy(dt) per
+ * cell ([ncells][N+1], y = rhoY_k and the T slot as integrated), it returns
+ * y(dt) in y_out, dL/dy0 in lam_y0 ([ncells][N+1]), dL/drX (the energy
+ * rhoe or rhoh) in lam_e ([ncells], may be NULL) and dL/dp summed over the
+ * cells in grad_params ([3R], may be NULL).  The step sizes and orders are
+ * those of the forward integration (frozen); the forward states are
+ * recomputed from checkpoints every opt.adjoint_checkpoint_interval accepted
+ * steps.  Per-cell status / counters: ppb_get_cell_status / _stats. */
+int ppb_adjoint_flat_device(ppb_reactor* r, const double* rY0, const double* rYsrc, const double* rX,
+                            const double* rX_src, double dt_react, int ncells, const double* lam_y, double* y_out,
+                            double* lam_y0, double* lam_e, double* grad_params, void* stream);
+/* Tangent-linear model of the same integration: the derivative of y(dt) in
+ * the direction (dy0 [ncells][N+1], drX [ncells], dparams [3R]); any
+ * direction pointer may be NULL (zero). */
+int ppb_tangent_flat_device(ppb_reactor* r, const double* rY0, const double* rYsrc, const double* rX,
+                            const double* rX_src, double dt_react, int ncells, const double* dy0, const double* drX,
+                            const double* dparams, double* y_out, double* dy_out, void* stream);
+/* Pointwise exact derivatives of the reactor right-hand side (fKernelSpec,
+ * with T from the energy constraint) on DEVICE arrays: f, df/dy
+ * ([ncells][(N+1)^2], column-major: entry j*(N+1)+i = d f_i / d y_j),
+ * df/drX, and for weights v ([ncells][N+1]) v^T df/dy, v^T df/drX and
+ * v^T df/dp ([ncells][3R]).  Any output may be NULL. */
+int ppb_rhs_exact(const char* mechanism, int reactor_type, double t, const double* y, const double* rhoe,
+                  const double* rhoesrc, const double* src, const double* v, double* f, double* dfdy, double* dfde,
+                  double* vjp_y, double* vjp_e, double* vjp_p, int ncells, void* stream);
 
 #ifdef __cplusplus
 }

@@ -98,6 +98,18 @@ int ppo_react_flat(
   double* rY, const double* rYsrc, double* rX, const double* rX_src, double dt,
   int ncells, int nthreads, long* nfe_out, int* status_out);
 
+// Same over explicit mechanism tables (use_ref_kernels must be 0).
+int ppo_react_flat_tables(
+  const PPBMechTables* M, int reactor_type, const PPOOptions* opt, int method,
+  double* rY, const double* rYsrc, double* rX, const double* rX_src, double dt,
+  int ncells, int nthreads, long* nfe_out, int* status_out);
+
+// A copy of `name`'s tables with the forward Arrhenius parameters replaced
+// (A in the tables' SI units, beta, Ea/R in K; arrays of R).  Free with
+// ppo_mech_free.  Used for finite-difference derivatives.
+PPBMechTables* ppo_mech_with_arrhenius(const char* name, const double* A, const double* beta, const double* EaR);
+void ppo_mech_free(PPBMechTables* M);
+
 // Select the reference kernels library (oracle/_ref/libref_<mech>.so) used
 // when opt->use_ref_kernels is set.  Returns 0 when loaded.
 int ppo_load_ref(const char* mech, const char* path);

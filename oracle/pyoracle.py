@@ -104,6 +104,11 @@ def lib():
                                     C.c_double, C.c_double]
         L.ppo_react_flat.argtypes = [C.c_char_p, C.c_int, C.POINTER(Options), C.c_int, _DP, _DP,
                                      _DP, _DP, C.c_double, C.c_int, C.c_int, _LP, _IP]
+        L.ppo_react_flat_tables.argtypes = [C.c_void_p, C.c_int, C.POINTER(Options), C.c_int, _DP, _DP,
+                                            _DP, _DP, C.c_double, C.c_int, C.c_int, _LP, _IP]
+        L.ppo_mech_with_arrhenius.argtypes = [C.c_char_p, _DP, _DP, _DP]
+        L.ppo_mech_with_arrhenius.restype = C.c_void_p
+        L.ppo_mech_free.argtypes = [C.c_void_p]
         L.ppo_load_ref.argtypes = [C.c_char_p, C.c_char_p]
         L.ppo_species_name.argtypes = [C.c_char_p, C.c_int]
         L.ppo_species_name.restype = C.c_char_p
@@ -279,6 +284,49 @@ def react_flat(mech, reactor_type, rY, rYsrc, rX, rX_src, dt, method=0, nthreads
     flag = lib().ppo_react_flat(mech.encode(), reactor_type, C.byref(o), method, _p(rY), _p(rYsrc),
                                 _p(rX), _p(rX_src), float(dt), ncells, nthreads,
                                 nfe.ctypes.data_as(_LP), st.ctypes.data_as(_IP))
+    return flag, nfe, st
+
+
+class _MechHead(C.Structure):
+    """Leading fields of PPBMechTables (mech_tables.h), up to rx_EaR."""
+
+    _fields_ = [("name", C.c_char_p), ("nsp", C.c_int), ("nrxn", C.c_int), ("species", C.c_void_p)] + [
+        (f, C.c_void_p) for f in ("mw", "imw", "tmid", "th_cv", "th_cp", "th_dcp", "th_u", "th_h", "th_g",
+                                  "rx_orig", "rx_kind", "rx_rev")
+    ] + [("rx_A", _DP), ("rx_beta", _DP), ("rx_EaR", _DP)]
+
+
+def arrhenius(mech):
+    """The mechanism tables' forward Arrhenius parameters (A SI, beta, Ea/R K)."""
+    M = Mech(mech).M
+    t = C.cast(C.c_void_p(M), C.POINTER(_MechHead)).contents
+    R = t.nrxn
+    A = np.ctypeslib.as_array(t.rx_A, shape=(R,)).copy()
+    b = np.ctypeslib.as_array(t.rx_beta, shape=(R,)).copy()
+    e = np.ctypeslib.as_array(t.rx_EaR, shape=(R,)).copy()
+    return A, b, e
+
+
+def react_flat_arrhenius(mech, A, beta, EaR, reactor_type, rY, rYsrc, rX, rX_src, dt, nthreads=0, **kw):
+    """react_flat (BDF, table-driven kernels) with replaced Arrhenius parameters."""
+    kw["use_ref_kernels"] = 0
+    o = options(**kw)
+    A = np.ascontiguousarray(A, float)
+    beta = np.ascontiguousarray(beta, float)
+    EaR = np.ascontiguousarray(EaR, float)
+    L = lib()
+    M = L.ppo_mech_with_arrhenius(mech.encode(), _p(A), _p(beta), _p(EaR))
+    if not M:
+        raise RuntimeError("ppo_mech_with_arrhenius failed")
+    try:
+        ncells = rX.shape[0]
+        nfe = np.zeros(ncells, dtype=np.int64)
+        st = np.zeros(ncells, dtype=np.int32)
+        flag = L.ppo_react_flat_tables(M, reactor_type, C.byref(o), 0, _p(rY), _p(rYsrc), _p(rX), _p(rX_src),
+                                       float(dt), ncells, nthreads, nfe.ctypes.data_as(_LP),
+                                       st.ctypes.data_as(_IP))
+    finally:
+        L.ppo_mech_free(M)
     return flag, nfe, st
 
 

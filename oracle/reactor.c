@@ -886,6 +886,46 @@ int ppo_react_flat(
 {
   const PPBMechTables* M = ppo_mech(mech);
   if (!M) return -100;
+  return ppo_react_flat_tables(M, reactor_type, opt, method, rY, rYsrc, rX, rX_src, dt, ncells, nthreads,
+                               nfe_out, status_out);
+}
+
+PPBMechTables* ppo_mech_with_arrhenius(const char* name, const double* A, const double* beta, const double* EaR)
+{
+  const PPBMechTables* M = ppo_mech(name);
+  if (!M) return 0;
+  PPBMechTables* C = (PPBMechTables*)malloc(sizeof(PPBMechTables));
+  double* buf = (double*)malloc(sizeof(double) * 3 * (size_t)M->nrxn);
+  if (!C || !buf) {
+    free(C);
+    free(buf);
+    return 0;
+  }
+  *C = *M;
+  for (int r = 0; r < M->nrxn; r++) {
+    buf[r] = A[r];
+    buf[M->nrxn + r] = beta[r];
+    buf[2 * M->nrxn + r] = EaR[r];
+  }
+  C->rx_A = buf;
+  C->rx_beta = buf + M->nrxn;
+  C->rx_EaR = buf + 2 * M->nrxn;
+  return C;
+}
+
+void ppo_mech_free(PPBMechTables* M)
+{
+  if (!M) return;
+  free((void*)M->rx_A);
+  free(M);
+}
+
+int ppo_react_flat_tables(
+  const PPBMechTables* M, int reactor_type, const PPOOptions* opt, int method,
+  double* rY, const double* rYsrc, double* rX, const double* rX_src, double dt,
+  int ncells, int nthreads, long* nfe_out, int* status_out)
+{
+  if (!M) return -100;
   const int N = M->nsp;
   int first_err = 0;
 #ifdef _OPENMP

@@ -41,6 +41,8 @@ class Options(C.Structure):
         ("refine_sweeps", C.c_int),
         ("warps_per_block", C.c_int),
         ("use_graph", C.c_int),
+        ("adjoint_checkpoint_interval", C.c_int),
+        ("adjoint_memory_mb", C.c_int),
     ]
 
 
@@ -110,6 +112,12 @@ def lib():
                                                 C.c_double, C.c_int, vp, ip]
     L.ppb_molecular_weights.argtypes = [C.c_char_p, dpp]
     L.ppb_pyt2re.argtypes = [C.c_char_p, C.c_int, dp, dp, dp, dp, dp, C.c_int, vp]
+    L.ppb_get_arrhenius.argtypes = [vp, dpp, dpp, dpp]
+    L.ppb_set_arrhenius.argtypes = [vp, dpp, dpp, dpp]
+    L.ppb_adjoint_flat_device.argtypes = [vp, dp, dp, dp, dp, C.c_double, C.c_int, dp, dp, dp, dp, dp, vp]
+    L.ppb_tangent_flat_device.argtypes = [vp, dp, dp, dp, dp, C.c_double, C.c_int, dp, dp, dp, dp, dp, vp]
+    L.ppb_rhs_exact.argtypes = [C.c_char_p, C.c_int, C.c_double, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp,
+                                C.c_int, vp]
     _lib = L
     return L
 

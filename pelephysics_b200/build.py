@@ -41,6 +41,8 @@ def _units():
     ]
     for ns in SPECIES_COUNTS:
         units.append((f"ppb_engine_ns{ns}.o", "ppb_engine_ns.cu", [f"-DPPB_NS={ns}"]))
+    for ns in SPECIES_COUNTS:
+        units.append((f"ppb_adjoint_ns{ns}.o", "ppb_adjoint_ns.cu", [f"-DPPB_NS={ns}"]))
     return units
 
 

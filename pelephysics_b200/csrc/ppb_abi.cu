@@ -7,6 +7,7 @@
 // paths can be replayed as a captured CUDA graph.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -103,7 +104,36 @@ struct ppb_reactor {
   cudaGraphExec_t gexec = nullptr;
   GraphKey gkey{};
   cudaStream_t cap_stream = nullptr;
+  // reactor-private mechanism tables (ppb_set_arrhenius)
+  PPBMechTables own_t{};
+  std::vector<double> own_A, own_beta, own_EaR;
+  DeviceMechanism* own = nullptr;
+  // adjoint scratch (grown on demand)
+  void *adj_cp = nullptr, *adj_tape = nullptr, *adj_ys = nullptr, *adj_gw = nullptr;
+  size_t adj_cp_bytes = 0, adj_tape_bytes = 0, adj_ys_bytes = 0, adj_gw_bytes = 0;
 };
+
+static void free_adjoint_scratch(ppb_reactor* r)
+{
+  cudaFree(r->adj_cp);
+  cudaFree(r->adj_tape);
+  cudaFree(r->adj_ys);
+  cudaFree(r->adj_gw);
+  r->adj_cp = r->adj_tape = r->adj_ys = r->adj_gw = nullptr;
+  r->adj_cp_bytes = r->adj_tape_bytes = r->adj_ys_bytes = r->adj_gw_bytes = 0;
+}
+
+static int grow(void*& p, size_t& cap, size_t bytes)
+{
+  if (p && bytes <= cap) return 0;
+  cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  if (bytes == 0) return 0;
+  PPB_CUDA(cudaMalloc(&p, bytes), "cudaMalloc (adjoint scratch)");
+  cap = bytes;
+  return 0;
+}
 
 static void free_scratch(ppb_reactor* r)
 {
@@ -227,6 +257,8 @@ void ppb_default_options(ppb_options* o)
   o->refine_sweeps = 1;
   o->warps_per_block = 0;
   o->use_graph = 1;
+  o->adjoint_checkpoint_interval = 16;
+  o->adjoint_memory_mb = 8192;
 }
 
 const char* ppb_last_error(void) { return g_err; }
@@ -294,8 +326,13 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
   if (r->opt.engine == PPB_ENGINE_PLAIN && r->opt.lu_fp32)
     return fail(PPB_E_ARG, "the plain engine is FP64 only");
   r->reactor_type = reactor_type;
-  int e = device_mechanism(r->t, &r->dm);
-  if (e) return e;
+  int e = 0;
+  if (r->own) {
+    r->dm = r->own;
+  } else {
+    e = device_mechanism(r->t, &r->dm);
+    if (e) return e;
+  }
   if (ncells > 0) {
     e = ensure_scratch(r, ncells);
     if (e) return e;
@@ -328,6 +365,7 @@ int ppb_close(ppb_reactor* r)
   r->cap_stream = nullptr;
   cudaFree(r->atolv);
   r->atolv = nullptr;
+  free_adjoint_scratch(r);
   r->inited = false;
   return 0;
 }
@@ -336,6 +374,10 @@ void ppb_destroy(ppb_reactor* r)
 {
   if (!r) return;
   ppb_close(r);
+  if (r->own) {
+    free_mechanism(r->own);
+    delete r->own;
+  }
   delete r;
 }
 
@@ -597,6 +639,192 @@ int ppb_probe_fp64_peak(double* gflops, void* stream)
 {
   if (!gflops) return fail(PPB_E_ARG, "ppb_probe_fp64_peak: null output");
   return cuda_fail(probe_fp64_peak(gflops, (cudaStream_t)stream), "probe_fp64_peak");
+}
+
+int ppb_get_arrhenius(ppb_reactor* r, double* A, double* beta, double* EaR)
+{
+  if (!r || !A || !beta || !EaR) return fail(PPB_E_ARG, "ppb_get_arrhenius: null argument");
+  const PPBMechTables* t = r->own ? &r->own_t : r->t;
+  for (int k = 0; k < t->nrxn; k++) {
+    A[k] = t->rx_A[k];
+    beta[k] = t->rx_beta[k];
+    EaR[k] = t->rx_EaR[k];
+  }
+  return 0;
+}
+
+int ppb_set_arrhenius(ppb_reactor* r, const double* A, const double* beta, const double* EaR)
+{
+  if (!r || !A || !beta || !EaR) return fail(PPB_E_ARG, "ppb_set_arrhenius: null argument");
+  const int R = r->t->nrxn;
+  r->own_A.assign(A, A + R);
+  r->own_beta.assign(beta, beta + R);
+  r->own_EaR.assign(EaR, EaR + R);
+  r->own_t = *r->t;
+  r->own_t.rx_A = r->own_A.data();
+  r->own_t.rx_beta = r->own_beta.data();
+  r->own_t.rx_EaR = r->own_EaR.data();
+  auto* m = new DeviceMechanism();
+  const int e = upload_mechanism(&r->own_t, m);
+  if (e) {
+    delete m;
+    return cuda_fail(e, "upload_mechanism");
+  }
+  if (r->own) {
+    free_mechanism(r->own);
+    delete r->own;
+  }
+  r->own = m;
+  if (r->inited) r->dm = m;
+  if (r->gexec) {
+    cudaGraphExecDestroy(r->gexec);
+    r->gexec = nullptr;
+  }
+  return 0;
+}
+
+// Shared set-up and launch of the adjoint (mode ADJ_REVERSE) and tangent
+// (ADJ_TANGENT) integrations.
+static int run_adjoint(ppb_reactor* r, int mode, AdjBatch b, double dt, double* grad, cudaStream_t st)
+{
+  if (!r || !r->inited) return fail(PPB_E_ARG, "adjoint: reactor not initialised");
+  if (r->method != METHOD_BDF)
+    return fail(PPB_E_ARG, "adjoint: only the BDF integrator (ReactorCvode) is differentiated");
+  if (r->opt.engine != PPB_ENGINE_TUNED) return fail(PPB_E_ARG, "adjoint: runs on the tuned engine only");
+  if (b.ncells < 0 || (b.ncells > 0 && (!b.y0 || !b.rhoe))) return fail(PPB_E_ARG, "adjoint: invalid arguments");
+  if (mode == ADJ_REVERSE && b.ncells > 0 && !b.lam_y) return fail(PPB_E_ARG, "adjoint: lam_y is required");
+  if (b.ncells == 0) {
+    if (grad) PPB_CUDA(cudaMemsetAsync(grad, 0, sizeof(double) * 3 * r->t->nrxn, st), "cudaMemsetAsync");
+    return 0;
+  }
+  int e = ensure_scratch(r, b.ncells);
+  if (e) return e;
+  const int N = r->t->nsp, n = N + 1, R = r->t->nrxn;
+  AdjPlan p;
+  e = plan_adjoint(*r->dm, mode, r->opt.lu_fp32, &p);
+  if (e) return cuda_fail(e, "plan_adjoint");
+  const int seg = r->opt.adjoint_checkpoint_interval > 0 ? r->opt.adjoint_checkpoint_interval : 16;
+  AdjLayout L{};
+  L.seg_steps = seg;
+  L.close_rec = 256;
+  L.cap_rec = L.close_rec + 2 * (r->opt.max_err_fails + 10) + 8;
+  L.close_y = 64;
+  L.cap_y = L.close_y + r->opt.max_err_fails + 2;
+  L.cp_stride = p.cp_stride;
+  L.cap_cp = (mode == ADJ_REVERSE) ? r->opt.max_steps / seg + 2 : 0;
+  L.warp_smem = p.warp_smem;
+  const size_t tape_w = (size_t)L.cap_rec * ADJ_TAPE_BYTES;
+  const size_t ys_w = (size_t)L.cap_y * n * 8;
+  const size_t gw_cell = (size_t)3 * R * 8;
+  // cells per launch: the per-cell gradients of one launch stay under 512 MiB
+  const int chunk = (int)std::min<size_t>((size_t)b.ncells, std::max<size_t>(1, (size_t(512) << 20) / gw_cell));
+  const size_t budget = (size_t)(r->opt.adjoint_memory_mb > 0 ? r->opt.adjoint_memory_mb : 8192) << 20;
+  // no more warps than cells, and within the memory budget
+  int blocks = std::min(p.blocks, (chunk + p.wpb - 1) / p.wpb);
+  size_t per_warp = (size_t)L.cap_cp * L.cp_stride + tape_w + ys_w;
+  if ((size_t)blocks * p.wpb * per_warp > budget) {
+    blocks = (int)std::max<size_t>(1, budget / (per_warp * p.wpb));
+    if ((size_t)blocks * p.wpb * per_warp > budget) {
+      const size_t room = budget / p.wpb;
+      if (room <= tape_w + ys_w + 2 * L.cp_stride)
+        return fail(PPB_E_ARG, "adjoint: adjoint_memory_mb too small for one block of checkpoints");
+      L.cap_cp = (int)((room - tape_w - ys_w) / L.cp_stride);
+    }
+  }
+  p.blocks = blocks;
+  const size_t W = (size_t)blocks * p.wpb;
+  if ((e = grow(r->adj_cp, r->adj_cp_bytes, W * L.cap_cp * L.cp_stride)) ||
+      (e = grow(r->adj_tape, r->adj_tape_bytes, W * tape_w)) || (e = grow(r->adj_ys, r->adj_ys_bytes, W * ys_w)) ||
+      (e = grow(r->adj_gw, r->adj_gw_bytes, mode == ADJ_REVERSE ? (size_t)chunk * gw_cell : 0)))
+    return e;
+  L.cp = (char*)r->adj_cp;
+  L.tape = r->adj_tape;
+  L.ys = (double*)r->adj_ys;
+  L.gw = mode == ADJ_REVERSE ? (double*)r->adj_gw : nullptr;
+  b.atolv = r->atolv;
+  b.status = r->status;
+  b.stats = r->stats;
+  const Options o = engine_options(r);
+  for (int c0 = 0; c0 < b.ncells; c0 += chunk) {
+    AdjBatch bc = b;
+    const size_t cn = (size_t)c0 * n, cN = (size_t)c0 * N;
+    bc.ncells = std::min(chunk, b.ncells - c0);
+    bc.y0 = b.y0 + cn;
+    bc.src = b.src ? b.src + cN : nullptr;
+    bc.rhoe = b.rhoe + c0;
+    bc.rhoesrc = b.rhoesrc ? b.rhoesrc + c0 : nullptr;
+    bc.lam_y = b.lam_y ? b.lam_y + cn : nullptr;
+    bc.dy0 = b.dy0 ? b.dy0 + cn : nullptr;
+    bc.dE = b.dE ? b.dE + c0 : nullptr;
+    bc.y_out = b.y_out ? b.y_out + cn : nullptr;
+    bc.lam_y0 = b.lam_y0 ? b.lam_y0 + cn : nullptr;
+    bc.lam_e = b.lam_e ? b.lam_e + c0 : nullptr;
+    bc.status = b.status + c0;
+    bc.stats = b.stats + (size_t)c0 * 7;
+    e = launch_adjoint(*r->dm, o, mode, r->opt.lu_fp32, p, bc, L, dt, r->queue, grad, c0 > 0 ? 1 : 0, st);
+    if (e) return cuda_fail(e, "launch_adjoint");
+  }
+  r->last_ncells = b.ncells;
+  std::vector<int> stat(b.ncells);
+  PPB_CUDA(cudaMemcpyAsync(stat.data(), r->status, (size_t)b.ncells * 4, cudaMemcpyDeviceToHost, st),
+           "cudaMemcpyAsync");
+  PPB_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  int bad = 0;
+  for (int c = 0; c < b.ncells; c++) bad += stat[c] < 0;
+  if (bad) return fail(PPB_E_INTEGRATE, std::to_string(bad) + " cell(s) failed in the adjoint integration");
+  return 0;
+}
+
+int ppb_adjoint_flat_device(ppb_reactor* r, const double* rY0, const double* rYsrc, const double* rX,
+                            const double* rX_src, double dt_react, int ncells, const double* lam_y, double* y_out,
+                            double* lam_y0, double* lam_e, double* grad_params, void* stream)
+{
+  AdjBatch b{};
+  b.y0 = rY0;
+  b.src = rYsrc;
+  b.rhoe = rX;
+  b.rhoesrc = rX_src;
+  b.lam_y = lam_y;
+  b.y_out = y_out;
+  b.lam_y0 = lam_y0;
+  b.lam_e = lam_e;
+  b.ncells = ncells;
+  return run_adjoint(r, ADJ_REVERSE, b, dt_react, grad_params, (cudaStream_t)stream);
+}
+
+int ppb_tangent_flat_device(ppb_reactor* r, const double* rY0, const double* rYsrc, const double* rX,
+                            const double* rX_src, double dt_react, int ncells, const double* dy0, const double* drX,
+                            const double* dparams, double* y_out, double* dy_out, void* stream)
+{
+  if (!dparams) return fail(PPB_E_ARG, "ppb_tangent_flat_device: dparams is required (zeros for none)");
+  AdjBatch b{};
+  b.y0 = rY0;
+  b.src = rYsrc;
+  b.rhoe = rX;
+  b.rhoesrc = rX_src;
+  b.dy0 = dy0;
+  b.dE = drX;
+  b.dp = dparams;
+  b.y_out = y_out;
+  b.lam_y0 = dy_out;
+  b.ncells = ncells;
+  return run_adjoint(r, ADJ_TANGENT, b, dt_react, nullptr, (cudaStream_t)stream);
+}
+
+int ppb_rhs_exact(const char* mechanism, int reactor_type, double t, const double* y, const double* rhoe,
+                  const double* rhoesrc, const double* src, const double* v, double* f, double* dfdy, double* dfde,
+                  double* vjp_y, double* vjp_e, double* vjp_p, int ncells, void* stream)
+{
+  DeviceMechanism* dm;
+  const PPBMechTables* tab = mechanism ? find_mechanism(mechanism) : nullptr;
+  if (!tab) return fail(PPB_E_MECH, std::string("unknown mechanism ") + (mechanism ? mechanism : "(null)"));
+  int e = device_mechanism(tab, &dm);
+  if (e) return e;
+  if (ncells < 0 || !y || !rhoe || (reactor_type != 1 && reactor_type != 2))
+    return fail(PPB_E_ARG, "ppb_rhs_exact: bad arguments");
+  return cuda_fail(launch_rhs_exact(*dm, reactor_type, t, y, rhoe, rhoesrc, src, v, f, dfdy, dfde, vjp_y, vjp_e,
+                                    vjp_p, ncells, (cudaStream_t)stream),
+                   "rhs_exact");
 }
 
 static int point_mech(const char* mechanism, DeviceMechanism** dm)

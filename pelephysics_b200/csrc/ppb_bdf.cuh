@@ -235,7 +235,15 @@ struct CellIn {
   double rhoe, rhoesrc;
 };
 
-template <int NS, int TEAM, typename LT>
+// Recorder interface of the integrator: every operation that changes the
+// Nordsieck history, with the coefficients it used, in execution order (the
+// discrete adjoint and tangent-linear sweeps replay these).  NoRec records
+// nothing and compiles away.
+struct NoRec {
+  static constexpr bool on = false;
+};
+
+template <int NS, int TEAM, typename LT, typename Rec = NoRec>
 struct Bdf {
   static constexpr int n = NS + 1;
   static constexpr int PER = (NS + TEAM - 1) / TEAM;
@@ -245,6 +253,7 @@ struct Bdf {
   Work<LT>& w;
   CellIn cin;
   BdfScalars s;
+  Rec rec;
 
   __device__ Bdf(const Team<TEAM>& t, const DevMech& m, const Options& op, Work<LT>& wk, CellIn ci)
     : tm(t), M(m), o(op), w(wk), cin(ci)
@@ -337,6 +346,7 @@ struct Bdf {
 
   __device__ void rescale()
   {
+    if constexpr (Rec::on) rec.rescale(tm, s.q, s.eta);
     double factor = s.eta;
     for (int j = 1; j <= s.q; j++) {
       for (int i = tm.lane; i < n; i += TEAM) w.zn[j][i] *= factor;
@@ -597,6 +607,7 @@ struct Bdf {
       for (int j = 2; j <= s.q; j++) w.zn[j][i] += s.l[j] * zL;
     }
     tm.sync();
+    if constexpr (Rec::on) rec.increase(tm, s.q, s.L, s.indx_acor, A1, s.l);
   }
 
   __device__ void decrease_bdf()
@@ -613,6 +624,7 @@ struct Bdf {
     for (int i = tm.lane; i < n; i += TEAM)
       for (int j = 2; j < s.q; j++) w.zn[j][i] -= s.l[j] * w.zn[s.q][i];
     tm.sync();
+    if constexpr (Rec::on) rec.decrease(tm, s.q, s.l);
   }
 
   __device__ void adjust_order(int deltaq)
@@ -670,6 +682,7 @@ struct Bdf {
     f(s.tn, w.zn[0], w.tempv);
     for (int i = tm.lane; i < n; i += TEAM) w.zn[1][i] = s.h * w.tempv[i];
     tm.sync();
+    if constexpr (Rec::on) rec.freset(tm, s.tn, s.h, w.zn[0]);
     return 5;
   }
 
@@ -681,6 +694,10 @@ struct Bdf {
     if ((s.q == 1) && (s.nst > 1)) s.tau[2] = s.tau[1];
     s.tau[1] = s.h;
     const bool save = ((s.qwait - 1) == 1) && (s.q != s.qmax);
+    if constexpr (Rec::on) {
+      rec.predict(tm, s.q);
+      rec.correct(tm, s.q, save, s.tn, s.gamma, s.rl1, s.l, w.zn[0], w.acor);
+    }
     for (int i = tm.lane; i < n; i += TEAM) {
       const double a = w.acor[i];
       for (int j = 0; j <= s.q; j++) w.zn[j][i] += s.l[j] * a;
@@ -750,6 +767,7 @@ struct Bdf {
       s.qprime = s.q + 1;
       for (int i = tm.lane; i < n; i += TEAM) w.zn[s.qmax][i] = w.acor[i];
       tm.sync();
+      if constexpr (Rec::on) rec.saveqmax(tm);
     }
     set_eta();
   }
@@ -797,11 +815,11 @@ struct Bdf {
     return ST_OK;
   }
 
-  // Integrate w.zn[0] (initial y, team-shared) over [0, tout]; result in w.y.
-  __device__ int run(double tout)
+  // Start of an integration of w.zn[0] (initial y, team-shared) towards
+  // tout: history, error weights, initial step (cvInitialSetup, cvHin).
+  __device__ int start(double tout)
   {
     s = BdfScalars{};
-    PPB_TIC(PH_TOTAL);
     s.qmax = o.max_order;
     s.q = 1;
     s.L = 2;
@@ -810,33 +828,56 @@ struct Bdf {
     s.tn = 0.0;
     set_ewt(w.zn[0]);
     f(s.tn, w.zn[0], w.zn[1]);
-    int flag = hin(tout);
+    const int flag = hin(tout);
     if (flag == ST_OK) {
       s.hscale = s.h;
       s.hprime = s.h;
       for (int i = tm.lane; i < n; i += TEAM) w.zn[1][i] *= s.h;
       tm.sync();
-      int nstloc = 0;
-      for (;;) {
-        if (s.nst > 0) set_ewt(w.zn[0]);
-        if (nstloc >= o.max_steps) {
-          flag = ST_TOO_MUCH_WORK;
-          break;
+      if constexpr (Rec::on) rec.init(tm, s.h, w.zn[0]);
+    }
+    return flag;
+  }
+
+  // Step until tout is passed (then interpolate to tout into w.y and set
+  // done) or, with a recorder, until the recorder closes its segment.
+  // nstloc counts the steps of this call to react.
+  __device__ int advance(double tout, int& nstloc, bool& done)
+  {
+    done = false;
+    for (;;) {
+      if (s.nst > 0) set_ewt(w.zn[0]);
+      if (nstloc >= o.max_steps) return ST_TOO_MUCH_WORK;
+      const int flag = step();
+      if (flag != ST_OK) return flag;
+      nstloc++;
+      if ((s.tn - tout) * s.h >= 0.0) {
+        const double sfac = (tout - s.tn) / s.h;
+        for (int i = tm.lane; i < n; i += TEAM) {
+          double v = w.zn[s.q][i];
+          for (int j = s.q - 1; j >= 0; j--) v = w.zn[j][i] + sfac * v;
+          w.y[i] = v;
         }
-        flag = step();
-        if (flag != ST_OK) break;
-        nstloc++;
-        if ((s.tn - tout) * s.h >= 0.0) {
-          const double sfac = (tout - s.tn) / s.h;
-          for (int i = tm.lane; i < n; i += TEAM) {
-            double v = w.zn[s.q][i];
-            for (int j = s.q - 1; j >= 0; j--) v = w.zn[j][i] + sfac * v;
-            w.y[i] = v;
-          }
-          tm.sync();
-          break;
-        }
+        tm.sync();
+        if constexpr (Rec::on) rec.output(tm, s.q, sfac);
+        done = true;
+        return ST_OK;
       }
+      if constexpr (Rec::on) {
+        if (rec.segment_full()) return ST_OK;
+      }
+    }
+  }
+
+  // Integrate w.zn[0] (initial y, team-shared) over [0, tout]; result in w.y.
+  __device__ int run(double tout)
+  {
+    PPB_TIC(PH_TOTAL);
+    int flag = start(tout);
+    if (flag == ST_OK) {
+      int nstloc = 0;
+      bool done = false;
+      flag = advance(tout, nstloc, done);
     }
     if (flag != ST_OK) {
       for (int i = tm.lane; i < n; i += TEAM) w.y[i] = w.zn[0][i];

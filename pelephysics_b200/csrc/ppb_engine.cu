@@ -536,6 +536,65 @@ int launch_production_rate(const DeviceMechanism& m, const double* sc, const dou
   return (int)cudaGetLastError();
 }
 
+#define PPB_ADJ_DECL(NS)                                                                                          \
+  int plan_adjoint_##NS(const DevMech& M, int mode, int lu_fp32, AdjPlan* p);                                      \
+  int launch_adjoint_##NS(const DevMech& M, const Options& o, int mode, int lu_fp32, const AdjPlan& p,             \
+                          const AdjBatch& b, const AdjLayout& L, double dt, int* queue, double* grad,              \
+                          int accumulate, cudaStream_t st);                                                        \
+  int launch_rhs_exact_##NS(const DevMech& M, int rtype, double t, const double* y, const double* rhoe,            \
+                            const double* rhoesrc, const double* src, const double* v, double* f_out,              \
+                            double* J_out, double* fE_out, double* vy_out, double* vE_out, double* vp_out,         \
+                            int ncells, cudaStream_t st);
+PPB_ADJ_DECL(9)
+PPB_ADJ_DECL(21)
+PPB_ADJ_DECL(53)
+PPB_ADJ_DECL(88)
+#undef PPB_ADJ_DECL
+
+int plan_adjoint(const DeviceMechanism& m, int mode, int lu_fp32, AdjPlan* p)
+{
+  const DevMech& M = *m.dm;
+  switch (M.nsp) {
+  case 9: return plan_adjoint_9(M, mode, lu_fp32, p);
+  case 21: return plan_adjoint_21(M, mode, lu_fp32, p);
+  case 53: return plan_adjoint_53(M, mode, lu_fp32, p);
+  case 88: return plan_adjoint_88(M, mode, lu_fp32, p);
+  default: return (int)cudaErrorNotSupported;
+  }
+}
+
+int launch_adjoint(const DeviceMechanism& m, const Options& o, int mode, int lu_fp32, const AdjPlan& p,
+                   const AdjBatch& b, const AdjLayout& L, double dt, int* queue, double* grad, int accumulate,
+                   cudaStream_t st)
+{
+  const DevMech& M = *m.dm;
+  switch (M.nsp) {
+  case 9: return launch_adjoint_9(M, o, mode, lu_fp32, p, b, L, dt, queue, grad, accumulate, st);
+  case 21: return launch_adjoint_21(M, o, mode, lu_fp32, p, b, L, dt, queue, grad, accumulate, st);
+  case 53: return launch_adjoint_53(M, o, mode, lu_fp32, p, b, L, dt, queue, grad, accumulate, st);
+  case 88: return launch_adjoint_88(M, o, mode, lu_fp32, p, b, L, dt, queue, grad, accumulate, st);
+  default: return (int)cudaErrorNotSupported;
+  }
+}
+
+int launch_rhs_exact(const DeviceMechanism& m, int rtype, double t, const double* y, const double* rhoe,
+                     const double* rhoesrc, const double* src, const double* v, double* f_out, double* J_out,
+                     double* fE_out, double* vy_out, double* vE_out, double* vp_out, int ncells, cudaStream_t st)
+{
+  const DevMech& M = *m.dm;
+#define PPB_RX(NS)                                                                                                 \
+  return launch_rhs_exact_##NS(M, rtype, t, y, rhoe, rhoesrc, src, v, f_out, J_out, fE_out, vy_out, vE_out, vp_out, \
+                               ncells, st)
+  switch (M.nsp) {
+  case 9: PPB_RX(9);
+  case 21: PPB_RX(21);
+  case 53: PPB_RX(53);
+  case 88: PPB_RX(88);
+  default: return (int)cudaErrorNotSupported;
+  }
+#undef PPB_RX
+}
+
 int launch_ajacobian(const DeviceMechanism& m, const double* sc, const double* T, int consP, double* J, int ncells,
                      int team, cudaStream_t st)
 {

@@ -108,4 +108,58 @@ int phase_cycles(unsigned long long* out, int reset);
 
 // Bytes of shared memory one team-integrated cell needs.
 size_t team_cell_bytes(const PPBMechTables* t, int lu_fp32);
+
+// ---------------------------------------------------------------- adjoint
+enum AdjMode { ADJ_REVERSE = 0, ADJ_TANGENT = 1 };
+
+// Cells of an adjoint or tangent-linear integration (device memory, YCOrder
+// cell-major: y0 / lam_y / dy0 / y_out / lam_y0 are [ncells][N+1]).
+struct AdjBatch {
+  const double* y0;
+  const double* src;     // [ncells][N] or nullptr
+  const double* rhoe;    // [ncells]
+  const double* rhoesrc; // [ncells] or nullptr
+  const double* atolv;   // typical-value tolerances or nullptr
+  const double* lam_y;   // reverse: dL/dy(t_end)
+  const double* dy0;     // tangent: direction in y0 (or nullptr)
+  const double* dE;      // tangent: direction in rhoe (or nullptr)
+  const double* dp;      // tangent: direction in [ln A | beta | Ea/R] (3R)
+  double* y_out;         // y(t_end)
+  double* lam_y0;        // reverse: dL/dy0; tangent: dy(t_end)
+  double* lam_e;         // reverse: dL/drhoe (or nullptr)
+  int* status;           // [ncells]
+  int* stats;            // [ncells][7] or nullptr
+  int ncells;
+};
+
+// Per-warp global scratch of the adjoint kernel.
+struct AdjLayout {
+  char* cp;          // [warps][cap_cp] checkpoints of cp_stride bytes
+  size_t cp_stride;
+  int cap_cp;
+  void* tape;        // [warps][cap_rec] tape records
+  int cap_rec, close_rec;
+  double* ys;        // [warps][cap_y][N+1]
+  int cap_y, close_y;
+  double* gw;        // [ncells][3R] per-cell parameter gradients
+  int seg_steps;     // accepted steps per checkpoint segment
+  size_t warp_smem;  // shared memory per warp
+};
+
+struct AdjPlan {
+  int wpb = 0, blocks = 0;
+  size_t warp_smem = 0, cp_stride = 0;
+};
+enum : int { ADJ_TAPE_BYTES = 112 };
+
+int plan_adjoint(const DeviceMechanism& m, int mode, int lu_fp32, AdjPlan* p);
+// grad (3R) receives (accumulate = 0) or gains (1) the cells' summed
+// parameter gradient, summed in cell order.
+int launch_adjoint(const DeviceMechanism& m, const Options& o, int mode, int lu_fp32, const AdjPlan& p,
+                   const AdjBatch& b, const AdjLayout& L, double dt, int* queue, double* grad, int accumulate,
+                   cudaStream_t st);
+// Pointwise exact derivatives of the reactor RHS (any output may be null).
+int launch_rhs_exact(const DeviceMechanism& m, int rtype, double t, const double* y, const double* rhoe,
+                     const double* rhoesrc, const double* src, const double* v, double* f_out, double* J_out,
+                     double* fE_out, double* vy_out, double* vE_out, double* vp_out, int ncells, cudaStream_t st);
 } // namespace ppb

@@ -626,6 +626,7 @@ __device__ void ajacobian_trow(
 // order as the reaction loop of ajacobian().
 struct RxJac {
   double q, dqdT, kf, kr, fac;
+  double dlnk; // d ln q / d ln k_f at fixed concentrations and T (k_inf for fall-off)
 };
 
 __device__ __forceinline__ RxJac rx_jac_packed(
@@ -753,6 +754,9 @@ __device__ __forceinline__ RxJac rx_jac_packed(
   o.kf = k_f;
   o.kr = k_r;
   o.fac = falloff ? q / alpha * (1.0 / (Pr + 1.0) + dlogFdlogPr) : q_nocor;
+  // fall-off: Pr = alpha k_0 / k_inf, so d ln(Pr/(1+Pr) F(Pr)) / d ln k_inf
+  // = -1/(1+Pr) - dlog F/dlog Pr
+  o.dlnk = falloff ? Pr / (1.0 + Pr) - dlogFdlogPr : 1.0;
   return o;
 }
 

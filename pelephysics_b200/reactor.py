@@ -97,6 +97,53 @@ class Reactor:
             check(code)
         return cost.value, dt.value, t.value, code
 
+    # ---- differentiation (no counterpart in the reference)
+    def get_arrhenius(self):
+        """Forward Arrhenius parameters (A in SI units, beta, Ea/R in K)."""
+        A, b, e = (np.zeros(self.nrxn) for _ in range(3))
+        dpp = C.POINTER(C.c_double)
+        check(lib().ppb_get_arrhenius(self._h, A.ctypes.data_as(dpp), b.ctypes.data_as(dpp), e.ctypes.data_as(dpp)))
+        return A, b, e
+
+    def set_arrhenius(self, A, beta, EaR):
+        dpp = C.POINTER(C.c_double)
+        A, beta, EaR = (np.ascontiguousarray(x, dtype=np.float64) for x in (A, beta, EaR))
+        assert A.size == beta.size == EaR.size == self.nrxn
+        check(lib().ppb_set_arrhenius(self._h, A.ctypes.data_as(dpp), beta.ctypes.data_as(dpp),
+                                      EaR.ctypes.data_as(dpp)))
+
+    def adjoint(self, rY0, rYsrc, rX, rX_src, dt_react, lam_y, stream=None):
+        """Discrete adjoint of react() (torch CUDA tensors, YCOrder).
+
+        Returns (y_out, lam_y0, lam_e, grad) with grad = [dL/dlnA | dL/dbeta |
+        dL/d(Ea/R)] summed over the cells.
+        """
+        import torch
+
+        n = rY0.shape[0]
+        y_out = torch.empty_like(rY0)
+        lam_y0 = torch.empty_like(rY0)
+        lam_e = torch.empty_like(rX)
+        grad = torch.empty(3 * self.nrxn, dtype=torch.float64, device=rY0.device)
+        check(lib().ppb_adjoint_flat_device(self._h, _ptr(rY0), _ptr(rYsrc), _ptr(rX), _ptr(rX_src),
+                                            float(dt_react), int(n), _ptr(lam_y), _ptr(y_out), _ptr(lam_y0),
+                                            _ptr(lam_e), _ptr(grad), _stream(stream)))
+        return y_out, lam_y0, lam_e, grad
+
+    def tangent(self, rY0, rYsrc, rX, rX_src, dt_react, dy0=None, drX=None, dparams=None, stream=None):
+        """Tangent-linear model of react(): returns (y_out, dy_out)."""
+        import torch
+
+        n = rY0.shape[0]
+        y_out = torch.empty_like(rY0)
+        dy_out = torch.empty_like(rY0)
+        if dparams is None:
+            dparams = torch.zeros(3 * self.nrxn, dtype=torch.float64, device=rY0.device)
+        check(lib().ppb_tangent_flat_device(self._h, _ptr(rY0), _ptr(rYsrc), _ptr(rX), _ptr(rX_src),
+                                            float(dt_react), int(n), _ptr(dy0), _ptr(drX), _ptr(dparams),
+                                            _ptr(y_out), _ptr(dy_out), _stream(stream)))
+        return y_out, dy_out
+
     def react_soa(self, y, src, rX, rX_src, dt_react, time=0.0, ld=None, ncells=None, stream=None,
                   raise_on_fail=True):
         """Species-major device arrays y[(N+1), ld], src[N, ld]."""

@@ -171,3 +171,15 @@ def drm19_field(n=64, device="cuda", seed=1, burnt_threshold=0.7, eos=None, spec
     rY[:, N] = T
     return Cells(mech, rY, np.zeros((ncells, N)), rhoE, np.zeros(ncells), 1, 1e-5,
                  {"T": T, "phi": phi, "burnt": burnt, "s": s})
+
+
+def drm19_adjoint(ncells=65536, device="cuda", eos=None, species=None, mw=None):
+    """The adjoint workload: drm19 homogeneous reactors of the h/c_p type
+    (constant rho), T = 1100 + 500 U, phi = 0.5 + 1.5 U (seed 3), 1 atm,
+    integrated over 5e-4 s; loss weights (w_T, w_OH) ~ N(0, 1) from seed 4
+    in meta["w"] (2 x ncells)."""
+    cells = premix_cells("drm19", ncells, 3, 1100.0, 500.0, 0.5, 1.5, reactor_type=2, dt=5e-4, device=device,
+                         eos=eos, species=species, mw=mw)
+    cells.meta["w"] = np.random.default_rng(4).normal(size=(2, ncells))
+    return cells
+
