@@ -164,6 +164,45 @@ __host__ __device__ inline size_t adj_bytes(int N, int R)
   return ((d * 8 + 4 * n) + 15) & ~size_t(15);
 }
 
+// Reverse sweeps run between a segment's recomputation and the restore of
+// the previous checkpoint, when the forward workspace holds nothing that is
+// still needed: its vectors, Jacobian, factor and pivots serve as sweep
+// scratch and only the adjoint history (lam, pend) and the per-reaction
+// factors need their own shared memory (plus an FP64 factor when the
+// forward factor is FP32).  The parameter gradient accumulates in global
+// memory, per cell.
+template <typename LT>
+__host__ __device__ inline size_t adj_rev_bytes(int N, int R)
+{
+  const size_t n = N + 1;
+  size_t d = 7 * n + 6 * (size_t)R;
+  if (sizeof(LT) != sizeof(double)) d += n * n;
+  return (d * 8 + 15) & ~size_t(15);
+}
+
+template <typename LT>
+__device__ inline void carve_adj_rev(AdjWork& a, char* base, Work<LT>& w, int N, int R)
+{
+  const int n = N + 1;
+  double* p = (double*)base;
+  a.lam = p; p += 6 * n;
+  a.pend = p; p += n;
+  a.jxa = p; p += 6 * (size_t)R;
+  a.AT = (sizeof(LT) == sizeof(double)) ? reinterpret_cast<double*>(w.A) : p;
+  a.Jc = w.J;
+  a.piv = w.piv;
+  a.fE = w.zn[0];
+  a.fy = w.zn[1];
+  a.ek = w.zn[2];
+  a.cvk = w.zn[3];
+  a.v = w.zn[4]; // n + 1: runs into zn[5], which follows it
+  a.mu = w.acor;
+  a.dcvk = w.tempv;
+  a.ybuf = w.ftemp;
+  a.tmp = w.delta;
+  a.gacc = nullptr; // set per cell
+}
+
 __device__ inline void carve_adj(AdjWork& a, char* base, int N, int R)
 {
   const int n = N + 1;
@@ -264,37 +303,35 @@ __device__ AdjPoint rhs_exact_jacobian(const Team<TEAM>& tm, const DevMech& M, i
     w.wdot[s] = wd;
     a.Jc[N * n + s] = d;
   }
-  // exact d wdot / d c: reactions in order, lane l owns columns l, l+TEAM, ...
-  for (int r = 0; r < R; r++) {
-    const RxPack p = load_rx(M, r);
-    const bool has_alpha = (p.kind == PPB_RX_THIRD) || (p.fo != 255);
-    const bool rev = p.rev != 0;
-    const double k_f = a.jxa[6 * r + 0];
-    const double k_r = a.jxa[6 * r + 1];
-    const double fac = a.jxa[6 * r + 2];
-    uint4 em = make_uint4(0u, 0u, 0u, 0u);
-    if (has_alpha) em = __ldg(reinterpret_cast<const uint4*>(M.effmask) + r);
-    const double* ed = M.effd + (size_t)p.aslot * N;
+  // exact d wdot / d c: lane l owns columns l, l+TEAM, ... and walks the
+  // reactions that reach its column
 #pragma unroll
-    for (int qq = 0; qq < PER; qq++) {
-      const int k = tm.lane + qq * TEAM;
-      if (k >= N) break;
+  for (int qq = 0; qq < PER; qq++) {
+    const int k = tm.lane + qq * TEAM;
+    if (k >= N) break;
+    double* Jk = a.Jc + k * n;
+    const unsigned word_i = (unsigned)(k >> 5), bit = 1u << (k & 31);
+    const int e1 = __ldg(M.jc_off + k + 1);
+    for (int ei = __ldg(M.jc_off + k); ei < e1; ei++) {
+      const int r = __ldg(M.jc_rx + ei);
+      const RxPack p = load_rx(M, r);
+      const bool has_alpha = (p.kind == PPB_RX_THIRD) || (p.fo != 255);
       const bool inr = slots_has(p.fsp, k);
-      const bool inp = rev && slots_has(p.rsp, k);
+      const bool inp = (p.rev != 0) && slots_has(p.rsp, k);
       double d = 0.0;
       bool apply = inr || inp;
       if (has_alpha) {
-        const unsigned word = (k >> 5) == 0 ? em.x : (k >> 5) == 1 ? em.y : (k >> 5) == 2 ? em.z : em.w;
-        const double e = ((word >> (k & 31)) & 1u) ? __ldg(ed + k) : 1.0;
-        d = e * fac;
+        const bool listed = (__ldg(M.effmask + 4 * r + word_i) & bit) != 0u;
+        const double e = listed ? __ldg(M.effd + (size_t)p.aslot * N + k) : 1.0;
+        d = e * a.jxa[6 * r + 2];
         apply = apply || (e != 0.0);
       }
-      if (inr) d += k_f * slots_dproduct(p.fsp, w.sc, k);
-      if (inp) d -= k_r * slots_dproduct(p.rsp, w.sc, k);
+      if (inr) d += a.jxa[6 * r + 0] * slots_dproduct(p.fsp, w.sc, k);
+      if (inp) d -= a.jxa[6 * r + 1] * slots_dproduct(p.rsp, w.sc, k);
       if (apply) {
         for (int j = 0; j < p.njn; j++) {
           const double nu = (double)p.jnc[j];
-          if (nu != 0) a.Jc[k * n + p.jns[j]] += nu * d;
+          if (nu != 0) Jk[p.jns[j]] += nu * d;
         }
       }
     }

@@ -106,7 +106,10 @@ __device__ void adjoint_cell(const Team<32>& tm, const DevMech& M, const Options
   double lamE = 0.0;
   int fst[7] = {0, 0, 0, 0, 0, 0, 0}; // counters of the forward integration
   const int R = M.nrxn;
-  for (int r = tm.lane; r < 3 * R; r += 32) a.gacc[r] = 0.0;
+  if (MODE != ADJ_TANGENT) {
+    a.gacc = L.gw + (size_t)c * 3 * R; // this cell's parameter gradient
+    for (int r = tm.lane; r < 3 * R; r += 32) a.gacc[r] = 0.0;
+  }
   for (int i = tm.lane; i < 6 * n; i += 32) a.lam[i] = 0.0;
   for (int i = tm.lane; i < n; i += 32) a.pend[i] = 0.0;
   tm.sync();
@@ -171,10 +174,10 @@ __device__ void adjoint_cell(const Team<32>& tm, const DevMech& M, const Options
     if (out_vec)
       for (int i = tm.lane; i < n; i += 32) out_vec[i] = (flag == ST_OK) ? a.lam[i] : 0.0;
     if (b.lam_e && tm.lane == 0) b.lam_e[c] = (flag == ST_OK) ? lamE : 0.0;
-    // this cell's parameter gradient (summed over the cells in cell order
-    // afterwards, so the result does not depend on which warp ran which cell)
-    if (L.gw)
-      for (int r = tm.lane; r < 3 * R; r += 32) L.gw[(size_t)c * 3 * R + r] = (flag == ST_OK) ? a.gacc[r] : 0.0;
+    // the per-cell gradients are summed in cell order afterwards, so the
+    // result does not depend on which warp ran which cell
+    if (flag != ST_OK)
+      for (int r = tm.lane; r < 3 * R; r += 32) a.gacc[r] = 0.0;
   }
   if (MODE == ADJ_TANGENT && b.y_out)
     for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = (flag == ST_OK) ? w.y[i] : w.zn[0][i];
@@ -211,7 +214,10 @@ __global__ void __launch_bounds__(256) k_adjoint(DevMech M, Options o, AdjBatch 
   Work<LT> w;
   carve<LT>(w, base, NS, R);
   AdjWork a;
-  carve_adj(a, base + team_bytes<LT>(NS, R), NS, R);
+  if (MODE == ADJ_TANGENT)
+    carve_adj(a, base + team_bytes<LT>(NS, R), NS, R);
+  else
+    carve_adj_rev<LT>(a, base + team_bytes<LT>(NS, R), w, NS, R);
   char* cpb = L.cp + gwarp * (size_t)L.cap_cp * L.cp_stride;
   TapeRec* tape = reinterpret_cast<TapeRec*>(L.tape) + gwarp * (size_t)L.cap_rec;
   double* ys = L.ys + gwarp * (size_t)L.cap_y * (NS + 1);
@@ -292,27 +298,38 @@ static __global__ void k_sum_cells(const double* gw, int nc, int np, double* out
 template <int NS, typename LT, int MODE>
 static size_t adj_warp_smem(const DevMech& M)
 {
-  return team_bytes<LT>(NS, M.nrxn) + adj_bytes(NS, M.nrxn);
+  return team_bytes<LT>(NS, M.nrxn) +
+         (MODE == ADJ_TANGENT ? adj_bytes(NS, M.nrxn) : adj_rev_bytes<LT>(NS, M.nrxn));
 }
 
+// Block size (warps) with the most resident warps per SM.
 template <int NS, typename LT, int MODE>
 static int plan_ns_t(const DevMech& M, AdjPlan* p)
 {
   const size_t wb = adj_warp_smem<NS, LT, MODE>(M);
-  int wpb = 8;
-  while (wpb > 1 && wb * wpb > 200 * 1024) wpb--;
-  const size_t shm = wb * wpb;
   auto kern = k_adjoint<NS, LT, MODE>;
-  cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  if (e != cudaSuccess) return (int)e;
-  int dev = 0, nsm = 0, per_sm = 0;
+  int dev = 0, nsm = 0, smem_max = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)kern, wpb * 32, shm);
-  if (e != cudaSuccess) return (int)e;
-  if (per_sm < 1) return (int)cudaErrorInvalidConfiguration;
-  p->wpb = wpb;
-  p->blocks = nsm * per_sm;
+  cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  int best_w = 0, best_blocks = 0, best_warps = 0;
+  for (int wpb = 8; wpb >= 1; wpb--) {
+    const size_t shm = wb * wpb;
+    if (shm > (size_t)smem_max) continue;
+    cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    if (e != cudaSuccess) return (int)e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)kern, wpb * 32, shm);
+    if (e != cudaSuccess) return (int)e;
+    if (per_sm * wpb > best_warps) {
+      best_warps = per_sm * wpb;
+      best_w = wpb;
+      best_blocks = per_sm;
+    }
+  }
+  if (best_warps < 1) return (int)cudaErrorInvalidConfiguration;
+  p->wpb = best_w;
+  p->blocks = nsm * best_blocks;
   p->warp_smem = wb;
   p->cp_stride = cp_bytes<LT>(NS);
   return 0;

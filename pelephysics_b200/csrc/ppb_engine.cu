@@ -295,6 +295,39 @@ static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
   if (N > 127 || nfo > 254) pk.overflow = true;
   pk.used = off_effd + (size_t)nalpha * N * sizeof(double);
   set_off(dm.effd, off_effd);
+  // Jacobian column lists (species -> reactions reaching its column)
+  {
+    auto reaches = [&](int r, int k) {
+      const int kind = t->rx_kind[r];
+      if (kind == PPB_RX_THIRD || kind == PPB_RX_TROE || kind == PPB_RX_LINDEMANN) return true;
+      for (int j = 0; j < t->rx_fps_n[r]; j++)
+        if (t->rx_fps_sp[r * PPB_MAXPS + j] == k) return true;
+      if (t->rx_rev[r])
+        for (int j = 0; j < t->rx_rps_n[r]; j++)
+          if (t->rx_rps_sp[r * PPB_MAXPS + j] == k) return true;
+      return false;
+    };
+    int tot = 0;
+    for (int k = 0; k < N; k++)
+      for (int r = 0; r < R; r++) tot += reaches(r, k);
+    const size_t off_jcoff = (pk.used + 15) & ~size_t(15);
+    const size_t off_jcrx = (off_jcoff + (N + 1) * sizeof(int) + 15) & ~size_t(15);
+    int e = 0;
+    for (int k = 0; k < N; k++) {
+      pk.put(off_jcoff + k * sizeof(int), &e, 1);
+      for (int r = 0; r < R; r++) {
+        if (!reaches(r, k)) continue;
+        const unsigned short rr = (unsigned short)r;
+        pk.put(off_jcrx + e * sizeof(unsigned short), &rr, 1);
+        e++;
+      }
+    }
+    pk.put(off_jcoff + N * sizeof(int), &e, 1);
+    if (R > 65535) pk.overflow = true;
+    pk.used = off_jcrx + (size_t)tot * sizeof(unsigned short);
+    set_off(dm.jc_off, off_jcoff);
+    set_off(dm.jc_rx, off_jcrx);
+  }
   set_off(dm.rxp, off_rxp);
   set_off(dm.fop, off_fop);
   set_off(dm.effmask, off_msk);

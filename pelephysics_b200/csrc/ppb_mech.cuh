@@ -57,6 +57,11 @@ struct DevMech {
   const struct FoPack* fop;
   const unsigned* effmask; // 4 words per reaction: species with a listed efficiency
   const double* effd;      // [third-body reactions][nsp] efficiencies, 1 where unlisted
+  // per species k, in reaction order, the reactions whose Jacobian row
+  // d q_r / d c_k can be nonzero: every third-body / fall-off reaction and
+  // the reactions with k in their forward or (reversible) reverse phase space
+  const int* jc_off;
+  const unsigned short* jc_rx;
   // species-major gather of the aJacobian net stoichiometry (jn lists)
   const int *jg_off, *jg_rx;
   const double* jg_c;
@@ -816,32 +821,35 @@ __device__ void ajacobian_packed(
     wdot[s] = w;
     J[N * n + s] = d;
   }
-  // (3) species columns, reactions in order
-  double dq[PER];
+  // (3) species columns: lane l owns columns l, l+TEAM, ... and walks the
+  // reactions that reach its column in reaction order (the per-entry
+  // accumulation order of the generated code; dq carries the last dq/dc_k of
+  // a third-body reaction, which the consP == 0 form reuses for a
+  // zero-efficiency species without a rate term)
 #pragma unroll
-  for (int q = 0; q < PER; q++) dq[q] = 0.0;
-  for (int r = 0; r < R; r++) {
-    const RxPack p = load_rx(M, r);
-    const bool falloff = (p.fo != 255);
-    const bool has_alpha = (p.kind == PPB_RX_THIRD) || falloff;
-    const bool rev = p.rev != 0;
-    const double k_f = jx[4 * r + 0];
-    const double k_r = jx[4 * r + 1];
-    const double fac = jx[4 * r + 2];
-    uint4 em = make_uint4(0u, 0u, 0u, 0u);
-    if (has_alpha) em = __ldg(reinterpret_cast<const uint4*>(M.effmask) + r);
-    const double* ed = M.effd + (size_t)p.aslot * N;
-#pragma unroll
-    for (int q = 0; q < PER; q++) {
-      const int k = tm.lane + q * TEAM;
-      if (k >= N) break;
+  for (int qq = 0; qq < PER; qq++) {
+    const int k = tm.lane + qq * TEAM;
+    if (k >= N) break;
+    double dq = 0.0;
+    double* Jk = J + k * n;
+    const unsigned word_i = (unsigned)(k >> 5), bit = 1u << (k & 31);
+    const int e1 = __ldg(M.jc_off + k + 1);
+    for (int ei = __ldg(M.jc_off + k); ei < e1; ei++) {
+      const int r = __ldg(M.jc_rx + ei);
+      const RxPack p = load_rx(M, r);
+      const bool falloff = (p.fo != 255);
+      const bool has_alpha = (p.kind == PPB_RX_THIRD) || falloff;
+      const bool rev = p.rev != 0;
+      const double k_f = jx[4 * r + 0];
+      const double k_r = jx[4 * r + 1];
+      const double fac = jx[4 * r + 2];
       const bool inr = slots_has(p.fsp, k);
       const bool inp = rev && slots_has(p.rsp, k);
       double d = 0.0;
       bool apply = false;
       if (has_alpha) {
-        const unsigned word = (k >> 5) == 0 ? em.x : (k >> 5) == 1 ? em.y : (k >> 5) == 2 ? em.z : em.w;
-        const bool listed = (word >> (k & 31)) & 1u;
+        const bool listed = (__ldg(M.effmask + 4 * r + word_i) & bit) != 0u;
+        const double* ed = M.effd + (size_t)p.aslot * N;
         if (consP == 1) {
           if (listed) {
             d = (__ldg(ed + k) - 1) * fac;
@@ -867,9 +875,9 @@ __device__ void ajacobian_packed(
               if (inr) d += k_f * slots_dproduct(p.fsp, sc, k);
               if (inp) d -= k_r * slots_dproduct(p.rsp, sc, k);
             }
-            dq[q] = d;
+            dq = d;
           }
-          d = dq[q];
+          d = dq;
           apply = true;
         }
       } else {
@@ -880,7 +888,7 @@ __device__ void ajacobian_packed(
       if (apply) {
         for (int j = 0; j < p.njn; j++) {
           const double nu = (double)p.jnc[j];
-          if (nu != 0) J[k * n + p.jns[j]] += nu * d;
+          if (nu != 0) Jk[p.jns[j]] += nu * d;
         }
       }
     }
