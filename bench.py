@@ -438,6 +438,88 @@ def adjoint_measure(dev, ncells):
             "mean_steps": float(fwd_stats[:, 0].mean())}
 
 
+def config_arm(args):
+    """The larger configurations, one JSON line each (not the headline):
+    dodecane_lu 128x128x64 (FP64 LU vs FP32 factor + FP64 refinement) and
+    heptane_lu_88sk 64^3 (the same two, plus RK64), with errors against the
+    FP64 CPU oracle on a seeded sample of cells."""
+    import torch
+
+    from oracle import pyoracle as po
+    from pelephysics_b200 import workloads as wl
+    from pelephysics_b200.reactor import Reactor
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    if args.config == "dodecane":
+        mech = "dodecane_lu"
+        cells = wl.dodecane_field(device=dev)
+        opts = dict(rtol=1e-10, atol=1e-10, max_order=5)
+        arms = [("bdf_fp64_lu", "ReactorCvode", dict(lu_fp32=0)),
+                ("bdf_fp32_lu_fp64_refine", "ReactorCvode", dict(lu_fp32=1, refine_sweeps=1))]
+        workload = "dodecane_lu 128x128x64 (1048576 cells), 40 atm, T 700+600 s(x), dt 2e-6 s, advective sources"
+    else:
+        mech = "heptane_lu_88sk"
+        cells = wl.heptane_cells(device=dev)
+        opts = dict(rtol=1e-8, atol=1e-12, max_order=5)
+        arms = [("bdf_fp64_lu", "ReactorCvode", dict(lu_fp32=0)),
+                ("bdf_fp32_lu_fp64_refine", "ReactorCvode", dict(lu_fp32=1, refine_sweeps=1)),
+                ("rk64", "ReactorRK64", dict())]
+        workload = "heptane_lu_88sk 262144 cells, 20 atm, T 750+650 U, phi 0.3+1.7 U, dt 1e-5 s"
+    n = cells.ncells
+    N = cells.rY.shape[1] - 1
+    y0 = torch.as_tensor(cells.rY.T.copy(), device=dev)
+    s0 = torch.as_tensor(cells.rYsrc.T.copy(), device=dev)
+    x0 = torch.as_tensor(cells.rX, device=dev)
+    xs = torch.as_tensor(cells.rX_src, device=dev)
+    idx = np.sort(np.random.default_rng(9).permutation(n)[:args.sample])
+    yc = cells.rY[idx].copy()
+    t0 = time.perf_counter()
+    flag, _, _ = po.react_flat(mech, 1, yc, np.ascontiguousarray(cells.rYsrc[idx]), cells.rX[idx].copy(),
+                               cells.rX_src[idx].copy(), cells.dt, use_ref_kernels=0, **opts)
+    cpu_s = time.perf_counter() - t0
+    out = {}
+    for name, integ, extra in arms:
+        r = Reactor(mech, integ)
+        r.init(1, n, engine=1, **opts, **extra)
+        y = y0.clone()
+        x = x0.clone()
+        r.react_soa(y, s0, x, xs, cells.dt)  # warm-up (allocations, graph)
+        ms = []
+        for _ in range(args.steps):
+            y.copy_(y0)
+            x.copy_(x0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            r.react_soa(y, s0, x, xs, cells.dt)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        yall = y.cpu().numpy()
+        finite = np.all(np.isfinite(yall), axis=0)
+        yg = yall.T[idx]
+        st, _ = r.cell_status(n)
+        ok = np.all(np.isfinite(yg), axis=1)
+        dT = np.abs(yg[ok, N] - yc[ok, N]) / yc[ok, N]
+        Yg = yg[ok, :N] / yg[ok, :N].sum(1, keepdims=True)
+        Yc = yc[ok, :N] / yc[ok, :N].sum(1, keepdims=True)
+        stats = r.cell_stats(n)
+        out[name] = {"cells_per_s": n * len(ms) / (sum(ms) / 1e3), "ms_per_react": sum(ms) / len(ms),
+                     "max_rel_T_vs_fp64_oracle": float(dT.max()) if ok.any() else None,
+                     "max_abs_Y_vs_fp64_oracle": float(np.abs(Yg - Yc).max()) if ok.any() else None,
+                     "nonfinite_cells": int(np.sum(~finite)),
+                     "failed_cells": int(np.sum(st < 0)),
+                     "per_cell_mean": dict(zip(["steps", "rhs", "jac", "lu", "newton", "err_fail", "conv_fail"],
+                                               [round(float(v), 3) for v in stats.mean(axis=0)]))}
+        r.close()
+    line = {"config": args.config, "workload": workload, "cells": n, "opts": opts, "arms": out,
+            "oracle_sample": {"cells": int(len(idx)), "seconds": cpu_s, "flag": int(flag),
+                              "kind": "oracle BDF (table-driven FP64 kernels), OpenMP"},
+            "dtype": "f64 state; LU as named"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def flops_probe():
     """One drm19 cell: reactor RHS and reactor Jacobian pointwise kernels,
     thread per cell (run under ncu to count FP64 operations)."""
@@ -555,6 +637,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-workload measurement")
     ap.add_argument("--adjoint-cells", type=int, default=65536)
+    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane"],
+                    help="drm19: the headline line; dodecane / heptane: the larger configurations")
+    ap.add_argument("--sample", type=int, default=256, help="oracle sample cells for --config dodecane/heptane")
     ap.add_argument("--edge", type=int, default=64, help="field edge (profiling runs use a smaller box)")
     ap.add_argument("--phase-probe", action="store_true",
                     help="per-phase cycle counters of one react (profiling build, PPB_LIB)")
@@ -571,6 +656,8 @@ def main():
         return phase_probe(args.edge)
     if args.impl == "reference":
         return reference_arm(args)
+    if args.config != "drm19":
+        return config_arm(args)
     return our_arm(args)
 
 

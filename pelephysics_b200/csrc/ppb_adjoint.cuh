@@ -250,7 +250,7 @@ __device__ AdjPoint rhs_exact_jacobian(const Team<TEAM>& tm, const DevMech& M, i
   AdjPoint pt;
   pt.T = T;
   pt.invT = 1.0 / T;
-  pt.logT = log(T);
+  pt.logT = ppb_log(T);
   const double RT = RU * T;
   double aden = 0.0, adden = 0.0, amix = 0.0;
   for (int s = tm.lane; s < N; s += TEAM) {
@@ -402,9 +402,10 @@ __device__ void jc_mul(const Team<TEAM>& tm, int n, const double* Jc, const doub
   tm.sync();
 }
 
-// FP64 LU of I - gamma Jc (transpose = false) or of its transpose.
+// FP64 LU of I - gamma Jc (transpose = false) or of its transpose (out of
+// line, as the solve below: the sweeps keep one copy of each).
 template <int TEAM>
-__device__ int adj_factor(const Team<TEAM>& tm, int n, const double* Jc, double gamma, bool transpose, double* A,
+__device__ __noinline__ int adj_factor(const Team<TEAM>& tm, int n, const double* Jc, double gamma, bool transpose, double* A,
                           int* piv)
 {
   for (int i = tm.lane; i < n; i += TEAM) {
@@ -417,6 +418,12 @@ __device__ int adj_factor(const Team<TEAM>& tm, int n, const double* Jc, double 
   }
   tm.sync();
   return lu_factor<TEAM, double>(tm, A, n, piv);
+}
+
+template <int TEAM>
+__device__ __noinline__ void adj_solve(const Team<TEAM>& tm, const double* A, int n, const int* piv, double* b)
+{
+  lu_solve<TEAM, double>(tm, A, n, piv, b);
 }
 
 // Parameter vector-Jacobian product at the last rhs_exact_jacobian point:
@@ -485,7 +492,7 @@ struct AdjSweep {
   CellIn cin;
   int n, qmax;
 
-  __device__ AdjPoint point(double t, const double* yg)
+  __device__ __noinline__ AdjPoint point(double t, const double* yg)
   {
     for (int i = tm.lane; i < n; i += TEAM) a.ybuf[i] = yg[i];
     tm.sync();
@@ -541,7 +548,7 @@ struct AdjSweep {
         tm.sync();
         const AdjPoint pt = point(tn, ys + (size_t)R.i2 * n);
         if (adj_factor(tm, n, a.Jc, gamma, true, a.AT, a.piv)) return ST_ADJ_SINGULAR;
-        lu_solve<TEAM, double>(tm, a.AT, n, a.piv, a.mu);
+        adj_solve<TEAM>(tm, a.AT, n, a.piv, a.mu);
         jc_tmul_add(tm, n, a.Jc, a.mu, gamma, a.lam);
         double s = 0.0;
         for (int i = tm.lane; i < n; i += TEAM) {
@@ -651,7 +658,7 @@ struct AdjSweep {
         for (int i = tm.lane; i < n; i += TEAM) a.mu[i] = gamma * a.mu[i] - rl1 * a.lam[n + i];
         tm.sync();
         if (adj_factor(tm, n, a.Jc, gamma, false, a.AT, a.piv)) return ST_ADJ_SINGULAR;
-        lu_solve<TEAM, double>(tm, a.AT, n, a.piv, a.mu);
+        adj_solve<TEAM>(tm, a.AT, n, a.piv, a.mu);
         for (int i = tm.lane; i < n; i += TEAM) {
           const double d = a.mu[i];
           for (int j = 0; j <= q; j++) a.lam[j * n + i] += R.c[3 + j] * d;

@@ -279,7 +279,8 @@ struct Bdf {
     tm.sync();
   }
 
-  __device__ void f(double t, const double* y, double* fy)
+  // out of line: one copy of the right-hand side in the kernel
+  __device__ __noinline__ void f(double t, const double* y, double* fy)
   {
     PPB_TIC(PH_RHS);
     reactor_rhs<TEAM>(tm, M, o.reactor_type, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,

@@ -17,7 +17,16 @@ recipe:
   burnt: they take the composition of a premixed cell of the nearest phi
   that was integrated for 1 ms at constant volume from 1700 K (the 256-entry
   pool data/drm19_burnt_pool.npz, made by data/make_burnt_pool.py), at the
-  cell's own T.
+  cell's own T;
+* ``dodecane_field``: dodecane_lu on 128 x 128 x 64 (1,048,576 cells),
+  P = 40 atm, T = 700 + 600 s(x) with s seed-2 white noise smoothed by a
+  Gaussian of sigma = 4 cells (periodic, by FFT) and [0,1]-normalised,
+  phi = 0.5 + 1.5 U, and advective species sources rYsrc_k ~ N(0,
+  (1e-3 rho Y_k / dt)^2) made mass-conserving by subtracting
+  Y_k sum_j rYsrc_j; dt = 2e-6 s;
+* ``heptane_cells``: heptane_lu_88sk, 262,144 cells, P = 20 atm,
+  T = 750 + 650 U, phi = 0.3 + 1.7 U (seed 5), dt = 1e-5 s (rtol 1e-8,
+  atol 1e-12 in the benchmark).
 
 Mass fractions are YCOrder per cell; energies are rho*e (reactor type 1) or
 rho*h (type 2).  Density and energy come from an EOS callable
@@ -182,4 +191,47 @@ def drm19_adjoint(ncells=65536, device="cuda", eos=None, species=None, mw=None):
                          eos=eos, species=species, mw=mw)
     cells.meta["w"] = np.random.default_rng(4).normal(size=(2, ncells))
     return cells
+
+
+def smoothed_field(shape, seed, sigma):
+    """White noise (default_rng(seed)) smoothed by a periodic Gaussian of
+    standard deviation sigma cells, normalised to [0, 1]."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(shape)
+    k = [np.fft.fftfreq(m) for m in shape]
+    kz, ky, kx = np.meshgrid(*k, indexing="ij")
+    g = np.exp(-2.0 * (np.pi * sigma) ** 2 * (kx ** 2 + ky ** 2 + kz ** 2))
+    s = np.real(np.fft.ifftn(np.fft.fftn(w) * g))
+    s -= s.min()
+    return s / s.max()
+
+
+def dodecane_field(shape=(64, 128, 128), device="cuda", seed=2, sigma=4.0, eos=None, species=None, mw=None):
+    """dodecane_lu on a 128 x 128 x 64 box (see module doc)."""
+    mech = "dodecane_lu"
+    species = species or _lib.species_names(mech)
+    mw = _lib.molecular_weights(mech) if mw is None else mw
+    eos = eos or device_eos(mech, device)
+    N = len(species)
+    dt = 2e-6
+    s = smoothed_field(shape, seed, sigma).reshape(-1)
+    ncells = s.size
+    rng = np.random.default_rng(seed + 100)
+    T = 700.0 + 600.0 * s
+    phi = 0.5 + 1.5 * rng.uniform(size=ncells)
+    Y = mass_fractions(mole_fractions(mech, phi, species), mw)
+    P = 40.0 * P_ATM
+    rho, rhoE = eos(T, Y, P, 1)
+    rY = np.zeros((ncells, N + 1))
+    rY[:, :N] = rho[:, None] * Y
+    rY[:, N] = T
+    src = rng.standard_normal((ncells, N)) * (1e-3 * rY[:, :N] / dt)
+    src -= Y * src.sum(axis=1, keepdims=True)
+    return Cells(mech, rY, src, rhoE, np.zeros(ncells), 1, dt, {"T": T, "phi": phi, "s": s, "P": P})
+
+
+def heptane_cells(ncells=262144, device="cuda", seed=5, eos=None, species=None, mw=None):
+    """heptane_lu_88sk, 64^3 cells (see module doc)."""
+    return premix_cells("heptane_lu_88sk", ncells, seed, 750.0, 650.0, 0.3, 1.7, P=20.0 * P_ATM, reactor_type=1,
+                        dt=1e-5, device=device, eos=eos, species=species, mw=mw)
 

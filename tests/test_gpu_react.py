@@ -76,6 +76,61 @@ def test_drm19_bdf(cuda, oracle, eng):
     compare(y, ref)
 
 
+# the thread-per-cell plain engine keeps a whole cell workspace (56 KB for
+# dodecane_lu, 142 KB for heptane_lu_88sk) in thread-local memory: it is the
+# drm19 baseline and is not exercised on the large mechanisms
+@pytest.mark.parametrize("eng", ENGINES[1:], ids=["tuned", "tuned_fp32"])
+def test_dodecane_bdf_with_sources(cuda, oracle, eng):
+    """dodecane_lu at 40 atm, dt 2e-6 s, with mass-conserving advective
+    species sources (the 128x128x64 configuration's recipe)."""
+    mech, rtype, dt, nc = "dodecane_lu", 1, 2e-6, 12
+    rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 2, 700.0, 600.0, 0.5, 1.5, P=40 * 1013250.0)
+    rng = np.random.default_rng(3)
+    Y = rY[:, :-1] / rY[:, :-1].sum(axis=1, keepdims=True)
+    src = rng.standard_normal(src.shape) * (1e-3 * rY[:, :-1] / dt)
+    src -= Y * src.sum(axis=1, keepdims=True)
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5)
+    ref, _, flag, _, _ = oracle_react(oracle, mech, rtype, rY, src, rX, rXs, dt, **opts)
+    assert flag == 0
+    r = Reactor(mech)
+    r.init(rtype, nc, **opts, **eng)
+    y = rY.copy()
+    r.react(y, src.copy(), rX.copy(), rXs.copy(), dt)
+    compare(y, ref)
+
+
+@pytest.mark.parametrize("eng", ENGINES[1:], ids=["tuned", "tuned_fp32"])
+def test_heptane_bdf(cuda, oracle, eng):
+    """heptane_lu_88sk (the 88x88 Newton matrix), 20 atm, rtol 1e-8,
+    atol 1e-12, as the 64^3 configuration."""
+    mech, rtype, dt, nc = "heptane_lu_88sk", 1, 1e-5, 6
+    rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 5, 750.0, 650.0, 0.3, 1.7, P=20 * 1013250.0)
+    opts = dict(rtol=1e-8, atol=1e-12, max_order=5)
+    ref, _, flag, _, _ = oracle_react(oracle, mech, rtype, rY, src, rX, rXs, dt, **opts)
+    assert flag == 0
+    r = Reactor(mech)
+    r.init(rtype, nc, **opts, **eng)
+    y = rY.copy()
+    r.react(y, src.copy(), rX.copy(), rXs.copy(), dt)
+    # rtol 1e-8 on the integration: the bar scales with it
+    compare(y, ref, T_rtol=1e-6, Y_atol=1e-7)
+
+
+@pytest.mark.parametrize("eng", ENGINES[1:2], ids=["tuned"])
+def test_heptane_rk64(cuda, oracle, eng):
+    """RK64 on heptane_lu_88sk at 20 atm over a step its 500-substep cap can
+    resolve (at 750-1400 K and dt = 1e-5 s the explicit scheme is unstable
+    on most cells, in the reference as here)."""
+    mech, rtype, dt, nc = "heptane_lu_88sk", 1, 1e-8, 4
+    rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 5, 750.0, 100.0, 0.3, 1.7, P=20 * 1013250.0)
+    ref, _, _, steps, _ = oracle_react(oracle, mech, rtype, rY, src, rX, rXs, dt, method=1, atol=1e-12)
+    r = Reactor(mech, "ReactorRK64")
+    r.init(rtype, nc, atol=1e-12, **eng)
+    y = rY.copy()
+    r.react(y, src.copy(), rX.copy(), rXs.copy(), dt)
+    compare(y, ref, T_rtol=1e-9, Y_atol=1e-11)
+
+
 @pytest.mark.parametrize("eng", ENGINES[:2], ids=["plain", "tuned"])
 def test_enthalpy_reactor_with_sources(cuda, oracle, eng):
     """Reactor type 2 with nonzero species and energy sources, default
