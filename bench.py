@@ -262,6 +262,7 @@ def our_arm(args):
     value = n * ws * args.steps / t_dev
     y_gpu = y.cpu().numpy().T.copy()
     stats = r.cell_stats(n)
+    wpb, team, regs, tune_ms = r.launch_config()
     status, _ = r.cell_status(n)
 
     # end to end through the public flat API on pinned host buffers
@@ -361,7 +362,10 @@ def our_arm(args):
             "data": "synthetic",
             "config": {"workload": "drm19 64^3 field (262144 cells/GPU), dt 1e-5 s, constant-volume, BDF q<=5, "
                                    "rtol=atol=1e-10", "cells_per_gpu": n, "l2": "flushed between timed steps",
-                       "engine": "tuned: warp per cell, persistent work queue, CUDA graph, FP64 LU"},
+                       "engine": "tuned: team of lanes per cell, persistent work queue, CUDA graph, FP64 LU",
+                       "autotuned_launch": {"warps_per_block": wpb, "lanes_per_cell": team,
+                                            "register_budget": "<=128 regs" if regs == 2 else "<=255 regs",
+                                            "sample_ms": tune_ms}},
             "e2e": {"value": e2e, "unit": "cells/s", "h2d_bytes_per_step": h2d * ws, "d2h_bytes_per_step": d2h * ws},
             "gpu_launches": 2 * args.steps,
             "roofline": roof,
@@ -511,6 +515,17 @@ def config_arm(args):
                      "failed_cells": int(np.sum(st < 0)),
                      "per_cell_mean": dict(zip(["steps", "rhs", "jac", "lu", "newton", "err_fail", "conv_fail"],
                                                [round(float(v), 3) for v in stats.mean(axis=0)]))}
+        if integ == "ReactorRK64":
+            # the oracle's RK64 on the sample: the explicit scheme's own answer
+            yk = cells.rY[idx].copy()
+            po.react_flat(mech, 1, yk, np.ascontiguousarray(cells.rYsrc[idx]), cells.rX[idx].copy(),
+                          cells.rX_src[idx].copy(), cells.dt, method=1, use_ref_kernels=0, **opts)
+            okk = np.all(np.isfinite(yk), axis=1)
+            both = okk & ok
+            out[name]["oracle_rk64_nonfinite_in_sample"] = int(np.sum(~okk))
+            out[name]["gpu_rk64_nonfinite_in_sample"] = int(np.sum(~ok))
+            if both.any():
+                out[name]["max_rel_T_vs_oracle_rk64"] = float(np.max(np.abs(yg[both, N] - yk[both, N]) / yk[both, N]))
         r.close()
     line = {"config": args.config, "workload": workload, "cells": n, "opts": opts, "arms": out,
             "oracle_sample": {"cells": int(len(idx)), "seconds": cpu_s, "flag": int(flag),

@@ -58,10 +58,13 @@ typedef struct ppb_options {
   int engine;               /* PPB_ENGINE_TUNED */
   int lu_fp32;              /* factor I - gamma J in FP32 + FP64 refinement, 0 */
   int refine_sweeps;        /* refinement sweeps with lu_fp32, 1 */
-  int warps_per_block;      /* tuned engine block size in warps, 0 = auto */
+  int warps_per_block;      /* tuned engine block size in warps; 0 = autotune the block size,
+                               lanes per cell and register budget on the first call */
   int use_graph;            /* replay react() as a captured CUDA graph, 1 */
   int adjoint_checkpoint_interval; /* accepted BDF steps between adjoint checkpoints, 16 */
   int adjoint_memory_mb;    /* device memory for adjoint checkpoints and tapes, 8192 */
+  int team_lanes;           /* with warps_per_block > 0: lanes per cell, 32 or 16 (<= 21 species) */
+  int register_budget;      /* with warps_per_block > 0: 2 (<= 128 registers) or 1 (<= 255) */
 } ppb_options;
 
 /* An amrex::Array4<Real>-compatible view: element (i,j,k,n) lives at
@@ -201,6 +204,14 @@ int ppb_pyt2re(const char* mechanism, int eh, const double* P, const double* T, 
 int ppb_react_flat_device_noalloc(const char* mechanism, const char* integrator, int reactor_type,
                                   const ppb_options* opt, double* rY, double* rYsrc, double* rX, double* rX_src,
                                   double dt_react, int ncells, void* stream, int* nfailed);
+
+/* Launch configuration of the tuned engine the reactor uses (after the
+ * autotuner ran, when warps_per_block was 0): block size in warps, lanes per
+ * cell, register budget, and the autotuner's measured time of the chosen
+ * configuration on its sample (ms; 0 when not tuned).  No counterpart in the
+ * reference. */
+int ppb_get_launch_config(ppb_reactor* r, int* warps_per_block, int* team_lanes, int* register_budget,
+                          double* tuned_ms);
 
 /* ---- Differentiation (no counterpart in the reference; the ReactorBase
  * interface has no derivative entry points).

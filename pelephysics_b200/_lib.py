@@ -43,6 +43,8 @@ class Options(C.Structure):
         ("use_graph", C.c_int),
         ("adjoint_checkpoint_interval", C.c_int),
         ("adjoint_memory_mb", C.c_int),
+        ("team_lanes", C.c_int),
+        ("register_budget", C.c_int),
     ]
 
 
@@ -112,6 +114,7 @@ def lib():
                                                 C.c_double, C.c_int, vp, ip]
     L.ppb_molecular_weights.argtypes = [C.c_char_p, dpp]
     L.ppb_pyt2re.argtypes = [C.c_char_p, C.c_int, dp, dp, dp, dp, dp, C.c_int, vp]
+    L.ppb_get_launch_config.argtypes = [vp, ip, ip, ip, dpp]
     L.ppb_get_arrhenius.argtypes = [vp, dpp, dpp, dpp]
     L.ppb_set_arrhenius.argtypes = [vp, dpp, dpp, dpp]
     L.ppb_adjoint_flat_device.argtypes = [vp, dp, dp, dp, dp, C.c_double, C.c_int, dp, dp, dp, dp, dp, vp]

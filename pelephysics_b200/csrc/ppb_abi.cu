@@ -196,21 +196,164 @@ static Options engine_options(const ppb_reactor* r)
   return o;
 }
 
+// ---- autotuner: per (mechanism tables, device, integrator, reactor type,
+// LU precision, typical values) the fastest tuned-engine configuration on a
+// sample of the first batch
+struct TuneEntry {
+  const PPBMechTables* t;
+  int dev, method, rtype, lu_fp32, typ;
+  LaunchConfig lc;
+  double ms;
+};
+static std::mutex g_tune_mu;
+static std::vector<TuneEntry> g_tune;
+
+static bool tuned_config(const ppb_reactor* r, LaunchConfig* lc, double* ms)
+{
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  for (const auto& e : g_tune) {
+    if (e.t == r->dm->host && e.dev == dev && e.method == r->method && e.rtype == r->reactor_type &&
+        e.lu_fp32 == r->opt.lu_fp32 && e.typ == (int)!r->typ_vals.empty()) {
+      *lc = e.lc;
+      if (ms) *ms = e.ms;
+      return true;
+    }
+  }
+  return false;
+}
+
 static LaunchConfig launch_config(const ppb_reactor* r)
 {
   LaunchConfig lc;
   lc.engine = r->opt.engine;
   lc.lu_fp32 = r->opt.lu_fp32;
-  lc.warps_per_block = r->opt.warps_per_block;
-  if (lc.warps_per_block <= 0) {
-    // largest block (<= 8 warps) whose shared-memory workspace still fits
-    const size_t cb = team_cell_bytes(r->t, r->opt.lu_fp32);
-    int w = 8;
-    while (w > 1 && cb * w > 200 * 1024) w--;
-    lc.warps_per_block = w;
-  }
   lc.persistent = 1;
+  if (r->opt.warps_per_block > 0) {
+    lc.warps_per_block = r->opt.warps_per_block;
+    lc.team = r->opt.team_lanes == 16 ? 16 : 32;
+    lc.minb = r->opt.register_budget == 1 ? 1 : 2;
+    return lc;
+  }
+  if (lc.engine == ENGINE_TUNED && tuned_config(r, &lc, nullptr)) {
+    lc.engine = ENGINE_TUNED;
+    lc.lu_fp32 = r->opt.lu_fp32;
+    return lc;
+  }
+  // untuned default: the largest block (<= 8 warps) that fits, one warp per
+  // cell, <= 128 registers
+  const size_t cb = team_cell_bytes(r->t, r->opt.lu_fp32);
+  int w = 8;
+  while (w > 1 && cb * w > 200 * 1024) w--;
+  lc.warps_per_block = w;
   return lc;
+}
+
+// Time the candidate configurations on a copy of (up to) four resident
+// waves of the batch's first cells and cache the fastest.  Not during a
+// stream capture (the caller checks).
+static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
+{
+  if (r->opt.engine != PPB_ENGINE_TUNED || r->opt.warps_per_block > 0) return 0;
+  LaunchConfig have;
+  if (tuned_config(r, &have, nullptr)) return 0;
+  const int N = r->t->nsp, n = N + 1;
+  std::vector<LaunchConfig> cand;
+  int max_res = 0;
+  for (int team : {32, 16}) {
+    if (team == 16 && N > 21) continue;
+    for (int minb : {2, 1}) {
+      if (minb == 1 && (r->method != METHOD_BDF || r->opt.lu_fp32)) continue;
+      for (int wpb : {8, 4, 2, 1}) {
+        LaunchConfig lc;
+        lc.engine = ENGINE_TUNED;
+        lc.lu_fp32 = r->opt.lu_fp32;
+        lc.warps_per_block = wpb;
+        lc.team = team;
+        lc.minb = minb;
+        const int res = react_occupancy(*r->dm, r->method, lc);
+        if (res <= 0) continue;
+        max_res = std::max(max_res, res);
+        cand.push_back(lc);
+      }
+    }
+  }
+  if (cand.empty()) return 0;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int m = (int)std::min<long>(b.ncells, 4L * max_res * nsm);
+  const size_t nm = (size_t)m;
+  double *y0 = nullptr, *y = nullptr, *sr = nullptr, *re = nullptr, *rs = nullptr;
+  int *stt = nullptr, *nfe = nullptr, *q = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int err = 0;
+  auto cleanup = [&]() {
+    cudaFree(y0);
+    cudaFree(y);
+    cudaFree(sr);
+    cudaFree(re);
+    cudaFree(rs);
+    cudaFree(stt);
+    cudaFree(nfe);
+    cudaFree(q);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  };
+  if ((err = cudaMalloc(&y0, n * nm * 8)) || (err = cudaMalloc(&y, n * nm * 8)) || (err = cudaMalloc(&sr, n * nm * 8)) ||
+      (err = cudaMalloc(&re, nm * 8)) || (err = cudaMalloc(&rs, nm * 8)) || (err = cudaMalloc(&stt, nm * 4)) ||
+      (err = cudaMalloc(&nfe, nm * 4)) || (err = cudaMalloc(&q, 16)) || (err = cudaEventCreate(&e0)) ||
+      (err = cudaEventCreate(&e1))) {
+    cleanup();
+    return cuda_fail(err, "autotune scratch");
+  }
+  err = cudaMemcpy2DAsync(y0, nm * 8, b.y, (size_t)b.ld * 8, nm * 8, n, cudaMemcpyDeviceToDevice, st);
+  if (!err) err = cudaMemcpy2DAsync(sr, nm * 8, b.src, (size_t)b.ld * 8, nm * 8, N, cudaMemcpyDeviceToDevice, st);
+  if (!err) err = cudaMemcpyAsync(re, b.rhoe, nm * 8, cudaMemcpyDeviceToDevice, st);
+  if (!err) err = cudaMemcpyAsync(rs, b.rhoesrc, nm * 8, cudaMemcpyDeviceToDevice, st);
+  const Options o = engine_options(r);
+  double best = 1e300;
+  LaunchConfig pick = cand[0];
+  for (size_t k = 0; k < cand.size() + 1 && !err; k++) {
+    const LaunchConfig& lc = cand[k == 0 ? 0 : k - 1]; // the first candidate twice: warm-up
+    Batch tb{};
+    tb.y = y;
+    tb.src = sr;
+    tb.rhoe = re;
+    tb.rhoesrc = rs;
+    tb.atolv = r->atolv;
+    tb.status = stt;
+    tb.nfe = nfe;
+    tb.ncells = m;
+    tb.ld = m;
+    err = cudaMemcpyAsync(y, y0, n * nm * 8, cudaMemcpyDeviceToDevice, st);
+    if (!err) err = cudaEventRecord(e0, st);
+    if (!err) err = launch_react(*r->dm, o, r->method, lc, tb, dt, q, st);
+    if (!err) err = cudaEventRecord(e1, st);
+    if (!err) err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (!err) err = cudaEventElapsedTime(&ms, e0, e1);
+    if (!err && k > 0 && ms < best) {
+      best = ms;
+      pick = lc;
+    }
+  }
+  cleanup();
+  if (err) return cuda_fail(err, "autotune");
+  TuneEntry te{r->dm->host, dev, r->method, r->reactor_type, r->opt.lu_fp32, (int)!r->typ_vals.empty(), pick, best};
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune.push_back(te);
+  return 0;
+}
+
+// Run the autotuner on this batch unless the stream is being captured.
+static int maybe_autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
+{
+  if (r->opt.engine != PPB_ENGINE_TUNED || r->opt.warps_per_block > 0) return 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return 0;
+  return autotune(r, b, dt, st);
 }
 
 // Capture body() on the reactor's private stream into r->gexec.
@@ -259,6 +402,8 @@ void ppb_default_options(ppb_options* o)
   o->use_graph = 1;
   o->adjoint_checkpoint_interval = 16;
   o->adjoint_memory_mb = 8192;
+  o->team_lanes = 32;
+  o->register_budget = 2;
 }
 
 const char* ppb_last_error(void) { return g_err; }
@@ -388,6 +533,8 @@ static int run_batch(ppb_reactor* r, Batch b, double dt, cudaStream_t st)
   b.status = r->status;
   b.nfe = r->nfe;
   b.stats = r->stats;
+  int te = maybe_autotune(r, b, dt, st);
+  if (te) return te;
   const Options o = engine_options(r);
   const LaunchConfig lc = launch_config(r);
   int e = launch_react(*r->dm, o, r->method, lc, b, dt, r->queue, st);
@@ -489,6 +636,20 @@ int ppb_react_flat_device(ppb_reactor* r, double* rY, double* rYsrc, double* rX,
     return 0;
   };
   if (r->opt.use_graph) {
+    if (!r->gexec || !(r->gkey == key)) {
+      // tune outside the capture, on the batch converted to species-major
+      PPB_CUDA(launch_aos_to_soa(rY, n, r->soa, ncells, n, ncells, st), "aos_to_soa");
+      PPB_CUDA(launch_aos_to_soa(rYsrc, N, r->soa_src, ncells, N, ncells, st), "aos_to_soa");
+      Batch tb{};
+      tb.y = r->soa;
+      tb.src = r->soa_src;
+      tb.rhoe = rX;
+      tb.rhoesrc = rX_src;
+      tb.ncells = ncells;
+      tb.ld = ncells;
+      e = maybe_autotune(r, tb, dt, st);
+      if (e) return e;
+    }
     e = capture(r, key, body);
     if (e) return e;
     PPB_CUDA(cudaGraphLaunch(r->gexec, st), "cudaGraphLaunch");
@@ -530,6 +691,10 @@ int ppb_react_soa_device(ppb_reactor* r, double* y, const double* src, double* r
     return ee;
   };
   if (r->opt.use_graph) {
+    if (!r->gexec || !(r->gkey == key)) {
+      e = maybe_autotune(r, b, dt, st); // outside the capture
+      if (e) return e;
+    }
     e = capture(r, key, body);
     if (e) return e;
     PPB_CUDA(cudaGraphLaunch(r->gexec, st), "cudaGraphLaunch");
@@ -639,6 +804,21 @@ int ppb_probe_fp64_peak(double* gflops, void* stream)
 {
   if (!gflops) return fail(PPB_E_ARG, "ppb_probe_fp64_peak: null output");
   return cuda_fail(probe_fp64_peak(gflops, (cudaStream_t)stream), "probe_fp64_peak");
+}
+
+int ppb_get_launch_config(ppb_reactor* r, int* warps_per_block, int* team_lanes, int* register_budget,
+                          double* tuned_ms)
+{
+  if (!r || !r->inited) return fail(PPB_E_STATE, "ppb_get_launch_config before init");
+  const LaunchConfig lc = launch_config(r);
+  double ms = 0.0;
+  LaunchConfig tl;
+  if (r->opt.warps_per_block <= 0) tuned_config(r, &tl, &ms);
+  if (warps_per_block) *warps_per_block = lc.warps_per_block;
+  if (team_lanes) *team_lanes = lc.team;
+  if (register_budget) *register_budget = lc.minb;
+  if (tuned_ms) *tuned_ms = ms;
+  return 0;
 }
 
 int ppb_get_arrhenius(ppb_reactor* r, double* A, double* beta, double* EaR)

@@ -404,7 +404,8 @@ size_t team_cell_bytes(const PPBMechTables* t, int lu_fp32)
 #define PPB_DECL(NS)                                                                                              \
   int launch_react_##NS(const DeviceMechanism&, const Options&, int, const LaunchConfig&, Batch, double, int*,      \
                         cudaStream_t);                                                                             \
-  int launch_ajacobian_##NS(const DevMech&, const double*, const double*, int, double*, int, int, cudaStream_t);
+  int launch_ajacobian_##NS(const DevMech&, const double*, const double*, int, double*, int, int, cudaStream_t);      \
+  int react_occupancy_##NS(const DevMech&, int, const LaunchConfig&);
 PPB_DECL(9)
 PPB_DECL(21)
 PPB_DECL(53)
@@ -424,6 +425,18 @@ int launch_react(const DeviceMechanism& m, const Options& o, int method, const L
     return launch_react_88(m, o, method, lc, b, dt, queue, st);
   default:
     return (int)cudaErrorNotSupported;
+  }
+}
+
+int react_occupancy(const DeviceMechanism& m, int method, const LaunchConfig& lc)
+{
+  const DevMech& M = *m.dm;
+  switch (M.nsp) {
+  case 9: return react_occupancy_9(M, method, lc);
+  case 21: return react_occupancy_21(M, method, lc);
+  case 53: return react_occupancy_53(M, method, lc);
+  case 88: return react_occupancy_88(M, method, lc);
+  default: return 0;
   }
 }
 

@@ -48,7 +48,12 @@ struct LaunchConfig {
   int warps_per_block = 4;
   int lu_fp32 = 0;
   int persistent = 1; // work queue
+  int team = 32;      // lanes per cell: 32, or 16 for mechanisms of <= 21 species
+  int minb = 2;       // register budget: >= minb blocks of 256 threads per SM
 };
+// Resident cells per SM of the tuned kernel in configuration lc (0: the
+// configuration does not fit or is not compiled).
+int react_occupancy(const DeviceMechanism& m, int method, const LaunchConfig& lc);
 
 // Integrate every cell of the batch over dt.  queue is a device int used by
 // the persistent kernel (reset inside the call).  Returns a cudaError_t.

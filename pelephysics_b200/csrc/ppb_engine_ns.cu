@@ -106,29 +106,59 @@ __global__ void __launch_bounds__(128) k_react_plain(DevMech M, Options o, Batch
   react_one<NS, 1, double, METHOD>(tm, M, o, w, b, c, dt);
 }
 
-// tuned: one warp per cell, shared-memory workspace, persistent work queue
-template <int NS, typename LT, int METHOD>
-__global__ void __launch_bounds__(256) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
-                                                    size_t cell_bytes, int persistent)
+// tuned: one team (a warp, or half a warp for small mechanisms) per cell,
+// shared-memory workspace, persistent work queue.  MINB is the register
+// budget: at least MINB blocks of 256 threads per SM (2: <= 128 registers a
+// thread, 1: <= 255).
+template <int NS, typename LT, int METHOD, int TEAM, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
+                                                          size_t cell_bytes, int persistent)
 {
   extern __shared__ __align__(16) char smem[];
-  Team<32> tm;
-  const int warp = threadIdx.x / 32;
+  Team<TEAM> tm;
+  const int team = threadIdx.x / TEAM;
   Work<LT> w;
-  carve<LT>(w, smem + (size_t)warp * cell_bytes, M.nsp, M.nrxn);
-  const int wpb = blockDim.x / 32;
+  carve<LT>(w, smem + (size_t)team * cell_bytes, M.nsp, M.nrxn);
+  const int tpb = blockDim.x / TEAM;
   if (persistent) {
     for (;;) {
       int c = 0;
       if (tm.lane == 0) c = atomicAdd(queue, 1);
-      c = __shfl_sync(0xffffffffu, c, 0);
+      c = __shfl_sync(tm.mask, c, 0, TEAM);
       if (c >= b.ncells) break;
-      react_one<NS, 32, LT, METHOD>(tm, M, o, w, b, c, dt);
+      react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, c, dt);
     }
   } else {
-    const int c = blockIdx.x * wpb + warp;
-    if (c < b.ncells) react_one<NS, 32, LT, METHOD>(tm, M, o, w, b, c, dt);
+    const int c = blockIdx.x * tpb + team;
+    if (c < b.ncells) react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, c, dt);
   }
+}
+
+typedef void (*TeamKernel)(DevMech, Options, Batch, double, int*, size_t, int);
+
+// The compiled variants: 32 lanes per cell with both register budgets for
+// the FP64 BDF kernel; 16 lanes per cell as well for mechanisms of at most
+// 21 species.
+template <int NS>
+static TeamKernel team_kernel(int method, bool fp32, int team, int minb)
+{
+  constexpr bool small = NS <= 21;
+  if (team == 16 && !small) return nullptr;
+  if (method == METHOD_RK64) {
+    if (team == 16) return small ? (TeamKernel)k_react_team<NS, double, METHOD_RK64, (small ? 16 : 32), 2> : nullptr;
+    return (TeamKernel)k_react_team<NS, double, METHOD_RK64, 32, 2>;
+  }
+  if (fp32) {
+    if (team == 16) return small ? (TeamKernel)k_react_team<NS, float, METHOD_BDF, (small ? 16 : 32), 2> : nullptr;
+    return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 2>;
+  }
+  if (team == 16) {
+    if (!small) return nullptr;
+    return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 1>
+                     : (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 2>;
+  }
+  return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1>
+                   : (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2>;
 }
 
 template <int NS>
@@ -148,12 +178,12 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
   }
   const int wpb = lc.warps_per_block > 0 ? lc.warps_per_block : 4;
   const bool fp32 = lc.lu_fp32 && method == METHOD_BDF;
+  const int team = lc.team == 16 ? 16 : 32;
+  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb);
+  if (!kern) return (int)cudaErrorInvalidConfiguration;
+  const int tpb = wpb * (32 / team); // cells per block
   const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
-  const size_t shm = cb * wpb;
-  typedef void (*KT)(DevMech, Options, Batch, double, int*, size_t, int);
-  KT kern = (method == METHOD_RK64) ? (KT)k_react_team<NS, double, METHOD_RK64>
-            : fp32                  ? (KT)k_react_team<NS, float, METHOD_BDF>
-                                    : (KT)k_react_team<NS, double, METHOD_BDF>;
+  const size_t shm = cb * tpb;
   cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   if (e != cudaSuccess) return (int)e;
   int blocks;
@@ -165,15 +195,37 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
     if (e != cudaSuccess) return (int)e;
     if (per_sm < 1) return (int)cudaErrorInvalidConfiguration;
     blocks = nsm * per_sm;
-    const int need = (b.ncells + wpb - 1) / wpb;
+    const int need = (b.ncells + tpb - 1) / tpb;
     if (blocks > need) blocks = need;
     e = cudaMemsetAsync(queue, 0, sizeof(int), st);
     if (e != cudaSuccess) return (int)e;
   } else {
-    blocks = (b.ncells + wpb - 1) / wpb;
+    blocks = (b.ncells + tpb - 1) / tpb;
   }
   kern<<<blocks, wpb * 32, shm, st>>>(M, o, b, dt, queue, cb, lc.persistent);
   return (int)cudaGetLastError();
+}
+
+// Resident cells per SM of a configuration (0: does not fit).
+template <int NS>
+static int occupancy_ns(const DevMech& M, int method, const LaunchConfig& lc)
+{
+  const bool fp32 = lc.lu_fp32 && method == METHOD_BDF;
+  const int team = lc.team == 16 ? 16 : 32;
+  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb);
+  if (!kern) return 0;
+  const int wpb = lc.warps_per_block > 0 ? lc.warps_per_block : 4;
+  const int tpb = wpb * (32 / team);
+  const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
+  const size_t shm = cb * tpb;
+  int dev = 0, smem_max = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (shm > (size_t)smem_max) return 0;
+  if (cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess)
+    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)kern, wpb * 32, shm) != cudaSuccess) return 0;
+  return per_sm * tpb;
 }
 
 template <int TEAM, int PER>
@@ -233,6 +285,10 @@ int PPB_CAT(launch_react_, PPB_NS)(const DeviceMechanism& m, const Options& o, i
                                    Batch b, double dt, int* queue, cudaStream_t st)
 {
   return launch_react_ns<PPB_NS>(m, o, method, lc, b, dt, queue, st);
+}
+int PPB_CAT(react_occupancy_, PPB_NS)(const DevMech& M, int method, const LaunchConfig& lc)
+{
+  return occupancy_ns<PPB_NS>(M, method, lc);
 }
 int PPB_CAT(launch_ajacobian_, PPB_NS)(const DevMech& M, const double* sc, const double* T, int consP, double* J,
                                        int ncells, int team, cudaStream_t st)

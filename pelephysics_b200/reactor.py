@@ -97,6 +97,14 @@ class Reactor:
             check(code)
         return cost.value, dt.value, t.value, code
 
+    def launch_config(self):
+        """(warps_per_block, team_lanes, register_budget, tuned_ms) of the
+        tuned engine (after the autotuner ran when warps_per_block was 0)."""
+        w, t, rb = C.c_int(), C.c_int(), C.c_int()
+        ms = C.c_double()
+        check(lib().ppb_get_launch_config(self._h, C.byref(w), C.byref(t), C.byref(rb), C.byref(ms)))
+        return w.value, t.value, rb.value, ms.value
+
     # ---- differentiation (no counterpart in the reference)
     def get_arrhenius(self):
         """Forward Arrhenius parameters (A in SI units, beta, Ea/R in K)."""

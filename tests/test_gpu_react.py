@@ -274,3 +274,35 @@ def test_empty_batch(cuda):
     e = np.zeros((0, 10))
     cost, dt, t, code = r.react(e, np.zeros((0, 9)), np.zeros(0), np.zeros(0), 1e-5, 1.0, ncells=0)
     assert code == 0 and cost == 0 and abs(t - (1.0 + 1e-5)) < 1e-15
+
+
+@pytest.mark.parametrize("mech", ["LiDryer", "drm19"])
+def test_autotuner_choice_is_reproducible(cuda, oracle, mech):
+    """warps_per_block = 0: the first react times the candidate launch
+    configurations (block size, lanes per cell, register budget) on the batch
+    and keeps the fastest; a reactor given that configuration explicitly
+    computes the same bits, and both meet the oracle bar."""
+    torch = cuda
+    rtype, dt, nc = 1, 1e-5, 600
+    rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 6, 1000.0, 800.0, 0.5, 1.5)
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5)
+    ra = Reactor(mech)
+    ra.init(rtype, nc, **opts)
+    y = torch.as_tensor(rY, device="cuda").contiguous()
+    x = torch.as_tensor(rX, device="cuda")
+    s = torch.as_tensor(src, device="cuda").contiguous()
+    xs = torch.as_tensor(rXs, device="cuda")
+    ra.react(y, s, x, xs, dt)
+    wpb, team, regs, ms = ra.launch_config()
+    assert ms > 0 and wpb in (1, 2, 4, 8) and team in (16, 32) and regs in (1, 2)
+    rb = Reactor(mech)
+    rb.init(rtype, nc, **opts, warps_per_block=wpb, team_lanes=team, register_budget=regs)
+    assert rb.launch_config()[:3] == (wpb, team, regs)
+    y2 = torch.as_tensor(rY, device="cuda").contiguous()
+    x2 = torch.as_tensor(rX, device="cuda")
+    rb.react(y2, s, x2, xs, dt)
+    np.testing.assert_array_equal(y.cpu().numpy(), y2.cpu().numpy())
+    sub = slice(0, 64)
+    ref, _, flag, _, _ = oracle_react(oracle, mech, rtype, rY[sub], src[sub], rX[sub], rXs[sub], dt, **opts)
+    compare(y.cpu().numpy()[sub], ref)
+
