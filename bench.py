@@ -224,7 +224,11 @@ def our_arm(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
 
     r = Reactor(MECH)
-    r.init(1, n, engine=1, **OPTS)
+    launch = {}
+    if args.launch:
+        w_, t_, g_ = (int(v) for v in args.launch.split(","))
+        launch = dict(warps_per_block=w_, team_lanes=t_, register_budget=g_)
+    r.init(1, n, engine=1, **OPTS, **launch)
     stream = torch.cuda.current_stream(dev)
 
     def step():
@@ -273,7 +277,7 @@ def our_arm(args):
     hs[:] = cells.rYsrc
     hxs[:] = cells.rX_src
     re2e = Reactor(MECH)
-    re2e.init(1, n, engine=1, **OPTS)
+    re2e.init(1, n, engine=1, **OPTS, **launch)
     hy[:] = cells.rY
     hx[:] = cells.rX
     re2e.react(hy, hs, hx, hxs, DT)  # warm
@@ -405,9 +409,10 @@ def adjoint_measure(dev, ncells):
     y0, s, x0, xs = g(cells.rY), g(cells.rYsrc), g(cells.rX), g(cells.rX_src)
     r = Reactor(MECH)
     r.init(2, n, engine=1, **OPTS)
-    # warm-up on a few cells (allocations, graph capture)
-    yw, xw = y0[:256].clone(), x0[:256].clone()
-    r.react(yw, s[:256].contiguous(), xw, xs[:256].contiguous(), t_end)
+    # warm-up: the full batch once (autotuner, graph capture), the adjoint on
+    # a few cells (its scratch)
+    yw, xw = y0.clone(), x0.clone()
+    r.react(yw, s, xw, xs, t_end)
     r.adjoint(y0[:256].contiguous(), s[:256].contiguous(), x0[:256].contiguous(), xs[:256].contiguous(), t_end,
               torch.zeros_like(y0[:256]))
     torch.cuda.synchronize()
@@ -643,6 +648,40 @@ def phase_probe(edge=64, engine=1, lu_fp32=0):
     return 0
 
 
+def adjoint_phase_probe(ncells):
+    """Cycle totals of the adjoint kernel's parts on the adjoint workload
+    (needs the profiling build: PPB_LIB=pelephysics_b200/libppb200_phase.so)."""
+    import ctypes as C
+
+    import torch
+
+    from pelephysics_b200 import _lib, workloads as wl
+    from pelephysics_b200.reactor import Reactor
+
+    L = _lib.lib()
+    if not hasattr(L, "ppb_adjoint_phase_cycles"):
+        raise SystemExit("needs PPB_LIB=pelephysics_b200/libppb200_phase.so")
+    cells = wl.drm19_adjoint(ncells)
+    n = cells.rY.shape[0]
+    g = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    r = Reactor(MECH)
+    r.init(2, n, engine=1, use_graph=0, **OPTS)
+    y = g(cells.rY)
+    lam = torch.ones_like(y)
+    buf = (C.c_ulonglong * 8)()
+    r.adjoint(y, g(cells.rYsrc), g(cells.rX), g(cells.rX_src), cells.dt, lam)
+    torch.cuda.synchronize()
+    L.ppb_adjoint_phase_cycles(buf, 1)
+    r.adjoint(y, g(cells.rYsrc), g(cells.rX), g(cells.rX_src), cells.dt, lam)
+    torch.cuda.synchronize()
+    L.ppb_adjoint_phase_cycles(buf, 1)
+    names = ["forward", "recompute", "sweep", "exact_jacobian", "factor_solve", "save", "restore", "cell"]
+    tot = buf[7]
+    print(json.dumps({"adjoint_phase_probe": {k: {"cycles_per_cell": buf[i] / n, "frac": buf[i] / tot}
+                                              for i, k in enumerate(names)}, "cells": n}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -655,9 +694,13 @@ def main():
     ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane"],
                     help="drm19: the headline line; dodecane / heptane: the larger configurations")
     ap.add_argument("--sample", type=int, default=256, help="oracle sample cells for --config dodecane/heptane")
+    ap.add_argument("--launch", default="", help="W,T,R: fixed warps per block, lanes per cell, register budget "
+                                                 "instead of the autotuner (profiling runs)")
     ap.add_argument("--edge", type=int, default=64, help="field edge (profiling runs use a smaller box)")
     ap.add_argument("--phase-probe", action="store_true",
                     help="per-phase cycle counters of one react (profiling build, PPB_LIB)")
+    ap.add_argument("--adjoint-phase-probe", action="store_true",
+                    help="cycle totals of the adjoint kernel's parts (profiling build, PPB_LIB)")
     ap.add_argument("--kernel-probe", action="store_true",
                     help="time the pointwise RHS / Jacobian / rate kernels on the field's cells")
     ap.add_argument("--flops-probe", action="store_true",
@@ -669,6 +712,8 @@ def main():
         return kernel_probe()
     if args.phase_probe:
         return phase_probe(args.edge)
+    if args.adjoint_phase_probe:
+        return adjoint_phase_probe(args.adjoint_cells)
     if args.impl == "reference":
         return reference_arm(args)
     if args.config != "drm19":

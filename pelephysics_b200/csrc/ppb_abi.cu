@@ -111,6 +111,11 @@ struct ppb_reactor {
   // adjoint scratch (grown on demand)
   void *adj_cp = nullptr, *adj_tape = nullptr, *adj_ys = nullptr, *adj_gw = nullptr;
   size_t adj_cp_bytes = 0, adj_tape_bytes = 0, adj_ys_bytes = 0, adj_gw_bytes = 0;
+  // batched reverse sweep
+  void *adj_yinfo = nullptr, *adj_cpidx = nullptr, *adj_ints = nullptr, *adj_dbl = nullptr, *adj_lam = nullptr,
+       *adj_items = nullptr, *adj_ioff = nullptr;
+  size_t adj_yinfo_bytes = 0, adj_cpidx_bytes = 0, adj_ints_bytes = 0, adj_dbl_bytes = 0, adj_lam_bytes = 0,
+         adj_items_bytes = 0, adj_ioff_bytes = 0;
 };
 
 static void free_adjoint_scratch(ppb_reactor* r)
@@ -121,6 +126,12 @@ static void free_adjoint_scratch(ppb_reactor* r)
   cudaFree(r->adj_gw);
   r->adj_cp = r->adj_tape = r->adj_ys = r->adj_gw = nullptr;
   r->adj_cp_bytes = r->adj_tape_bytes = r->adj_ys_bytes = r->adj_gw_bytes = 0;
+  for (void** q : {&r->adj_yinfo, &r->adj_cpidx, &r->adj_ints, &r->adj_dbl, &r->adj_lam, &r->adj_items, &r->adj_ioff}) {
+    cudaFree(*q);
+    *q = nullptr;
+  }
+  r->adj_yinfo_bytes = r->adj_cpidx_bytes = r->adj_ints_bytes = r->adj_dbl_bytes = r->adj_lam_bytes = 0;
+  r->adj_items_bytes = r->adj_ioff_bytes = 0;
 }
 
 static int grow(void*& p, size_t& cap, size_t bytes)
@@ -204,24 +215,34 @@ struct TuneEntry {
   int dev, method, rtype, lu_fp32, typ;
   LaunchConfig lc;
   double ms;
+  int sample, target; // cells timed, and the sample size wanted (four resident waves)
 };
 static std::mutex g_tune_mu;
 static std::vector<TuneEntry> g_tune;
 
-static bool tuned_config(const ppb_reactor* r, LaunchConfig* lc, double* ms)
+static TuneEntry* find_tune(const ppb_reactor* r)
 {
   int dev = 0;
   cudaGetDevice(&dev);
-  std::lock_guard<std::mutex> lk(g_tune_mu);
-  for (const auto& e : g_tune) {
+  for (auto& e : g_tune) {
     if (e.t == r->dm->host && e.dev == dev && e.method == r->method && e.rtype == r->reactor_type &&
-        e.lu_fp32 == r->opt.lu_fp32 && e.typ == (int)!r->typ_vals.empty()) {
-      *lc = e.lc;
-      if (ms) *ms = e.ms;
-      return true;
-    }
+        e.lu_fp32 == r->opt.lu_fp32 && e.typ == (int)!r->typ_vals.empty())
+      return &e;
   }
-  return false;
+  return nullptr;
+}
+
+static bool tuned_config(const ppb_reactor* r, LaunchConfig* lc, double* ms, int* sample = nullptr,
+                         int* target = nullptr)
+{
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  const TuneEntry* e = find_tune(r);
+  if (!e) return false;
+  *lc = e->lc;
+  if (ms) *ms = e->ms;
+  if (sample) *sample = e->sample;
+  if (target) *target = e->target;
+  return true;
 }
 
 static LaunchConfig launch_config(const ppb_reactor* r)
@@ -251,13 +272,15 @@ static LaunchConfig launch_config(const ppb_reactor* r)
 }
 
 // Time the candidate configurations on a copy of (up to) four resident
-// waves of the batch's first cells and cache the fastest.  Not during a
-// stream capture (the caller checks).
+// waves of the batch's first cells and cache the fastest; a batch that gives
+// at least twice the cells of an earlier, smaller-than-wanted sample tunes
+// again.  Not during a stream capture (the caller checks).
 static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
 {
   if (r->opt.engine != PPB_ENGINE_TUNED || r->opt.warps_per_block > 0) return 0;
   LaunchConfig have;
-  if (tuned_config(r, &have, nullptr)) return 0;
+  int had = 0, want = 0;
+  if (tuned_config(r, &have, nullptr, &had, &want) && (had >= want || b.ncells < 2 * had)) return 0;
   const int N = r->t->nsp, n = N + 1;
   std::vector<LaunchConfig> cand;
   int max_res = 0;
@@ -341,9 +364,19 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
   }
   cleanup();
   if (err) return cuda_fail(err, "autotune");
-  TuneEntry te{r->dm->host, dev, r->method, r->reactor_type, r->opt.lu_fp32, (int)!r->typ_vals.empty(), pick, best};
+  const int target = (int)std::min<long>(1L << 30, 4L * max_res * nsm);
+  TuneEntry te{r->dm->host, dev, r->method, r->reactor_type, r->opt.lu_fp32, (int)!r->typ_vals.empty(), pick, best,
+               m, target};
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune.push_back(te);
+  if (TuneEntry* e = find_tune(r)) {
+    *e = te;
+  } else {
+    g_tune.push_back(te);
+  }
+  if (r->gexec) { // a graph captured with the earlier choice
+    cudaGraphExecDestroy(r->gexec);
+    r->gexec = nullptr;
+  }
   return 0;
 }
 
@@ -401,7 +434,7 @@ void ppb_default_options(ppb_options* o)
   o->warps_per_block = 0;
   o->use_graph = 1;
   o->adjoint_checkpoint_interval = 16;
-  o->adjoint_memory_mb = 8192;
+  o->adjoint_memory_mb = 16384;
   o->team_lanes = 32;
   o->register_budget = 2;
 }
@@ -863,6 +896,99 @@ int ppb_set_arrhenius(ppb_reactor* r, const double* A, const double* beta, const
   return 0;
 }
 
+static int grow_items(void* ctx, void** p, size_t bytes)
+{
+  ppb_reactor* r = static_cast<ppb_reactor*>(ctx);
+  r->adj_items = *p;
+  const int e = grow(r->adj_items, r->adj_items_bytes, bytes);
+  *p = r->adj_items;
+  return e;
+}
+
+// The adjoint integration, batched over cells segment by segment (chunks of
+// cells within adjoint_memory_mb).
+static int run_adjoint_batched(ppb_reactor* r, AdjBatch b, double dt, double* grad, cudaStream_t st)
+{
+  const int N = r->t->nsp, n = N + 1, R = r->t->nrxn;
+  const int seg = r->opt.adjoint_checkpoint_interval > 0 ? r->opt.adjoint_checkpoint_interval : 16;
+  AdjCells C{};
+  C.seg_steps = seg;
+  C.close_rec = 128;
+  C.cap_rec = C.close_rec + 2 * (r->opt.max_err_fails + 10) + 8;
+  C.close_y = 32;
+  C.cap_y = C.close_y + r->opt.max_err_fails + 2;
+  C.max_seg = r->opt.max_steps / seg + 2;
+  C.cp_stride = adj_cp_bytes(N, r->opt.lu_fp32);
+  const size_t item_b = adj_item_bytes(N, R);
+  const size_t budget = (size_t)(r->opt.adjoint_memory_mb > 0 ? r->opt.adjoint_memory_mb : 16384) << 20;
+  const size_t per_cell = (size_t)C.max_seg * 4 + (size_t)C.cap_rec * ADJ_TAPE_BYTES + (size_t)C.cap_y * (8 * n + 16) +
+                          3 * 4 + 8 + (size_t)7 * n * 8 + 8 + (size_t)3 * R * 8 + 4;
+  const long cells = std::max<long>(1, std::min<long>(b.ncells, (long)(budget * 2 / 5 / per_cell)));
+  const size_t pool_bytes = budget * 7 / 20;
+  C.pool_cap = (int)std::min<size_t>(pool_bytes / C.cp_stride, 1u << 30);
+  C.items_cap = std::max<long>((long)(budget / 4 / item_b), C.cap_y + 1);
+  if (C.pool_cap < 2) return fail(PPB_E_ARG, "adjoint: adjoint_memory_mb too small for the checkpoints");
+  const size_t nc = (size_t)cells;
+  int e;
+  if ((e = grow(r->adj_cp, r->adj_cp_bytes, (size_t)C.pool_cap * C.cp_stride + 16)) ||
+      (e = grow(r->adj_cpidx, r->adj_cpidx_bytes, nc * C.max_seg * 4)) ||
+      (e = grow(r->adj_tape, r->adj_tape_bytes, nc * C.cap_rec * ADJ_TAPE_BYTES)) ||
+      (e = grow(r->adj_ys, r->adj_ys_bytes, nc * C.cap_y * n * 8)) ||
+      (e = grow(r->adj_yinfo, r->adj_yinfo_bytes, nc * C.cap_y * 16)) ||
+      (e = grow(r->adj_ints, r->adj_ints_bytes, nc * 3 * 4 + 16)) ||
+      (e = grow(r->adj_dbl, r->adj_dbl_bytes, nc * 2 * 8)) || (e = grow(r->adj_lam, r->adj_lam_bytes, nc * 7 * n * 8)) ||
+      (e = grow(r->adj_gw, r->adj_gw_bytes, nc * 3 * R * 8)) ||
+      (e = grow(r->adj_items, r->adj_items_bytes, (size_t)C.items_cap * item_b)) ||
+      (e = grow(r->adj_ioff, r->adj_ioff_bytes, (nc + 1) * 4)))
+    return e;
+  C.cp_pool = (char*)r->adj_cp;
+  C.pool_next = (int*)((char*)r->adj_cp + (size_t)C.pool_cap * C.cp_stride);
+  C.cp_idx = (int*)r->adj_cpidx;
+  C.tape = r->adj_tape;
+  C.ys = (double*)r->adj_ys;
+  C.yinfo = (double*)r->adj_yinfo;
+  C.nrec = (int*)r->adj_ints;
+  C.ny = C.nrec + nc;
+  C.nseg = C.ny + nc;
+  C.h0 = (double*)r->adj_dbl;
+  C.lamE = C.h0 + nc;
+  C.lam = (double*)r->adj_lam;
+  C.gw = (double*)r->adj_gw;
+  C.items = (double*)r->adj_items;
+  C.item_off = (int*)r->adj_ioff;
+  b.atolv = r->atolv;
+  b.status = r->status;
+  b.stats = r->stats;
+  const Options o = engine_options(r);
+  for (long c0 = 0; c0 < b.ncells; c0 += cells) {
+    AdjBatch bc = b;
+    const size_t cn = (size_t)c0 * n, cN = (size_t)c0 * N;
+    bc.ncells = (int)std::min<long>(cells, b.ncells - c0);
+    bc.y0 = b.y0 + cn;
+    bc.src = b.src ? b.src + cN : nullptr;
+    bc.rhoe = b.rhoe + c0;
+    bc.rhoesrc = b.rhoesrc ? b.rhoesrc + c0 : nullptr;
+    bc.lam_y = b.lam_y + cn;
+    bc.y_out = b.y_out ? b.y_out + cn : nullptr;
+    bc.lam_y0 = b.lam_y0 ? b.lam_y0 + cn : nullptr;
+    bc.lam_e = b.lam_e ? b.lam_e + c0 : nullptr;
+    bc.status = b.status + c0;
+    bc.stats = b.stats + (size_t)c0 * 7;
+    e = launch_adjoint_batched(*r->dm, o, r->opt.lu_fp32, bc, C, dt, r->queue, grad, c0 > 0 ? 1 : 0, grow_items, r,
+                               st);
+    if (e) return cuda_fail(e, "launch_adjoint_batched");
+  }
+  r->last_ncells = b.ncells;
+  std::vector<int> stat(b.ncells);
+  PPB_CUDA(cudaMemcpyAsync(stat.data(), r->status, (size_t)b.ncells * 4, cudaMemcpyDeviceToHost, st),
+           "cudaMemcpyAsync");
+  PPB_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  int bad = 0;
+  for (int c = 0; c < b.ncells; c++) bad += stat[c] < 0;
+  if (bad) return fail(PPB_E_INTEGRATE, std::to_string(bad) + " cell(s) failed in the adjoint integration");
+  return 0;
+}
+
 // Shared set-up and launch of the adjoint (mode ADJ_REVERSE) and tangent
 // (ADJ_TANGENT) integrations.
 static int run_adjoint(ppb_reactor* r, int mode, AdjBatch b, double dt, double* grad, cudaStream_t st)
@@ -879,6 +1005,7 @@ static int run_adjoint(ppb_reactor* r, int mode, AdjBatch b, double dt, double* 
   }
   int e = ensure_scratch(r, b.ncells);
   if (e) return e;
+  if (mode == ADJ_REVERSE) return run_adjoint_batched(r, b, dt, grad, st);
   const int N = r->t->nsp, n = N + 1, R = r->t->nrxn;
   AdjPlan p;
   e = plan_adjoint(*r->dm, mode, r->opt.lu_fp32, &p);
@@ -1070,6 +1197,10 @@ int ppb_pyt2re(const char* mechanism, int eh, const double* P, const double* T, 
 #ifdef PPB_PHASE_TIMERS
 // Profiling builds only: per-phase cycle totals of the BDF kernels.
 int ppb_phase_cycles(unsigned long long* out, int reset) { return cuda_fail(phase_cycles(out, reset), "phase"); }
+int ppb_adjoint_phase_cycles(unsigned long long* out, int reset)
+{
+  return cuda_fail(adj_phase_cycles(out, reset), "adjoint phase");
+}
 #endif
 
 } // extern "C"

@@ -37,7 +37,19 @@
 
 namespace ppb {
 
-enum { ST_ADJ_CAPACITY = -40, ST_ADJ_SINGULAR = -41 };
+enum { ST_ADJ_CAPACITY = -40, ST_ADJ_SINGULAR = -41, ST_ADJ_REPLAY = -42 };
+
+// Profiling builds (-DPPB_PHASE_TIMERS): clock64() totals of the adjoint's
+// parts (forward, recomputation, sweeps, exact Jacobians, factor + solve,
+// checkpoint save, restore, whole cell), one accumulator set per lane.
+enum AdjPhase { AP_FWD = 0, AP_REPLAY, AP_SWEEP, AP_POINT, AP_LU, AP_SAVE, AP_RESTORE, AP_CELL, AP_COUNT };
+#ifdef PPB_PHASE_TIMERS
+#define PPB_ATIC(ph) const long long _atic_##ph = clock64()
+#define PPB_ATOC(acc, ph) (acc)[ph] += clock64() - _atic_##ph
+#else
+#define PPB_ATIC(ph)
+#define PPB_ATOC(acc, ph)
+#endif
 
 enum TapeOp : int {
   TP_FRESET = 1,
@@ -64,7 +76,8 @@ template <int TEAM>
 struct AdjRec {
   static constexpr bool on = true;
   TapeRec* tape = nullptr;
-  double* ys = nullptr; // [cap_y][n] states at which f was differentiated
+  double* ys = nullptr;    // [cap_y][n] states at which f was differentiated
+  double* yinfo = nullptr; // [cap_y][2] their time and gamma (0: no matrix), or nullptr
   int n = 0;
   int nrec = 0, ny = 0, nsteps = 0;
   int seg_steps = 16, close_rec = 0, close_y = 0;
@@ -106,6 +119,10 @@ struct AdjRec {
     double c[9] = {tn, gamma, rl1, 0, 0, 0, 0, 0, 0};
     for (int j = 0; j <= q; j++) c[3 + j] = l[j];
     put(tm, TP_CORRECT, q, save ? 1 : 0, ny, c, 9);
+    if (yinfo && tm.lane == 0) {
+      yinfo[2 * ny] = tn;
+      yinfo[2 * ny + 1] = gamma;
+    }
     ny++;
     nsteps++;
   }
@@ -128,6 +145,10 @@ struct AdjRec {
     for (int i = tm.lane; i < n; i += TEAM) yv[i] = z0[i];
     const double c[2] = {tn, h};
     put(tm, TP_FRESET, 1, 0, ny, c, 2);
+    if (yinfo && tm.lane == 0) {
+      yinfo[2 * ny] = tn;
+      yinfo[2 * ny + 1] = 0.0;
+    }
     ny++;
   }
   __device__ void output(const Team<TEAM>& tm, int q, double sfac)
@@ -152,7 +173,7 @@ struct AdjWork {
   double* tmp;  // [n]
   double* Jc;   // [n * n] df/dy, column-major Jc[j*n + i] = d f_i / d y_j
   double* AT;   // [n * n] FP64 LU of I - gamma Jc or of its transpose
-  double* jxa;  // [6R] per-reaction factors kf, kr, fac, dq/dT, dq/dlnk, (jvp)
+  double* jxa;  // [5R] per-reaction factors kf, kr, fac, dq/dT, dq/dlnk
   double* gacc; // [3R] parameter gradient of this warp's cells
   int* piv;     // [n]
 };
@@ -175,7 +196,7 @@ template <typename LT>
 __host__ __device__ inline size_t adj_rev_bytes(int N, int R)
 {
   const size_t n = N + 1;
-  size_t d = 7 * n + 6 * (size_t)R;
+  size_t d = 7 * n;
   if (sizeof(LT) != sizeof(double)) d += n * n;
   return (d * 8 + 15) & ~size_t(15);
 }
@@ -187,7 +208,9 @@ __device__ inline void carve_adj_rev(AdjWork& a, char* base, Work<LT>& w, int N,
   double* p = (double*)base;
   a.lam = p; p += 6 * n;
   a.pend = p; p += n;
-  a.jxa = p; p += 6 * (size_t)R;
+  // the per-reaction factors (5 R doubles) and then the FP64 factor of the
+  // adjoint matrix share the Newton-matrix region
+  a.jxa = reinterpret_cast<double*>(w.A);
   a.AT = (sizeof(LT) == sizeof(double)) ? reinterpret_cast<double*>(w.A) : p;
   a.Jc = w.J;
   a.piv = w.piv;
@@ -283,11 +306,11 @@ __device__ AdjPoint rhs_exact_jacobian(const Team<TEAM>& tm, const DevMech& M, i
     const RxJac f =
       rx_jac_packed(M, p, T, pt.invT, pt.invT * pt.invT, pt.logT, refC, refCinv, mixture, w.sc, w.g, w.h1);
     w.qd[r] = f.q;
-    a.jxa[6 * r + 0] = f.kf;
-    a.jxa[6 * r + 1] = f.kr;
-    a.jxa[6 * r + 2] = f.fac;
-    a.jxa[6 * r + 3] = f.dqdT;
-    a.jxa[6 * r + 4] = f.q * f.dlnk;
+    a.jxa[5 * r + 0] = f.kf;
+    a.jxa[5 * r + 1] = f.kr;
+    a.jxa[5 * r + 2] = f.fac;
+    a.jxa[5 * r + 3] = f.dqdT;
+    a.jxa[5 * r + 4] = f.q * f.dlnk;
   }
   tm.sync();
   // wdot and d wdot / dT (held in column N until the assembly)
@@ -298,41 +321,57 @@ __device__ AdjPoint rhs_exact_jacobian(const Team<TEAM>& tm, const DevMech& M, i
       const int r = __ldg(M.jg_rx + gi);
       const double nu = __ldg(M.jg_c + gi);
       wd += nu * w.qd[r];
-      d += nu * a.jxa[6 * r + 3];
+      d += nu * a.jxa[5 * r + 3];
     }
     w.wdot[s] = wd;
     a.Jc[N * n + s] = d;
   }
-  // exact d wdot / d c: lane l owns columns l, l+TEAM, ... and walks the
-  // reactions that reach its column
+  tm.sync();
+  // from here on qd holds dq/d ln k (the parameter derivatives outlive the
+  // per-reaction factors, whose storage the Newton-matrix factor may reuse)
+  for (int r = tm.lane; r < R; r += TEAM) w.qd[r] = a.jxa[5 * r + 4];
+  // third-body / fall-off terms: a rank-one update e_k fac_r nu_r per
+  // reaction, all lanes on the same reaction, lane l on columns l, l+TEAM, ..
+  {
+    const int na = __ldg(M.al_off + 1);
+    for (int ai = 0; ai < na; ai++) {
+      const int r = __ldg(M.al_rx + ai);
+      const RxPack p = load_rx(M, r);
+      const double fac = a.jxa[5 * r + 2];
+      const double* ed = M.effd + (size_t)p.aslot * N;
+#pragma unroll
+      for (int qq = 0; qq < PER; qq++) {
+        const int k = tm.lane + qq * TEAM;
+        if (k >= N) break;
+        const double d = __ldg(ed + k) * fac;
+        if (d == 0.0) continue;
+        double* Jk = a.Jc + k * n;
+        for (int j = 0; j < p.njn; j++) {
+          const double nu = (double)p.jnc[j];
+          if (nu != 0) Jk[p.jns[j]] += nu * d;
+        }
+      }
+    }
+  }
+  // phase-space terms: lane l owns columns l, l+TEAM, ... and walks the
+  // reactions with its species in their phase space
 #pragma unroll
   for (int qq = 0; qq < PER; qq++) {
     const int k = tm.lane + qq * TEAM;
     if (k >= N) break;
     double* Jk = a.Jc + k * n;
-    const unsigned word_i = (unsigned)(k >> 5), bit = 1u << (k & 31);
-    const int e1 = __ldg(M.jc_off + k + 1);
-    for (int ei = __ldg(M.jc_off + k); ei < e1; ei++) {
-      const int r = __ldg(M.jc_rx + ei);
+    const int e1 = __ldg(M.jm_off + k + 1);
+    for (int ei = __ldg(M.jm_off + k); ei < e1; ei++) {
+      const int r = __ldg(M.jm_rx + ei);
       const RxPack p = load_rx(M, r);
-      const bool has_alpha = (p.kind == PPB_RX_THIRD) || (p.fo != 255);
       const bool inr = slots_has(p.fsp, k);
       const bool inp = (p.rev != 0) && slots_has(p.rsp, k);
       double d = 0.0;
-      bool apply = inr || inp;
-      if (has_alpha) {
-        const bool listed = (__ldg(M.effmask + 4 * r + word_i) & bit) != 0u;
-        const double e = listed ? __ldg(M.effd + (size_t)p.aslot * N + k) : 1.0;
-        d = e * a.jxa[6 * r + 2];
-        apply = apply || (e != 0.0);
-      }
-      if (inr) d += a.jxa[6 * r + 0] * slots_dproduct(p.fsp, w.sc, k);
-      if (inp) d -= a.jxa[6 * r + 1] * slots_dproduct(p.rsp, w.sc, k);
-      if (apply) {
-        for (int j = 0; j < p.njn; j++) {
-          const double nu = (double)p.jnc[j];
-          if (nu != 0) Jk[p.jns[j]] += nu * d;
-        }
+      if (inr) d += a.jxa[5 * r + 0] * slots_dproduct(p.fsp, w.sc, k);
+      if (inp) d -= a.jxa[5 * r + 1] * slots_dproduct(p.rsp, w.sc, k);
+      for (int j = 0; j < p.njn; j++) {
+        const double nu = (double)p.jnc[j];
+        if (nu != 0) Jk[p.jns[j]] += nu * d;
       }
     }
   }
@@ -429,8 +468,8 @@ __device__ __noinline__ void adj_solve(const Team<TEAM>& tm, const double* A, in
 // Parameter vector-Jacobian product at the last rhs_exact_jacobian point:
 // gacc += scale * (df/dp)^T u, p = (ln A_r, beta_r, Ea_r / R) per reaction.
 template <int TEAM>
-__device__ void param_vjp(const Team<TEAM>& tm, const DevMech& M, const AdjPoint& pt, AdjWork& a, const double* u,
-                          double scale)
+__device__ void param_vjp(const Team<TEAM>& tm, const DevMech& M, const AdjPoint& pt, AdjWork& a,
+                          const double* dqdlnk, const double* u, double scale)
 {
   const int N = M.nsp, R = M.nrxn;
   // species weights: d(u . f)/d wdot_k (f_N depends on wdot through the
@@ -445,7 +484,7 @@ __device__ void param_vjp(const Team<TEAM>& tm, const DevMech& M, const AdjPoint
 #pragma unroll
     for (int j = 0; j < 6; j++)
       if (p.jnc[j]) g += (double)p.jnc[j] * a.v[p.jns[j]];
-    g *= scale * a.jxa[6 * r + 4];
+    g *= scale * dqdlnk[r];
     a.gacc[r] += g;
     a.gacc[R + r] += g * pt.logT;
     a.gacc[2 * R + r] -= g * pt.invT;
@@ -456,18 +495,19 @@ __device__ void param_vjp(const Team<TEAM>& tm, const DevMech& M, const AdjPoint
 // Parameter Jacobian-vector product: out = (df/dp) dp at the last
 // rhs_exact_jacobian point (dp = [d ln A | d beta | d Ea/R]).
 template <int TEAM>
-__device__ void param_jvp(const Team<TEAM>& tm, const DevMech& M, const AdjPoint& pt, AdjWork& a, const double* dp,
-                          double* out)
+__device__ void param_jvp(const Team<TEAM>& tm, const DevMech& M, const AdjPoint& pt, AdjWork& a,
+                          const double* dqdlnk, const double* dp, double* out)
 {
   const int N = M.nsp, R = M.nrxn;
+  // a.jxa is free once the Jacobian is assembled: the rate tangents
   for (int r = tm.lane; r < R; r += TEAM)
-    a.jxa[6 * r + 5] = a.jxa[6 * r + 4] * (__ldg(dp + r) + pt.logT * __ldg(dp + R + r) - pt.invT * __ldg(dp + 2 * R + r));
+    a.jxa[r] = dqdlnk[r] * (__ldg(dp + r) + pt.logT * __ldg(dp + R + r) - pt.invT * __ldg(dp + 2 * R + r));
   tm.sync();
   double ae = 0.0;
   for (int k = tm.lane; k < N; k += TEAM) {
     double sk = 0.0;
     const int g1 = __ldg(M.jg_off + k + 1);
-    for (int gi = __ldg(M.jg_off + k); gi < g1; gi++) sk += __ldg(M.jg_c + gi) * a.jxa[6 * __ldg(M.jg_rx + gi) + 5];
+    for (int gi = __ldg(M.jg_off + k); gi < g1; gi++) sk += __ldg(M.jg_c + gi) * a.jxa[__ldg(M.jg_rx + gi)];
     const double ok = 1.0e-6 * __ldg(M.mw + k) * sk;
     out[k] = ok;
     ae += ok * a.ek[k];
@@ -476,6 +516,79 @@ __device__ void param_jvp(const Team<TEAM>& tm, const DevMech& M, const AdjPoint
   tm.sync();
   if (tm.lane == 0) out[N] = oN;
   tm.sync();
+}
+
+// The transposes of the operations that do not touch f (output, saved
+// correction, predict, rescale, order change) on the adjoint history lam and
+// pending correction adjoint pend; false for TP_CORRECT / TP_FRESET.
+template <int TEAM>
+__device__ bool rev_linear(const Team<TEAM>& tm, int n, int qmax, const TapeRec& R, AdjWork& a, const double* lam_y)
+{
+  const int q = R.q;
+  switch (R.op) {
+  case TP_OUTPUT: {
+    // y(tout) = sum_j s^j z_j
+    for (int i = tm.lane; i < n; i += TEAM) {
+      double pw = 1.0;
+      for (int j = 0; j <= q; j++) {
+        a.lam[j * n + i] += pw * lam_y[i];
+        pw *= R.c[0];
+      }
+    }
+    tm.sync();
+    break;
+  }
+  case TP_SAVEQMAX: {
+    for (int i = tm.lane; i < n; i += TEAM) {
+      a.pend[i] += a.lam[qmax * n + i];
+      a.lam[qmax * n + i] = 0.0;
+    }
+    tm.sync();
+    break;
+  }
+  case TP_PREDICT: {
+    // forward: for k = 1..q, j = q..k: z_{j-1} += z_j
+    for (int i = tm.lane; i < n; i += TEAM)
+      for (int kk = q; kk >= 1; kk--)
+        for (int j = kk; j <= q; j++) a.lam[j * n + i] += a.lam[(j - 1) * n + i];
+    tm.sync();
+    break;
+  }
+  case TP_RESCALE: {
+    for (int i = tm.lane; i < n; i += TEAM) {
+      double f = R.c[0];
+      for (int j = 1; j <= q; j++) {
+        a.lam[j * n + i] *= f;
+        f *= R.c[0];
+      }
+    }
+    tm.sync();
+    break;
+  }
+  case TP_INCREASE: {
+    const int L = R.i1, idx = R.i2;
+    for (int i = tm.lane; i < n; i += TEAM) {
+      double lz = a.lam[L * n + i];
+      for (int j = 2; j <= q; j++) lz += R.c[j - 1] * a.lam[j * n + i];
+      a.lam[L * n + i] = 0.0;
+      a.lam[idx * n + i] += R.c[0] * lz;
+    }
+    tm.sync();
+    break;
+  }
+  case TP_DECREASE: {
+    for (int i = tm.lane; i < n; i += TEAM) {
+      double s = 0.0;
+      for (int j = 2; j < q; j++) s += R.c[j - 2] * a.lam[j * n + i];
+      a.lam[q * n + i] -= s;
+    }
+    tm.sync();
+    break;
+  }
+  default:
+    return false;
+  }
+  return true;
 }
 
 // Sweeps over one tape segment.  lam holds the adjoint (reverse) or the
@@ -491,6 +604,7 @@ struct AdjSweep {
   AdjWork& a;
   CellIn cin;
   int n, qmax;
+  long long* acc; // profiling accumulators (AP_*), or nullptr
 
   __device__ __noinline__ AdjPoint point(double t, const double* yg)
   {
@@ -512,7 +626,7 @@ struct AdjSweep {
     double s = 0.0;
     for (int i = tm.lane; i < n; i += TEAM) s += a.fE[i] * a.mu[i];
     lamE += h * tm.sum(s);
-    param_vjp(tm, M, pt, a, a.mu, h);
+    param_vjp(tm, M, pt, a, w.qd, a.mu, h);
   }
 
   __device__ int reverse(const TapeRec* tape, int nrec, const double* ys, const double* lam_y, double& lamE)
@@ -546,9 +660,13 @@ struct AdjSweep {
           a.pend[i] = 0.0;
         }
         tm.sync();
+        PPB_ATIC(AP_POINT);
         const AdjPoint pt = point(tn, ys + (size_t)R.i2 * n);
+        PPB_ATOC(acc, AP_POINT);
+        PPB_ATIC(AP_LU);
         if (adj_factor(tm, n, a.Jc, gamma, true, a.AT, a.piv)) return ST_ADJ_SINGULAR;
         adj_solve<TEAM>(tm, a.AT, n, a.piv, a.mu);
+        PPB_ATOC(acc, AP_LU);
         jc_tmul_add(tm, n, a.Jc, a.mu, gamma, a.lam);
         double s = 0.0;
         for (int i = tm.lane; i < n; i += TEAM) {
@@ -557,7 +675,7 @@ struct AdjSweep {
         }
         lamE += gamma * tm.sum(s);
         tm.sync();
-        param_vjp(tm, M, pt, a, a.mu, gamma);
+        param_vjp(tm, M, pt, a, w.qd, a.mu, gamma);
         break;
       }
       case TP_SAVEQMAX: {
@@ -623,7 +741,7 @@ struct AdjSweep {
   __device__ void tangent_rhs(const AdjPoint& pt, const double* z, double dE, const double* dp, double* out)
   {
     jc_mul(tm, n, a.Jc, z, a.tmp);
-    param_jvp(tm, M, pt, a, dp, out);
+    param_jvp(tm, M, pt, a, w.qd, dp, out);
     for (int i = tm.lane; i < n; i += TEAM) out[i] += a.tmp[i] + a.fE[i] * dE;
     tm.sync();
   }
@@ -718,5 +836,166 @@ struct AdjSweep {
     return ST_OK;
   }
 };
+
+// ---------------------------------------------------------------- batched
+// The batched reverse sweep evaluates, for every differentiated point of a
+// segment of every cell at once, the exact Jacobian, df/dE, the rate
+// derivatives and (for corrections) the FP64 factor of (I - gamma Jc)^T --
+// none of which depends on the adjoint state -- and stores them per point;
+// the sequential sweep then needs only solves and products.
+struct ItemLayout {
+  size_t at, fe, ek, dq, sc, piv, stride; // offsets in doubles
+  __host__ __device__ ItemLayout(int N, int R)
+  {
+    const size_t n = N + 1;
+    at = n * n;
+    fe = 2 * n * n;
+    ek = fe + n;
+    dq = ek + n;
+    sc = dq + (size_t)R;
+    piv = sc + 4;
+    stride = piv + (n + 1) / 2;
+    stride = (stride + 1) & ~size_t(1);
+  }
+};
+
+// shared memory of one item evaluation
+__host__ __device__ inline size_t item_bytes(int N, int R)
+{
+  const size_t n = N + 1;
+  return ((8 * (13 * n + 6 * (size_t)R + 2 * n * n) + 4 * n) + 15) & ~size_t(15);
+}
+
+template <int TEAM, int PER>
+__device__ void eval_item(const Team<TEAM>& tm, const DevMech& M, int rtype, double t, double gamma, const double* yg,
+                          double rhoe, double rhoesrc, const double* srcg, char* smem, double* item,
+                          const ItemLayout& IL)
+{
+  const int N = M.nsp, n = N + 1, R = M.nrxn;
+  double* p = (double*)smem;
+  Work<double> w{};
+  AdjWork a{};
+  w.Y = p; p += n;
+  w.sc = p; p += n;
+  w.g = p; p += n;
+  w.h1 = p; p += n;
+  w.wdot = p; p += n;
+  w.src = p; p += n;
+  w.qd = p; p += R;
+  a.ek = p; p += n;
+  a.cvk = p; p += n;
+  a.dcvk = p; p += n;
+  a.fy = p; p += n;
+  a.fE = p; p += n;
+  a.ybuf = p; p += n;
+  a.Jc = p; p += (size_t)n * n;
+  a.AT = p; p += (size_t)n * n;
+  a.jxa = p; p += 5 * (size_t)R;
+  a.piv = (int*)p;
+  for (int i = tm.lane; i < n; i += TEAM) {
+    a.ybuf[i] = yg[i];
+    w.src[i] = (i < N && srcg) ? srcg[i] : 0.0;
+  }
+  tm.sync();
+  const AdjPoint pt = rhs_exact_jacobian<TEAM, PER, double>(tm, M, rtype, t, a.ybuf, rhoe, rhoesrc, w.src, w, a);
+  int sing = 0;
+  if (gamma != 0.0) sing = adj_factor(tm, n, a.Jc, gamma, true, a.AT, a.piv);
+  for (int i = tm.lane; i < n * n; i += TEAM) item[i] = a.Jc[i];
+  if (gamma != 0.0)
+    for (int i = tm.lane; i < n * n; i += TEAM) item[IL.at + i] = a.AT[i];
+  for (int i = tm.lane; i < n; i += TEAM) {
+    item[IL.fe + i] = a.fE[i];
+    item[IL.ek + i] = a.ek[i];
+  }
+  for (int r = tm.lane; r < R; r += TEAM) item[IL.dq + r] = w.qd[r];
+  int* ip = reinterpret_cast<int*>(item + IL.piv);
+  for (int i = tm.lane; i < n; i += TEAM) ip[i] = (sing && i == 0) ? -1 : a.piv[i];
+  if (tm.lane == 0) {
+    item[IL.sc + 0] = pt.Den;
+    item[IL.sc + 1] = pt.logT;
+    item[IL.sc + 2] = pt.invT;
+    item[IL.sc + 3] = pt.T;
+  }
+}
+
+// z_1 = h f(t, z_0) at a stored point: lam_0 += h Jc^T lam_1, lamE += h fE .
+// lam_1, gradient, lam_1 = 0
+template <int TEAM>
+__device__ void rev_item_freset(const Team<TEAM>& tm, const DevMech& M, int n, AdjWork& a, const double* it,
+                                const ItemLayout& IL, double h, double& lamE)
+{
+  double* l1 = a.lam + n;
+  for (int i = tm.lane; i < n; i += TEAM) a.mu[i] = l1[i];
+  tm.sync();
+  for (int i = tm.lane; i < n; i += TEAM) l1[i] = 0.0;
+  jc_tmul_add(tm, n, it, a.mu, h, a.lam);
+  double s = 0.0;
+  for (int i = tm.lane; i < n; i += TEAM) s += it[IL.fe + i] * a.mu[i];
+  lamE += h * tm.sum(s);
+  AdjPoint pt;
+  pt.Den = it[IL.sc + 0];
+  pt.logT = it[IL.sc + 1];
+  pt.invT = it[IL.sc + 2];
+  pt.T = it[IL.sc + 3];
+  pt.dDen = 0.0;
+  AdjWork av = a;
+  av.ek = const_cast<double*>(it + IL.ek);
+  param_vjp(tm, M, pt, av, it + IL.dq, a.mu, h);
+}
+
+// Reverse sweep of one tape segment with the segment's points evaluated
+// beforehand (items: point k at items + k * IL.stride).  a.AT / a.piv are
+// shared-memory copies of the factors.
+template <int TEAM>
+__device__ int sweep_items(const Team<TEAM>& tm, const DevMech& M, int n, int qmax, AdjWork& a, const TapeRec* tape,
+                           int nrec, const double* items, const ItemLayout& IL, const double* lam_y, double& lamE)
+{
+  for (int k = nrec - 1; k >= 0; k--) {
+    const TapeRec R = tape[k];
+    if (rev_linear(tm, n, qmax, R, a, lam_y)) continue;
+    const double* it = items + (size_t)R.i2 * IL.stride;
+    if (R.op == TP_FRESET) {
+      rev_item_freset(tm, M, n, a, it, IL, R.c[1], lamE);
+      continue;
+    }
+    if (R.op != TP_CORRECT) continue;
+    const int q = R.q;
+    const double gamma = R.c[1], rl1 = R.c[2];
+    for (int i = tm.lane; i < n; i += TEAM) {
+      double la = a.pend[i];
+      for (int j = 0; j <= q; j++) la += R.c[3 + j] * a.lam[j * n + i];
+      if (R.i1) {
+        la += a.lam[qmax * n + i];
+        a.lam[qmax * n + i] = 0.0;
+      }
+      a.mu[i] = la;
+      a.pend[i] = 0.0;
+    }
+    const int* ip = reinterpret_cast<const int*>(it + IL.piv);
+    if (ip[0] < 0) return ST_ADJ_SINGULAR;
+    for (int i = tm.lane; i < n * n; i += TEAM) a.AT[i] = it[IL.at + i];
+    for (int i = tm.lane; i < n; i += TEAM) a.piv[i] = ip[i];
+    tm.sync();
+    adj_solve<TEAM>(tm, a.AT, n, a.piv, a.mu);
+    jc_tmul_add(tm, n, it, a.mu, gamma, a.lam);
+    double s = 0.0;
+    for (int i = tm.lane; i < n; i += TEAM) {
+      a.lam[n + i] -= rl1 * a.mu[i];
+      s += it[IL.fe + i] * a.mu[i];
+    }
+    lamE += gamma * tm.sum(s);
+    tm.sync();
+    AdjPoint pt;
+    pt.Den = it[IL.sc + 0];
+    pt.logT = it[IL.sc + 1];
+    pt.invT = it[IL.sc + 2];
+    pt.T = it[IL.sc + 3];
+    pt.dDen = 0.0;
+    AdjWork av = a;
+    av.ek = const_cast<double*>(it + IL.ek);
+    param_vjp(tm, M, pt, av, it + IL.dq, a.mu, gamma);
+  }
+  return ST_OK;
+}
 
 } // namespace ppb

@@ -10,6 +10,9 @@
 // recomputing it (bit for bit: the same code path runs on the same state) to
 // rebuild its tape, and applies the transposed operations in reverse order.
 // Tangent: each segment's tape is swept forward right after it is recorded.
+#include <algorithm>
+#include <vector>
+
 #include "ppb_adjoint.cuh"
 #include "ppb_engine.h"
 #include "ppb_work.cuh"
@@ -19,6 +22,10 @@
 #endif
 
 namespace ppb {
+
+#ifdef PPB_PHASE_TIMERS
+static __device__ unsigned long long g_adj_cycles[AP_COUNT];
+#endif
 
 // checkpoint layout: [BdfScalars | nstloc][zn 6n][ewt n][J n*n][A n*n LT][piv n]
 template <typename LT>
@@ -99,7 +106,9 @@ __device__ void adjoint_cell(const Team<32>& tm, const DevMech& M, const Options
   bdf.rec.close_rec = L.close_rec;
   bdf.rec.close_y = L.close_y;
   bdf.rec.begin();
-  AdjSweep<32, PER, LT> sw{tm, M, o, w, a, cin, n, o.max_order};
+  long long acc[AP_COUNT] = {};
+  AdjSweep<32, PER, LT> sw{tm, M, o, w, a, cin, n, o.max_order, acc};
+  PPB_ATIC(AP_CELL);
   int flag = bdf.start(dt);
   int nstloc = 0;
   bool done = false;
@@ -140,13 +149,21 @@ __device__ void adjoint_cell(const Team<32>& tm, const DevMech& M, const Options
           flag = ST_ADJ_CAPACITY;
           break;
         }
+        PPB_ATIC(AP_SAVE);
         save_cp<NS, LT>(tm, cpb + (size_t)ncp * L.cp_stride, bdf, w, nstloc);
+        PPB_ATOC(acc, AP_SAVE);
         ncp++;
       } else {
+        PPB_ATIC(AP_RESTORE);
         restore_cp<NS, LT>(tm, cpb + (size_t)seg * L.cp_stride, bdf, w, nstloc);
+        PPB_ATOC(acc, AP_RESTORE);
       }
       bdf.rec.begin();
+      PPB_ATIC(AP_FWD);
       flag = bdf.advance(dt, nstloc, done);
+#ifdef PPB_PHASE_TIMERS
+      acc[fwd ? AP_FWD : AP_REPLAY] += clock64() - _atic_AP_FWD;
+#endif
       if (flag != ST_OK) break;
       if (fwd) {
         if (!done) continue;
@@ -163,7 +180,9 @@ __device__ void adjoint_cell(const Team<32>& tm, const DevMech& M, const Options
           for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = w.y[i];
         tm.sync();
       }
+      PPB_ATIC(AP_SWEEP);
       flag = sw.reverse(tape, bdf.rec.nrec, ys, b.lam_y + (size_t)c * n, lamE);
+      PPB_ATOC(acc, AP_SWEEP);
       if (flag != ST_OK) break;
       if (seg == 0) {
         sw.rev_freset(0.0, bdf.rec.h0, y0, lamE);
@@ -183,6 +202,11 @@ __device__ void adjoint_cell(const Team<32>& tm, const DevMech& M, const Options
     for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = (flag == ST_OK) ? w.y[i] : w.zn[0][i];
   if (MODE != ADJ_TANGENT && flag != ST_OK && b.y_out)
     for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = w.zn[0][i];
+  PPB_ATOC(acc, AP_CELL);
+#ifdef PPB_PHASE_TIMERS
+  if (tm.lane == 0)
+    for (int q = 0; q < AP_COUNT; q++) atomicAdd(&g_adj_cycles[q], (unsigned long long)acc[q]);
+#endif
   if (tm.lane == 0) {
     if (b.status) b.status[c] = flag;
     if (b.stats) {
@@ -279,7 +303,7 @@ __global__ void __launch_bounds__(128) k_rhs_exact(DevMech M, int rtype, double 
     }
     s = tm.sum(s);
     if (vE_out && tm.lane == 0) vE_out[c] = s;
-    param_vjp(tm, M, pt, a, a.mu, 1.0);
+    param_vjp(tm, M, pt, a, w.qd, a.mu, 1.0);
     if (vp_out)
       for (int r = tm.lane; r < 3 * R; r += 32) vp_out[(size_t)c * 3 * R + r] = a.gacc[r];
   }
@@ -338,9 +362,9 @@ static int plan_ns_t(const DevMech& M, AdjPlan* p)
 template <int NS>
 static int plan_ns(const DevMech& M, int mode, int lu_fp32, AdjPlan* p)
 {
-  if (mode == ADJ_TANGENT)
-    return lu_fp32 ? plan_ns_t<NS, float, ADJ_TANGENT>(M, p) : plan_ns_t<NS, double, ADJ_TANGENT>(M, p);
-  return lu_fp32 ? plan_ns_t<NS, float, ADJ_REVERSE>(M, p) : plan_ns_t<NS, double, ADJ_REVERSE>(M, p);
+  // the reverse integration runs batched (launch_adjoint_batched)
+  if (mode != ADJ_TANGENT) return (int)cudaErrorNotSupported;
+  return lu_fp32 ? plan_ns_t<NS, float, ADJ_TANGENT>(M, p) : plan_ns_t<NS, double, ADJ_TANGENT>(M, p);
 }
 
 template <int NS>
@@ -352,8 +376,8 @@ static int launch_ns(const DevMech& M, const Options& o, int mode, int lu_fp32, 
   if (e != cudaSuccess) return (int)e;
   const size_t shm = p.warp_smem * p.wpb;
   typedef void (*KT)(DevMech, Options, AdjBatch, AdjLayout, double, int*);
-  KT kern = (mode == ADJ_TANGENT) ? (lu_fp32 ? (KT)k_adjoint<NS, float, ADJ_TANGENT> : (KT)k_adjoint<NS, double, ADJ_TANGENT>)
-                                  : (lu_fp32 ? (KT)k_adjoint<NS, float, ADJ_REVERSE> : (KT)k_adjoint<NS, double, ADJ_REVERSE>);
+  if (mode != ADJ_TANGENT) return (int)cudaErrorNotSupported;
+  KT kern = lu_fp32 ? (KT)k_adjoint<NS, float, ADJ_TANGENT> : (KT)k_adjoint<NS, double, ADJ_TANGENT>;
   e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   if (e != cudaSuccess) return (int)e;
   kern<<<p.blocks, p.wpb * 32, shm, st>>>(M, o, b, L, dt, queue);
@@ -386,8 +410,354 @@ static int launch_rhs_exact_ns(const DevMech& M, int rtype, double t, const doub
   return (int)cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- batched
+// Forward (replay = 0: every cell from its initial state, a checkpoint at
+// the start of each segment, the last segment's tape left in place) or
+// recomputation of segment seg of every cell that has an earlier segment
+// (replay = 1).  One call site of the integrator serves both, so the
+// recomputation repeats the forward bit for bit; it is checked against the
+// next checkpoint.
+template <int NS, typename LT>
+__global__ void __launch_bounds__(256) k_adj_seg(DevMech M, Options o, AdjBatch b, AdjCells C, double dt, int* queue,
+                                                 int seg, int replay, size_t warp_smem)
+{
+  extern __shared__ __align__(16) char smem[];
+  Team<32> tm;
+  constexpr int n = NS + 1;
+  const int R = M.nrxn;
+  const int warp = threadIdx.x / 32;
+  Work<LT> w;
+  carve<LT>(w, smem + (size_t)warp * warp_smem, NS, R);
+  for (;;) {
+    int c = 0;
+    if (tm.lane == 0) c = atomicAdd(queue, 1);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= b.ncells) break;
+    if (replay) {
+      // cells without a segment seg are idle; for a cell whose last segment
+      // is seg, the forward run left the tape (and its counts) in place
+      const int ns = C.nseg[c];
+      if (seg >= ns - 1) continue;
+    }
+    const double* y0 = b.y0 + (size_t)c * n;
+    for (int i = tm.lane; i < n; i += 32) {
+      w.src[i] = (i < NS && b.src) ? b.src[(size_t)c * NS + i] : 0.0;
+      if (o.use_typ_vals) w.atolv[i] = b.atolv[i];
+      if (!replay) {
+        w.zn[0][i] = y0[i];
+        w.y[i] = y0[i];
+      }
+    }
+    tm.sync();
+    const CellIn cin{b.rhoe[c], b.rhoesrc ? b.rhoesrc[c] : 0.0};
+    Bdf<NS, 32, LT, AdjRec<32>> bdf(tm, M, o, w, cin);
+    bdf.rec.tape = reinterpret_cast<TapeRec*>(C.tape) + (size_t)c * C.cap_rec;
+    bdf.rec.ys = C.ys + (size_t)c * C.cap_y * n;
+    bdf.rec.yinfo = C.yinfo + (size_t)c * C.cap_y * 2;
+    bdf.rec.n = n;
+    bdf.rec.seg_steps = C.seg_steps;
+    bdf.rec.close_rec = C.close_rec;
+    bdf.rec.close_y = C.close_y;
+    bdf.rec.begin();
+    int nstloc = 0, ncp = 0, flag = ST_OK;
+    bool done = false;
+    int* cpi = C.cp_idx + (size_t)c * C.max_seg;
+    if (!replay) {
+      flag = bdf.start(dt);
+      for (int i = tm.lane; i < 7 * n; i += 32) C.lam[(size_t)c * 7 * n + i] = 0.0;
+      for (int r = tm.lane; r < 3 * R; r += 32) C.gw[(size_t)c * 3 * R + r] = 0.0;
+      if (b.lam_y0)
+        for (int i = tm.lane; i < n; i += 32) b.lam_y0[(size_t)c * n + i] = 0.0;
+      if (tm.lane == 0) {
+        C.lamE[c] = 0.0;
+        if (b.lam_e) b.lam_e[c] = 0.0;
+      }
+    }
+    for (;;) {
+      if (flag != ST_OK) break;
+      if (!replay) {
+        if (ncp >= C.max_seg) {
+          flag = ST_ADJ_CAPACITY;
+          break;
+        }
+        int slot = 0;
+        if (tm.lane == 0) slot = atomicAdd(C.pool_next, 1);
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (slot >= C.pool_cap) {
+          flag = ST_ADJ_CAPACITY;
+          break;
+        }
+        if (tm.lane == 0) cpi[ncp] = slot;
+        save_cp<NS, LT>(tm, C.cp_pool + (size_t)slot * C.cp_stride, bdf, w, nstloc);
+        ncp++;
+      } else {
+        restore_cp<NS, LT>(tm, C.cp_pool + (size_t)cpi[seg] * C.cp_stride, bdf, w, nstloc);
+      }
+      bdf.rec.begin();
+      flag = bdf.advance(dt, nstloc, done);
+      if (flag != ST_OK || done || replay) break;
+    }
+    if (!replay) {
+      if (b.y_out)
+        for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = (flag == ST_OK) ? w.y[i] : w.zn[0][i];
+      if (tm.lane == 0) {
+        if (b.status) b.status[c] = flag;
+        if (b.stats) {
+          int* st = b.stats + (size_t)c * 7;
+          st[0] = bdf.s.nst;
+          st[1] = bdf.s.nfe;
+          st[2] = bdf.s.nje;
+          st[3] = bdf.s.nsetups;
+          st[4] = bdf.s.nni;
+          st[5] = bdf.s.netf;
+          st[6] = bdf.s.ncfn;
+        }
+        C.nseg[c] = (flag == ST_OK) ? ncp : 0;
+        C.h0[c] = bdf.rec.h0;
+        C.nrec[c] = bdf.rec.nrec;
+        C.ny[c] = bdf.rec.ny;
+      }
+    } else {
+      if (flag == ST_OK) {
+        // the recomputed segment must end where the forward run did
+        const BdfScalars* nx = reinterpret_cast<const BdfScalars*>(C.cp_pool + (size_t)cpi[seg + 1] * C.cp_stride);
+        if (nx->tn != bdf.s.tn || nx->nst != bdf.s.nst || nx->h != bdf.s.h) flag = ST_ADJ_REPLAY;
+      }
+      if (tm.lane == 0) {
+        if (flag != ST_OK) {
+          if (b.status) b.status[c] = flag;
+          C.nseg[c] = 0;
+          C.nrec[c] = 0;
+          C.ny[c] = 0;
+        } else {
+          C.nrec[c] = bdf.rec.nrec;
+          C.ny[c] = bdf.rec.ny;
+        }
+      }
+    }
+    tm.sync();
+  }
+}
+
+// Every differentiated point of items [i0, i1) of segment seg (item i of
+// cell c is slot i - item_off[c]; at seg 0 the slot after the last is the
+// initial state).
+template <int NS>
+__global__ void __launch_bounds__(256) k_adj_items(DevMech M, int rtype, AdjBatch b, AdjCells C, int seg, int c0,
+                                                   int c1, int i0, int i1, size_t warp_smem)
+{
+  extern __shared__ __align__(16) char smem[];
+  Team<32> tm;
+  constexpr int n = NS + 1;
+  constexpr int PER = (NS + 31) / 32;
+  const int warp = threadIdx.x / 32;
+  const int i = i0 + blockIdx.x * (blockDim.x / 32) + warp;
+  if (i >= i1) return;
+  // the cell owning item i: the last c in [c0, c1) with item_off[c] <= i
+  int lo = c0, hi = c1 - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (C.item_off[mid] <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  const int c = lo;
+  const int slot = i - C.item_off[c];
+  const double* yg;
+  double t, gamma;
+  if (seg == 0 && slot == C.ny[c]) {
+    yg = b.y0 + (size_t)c * n;
+    t = 0.0;
+    gamma = 0.0;
+  } else {
+    const size_t k = (size_t)c * C.cap_y + slot;
+    yg = C.ys + k * n;
+    t = C.yinfo[2 * k];
+    gamma = C.yinfo[2 * k + 1];
+  }
+  const ItemLayout IL(NS, M.nrxn);
+  eval_item<32, PER>(tm, M, rtype, t, gamma, yg, b.rhoe[c], b.rhoesrc ? b.rhoesrc[c] : 0.0,
+                     b.src ? b.src + (size_t)c * NS : nullptr, smem + (size_t)warp * warp_smem,
+                     C.items + (size_t)(i - i0) * IL.stride, IL);
+}
+
+// The reverse sweep of segment seg for cells [c0, c1), whose items start at
+// global item index i0 in C.items.
+template <int NS>
+__global__ void __launch_bounds__(256) k_adj_sweep(DevMech M, Options o, AdjBatch b, AdjCells C, int seg, int c0,
+                                                   int c1, int i0, size_t warp_smem)
+{
+  extern __shared__ __align__(16) char smem[];
+  Team<32> tm;
+  constexpr int n = NS + 1;
+  const int R = M.nrxn;
+  const int warp = threadIdx.x / 32;
+  const int c = c0 + blockIdx.x * (blockDim.x / 32) + warp;
+  if (c >= c1) return;
+  if (seg >= C.nseg[c]) return;
+  double* p = reinterpret_cast<double*>(smem + (size_t)warp * warp_smem);
+  AdjWork a{};
+  a.lam = p; p += 6 * n;
+  a.pend = p; p += n;
+  a.mu = p; p += n;
+  a.v = p; p += n + 1;
+  a.AT = p; p += (size_t)n * n;
+  a.piv = reinterpret_cast<int*>(p);
+  a.gacc = C.gw + (size_t)c * 3 * R;
+  double* lg = C.lam + (size_t)c * 7 * n;
+  for (int i = tm.lane; i < 7 * n; i += 32) a.lam[i] = lg[i]; // lam then pend
+  double lamE = C.lamE[c];
+  tm.sync();
+  const ItemLayout IL(NS, R);
+  const double* items = C.items + (size_t)(C.item_off[c] - i0) * IL.stride;
+  const TapeRec* tape = reinterpret_cast<const TapeRec*>(C.tape) + (size_t)c * C.cap_rec;
+  int flag = sweep_items<32>(tm, M, n, o.max_order, a, tape, C.nrec[c], items, IL, b.lam_y + (size_t)c * n, lamE);
+  if (flag == ST_OK && seg == 0) {
+    // z_0 = y0, z_1 = h0 f(0, y0)
+    rev_item_freset<32>(tm, M, n, a, items + (size_t)C.ny[c] * IL.stride, IL, C.h0[c], lamE);
+    if (b.lam_y0)
+      for (int i = tm.lane; i < n; i += 32) b.lam_y0[(size_t)c * n + i] = a.lam[i];
+    if (b.lam_e && tm.lane == 0) b.lam_e[c] = lamE;
+  }
+  if (flag != ST_OK) {
+    for (int r = tm.lane; r < 3 * R; r += 32) a.gacc[r] = 0.0;
+    if (tm.lane == 0) {
+      if (b.status) b.status[c] = flag;
+      C.nseg[c] = 0;
+    }
+  }
+  tm.sync();
+  for (int i = tm.lane; i < 7 * n; i += 32) lg[i] = a.lam[i];
+  if (tm.lane == 0) C.lamE[c] = lamE;
+}
+
+// Block size (warps) with the most resident warps per SM for a kernel with
+// wb bytes of shared memory per warp.
+static int best_blocks(const void* kern, size_t wb, int* wpb_out, int* per_sm_out)
+{
+  int dev = 0, smem_max = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  int best_w = 0, best_b = 0, best = 0;
+  for (int wpb = 8; wpb >= 1; wpb--) {
+    const size_t shm = wb * wpb;
+    if (shm > (size_t)smem_max) continue;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    if (e != cudaSuccess) return (int)e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, wpb * 32, shm);
+    if (e != cudaSuccess) return (int)e;
+    if (per_sm * wpb > best) {
+      best = per_sm * wpb;
+      best_w = wpb;
+      best_b = per_sm;
+    }
+  }
+  if (best < 1) return (int)cudaErrorInvalidConfiguration;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(wb * best_w));
+  *wpb_out = best_w;
+  *per_sm_out = best_b;
+  return 0;
+}
+
+template <int NS, typename LT>
+static int batched_ns_t(const DevMech& M, const Options& o, const AdjBatch& b, AdjCells& C, double dt, int* queue,
+                        double* grad, int accumulate, AdjGrow grow, void* ctx, cudaStream_t st)
+{
+  constexpr int n = NS + 1;
+  const int R = M.nrxn, nc = b.ncells;
+  if (nc <= 0) return 0;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e;
+  // launch shapes
+  const size_t seg_wb = team_bytes<LT>(NS, R);
+  int seg_w = 0, seg_b = 0, it_w = 0, it_b = 0, sw_w = 0, sw_b = 0;
+  int err = best_blocks((const void*)k_adj_seg<NS, LT>, seg_wb, &seg_w, &seg_b);
+  if (err) return err;
+  const size_t it_wb = item_bytes(NS, R);
+  if ((err = best_blocks((const void*)k_adj_items<NS>, it_wb, &it_w, &it_b))) return err;
+  const size_t sw_wb = ((8 * (9 * (size_t)n + 1 + (size_t)n * n) + 4 * n) + 15) & ~size_t(15);
+  if ((err = best_blocks((const void*)k_adj_sweep<NS>, sw_wb, &sw_w, &sw_b))) return err;
+  const int seg_grid = std::min(nsm * seg_b, (nc + seg_w - 1) / seg_w);
+  const ItemLayout IL(NS, R);
+  // forward with checkpoints
+  if ((e = cudaMemsetAsync(C.pool_next, 0, sizeof(int), st)) || (e = cudaMemsetAsync(queue, 0, sizeof(int), st)))
+    return (int)e;
+  k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, o, b, C, dt, queue, 0, 0, seg_wb);
+  if ((e = cudaGetLastError())) return (int)e;
+  std::vector<int> nseg(nc), ny(nc), off(nc + 1);
+  if ((e = cudaMemcpyAsync(nseg.data(), C.nseg, nc * sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaStreamSynchronize(st)))
+    return (int)e;
+  int maxseg = 0;
+  for (int c = 0; c < nc; c++) maxseg = std::max(maxseg, nseg[c]);
+  for (int s = maxseg - 1; s >= 0; s--) {
+    if ((e = cudaMemsetAsync(queue, 0, sizeof(int), st))) return (int)e;
+    k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, o, b, C, dt, queue, s, 1, seg_wb);
+    if ((e = cudaGetLastError())) return (int)e;
+    if ((e = cudaMemcpyAsync(nseg.data(), C.nseg, nc * sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaMemcpyAsync(ny.data(), C.ny, nc * sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaStreamSynchronize(st)))
+      return (int)e;
+    long tot = 0;
+    int most = 0;
+    for (int c = 0; c < nc; c++) {
+      off[c] = (int)tot;
+      const int k = (s < nseg[c]) ? ny[c] + (s == 0 ? 1 : 0) : 0;
+      most = std::max(most, k);
+      tot += k;
+    }
+    off[nc] = (int)tot;
+    if (tot == 0) continue;
+    if (C.items_cap < most) {
+      void* pi = C.items;
+      if ((err = grow(ctx, &pi, (size_t)most * IL.stride * 8))) return err;
+      C.items = (double*)pi;
+      C.items_cap = most;
+    }
+    if ((e = cudaMemcpyAsync(C.item_off, off.data(), (nc + 1) * sizeof(int), cudaMemcpyHostToDevice, st)))
+      return (int)e;
+    // groups of cells whose items fit the buffer
+    int c0 = 0;
+    while (c0 < nc) {
+      int c1 = c0;
+      while (c1 < nc && (long)off[c1 + 1] - off[c0] <= C.items_cap) c1++;
+      if (c1 == c0) c1 = c0 + 1;
+      const int i0 = off[c0], i1 = off[c1];
+      if (i1 > i0) {
+        const int ni = i1 - i0;
+        k_adj_items<NS><<<(ni + it_w - 1) / it_w, it_w * 32, it_wb * it_w, st>>>(M, o.reactor_type, b, C, s, c0, c1,
+                                                                               i0, i1, it_wb);
+        if ((e = cudaGetLastError())) return (int)e;
+        k_adj_sweep<NS><<<(c1 - c0 + sw_w - 1) / sw_w, sw_w * 32, sw_wb * sw_w, st>>>(M, o, b, C, s, c0, c1, i0,
+                                                                                   sw_wb);
+        if ((e = cudaGetLastError())) return (int)e;
+      }
+      c0 = c1;
+    }
+  }
+  if (grad) {
+    const int np = 3 * R;
+    k_sum_cells<<<(np + 127) / 128, 128, 0, st>>>(C.gw, nc, np, grad, accumulate);
+    if ((e = cudaGetLastError())) return (int)e;
+  }
+  return 0;
+}
+
 #define PPB_CAT2(a, b) a##b
 #define PPB_CAT(a, b) PPB_CAT2(a, b)
+#ifdef PPB_PHASE_TIMERS
+int PPB_CAT(adj_phase_cycles_, PPB_NS)(unsigned long long* out, int reset)
+{
+  cudaError_t e = cudaMemcpyFromSymbol(out, g_adj_cycles, sizeof(unsigned long long) * AP_COUNT);
+  if (e == cudaSuccess && reset) {
+    unsigned long long z[AP_COUNT] = {};
+    e = cudaMemcpyToSymbol(g_adj_cycles, z, sizeof(z));
+  }
+  return (int)e;
+}
+#endif
 int PPB_CAT(plan_adjoint_, PPB_NS)(const DevMech& M, int mode, int lu_fp32, AdjPlan* p)
 {
   return plan_ns<PPB_NS>(M, mode, lu_fp32, p);
@@ -398,6 +768,14 @@ int PPB_CAT(launch_adjoint_, PPB_NS)(const DevMech& M, const Options& o, int mod
 {
   return launch_ns<PPB_NS>(M, o, mode, lu_fp32, p, b, L, dt, queue, grad, accumulate, st);
 }
+int PPB_CAT(launch_adjoint_batched_, PPB_NS)(const DevMech& M, const Options& o, int lu_fp32, const AdjBatch& b,
+                                             AdjCells& C, double dt, int* queue, double* grad, int accumulate,
+                                             AdjGrow grow, void* ctx, cudaStream_t st)
+{
+  return lu_fp32 ? batched_ns_t<PPB_NS, float>(M, o, b, C, dt, queue, grad, accumulate, grow, ctx, st)
+                 : batched_ns_t<PPB_NS, double>(M, o, b, C, dt, queue, grad, accumulate, grow, ctx, st);
+}
+size_t PPB_CAT(adj_cp_bytes_, PPB_NS)(int lu_fp32) { return lu_fp32 ? cp_bytes<float>(PPB_NS) : cp_bytes<double>(PPB_NS); }
 int PPB_CAT(launch_rhs_exact_, PPB_NS)(const DevMech& M, int rtype, double t, const double* y, const double* rhoe,
                                        const double* rhoesrc, const double* src, const double* v, double* f_out,
                                        double* J_out, double* fE_out, double* vy_out, double* vE_out,

@@ -327,6 +327,49 @@ static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
     pk.used = off_jcrx + (size_t)tot * sizeof(unsigned short);
     set_off(dm.jc_off, off_jcoff);
     set_off(dm.jc_rx, off_jcrx);
+    // member lists (phase-space species only) and the third-body list
+    auto member = [&](int r, int k) {
+      for (int j = 0; j < t->rx_fps_n[r]; j++)
+        if (t->rx_fps_sp[r * PPB_MAXPS + j] == k) return true;
+      if (t->rx_rev[r])
+        for (int j = 0; j < t->rx_rps_n[r]; j++)
+          if (t->rx_rps_sp[r * PPB_MAXPS + j] == k) return true;
+      return false;
+    };
+    int mtot = 0;
+    for (int k = 0; k < N; k++)
+      for (int r = 0; r < R; r++) mtot += member(r, k);
+    const size_t off_jmoff = (pk.used + 15) & ~size_t(15);
+    const size_t off_jmrx = (off_jmoff + (N + 1) * sizeof(int) + 15) & ~size_t(15);
+    e = 0;
+    for (int k = 0; k < N; k++) {
+      pk.put(off_jmoff + k * sizeof(int), &e, 1);
+      for (int r = 0; r < R; r++) {
+        if (!member(r, k)) continue;
+        const unsigned short rr = (unsigned short)r;
+        pk.put(off_jmrx + e * sizeof(unsigned short), &rr, 1);
+        e++;
+      }
+    }
+    pk.put(off_jmoff + N * sizeof(int), &e, 1);
+    pk.used = off_jmrx + (size_t)mtot * sizeof(unsigned short);
+    const size_t off_aloff = (pk.used + 15) & ~size_t(15);
+    const size_t off_alrx = off_aloff + 16;
+    int na = 0;
+    for (int r = 0; r < R; r++) {
+      const int kind = t->rx_kind[r];
+      if (kind != PPB_RX_THIRD && kind != PPB_RX_TROE && kind != PPB_RX_LINDEMANN) continue;
+      const unsigned short rr = (unsigned short)r;
+      pk.put(off_alrx + na * sizeof(unsigned short), &rr, 1);
+      na++;
+    }
+    const int al[2] = {0, na};
+    pk.put(off_aloff, al, 2);
+    pk.used = off_alrx + (size_t)na * sizeof(unsigned short);
+    set_off(dm.jm_off, off_jmoff);
+    set_off(dm.jm_rx, off_jmrx);
+    set_off(dm.al_off, off_aloff);
+    set_off(dm.al_rx, off_alrx);
   }
   set_off(dm.rxp, off_rxp);
   set_off(dm.fop, off_fop);
@@ -596,6 +639,52 @@ PPB_ADJ_DECL(21)
 PPB_ADJ_DECL(53)
 PPB_ADJ_DECL(88)
 #undef PPB_ADJ_DECL
+#define PPB_ADJB_DECL(NS)                                                                                         \
+  int launch_adjoint_batched_##NS(const DevMech& M, const Options& o, int lu_fp32, const AdjBatch& b, AdjCells& C, \
+                                  double dt, int* queue, double* grad, int accumulate, AdjGrow grow, void* ctx,    \
+                                  cudaStream_t st);                                                               \
+  size_t adj_cp_bytes_##NS(int lu_fp32);
+PPB_ADJB_DECL(9)
+PPB_ADJB_DECL(21)
+PPB_ADJB_DECL(53)
+PPB_ADJB_DECL(88)
+#undef PPB_ADJB_DECL
+
+int launch_adjoint_batched(const DeviceMechanism& m, const Options& o, int lu_fp32, const AdjBatch& b, AdjCells& C,
+                           double dt, int* queue, double* grad, int accumulate, AdjGrow grow, void* grow_ctx,
+                           cudaStream_t st)
+{
+  const DevMech& M = *m.dm;
+#define PPB_B(NS) return launch_adjoint_batched_##NS(M, o, lu_fp32, b, C, dt, queue, grad, accumulate, grow, grow_ctx, st)
+  switch (M.nsp) {
+  case 9: PPB_B(9);
+  case 21: PPB_B(21);
+  case 53: PPB_B(53);
+  case 88: PPB_B(88);
+  default: return (int)cudaErrorNotSupported;
+  }
+#undef PPB_B
+}
+
+size_t adj_cp_bytes(int N, int lu_fp32)
+{
+  switch (N) {
+  case 9: return adj_cp_bytes_9(lu_fp32);
+  case 21: return adj_cp_bytes_21(lu_fp32);
+  case 53: return adj_cp_bytes_53(lu_fp32);
+  case 88: return adj_cp_bytes_88(lu_fp32);
+  default: return 0;
+  }
+}
+
+size_t adj_item_bytes(int N, int R)
+{
+  // [Jc n*n][AT n*n][fE n][ek n][dq R][4 scalars][n pivots], 16-byte aligned
+  const size_t n = N + 1;
+  size_t stride = 2 * n * n + 2 * n + (size_t)R + 4 + (n + 1) / 2;
+  stride = (stride + 1) & ~size_t(1);
+  return stride * 8;
+}
 
 int plan_adjoint(const DeviceMechanism& m, int mode, int lu_fp32, AdjPlan* p)
 {
@@ -817,6 +906,25 @@ int phase_cycles(unsigned long long* out, int reset)
     const int e = fn(part, reset);
     if (e) return e;
     for (int q = 0; q < PH_COUNT; q++) out[q] += part[q];
+  }
+  return 0;
+}
+
+int adj_phase_cycles_9(unsigned long long*, int);
+int adj_phase_cycles_21(unsigned long long*, int);
+int adj_phase_cycles_53(unsigned long long*, int);
+int adj_phase_cycles_88(unsigned long long*, int);
+
+int adj_phase_cycles(unsigned long long* out, int reset)
+{
+  for (int q = 0; q < 8; q++) out[q] = 0;
+  int (*fns[4])(unsigned long long*, int) = {adj_phase_cycles_9, adj_phase_cycles_21, adj_phase_cycles_53,
+                                             adj_phase_cycles_88};
+  for (auto fn : fns) {
+    unsigned long long part[8];
+    const int e = fn(part, reset);
+    if (e) return e;
+    for (int q = 0; q < 8; q++) out[q] += part[q];
   }
   return 0;
 }

@@ -109,6 +109,9 @@ void set_error(const char* msg);
 
 #ifdef PPB_PHASE_TIMERS
 int phase_cycles(unsigned long long* out, int reset);
+// adjoint kernel parts: forward, recomputation, sweeps, exact Jacobians,
+// factor + solve, checkpoint save, restore, whole cell (8 totals)
+int adj_phase_cycles(unsigned long long* out, int reset);
 #endif
 
 // Bytes of shared memory one team-integrated cell needs.
@@ -151,6 +154,33 @@ struct AdjLayout {
   size_t warp_smem;  // shared memory per warp
 };
 
+// Per-cell global state of the batched reverse sweep (one chunk of cells).
+struct AdjCells {
+  char* cp_pool;        // checkpoint slots of cp_stride bytes
+  size_t cp_stride;
+  int pool_cap;         // slots
+  int* pool_next;       // slot counter (device)
+  int* cp_idx;          // [cells][max_seg] slot of each segment's checkpoint
+  int max_seg;
+  void* tape;           // [cells][cap_rec] records
+  int cap_rec, close_rec;
+  double* ys;           // [cells][cap_y][N+1]
+  double* yinfo;        // [cells][cap_y][2] time, gamma
+  int cap_y, close_y;
+  int *nrec, *ny, *nseg; // [cells]
+  double* h0;           // [cells] initial step
+  double* lam;          // [cells][7(N+1)] adjoint history and pending correction
+  double* lamE;         // [cells]
+  double* gw;           // [cells][3R] parameter gradient per cell
+  double* items;        // [items][stride] evaluated points of one segment
+  int* item_off;        // [cells + 1] first item of each cell
+  int* item_cell;       // [items]
+  long items_cap;       // items the buffer holds
+  int seg_steps;
+};
+// Host callback growing a device buffer (returns a cudaError_t).
+typedef int (*AdjGrow)(void* ctx, void** p, size_t bytes);
+
 struct AdjPlan {
   int wpb = 0, blocks = 0;
   size_t warp_smem = 0, cp_stride = 0;
@@ -163,6 +193,17 @@ int plan_adjoint(const DeviceMechanism& m, int mode, int lu_fp32, AdjPlan* p);
 int launch_adjoint(const DeviceMechanism& m, const Options& o, int mode, int lu_fp32, const AdjPlan& p,
                    const AdjBatch& b, const AdjLayout& L, double dt, int* queue, double* grad, int accumulate,
                    cudaStream_t st);
+// The reverse (adjoint) integration of one chunk of cells, batched over the
+// cells segment by segment: forward with checkpoints, then per segment
+// (last first) recomputation, evaluation of every point, and the sweeps.
+// grow enlarges C.items (passing its capacity in C.items_cap) when a segment
+// needs more; the item bytes per point are adj_item_bytes().
+int launch_adjoint_batched(const DeviceMechanism& m, const Options& o, int lu_fp32, const AdjBatch& b, AdjCells& C,
+                           double dt, int* queue, double* grad, int accumulate, AdjGrow grow, void* grow_ctx,
+                           cudaStream_t st);
+size_t adj_item_bytes(int N, int R);
+size_t adj_cp_bytes(int N, int lu_fp32);
+
 // Pointwise exact derivatives of the reactor RHS (any output may be null).
 int launch_rhs_exact(const DeviceMechanism& m, int rtype, double t, const double* y, const double* rhoe,
                      const double* rhoesrc, const double* src, const double* v, double* f_out, double* J_out,

@@ -69,6 +69,13 @@ struct DevMech {
   // the reactions with k in their forward or (reversible) reverse phase space
   const int* jc_off;
   const unsigned short* jc_rx;
+  // per species k, in reaction order, the reactions with k in their forward
+  // or (reversible) reverse phase space; and the third-body / fall-off
+  // reactions (al_off = {0, count})
+  const int* jm_off;
+  const unsigned short* jm_rx;
+  const int* al_off;
+  const unsigned short* al_rx;
   // species-major gather of the aJacobian net stoichiometry (jn lists)
   const int *jg_off, *jg_rx;
   const double* jg_c;

@@ -4,15 +4,16 @@
 
 namespace ppb {
 // ------------------------------------------------------------ workspace
-// Newton-matrix region: the n x n factor, or the 4 doubles per reaction of
-// the warp-cooperative Jacobian evaluation, which uses it while the matrix is
-// not live, whichever is larger.
+// Newton-matrix region: the n x n factor, or the per-reaction factors of
+// the warp-cooperative Jacobian evaluations (4 doubles per reaction; 5 in the
+// adjoint's exact Jacobian), which use it while the matrix is not live,
+// whichever is larger.
 template <typename LT>
 __host__ __device__ inline size_t a_region_bytes(int N, int R)
 {
   const size_t n = N + 1;
   size_t a = n * n * sizeof(LT);
-  const size_t jx = 32 * (size_t)R;
+  const size_t jx = 40 * (size_t)R;
   if (jx > a) a = jx;
   return (a + 15) & ~size_t(15);
 }
