@@ -648,40 +648,6 @@ def phase_probe(edge=64, engine=1, lu_fp32=0):
     return 0
 
 
-def adjoint_phase_probe(ncells):
-    """Cycle totals of the adjoint kernel's parts on the adjoint workload
-    (needs the profiling build: PPB_LIB=pelephysics_b200/libppb200_phase.so)."""
-    import ctypes as C
-
-    import torch
-
-    from pelephysics_b200 import _lib, workloads as wl
-    from pelephysics_b200.reactor import Reactor
-
-    L = _lib.lib()
-    if not hasattr(L, "ppb_adjoint_phase_cycles"):
-        raise SystemExit("needs PPB_LIB=pelephysics_b200/libppb200_phase.so")
-    cells = wl.drm19_adjoint(ncells)
-    n = cells.rY.shape[0]
-    g = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
-    r = Reactor(MECH)
-    r.init(2, n, engine=1, use_graph=0, **OPTS)
-    y = g(cells.rY)
-    lam = torch.ones_like(y)
-    buf = (C.c_ulonglong * 8)()
-    r.adjoint(y, g(cells.rYsrc), g(cells.rX), g(cells.rX_src), cells.dt, lam)
-    torch.cuda.synchronize()
-    L.ppb_adjoint_phase_cycles(buf, 1)
-    r.adjoint(y, g(cells.rYsrc), g(cells.rX), g(cells.rX_src), cells.dt, lam)
-    torch.cuda.synchronize()
-    L.ppb_adjoint_phase_cycles(buf, 1)
-    names = ["forward", "recompute", "sweep", "exact_jacobian", "factor_solve", "save", "restore", "cell"]
-    tot = buf[7]
-    print(json.dumps({"adjoint_phase_probe": {k: {"cycles_per_cell": buf[i] / n, "frac": buf[i] / tot}
-                                              for i, k in enumerate(names)}, "cells": n}), flush=True)
-    return 0
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -699,8 +665,6 @@ def main():
     ap.add_argument("--edge", type=int, default=64, help="field edge (profiling runs use a smaller box)")
     ap.add_argument("--phase-probe", action="store_true",
                     help="per-phase cycle counters of one react (profiling build, PPB_LIB)")
-    ap.add_argument("--adjoint-phase-probe", action="store_true",
-                    help="cycle totals of the adjoint kernel's parts (profiling build, PPB_LIB)")
     ap.add_argument("--kernel-probe", action="store_true",
                     help="time the pointwise RHS / Jacobian / rate kernels on the field's cells")
     ap.add_argument("--flops-probe", action="store_true",
@@ -712,8 +676,6 @@ def main():
         return kernel_probe()
     if args.phase_probe:
         return phase_probe(args.edge)
-    if args.adjoint_phase_probe:
-        return adjoint_phase_probe(args.adjoint_cells)
     if args.impl == "reference":
         return reference_arm(args)
     if args.config != "drm19":

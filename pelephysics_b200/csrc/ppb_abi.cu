@@ -1197,10 +1197,6 @@ int ppb_pyt2re(const char* mechanism, int eh, const double* P, const double* T, 
 #ifdef PPB_PHASE_TIMERS
 // Profiling builds only: per-phase cycle totals of the BDF kernels.
 int ppb_phase_cycles(unsigned long long* out, int reset) { return cuda_fail(phase_cycles(out, reset), "phase"); }
-int ppb_adjoint_phase_cycles(unsigned long long* out, int reset)
-{
-  return cuda_fail(adj_phase_cycles(out, reset), "adjoint phase");
-}
 #endif
 
 } // extern "C"

@@ -39,17 +39,6 @@ namespace ppb {
 
 enum { ST_ADJ_CAPACITY = -40, ST_ADJ_SINGULAR = -41, ST_ADJ_REPLAY = -42 };
 
-// Profiling builds (-DPPB_PHASE_TIMERS): clock64() totals of the adjoint's
-// parts (forward, recomputation, sweeps, exact Jacobians, factor + solve,
-// checkpoint save, restore, whole cell), one accumulator set per lane.
-enum AdjPhase { AP_FWD = 0, AP_REPLAY, AP_SWEEP, AP_POINT, AP_LU, AP_SAVE, AP_RESTORE, AP_CELL, AP_COUNT };
-#ifdef PPB_PHASE_TIMERS
-#define PPB_ATIC(ph) const long long _atic_##ph = clock64()
-#define PPB_ATOC(acc, ph) (acc)[ph] += clock64() - _atic_##ph
-#else
-#define PPB_ATIC(ph)
-#define PPB_ATOC(acc, ph)
-#endif
 
 enum TapeOp : int {
   TP_FRESET = 1,
@@ -185,46 +174,6 @@ __host__ __device__ inline size_t adj_bytes(int N, int R)
   return ((d * 8 + 4 * n) + 15) & ~size_t(15);
 }
 
-// Reverse sweeps run between a segment's recomputation and the restore of
-// the previous checkpoint, when the forward workspace holds nothing that is
-// still needed: its vectors, Jacobian, factor and pivots serve as sweep
-// scratch and only the adjoint history (lam, pend) and the per-reaction
-// factors need their own shared memory (plus an FP64 factor when the
-// forward factor is FP32).  The parameter gradient accumulates in global
-// memory, per cell.
-template <typename LT>
-__host__ __device__ inline size_t adj_rev_bytes(int N, int R)
-{
-  const size_t n = N + 1;
-  size_t d = 7 * n;
-  if (sizeof(LT) != sizeof(double)) d += n * n;
-  return (d * 8 + 15) & ~size_t(15);
-}
-
-template <typename LT>
-__device__ inline void carve_adj_rev(AdjWork& a, char* base, Work<LT>& w, int N, int R)
-{
-  const int n = N + 1;
-  double* p = (double*)base;
-  a.lam = p; p += 6 * n;
-  a.pend = p; p += n;
-  // the per-reaction factors (5 R doubles) and then the FP64 factor of the
-  // adjoint matrix share the Newton-matrix region
-  a.jxa = reinterpret_cast<double*>(w.A);
-  a.AT = (sizeof(LT) == sizeof(double)) ? reinterpret_cast<double*>(w.A) : p;
-  a.Jc = w.J;
-  a.piv = w.piv;
-  a.fE = w.zn[0];
-  a.fy = w.zn[1];
-  a.ek = w.zn[2];
-  a.cvk = w.zn[3];
-  a.v = w.zn[4]; // n + 1: runs into zn[5], which follows it
-  a.mu = w.acor;
-  a.dcvk = w.tempv;
-  a.ybuf = w.ftemp;
-  a.tmp = w.delta;
-  a.gacc = nullptr; // set per cell
-}
 
 __device__ inline void carve_adj(AdjWork& a, char* base, int N, int R)
 {
@@ -604,136 +553,12 @@ struct AdjSweep {
   AdjWork& a;
   CellIn cin;
   int n, qmax;
-  long long* acc; // profiling accumulators (AP_*), or nullptr
 
   __device__ __noinline__ AdjPoint point(double t, const double* yg)
   {
     for (int i = tm.lane; i < n; i += TEAM) a.ybuf[i] = yg[i];
     tm.sync();
     return rhs_exact_jacobian<TEAM, PER, LT>(tm, M, o.reactor_type, t, a.ybuf, cin.rhoe, cin.rhoesrc, w.src, w, a);
-  }
-
-  // ---- reverse
-  // z_1 = h f(t, z_0): lam_0 += h Jc^T lam_1, lamE += h fE . lam_1, grad
-  __device__ void rev_freset(double t, double h, const double* yg, double& lamE)
-  {
-    double* l1 = a.lam + n;
-    for (int i = tm.lane; i < n; i += TEAM) a.mu[i] = l1[i];
-    tm.sync();
-    for (int i = tm.lane; i < n; i += TEAM) l1[i] = 0.0;
-    const AdjPoint pt = point(t, yg);
-    jc_tmul_add(tm, n, a.Jc, a.mu, h, a.lam);
-    double s = 0.0;
-    for (int i = tm.lane; i < n; i += TEAM) s += a.fE[i] * a.mu[i];
-    lamE += h * tm.sum(s);
-    param_vjp(tm, M, pt, a, w.qd, a.mu, h);
-  }
-
-  __device__ int reverse(const TapeRec* tape, int nrec, const double* ys, const double* lam_y, double& lamE)
-  {
-    for (int k = nrec - 1; k >= 0; k--) {
-      const TapeRec R = tape[k];
-      const int q = R.q;
-      switch (R.op) {
-      case TP_OUTPUT: {
-        // y(tout) = sum_j s^j z_j
-        for (int i = tm.lane; i < n; i += TEAM) {
-          double pw = 1.0;
-          for (int j = 0; j <= q; j++) {
-            a.lam[j * n + i] += pw * lam_y[i];
-            pw *= R.c[0];
-          }
-        }
-        tm.sync();
-        break;
-      }
-      case TP_CORRECT: {
-        const double tn = R.c[0], gamma = R.c[1], rl1 = R.c[2];
-        for (int i = tm.lane; i < n; i += TEAM) {
-          double la = a.pend[i];
-          for (int j = 0; j <= q; j++) la += R.c[3 + j] * a.lam[j * n + i];
-          if (R.i1) {
-            la += a.lam[qmax * n + i];
-            a.lam[qmax * n + i] = 0.0;
-          }
-          a.mu[i] = la;
-          a.pend[i] = 0.0;
-        }
-        tm.sync();
-        PPB_ATIC(AP_POINT);
-        const AdjPoint pt = point(tn, ys + (size_t)R.i2 * n);
-        PPB_ATOC(acc, AP_POINT);
-        PPB_ATIC(AP_LU);
-        if (adj_factor(tm, n, a.Jc, gamma, true, a.AT, a.piv)) return ST_ADJ_SINGULAR;
-        adj_solve<TEAM>(tm, a.AT, n, a.piv, a.mu);
-        PPB_ATOC(acc, AP_LU);
-        jc_tmul_add(tm, n, a.Jc, a.mu, gamma, a.lam);
-        double s = 0.0;
-        for (int i = tm.lane; i < n; i += TEAM) {
-          a.lam[n + i] -= rl1 * a.mu[i];
-          s += a.fE[i] * a.mu[i];
-        }
-        lamE += gamma * tm.sum(s);
-        tm.sync();
-        param_vjp(tm, M, pt, a, w.qd, a.mu, gamma);
-        break;
-      }
-      case TP_SAVEQMAX: {
-        for (int i = tm.lane; i < n; i += TEAM) {
-          a.pend[i] += a.lam[qmax * n + i];
-          a.lam[qmax * n + i] = 0.0;
-        }
-        tm.sync();
-        break;
-      }
-      case TP_PREDICT: {
-        // forward: for k = 1..q, j = q..k: z_{j-1} += z_j
-        for (int i = tm.lane; i < n; i += TEAM)
-          for (int kk = q; kk >= 1; kk--)
-            for (int j = kk; j <= q; j++) a.lam[j * n + i] += a.lam[(j - 1) * n + i];
-        tm.sync();
-        break;
-      }
-      case TP_RESCALE: {
-        for (int i = tm.lane; i < n; i += TEAM) {
-          double f = R.c[0];
-          for (int j = 1; j <= q; j++) {
-            a.lam[j * n + i] *= f;
-            f *= R.c[0];
-          }
-        }
-        tm.sync();
-        break;
-      }
-      case TP_INCREASE: {
-        const int L = R.i1, idx = R.i2;
-        for (int i = tm.lane; i < n; i += TEAM) {
-          double lz = a.lam[L * n + i];
-          for (int j = 2; j <= q; j++) lz += R.c[j - 1] * a.lam[j * n + i];
-          a.lam[L * n + i] = 0.0;
-          a.lam[idx * n + i] += R.c[0] * lz;
-        }
-        tm.sync();
-        break;
-      }
-      case TP_DECREASE: {
-        for (int i = tm.lane; i < n; i += TEAM) {
-          double s = 0.0;
-          for (int j = 2; j < q; j++) s += R.c[j - 2] * a.lam[j * n + i];
-          a.lam[q * n + i] -= s;
-        }
-        tm.sync();
-        break;
-      }
-      case TP_FRESET: {
-        rev_freset(R.c[0], R.c[1], ys + (size_t)R.i2 * n, lamE);
-        break;
-      }
-      default:
-        break;
-      }
-    }
-    return ST_OK;
   }
 
   // ---- forward (tangent-linear)

@@ -1,15 +1,21 @@
 // Discrete adjoint / tangent-linear kernels of the BDF integration for one
 // species count (compiled once per mechanism size with -DPPB_NS=<N>).
 //
-// One warp integrates one cell at a time, pulling cells from a work queue.
-// Adjoint: the forward integration saves a checkpoint of the whole integrator
-// state (scalars, Nordsieck history, Jacobian, Newton-matrix factor) at the
-// start of every segment of `seg_steps` accepted steps, recording each
-// segment's operations on the warp's tape; the reverse sweep then walks the
-// segments from last to first, restoring the segment's checkpoint and
-// recomputing it (bit for bit: the same code path runs on the same state) to
-// rebuild its tape, and applies the transposed operations in reverse order.
-// Tangent: each segment's tape is swept forward right after it is recorded.
+// Adjoint (batched over the cells, segment by segment):
+//   1. k_adj_seg (forward): one warp per cell integrates from y0, saving a
+//      checkpoint of the whole integrator state (scalars, Nordsieck history,
+//      error weights, Jacobian, Newton-matrix factor) at the start of every
+//      segment of seg_steps accepted steps into a shared pool, and recording
+//      each segment's operations on the cell's tape (the last one stays);
+//   2. for each segment s, last first: k_adj_seg (replay) restores every
+//      cell's checkpoint s and recomputes the segment through the same code
+//      (bit for bit, checked against checkpoint s+1) to rebuild its tape;
+//      k_adj_items evaluates, for every point of every cell's segment at
+//      once, the exact Jacobian, df/dE, the rate derivatives and the FP64
+//      factor of (I - gamma Jc)^T; k_adj_sweep applies the transposed
+//      operations in reverse order with those stored factors.
+// Tangent (k_tangent): each segment's tape is swept forward right after it
+// is recorded, one warp per cell.
 #include <algorithm>
 #include <vector>
 
@@ -22,10 +28,6 @@
 #endif
 
 namespace ppb {
-
-#ifdef PPB_PHASE_TIMERS
-static __device__ unsigned long long g_adj_cycles[AP_COUNT];
-#endif
 
 // checkpoint layout: [BdfScalars | nstloc][zn 6n][ewt n][J n*n][A n*n LT][piv n]
 template <typename LT>
@@ -82,10 +84,11 @@ __device__ void restore_cp(const Team<32>& tm, const char* src, B& bdf, Work<LT>
   tm.sync();
 }
 
-template <int NS, typename LT, int MODE>
-__device__ void adjoint_cell(const Team<32>& tm, const DevMech& M, const Options& o, Work<LT>& w, AdjWork& a,
-                             const AdjBatch& b, const AdjLayout& L, char* cpb, TapeRec* tape, double* ys, int c,
-                             double dt)
+// Tangent-linear integration of one cell: each segment's tape is swept
+// forward right after it is recorded.
+template <int NS, typename LT>
+__device__ void tangent_cell(const Team<32>& tm, const DevMech& M, const Options& o, Work<LT>& w, AdjWork& a,
+                             const AdjBatch& b, const AdjLayout& L, TapeRec* tape, double* ys, int c, double dt)
 {
   constexpr int n = NS + 1;
   constexpr int PER = (NS + 31) / 32;
@@ -106,128 +109,49 @@ __device__ void adjoint_cell(const Team<32>& tm, const DevMech& M, const Options
   bdf.rec.close_rec = L.close_rec;
   bdf.rec.close_y = L.close_y;
   bdf.rec.begin();
-  long long acc[AP_COUNT] = {};
-  AdjSweep<32, PER, LT> sw{tm, M, o, w, a, cin, n, o.max_order, acc};
-  PPB_ATIC(AP_CELL);
+  AdjSweep<32, PER, LT> sw{tm, M, o, w, a, cin, n, o.max_order};
   int flag = bdf.start(dt);
   int nstloc = 0;
   bool done = false;
-  double lamE = 0.0;
-  int fst[7] = {0, 0, 0, 0, 0, 0, 0}; // counters of the forward integration
-  const int R = M.nrxn;
-  if (MODE != ADJ_TANGENT) {
-    a.gacc = L.gw + (size_t)c * 3 * R; // this cell's parameter gradient
-    for (int r = tm.lane; r < 3 * R; r += 32) a.gacc[r] = 0.0;
-  }
   for (int i = tm.lane; i < 6 * n; i += 32) a.lam[i] = 0.0;
   for (int i = tm.lane; i < n; i += 32) a.pend[i] = 0.0;
   tm.sync();
-  double* out_vec = b.lam_y0 ? b.lam_y0 + (size_t)c * n : nullptr;
-  if (MODE == ADJ_TANGENT) {
-    const double dE = b.dE ? b.dE[c] : 0.0;
-    if (flag == ST_OK) {
-      // z_0 = y0, z_1 = h0 f(0, y0)
-      for (int i = tm.lane; i < n; i += 32) a.lam[i] = b.dy0 ? b.dy0[(size_t)c * n + i] : 0.0;
-      tm.sync();
-      sw.fwd_freset(0.0, bdf.rec.h0, y0, dE, b.dp);
-      for (;;) {
-        flag = bdf.advance(dt, nstloc, done);
-        if (flag != ST_OK) break;
-        flag = sw.forward(tape, bdf.rec.nrec, ys, dE, b.dp, a.tmp);
-        if (flag != ST_OK || done) break;
-        bdf.rec.begin();
-      }
-    }
-    if (out_vec)
-      for (int i = tm.lane; i < n; i += 32) out_vec[i] = (flag == ST_OK) ? a.tmp[i] : 0.0;
-  } else {
-    int ncp = 0, seg = 0;
-    bool fwd = true;
-    while (flag == ST_OK) {
-      if (fwd) {
-        if (ncp >= L.cap_cp) {
-          flag = ST_ADJ_CAPACITY;
-          break;
-        }
-        PPB_ATIC(AP_SAVE);
-        save_cp<NS, LT>(tm, cpb + (size_t)ncp * L.cp_stride, bdf, w, nstloc);
-        PPB_ATOC(acc, AP_SAVE);
-        ncp++;
-      } else {
-        PPB_ATIC(AP_RESTORE);
-        restore_cp<NS, LT>(tm, cpb + (size_t)seg * L.cp_stride, bdf, w, nstloc);
-        PPB_ATOC(acc, AP_RESTORE);
-      }
-      bdf.rec.begin();
-      PPB_ATIC(AP_FWD);
+  const double dE = b.dE ? b.dE[c] : 0.0;
+  if (flag == ST_OK) {
+    // z_0 = y0, z_1 = h0 f(0, y0)
+    for (int i = tm.lane; i < n; i += 32) a.lam[i] = b.dy0 ? b.dy0[(size_t)c * n + i] : 0.0;
+    tm.sync();
+    sw.fwd_freset(0.0, bdf.rec.h0, y0, dE, b.dp);
+    for (;;) {
       flag = bdf.advance(dt, nstloc, done);
-#ifdef PPB_PHASE_TIMERS
-      acc[fwd ? AP_FWD : AP_REPLAY] += clock64() - _atic_AP_FWD;
-#endif
       if (flag != ST_OK) break;
-      if (fwd) {
-        if (!done) continue;
-        fwd = false;
-        seg = ncp - 1;
-        fst[0] = bdf.s.nst;
-        fst[1] = bdf.s.nfe;
-        fst[2] = bdf.s.nje;
-        fst[3] = bdf.s.nsetups;
-        fst[4] = bdf.s.nni;
-        fst[5] = bdf.s.netf;
-        fst[6] = bdf.s.ncfn;
-        if (b.y_out)
-          for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = w.y[i];
-        tm.sync();
-      }
-      PPB_ATIC(AP_SWEEP);
-      flag = sw.reverse(tape, bdf.rec.nrec, ys, b.lam_y + (size_t)c * n, lamE);
-      PPB_ATOC(acc, AP_SWEEP);
-      if (flag != ST_OK) break;
-      if (seg == 0) {
-        sw.rev_freset(0.0, bdf.rec.h0, y0, lamE);
-        break;
-      }
-      seg--;
+      flag = sw.forward(tape, bdf.rec.nrec, ys, dE, b.dp, a.tmp);
+      if (flag != ST_OK || done) break;
+      bdf.rec.begin();
     }
-    if (out_vec)
-      for (int i = tm.lane; i < n; i += 32) out_vec[i] = (flag == ST_OK) ? a.lam[i] : 0.0;
-    if (b.lam_e && tm.lane == 0) b.lam_e[c] = (flag == ST_OK) ? lamE : 0.0;
-    // the per-cell gradients are summed in cell order afterwards, so the
-    // result does not depend on which warp ran which cell
-    if (flag != ST_OK)
-      for (int r = tm.lane; r < 3 * R; r += 32) a.gacc[r] = 0.0;
   }
-  if (MODE == ADJ_TANGENT && b.y_out)
+  if (b.lam_y0)
+    for (int i = tm.lane; i < n; i += 32) b.lam_y0[(size_t)c * n + i] = (flag == ST_OK) ? a.tmp[i] : 0.0;
+  if (b.y_out)
     for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = (flag == ST_OK) ? w.y[i] : w.zn[0][i];
-  if (MODE != ADJ_TANGENT && flag != ST_OK && b.y_out)
-    for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = w.zn[0][i];
-  PPB_ATOC(acc, AP_CELL);
-#ifdef PPB_PHASE_TIMERS
-  if (tm.lane == 0)
-    for (int q = 0; q < AP_COUNT; q++) atomicAdd(&g_adj_cycles[q], (unsigned long long)acc[q]);
-#endif
   if (tm.lane == 0) {
     if (b.status) b.status[c] = flag;
     if (b.stats) {
       int* st = b.stats + (size_t)c * 7;
-      if (MODE == ADJ_TANGENT) {
-        fst[0] = bdf.s.nst;
-        fst[1] = bdf.s.nfe;
-        fst[2] = bdf.s.nje;
-        fst[3] = bdf.s.nsetups;
-        fst[4] = bdf.s.nni;
-        fst[5] = bdf.s.netf;
-        fst[6] = bdf.s.ncfn;
-      }
-      for (int q = 0; q < 7; q++) st[q] = fst[q];
+      st[0] = bdf.s.nst;
+      st[1] = bdf.s.nfe;
+      st[2] = bdf.s.nje;
+      st[3] = bdf.s.nsetups;
+      st[4] = bdf.s.nni;
+      st[5] = bdf.s.netf;
+      st[6] = bdf.s.ncfn;
     }
   }
   tm.sync();
 }
 
-template <int NS, typename LT, int MODE>
-__global__ void __launch_bounds__(256) k_adjoint(DevMech M, Options o, AdjBatch b, AdjLayout L, double dt, int* queue)
+template <int NS, typename LT>
+__global__ void __launch_bounds__(256) k_tangent(DevMech M, Options o, AdjBatch b, AdjLayout L, double dt, int* queue)
 {
   extern __shared__ __align__(16) char smem[];
   Team<32> tm;
@@ -238,11 +162,7 @@ __global__ void __launch_bounds__(256) k_adjoint(DevMech M, Options o, AdjBatch 
   Work<LT> w;
   carve<LT>(w, base, NS, R);
   AdjWork a;
-  if (MODE == ADJ_TANGENT)
-    carve_adj(a, base + team_bytes<LT>(NS, R), NS, R);
-  else
-    carve_adj_rev<LT>(a, base + team_bytes<LT>(NS, R), w, NS, R);
-  char* cpb = L.cp + gwarp * (size_t)L.cap_cp * L.cp_stride;
+  carve_adj(a, base + team_bytes<LT>(NS, R), NS, R);
   TapeRec* tape = reinterpret_cast<TapeRec*>(L.tape) + gwarp * (size_t)L.cap_rec;
   double* ys = L.ys + gwarp * (size_t)L.cap_y * (NS + 1);
   for (;;) {
@@ -250,7 +170,7 @@ __global__ void __launch_bounds__(256) k_adjoint(DevMech M, Options o, AdjBatch 
     if (tm.lane == 0) c = atomicAdd(queue, 1);
     c = __shfl_sync(0xffffffffu, c, 0);
     if (c >= b.ncells) break;
-    adjoint_cell<NS, LT, MODE>(tm, M, o, w, a, b, L, cpb, tape, ys, c, dt);
+    tangent_cell<NS, LT>(tm, M, o, w, a, b, L, tape, ys, c, dt);
   }
 }
 
@@ -319,19 +239,18 @@ static __global__ void k_sum_cells(const double* gw, int nc, int np, double* out
   out[p] = s;
 }
 
-template <int NS, typename LT, int MODE>
+template <int NS, typename LT>
 static size_t adj_warp_smem(const DevMech& M)
 {
-  return team_bytes<LT>(NS, M.nrxn) +
-         (MODE == ADJ_TANGENT ? adj_bytes(NS, M.nrxn) : adj_rev_bytes<LT>(NS, M.nrxn));
+  return team_bytes<LT>(NS, M.nrxn) + adj_bytes(NS, M.nrxn);
 }
 
 // Block size (warps) with the most resident warps per SM.
-template <int NS, typename LT, int MODE>
+template <int NS, typename LT>
 static int plan_ns_t(const DevMech& M, AdjPlan* p)
 {
-  const size_t wb = adj_warp_smem<NS, LT, MODE>(M);
-  auto kern = k_adjoint<NS, LT, MODE>;
+  const size_t wb = adj_warp_smem<NS, LT>(M);
+  auto kern = k_tangent<NS, LT>;
   int dev = 0, nsm = 0, smem_max = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -364,7 +283,7 @@ static int plan_ns(const DevMech& M, int mode, int lu_fp32, AdjPlan* p)
 {
   // the reverse integration runs batched (launch_adjoint_batched)
   if (mode != ADJ_TANGENT) return (int)cudaErrorNotSupported;
-  return lu_fp32 ? plan_ns_t<NS, float, ADJ_TANGENT>(M, p) : plan_ns_t<NS, double, ADJ_TANGENT>(M, p);
+  return lu_fp32 ? plan_ns_t<NS, float>(M, p) : plan_ns_t<NS, double>(M, p);
 }
 
 template <int NS>
@@ -377,17 +296,12 @@ static int launch_ns(const DevMech& M, const Options& o, int mode, int lu_fp32, 
   const size_t shm = p.warp_smem * p.wpb;
   typedef void (*KT)(DevMech, Options, AdjBatch, AdjLayout, double, int*);
   if (mode != ADJ_TANGENT) return (int)cudaErrorNotSupported;
-  KT kern = lu_fp32 ? (KT)k_adjoint<NS, float, ADJ_TANGENT> : (KT)k_adjoint<NS, double, ADJ_TANGENT>;
+  KT kern = lu_fp32 ? (KT)k_tangent<NS, float> : (KT)k_tangent<NS, double>;
   e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   if (e != cudaSuccess) return (int)e;
   kern<<<p.blocks, p.wpb * 32, shm, st>>>(M, o, b, L, dt, queue);
   e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
-  if (mode == ADJ_REVERSE && grad && L.gw) {
-    const int np = 3 * M.nrxn;
-    k_sum_cells<<<(np + 127) / 128, 128, 0, st>>>(L.gw, b.ncells, np, grad, accumulate);
-    e = cudaGetLastError();
-  }
   return (int)e;
 }
 
@@ -747,17 +661,6 @@ static int batched_ns_t(const DevMech& M, const Options& o, const AdjBatch& b, A
 
 #define PPB_CAT2(a, b) a##b
 #define PPB_CAT(a, b) PPB_CAT2(a, b)
-#ifdef PPB_PHASE_TIMERS
-int PPB_CAT(adj_phase_cycles_, PPB_NS)(unsigned long long* out, int reset)
-{
-  cudaError_t e = cudaMemcpyFromSymbol(out, g_adj_cycles, sizeof(unsigned long long) * AP_COUNT);
-  if (e == cudaSuccess && reset) {
-    unsigned long long z[AP_COUNT] = {};
-    e = cudaMemcpyToSymbol(g_adj_cycles, z, sizeof(z));
-  }
-  return (int)e;
-}
-#endif
 int PPB_CAT(plan_adjoint_, PPB_NS)(const DevMech& M, int mode, int lu_fp32, AdjPlan* p)
 {
   return plan_ns<PPB_NS>(M, mode, lu_fp32, p);

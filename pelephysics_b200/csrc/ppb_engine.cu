@@ -910,24 +910,6 @@ int phase_cycles(unsigned long long* out, int reset)
   return 0;
 }
 
-int adj_phase_cycles_9(unsigned long long*, int);
-int adj_phase_cycles_21(unsigned long long*, int);
-int adj_phase_cycles_53(unsigned long long*, int);
-int adj_phase_cycles_88(unsigned long long*, int);
-
-int adj_phase_cycles(unsigned long long* out, int reset)
-{
-  for (int q = 0; q < 8; q++) out[q] = 0;
-  int (*fns[4])(unsigned long long*, int) = {adj_phase_cycles_9, adj_phase_cycles_21, adj_phase_cycles_53,
-                                             adj_phase_cycles_88};
-  for (auto fn : fns) {
-    unsigned long long part[8];
-    const int e = fn(part, reset);
-    if (e) return e;
-    for (int q = 0; q < 8; q++) out[q] += part[q];
-  }
-  return 0;
-}
 #endif
 
 int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells, cudaStream_t st)

@@ -109,9 +109,6 @@ void set_error(const char* msg);
 
 #ifdef PPB_PHASE_TIMERS
 int phase_cycles(unsigned long long* out, int reset);
-// adjoint kernel parts: forward, recomputation, sweeps, exact Jacobians,
-// factor + solve, checkpoint save, restore, whole cell (8 totals)
-int adj_phase_cycles(unsigned long long* out, int reset);
 #endif
 
 // Bytes of shared memory one team-integrated cell needs.
