@@ -44,6 +44,11 @@ METRIC = "cells/s per dt (drm19 64^3, tuned engine)"
 FLOPS_RHS = {"drm19": 12023.0}
 FLOPS_JAC = {"drm19": 22943.0}
 CPU_SAMPLE = 8192  # cells of the field integrated by the CPU baseline
+# DRAM bytes (read + write) per cell of one launch of the tuned kernel,
+# from an ncu capture of the same kernel on the 16^3 field (4096 cells:
+# 16.84 MB + 74.83 MB); profiles/k_react_team_drm19_16cubed.md has the
+# command.  Scaled by the cells of a launch (the traffic grows with them).
+TRAFFIC_PER_CELL = (16.841728e6 + 74.83392e6) / 4096
 
 
 def log(*a):
@@ -349,7 +354,8 @@ def our_arm(args):
             achieved = out["flops"] / t_step / 1e12
             peak_t = out["fp64_peak_gflops"] / 1e3
             roof = {"bound": "fp64", "achieved": achieved, "peak": peak_t, "unit": "TFLOP/s",
-                    "frac": achieved / peak_t, "traffic": None,
+                    "frac": achieved / peak_t, "traffic": TRAFFIC_PER_CELL * n,
+                    "traffic_note": "bytes per launch, scaled from the 16^3 ncu capture by cells",
                     "peak_source": "measured FP64 FMA probe on this GPU (ppb_probe_fp64_peak)"}
         line = {
             "metric": METRIC,
