@@ -519,7 +519,9 @@ def config_arm(args):
         Yg = yg[ok, :N] / yg[ok, :N].sum(1, keepdims=True)
         Yc = yc[ok, :N] / yc[ok, :N].sum(1, keepdims=True)
         stats = r.cell_stats(n)
+        wpb, team, regs, _ = r.launch_config()
         out[name] = {"cells_per_s": n * len(ms) / (sum(ms) / 1e3), "ms_per_react": sum(ms) / len(ms),
+                     "autotuned_launch": {"warps_per_block": wpb, "team_lanes": team, "register_budget": regs},
                      "max_rel_T_vs_fp64_oracle": float(dT.max()) if ok.any() else None,
                      "max_abs_Y_vs_fp64_oracle": float(np.abs(Yg - Yc).max()) if ok.any() else None,
                      "nonfinite_cells": int(np.sum(~finite)),

@@ -63,7 +63,8 @@ typedef struct ppb_options {
   int use_graph;            /* replay react() as a captured CUDA graph, 1 */
   int adjoint_checkpoint_interval; /* accepted BDF steps between adjoint checkpoints, 16 */
   int adjoint_memory_mb;    /* device memory for adjoint checkpoints, tapes and points, 16384 */
-  int team_lanes;           /* with warps_per_block > 0: lanes per cell, 32 or 16 (<= 21 species) */
+  int team_lanes;           /* with warps_per_block > 0: lanes per cell, 32, 16 (<= 21 species), 64
+                               (33..64 species) or 128 (65..128 species; one cell per block) */
   int register_budget;      /* with warps_per_block > 0: 2 (<= 128 registers) or 1 (<= 255) */
 } ppb_options;
 

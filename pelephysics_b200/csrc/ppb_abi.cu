@@ -253,8 +253,12 @@ static LaunchConfig launch_config(const ppb_reactor* r)
   lc.persistent = 1;
   if (r->opt.warps_per_block > 0) {
     lc.warps_per_block = r->opt.warps_per_block;
-    lc.team = r->opt.team_lanes == 16 ? 16 : 32;
+    lc.team = (r->opt.team_lanes == 16 || r->opt.team_lanes == 64 || r->opt.team_lanes == 128) ? r->opt.team_lanes : 32;
     lc.minb = r->opt.register_budget == 1 ? 1 : 2;
+    if (lc.team > 32) { // one cell per block of team / 32 warps, <= 255 registers
+      lc.warps_per_block = lc.team / 32;
+      lc.minb = 1;
+    }
     return lc;
   }
   if (lc.engine == ENGINE_TUNED && tuned_config(r, &lc, nullptr)) {
@@ -284,11 +288,14 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
   const int N = r->t->nsp, n = N + 1;
   std::vector<LaunchConfig> cand;
   int max_res = 0;
-  for (int team : {32, 16}) {
-    if (team == 16 && N > 21) continue;
+  const int big = N <= 21 ? 0 : N <= 64 ? 64 : 128;
+  for (int team : {32, 16, big}) {
+    if (team == 0 || (team == 16 && N > 21)) continue;
     for (int minb : {2, 1}) {
-      if (minb == 1 && (r->method != METHOD_BDF || r->opt.lu_fp32)) continue;
+      if (minb == 1 && (r->method != METHOD_BDF || r->opt.lu_fp32) && team <= 32) continue;
+      if (team > 32 && minb != 1) continue;
       for (int wpb : {8, 4, 2, 1}) {
+        if (team > 32 && wpb != team / 32) continue;
         LaunchConfig lc;
         lc.engine = ENGINE_TUNED;
         lc.lu_fp32 = r->opt.lu_fp32;

@@ -48,7 +48,8 @@ struct LaunchConfig {
   int warps_per_block = 4;
   int lu_fp32 = 0;
   int persistent = 1; // work queue
-  int team = 32;      // lanes per cell: 32, or 16 for mechanisms of <= 21 species
+  int team = 32;      // lanes per cell: 32; 16 for <= 21 species; 64 (33..64 species) or 128 (65..128): one
+                      // multi-warp team per block
   int minb = 2;       // register budget: >= minb blocks of 256 threads per SM
 };
 // Resident cells per SM of the tuned kernel in configuration lc (0: the

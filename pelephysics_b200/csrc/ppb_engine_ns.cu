@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, 
                                                           size_t cell_bytes, int persistent)
 {
   extern __shared__ __align__(16) char smem[];
-  Team<TEAM> tm;
+  __shared__ double red[TEAM > 32 ? 16 : 1]; // reductions of a multi-warp team
+  Team<TEAM> tm(red);
   const int team = threadIdx.x / TEAM;
   Work<LT> w;
   carve<LT>(w, smem + (size_t)team * cell_bytes, M.nsp, M.nrxn);
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, 
     for (;;) {
       int c = 0;
       if (tm.lane == 0) c = atomicAdd(queue, 1);
-      c = __shfl_sync(tm.mask, c, 0, TEAM);
+      c = tm.bcast_int(c, 0);
       if (c >= b.ncells) break;
       react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, c, dt);
     }
@@ -136,13 +137,32 @@ __global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, 
 
 typedef void (*TeamKernel)(DevMech, Options, Batch, double, int*, size_t, int);
 
+// Lanes per cell of the multi-warp team compiled for a mechanism: one lane
+// per species (64 for 33..64 species, 128 for 65..128), 0 for <= 21 species.
+template <int NS>
+constexpr int big_team()
+{
+  return NS <= 21 ? 0 : NS <= 64 ? 64 : 128;
+}
+
 // The compiled variants: 32 lanes per cell with both register budgets for
 // the FP64 BDF kernel; 16 lanes per cell as well for mechanisms of at most
-// 21 species.
+// 21 species, and a multi-warp team (one cell per block, one lane per
+// species) for larger ones.
 template <int NS>
 static TeamKernel team_kernel(int method, bool fp32, int team, int minb)
 {
   constexpr bool small = NS <= 21;
+  if (team > 32) {
+    if constexpr (big_team<NS>() > 0) {
+      constexpr int BT = big_team<NS>();
+      if (team != BT) return nullptr;
+      if (method == METHOD_RK64) return (TeamKernel)k_react_team<NS, double, METHOD_RK64, BT, 1>;
+      if (fp32) return (TeamKernel)k_react_team<NS, float, METHOD_BDF, BT, 1>;
+      return (TeamKernel)k_react_team<NS, double, METHOD_BDF, BT, 1>;
+    }
+    return nullptr;
+  }
   if (team == 16 && !small) return nullptr;
   if (method == METHOD_RK64) {
     if (team == 16) return small ? (TeamKernel)k_react_team<NS, double, METHOD_RK64, (small ? 16 : 32), 2> : nullptr;
@@ -176,12 +196,13 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
       k_react_plain<NS, METHOD_RK64><<<blocks, threads, 0, st>>>(M, o, b, dt);
     return (int)cudaGetLastError();
   }
-  const int wpb = lc.warps_per_block > 0 ? lc.warps_per_block : 4;
   const bool fp32 = lc.lu_fp32 && method == METHOD_BDF;
-  const int team = lc.team == 16 ? 16 : 32;
+  const int team = (lc.team == 16 || lc.team > 32) ? lc.team : 32;
+  // a multi-warp team is one block
+  const int wpb = team > 32 ? team / 32 : (lc.warps_per_block > 0 ? lc.warps_per_block : 4);
   TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb);
   if (!kern) return (int)cudaErrorInvalidConfiguration;
-  const int tpb = wpb * (32 / team); // cells per block
+  const int tpb = team > 32 ? 1 : wpb * (32 / team); // cells per block
   const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
   const size_t shm = cb * tpb;
   cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -211,11 +232,11 @@ template <int NS>
 static int occupancy_ns(const DevMech& M, int method, const LaunchConfig& lc)
 {
   const bool fp32 = lc.lu_fp32 && method == METHOD_BDF;
-  const int team = lc.team == 16 ? 16 : 32;
+  const int team = (lc.team == 16 || lc.team > 32) ? lc.team : 32;
   TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb);
   if (!kern) return 0;
-  const int wpb = lc.warps_per_block > 0 ? lc.warps_per_block : 4;
-  const int tpb = wpb * (32 / team);
+  const int wpb = team > 32 ? team / 32 : (lc.warps_per_block > 0 ? lc.warps_per_block : 4);
+  const int tpb = team > 32 ? 1 : wpb * (32 / team);
   const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
   const size_t shm = cb * tpb;
   int dev = 0, smem_max = 0, per_sm = 0;

@@ -109,14 +109,33 @@ struct alignas(16) FoPack {
 };
 static_assert(sizeof(FoPack) == 112, "FoPack is seven 16-byte words");
 
+// A team of TEAM lanes integrates one cell: TEAM = 1 (one thread), 16 or 32
+// (part of or a whole warp: shuffles and __syncwarp), or 64 / 128 (several
+// warps, one team per block: warp shuffles, then the warps' partial results
+// through a small shared scratch and __syncthreads).  Every reduction returns
+// the same bits on every lane (fixed combination order).
+// The block-shared scratch of a multi-warp team (2 * warps doubles); warp
+// teams carry none.
+template <int TEAM, bool MULTI = (TEAM > 32)>
+struct TeamScratch {
+  __device__ __forceinline__ TeamScratch(double*) {}
+};
 template <int TEAM>
-struct Team {
+struct TeamScratch<TEAM, true> {
+  double* red;
+  __device__ __forceinline__ TeamScratch(double* s) : red(s) {}
+};
+
+template <int TEAM>
+struct Team : TeamScratch<TEAM> {
+  static constexpr int W = TEAM < 32 ? TEAM : 32; // lanes per warp in the team
+  static constexpr int NW = TEAM > 32 ? TEAM / 32 : 1;
   int lane;
   unsigned mask;
-  __device__ __forceinline__ Team()
+  __device__ __forceinline__ Team(double* scratch = nullptr) : TeamScratch<TEAM>(scratch)
   {
     lane = (TEAM == 1) ? 0 : (int)(threadIdx.x % TEAM);
-    if (TEAM == 32) {
+    if (TEAM >= 32) {
       mask = 0xffffffffu;
     } else if (TEAM == 1) {
       mask = 1u << (threadIdx.x % 32);
@@ -126,30 +145,102 @@ struct Team {
   }
   __device__ __forceinline__ void sync() const
   {
-    if (TEAM > 1) __syncwarp(mask);
+    if (TEAM > 32) {
+      __syncthreads();
+    } else if (TEAM > 1) {
+      __syncwarp(mask);
+    }
+  }
+  template <typename T, typename Op>
+  __device__ __forceinline__ T reduce(T x, Op op) const
+  {
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) x = op(x, __shfl_xor_sync(mask, x, o, W));
+    if constexpr (TEAM > 32) {
+      T* r = reinterpret_cast<T*>(this->red);
+      if ((lane & 31) == 0) r[lane >> 5] = x;
+      __syncthreads();
+      x = r[0];
+#pragma unroll
+      for (int i = 1; i < NW; i++) x = op(x, r[i]);
+      __syncthreads();
+    }
+    return x;
   }
   __device__ __forceinline__ double sum(double x) const
   {
-#pragma unroll
-    for (int o = TEAM / 2; o > 0; o >>= 1) x += __shfl_xor_sync(mask, x, o, TEAM);
-    return x;
+    return reduce(x, [](double a, double b) { return a + b; });
   }
   __device__ __forceinline__ double max(double x) const
   {
-#pragma unroll
-    for (int o = TEAM / 2; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(mask, x, o, TEAM));
-    return x;
+    return reduce(x, [](double a, double b) { return fmax(a, b); });
   }
   __device__ __forceinline__ int imax(int x) const
   {
-#pragma unroll
-    for (int o = TEAM / 2; o > 0; o >>= 1) x = ::max(x, __shfl_xor_sync(mask, x, o, TEAM));
-    return x;
+    return reduce(x, [](int a, int b) { return ::max(a, b); });
   }
   // broadcast from team lane src
   __device__ __forceinline__ double bcast(double x, int src) const
   {
-    return (TEAM == 1) ? x : __shfl_sync(mask, x, src, TEAM);
+    if constexpr (TEAM == 1) {
+      return x;
+    } else if constexpr (TEAM <= 32) {
+      return __shfl_sync(mask, x, src, TEAM);
+    } else {
+      if (lane == src) this->red[0] = x;
+      __syncthreads();
+      const double v = this->red[0];
+      __syncthreads();
+      return v;
+    }
+  }
+  __device__ __forceinline__ int bcast_int(int x, int src) const
+  {
+    if constexpr (TEAM == 1) {
+      return x;
+    } else if constexpr (TEAM <= 32) {
+      return __shfl_sync(mask, x, src, TEAM);
+    } else {
+      int* r = reinterpret_cast<int*>(this->red);
+      if (lane == src) r[0] = x;
+      __syncthreads();
+      const int v = r[0];
+      __syncthreads();
+      return v;
+    }
+  }
+  // largest best over the team, ties to the smallest index bi
+  __device__ __forceinline__ void argmax(double& best, int& bi) const
+  {
+    if constexpr (TEAM > 1) {
+#pragma unroll
+      for (int o = W / 2; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(mask, best, o, W);
+        const int oi = __shfl_xor_sync(mask, bi, o, W);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+    }
+    if constexpr (TEAM > 32) {
+      int* ri = reinterpret_cast<int*>(this->red + NW);
+      if ((lane & 31) == 0) {
+        this->red[lane >> 5] = best;
+        ri[lane >> 5] = bi;
+      }
+      __syncthreads();
+      best = this->red[0];
+      bi = ri[0];
+#pragma unroll
+      for (int i = 1; i < NW; i++) {
+        if (this->red[i] > best || (this->red[i] == best && ri[i] < bi)) {
+          best = this->red[i];
+          bi = ri[i];
+        }
+      }
+      __syncthreads();
+    }
   }
 };
 

@@ -79,7 +79,22 @@ def test_drm19_bdf(cuda, oracle, eng):
 # the thread-per-cell plain engine keeps a whole cell workspace (56 KB for
 # dodecane_lu, 142 KB for heptane_lu_88sk) in thread-local memory: it is the
 # drm19 baseline and is not exercised on the large mechanisms
-@pytest.mark.parametrize("eng", ENGINES[1:], ids=["tuned", "tuned_fp32"])
+def multi_warp(team):
+    """The tuned engine pinned to one multi-warp team (team lanes) per cell."""
+    return [dict(engine=1, warps_per_block=1, team_lanes=team),
+            dict(engine=1, warps_per_block=1, team_lanes=team, lu_fp32=1, refine_sweeps=1)]
+
+
+def check_pinned(r, eng):
+    """A pinned multi-warp team runs as one block of team/32 warps with the
+    255-register budget, and the launch-config query says so."""
+    team = eng.get("team_lanes", 0)
+    if team > 32:
+        assert r.launch_config()[:3] == (team // 32, team, 1)
+
+
+@pytest.mark.parametrize("eng", ENGINES[1:] + multi_warp(64),
+                         ids=["tuned", "tuned_fp32", "team64", "team64_fp32"])
 def test_dodecane_bdf_with_sources(cuda, oracle, eng):
     """dodecane_lu at 40 atm, dt 2e-6 s, with mass-conserving advective
     species sources (the 128x128x64 configuration's recipe)."""
@@ -94,12 +109,14 @@ def test_dodecane_bdf_with_sources(cuda, oracle, eng):
     assert flag == 0
     r = Reactor(mech)
     r.init(rtype, nc, **opts, **eng)
+    check_pinned(r, eng)
     y = rY.copy()
     r.react(y, src.copy(), rX.copy(), rXs.copy(), dt)
     compare(y, ref)
 
 
-@pytest.mark.parametrize("eng", ENGINES[1:], ids=["tuned", "tuned_fp32"])
+@pytest.mark.parametrize("eng", ENGINES[1:] + multi_warp(128),
+                         ids=["tuned", "tuned_fp32", "team128", "team128_fp32"])
 def test_heptane_bdf(cuda, oracle, eng):
     """heptane_lu_88sk (the 88x88 Newton matrix), 20 atm, rtol 1e-8,
     atol 1e-12, as the 64^3 configuration."""
@@ -110,13 +127,14 @@ def test_heptane_bdf(cuda, oracle, eng):
     assert flag == 0
     r = Reactor(mech)
     r.init(rtype, nc, **opts, **eng)
+    check_pinned(r, eng)
     y = rY.copy()
     r.react(y, src.copy(), rX.copy(), rXs.copy(), dt)
     # rtol 1e-8 on the integration: the bar scales with it
     compare(y, ref, T_rtol=1e-6, Y_atol=1e-7)
 
 
-@pytest.mark.parametrize("eng", ENGINES[1:2], ids=["tuned"])
+@pytest.mark.parametrize("eng", ENGINES[1:2] + multi_warp(128)[:1], ids=["tuned", "team128"])
 def test_heptane_rk64(cuda, oracle, eng):
     """RK64 on heptane_lu_88sk at 20 atm over a step its 500-substep cap can
     resolve (at 750-1400 K and dt = 1e-5 s the explicit scheme is unstable
