@@ -548,6 +548,82 @@ def config_arm(args):
     return 0
 
 
+def arkode_arm(args):
+    """ReactorArkode (the batch-coupled explicit reactor) on the drm19 64^3
+    field: the whole field as one integration on the GPU (cells/s per
+    dt_react), and on a 4096-cell batch of the field the GPU against the
+    oracle's restatement (same step and RHS counts, state differences) and the
+    oracle's CPU time (OpenMP over the host cores)."""
+    import torch
+
+    from oracle import pyoracle as po
+    from pelephysics_b200 import workloads as wl
+    from pelephysics_b200.reactor import Reactor
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    dt, opts = 1e-6, dict(rtol=1e-6, atol=1e-10)  # ode.rtol / ode.atol defaults
+    cells = wl.drm19_field(args.edge, device=dev)
+    n = cells.ncells
+    N = cells.rY.shape[1] - 1
+    r = Reactor(MECH, "ReactorArkode")
+    r.init(1, n, **opts)
+    y0 = torch.as_tensor(cells.rY, device=dev).contiguous()
+    s0 = torch.as_tensor(cells.rYsrc, device=dev).contiguous()
+    x0 = torch.as_tensor(cells.rX, device=dev)
+    xs = torch.as_tensor(cells.rX_src, device=dev)
+    y = y0.clone()
+    x = x0.clone()
+    for _ in range(max(args.warmup, 1)):
+        y.copy_(y0)
+        x.copy_(x0)
+        r.react(y, s0, x, xs, dt)
+    ms = []
+    for _ in range(args.steps):
+        y.copy_(y0)
+        x.copy_(x0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        cost, _, _, _ = r.react(y, s0, x, xs, dt)
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    stats = r.cell_stats(n)[0]
+    full = {"cells_per_s": n * len(ms) / (sum(ms) / 1e3), "ms_per_react": sum(ms) / len(ms),
+            "steps": int(stats[0]), "rhs_evals": int(stats[1]), "err_test_fails": int(stats[5]),
+            "cell_rhs_per_s": n * int(stats[1]) * len(ms) / (sum(ms) / 1e3)}
+    r.close()
+    # a 4096-cell batch: GPU vs the oracle, and the oracle's CPU time
+    nb = min(4096, n)
+    rb = Reactor(MECH, "ReactorArkode")
+    rb.init(1, nb, **opts)
+    yb = cells.rY[:nb].copy()
+    xb = cells.rX[:nb].copy()
+    gcost, _, _, _ = rb.react(yb, cells.rYsrc[:nb].copy(), xb, cells.rX_src[:nb].copy(), dt)
+    gst = rb.cell_stats(nb)[0]
+    rb.close()
+    yc = cells.rY[:nb].copy()
+    t0 = time.perf_counter()
+    flag, st = po.react_arkode(MECH, 1, yc, np.ascontiguousarray(cells.rYsrc[:nb]), cells.rX[:nb].copy(),
+                               cells.rX_src[:nb].copy(), dt, **opts)
+    cpu_s = time.perf_counter() - t0
+    dT = np.abs(yb[:, N] - yc[:, N]) / yc[:, N]
+    Yg = yb[:, :N] / yb[:, :N].sum(1, keepdims=True)
+    Yc = yc[:, :N] / yc[:, :N].sum(1, keepdims=True)
+    line = {"config": "arkode", "workload": f"drm19 {args.edge}^3 field ({n} cells), dt {dt} s, rtol 1e-6, "
+                                            "atol 1e-10, ZONNEVELD_5_3_4 + PID (the flat path's defaults), "
+                                            "one batch-coupled integration",
+            "gpu": full,
+            "batch_4096": {"gpu_steps": int(gst[0]), "oracle_steps": st["nst"], "gpu_rhs_evals": int(gcost),
+                           "oracle_rhs_evals": st["nfe"], "oracle_flag": int(flag),
+                           "max_rel_T_vs_oracle": float(dT.max()),
+                           "max_abs_Y_vs_oracle": float(np.abs(Yg - Yc).max()),
+                           "oracle_cpu_s": cpu_s, "oracle_cells_per_s": nb / cpu_s, "cores": os.cpu_count()},
+            "dtype": "f64"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def flops_probe():
     """One drm19 cell: reactor RHS and reactor Jacobian pointwise kernels,
     thread per cell (run under ncu to count FP64 operations)."""
@@ -665,8 +741,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-workload measurement")
     ap.add_argument("--adjoint-cells", type=int, default=65536)
-    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane"],
-                    help="drm19: the headline line; dodecane / heptane: the larger configurations")
+    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane", "arkode"],
+                    help="drm19: the headline line; dodecane / heptane: the larger configurations; arkode: "
+                         "the ReactorArkode integrator on the drm19 field")
     ap.add_argument("--sample", type=int, default=256, help="oracle sample cells for --config dodecane/heptane")
     ap.add_argument("--launch", default="", help="W,T,R: fixed warps per block, lanes per cell, register budget "
                                                  "instead of the autotuner (profiling runs)")
@@ -686,6 +763,8 @@ def main():
         return phase_probe(args.edge)
     if args.impl == "reference":
         return reference_arm(args)
+    if args.config == "arkode":
+        return arkode_arm(args)
     if args.config != "drm19":
         return config_arm(args)
     return our_arm(args)

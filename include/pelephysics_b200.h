@@ -66,6 +66,11 @@ typedef struct ppb_options {
   int team_lanes;           /* with warps_per_block > 0: lanes per cell, 32, 16 (<= 21 species), 64
                                (33..64 species) or 128 (65..128 species; one cell per block) */
   int register_budget;      /* with warps_per_block > 0: 2 (<= 128 registers) or 1 (<= 255) */
+  /* ReactorArkode (ReactorArkode.cpp:10-20, ReactorArkode.H:131-137) */
+  int rk_method;            /* ode.rk_method, 40 (ZONNEVELD_5_3_4); box path only, as in the reference */
+  int rk_controller;        /* ode.rk_controller, 0 (PID), 1 PI, 2 I, 3 explicit Gustafsson; box path only */
+  int use_erkstep;          /* ode.use_erkstep, 1 (ERKStep and an explicit-only ARKStep integrate alike) */
+  int arkode_max_steps;     /* internal steps per react call, 500 (the ARKODE default; the reference sets none) */
 } ppb_options;
 
 /* An amrex::Array4<Real>-compatible view: element (i,j,k,n) lives at
@@ -101,7 +106,15 @@ const char* ppb_species_name(const char* mechanism, int k);
 int ppb_molecular_weights(const char* mechanism, double* mw);
 
 /* ReactorBase::create (Factory.H:72-81).  integrator is "ReactorCvode"
- * (BDF, the ReactorCvode drop-in) or "ReactorRK64" (explicit RK64). */
+ * (BDF, the ReactorCvode drop-in), "ReactorRK64" (explicit RK64) or
+ * "ReactorArkode" (explicit embedded RK over the whole batch with one
+ * adaptive step, the ReactorArkode drop-in: ReactorArkode.cpp:134-398; the
+ * flat paths use the default order-4 table and PID controller, the box path
+ * rk_method / rk_controller, as the reference does).  For ReactorArkode a
+ * call that stops early (arkode_max_steps reached, repeated error-test
+ * failures) returns PPB_E_INTEGRATE with *dt_react set to the interval
+ * actually integrated (the reference's MOD_REACTOR bookkeeping,
+ * ReactorArkode.cpp:223-226) and rX advanced by that interval. */
 int ppb_create(const char* mechanism, const char* integrator, ppb_reactor** out);
 /* ReactorBase::init(reactor_type, ncells) (ReactorBase.H:19) with options. */
 int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* opt);

@@ -3,9 +3,9 @@
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/liboracle.so"
-SRC=("$HERE/mech_eval.c" "$HERE/reactor.c")
+SRC=("$HERE/mech_eval.c" "$HERE/reactor.c" "$HERE/arkode.c")
 newest=0
-for f in "${SRC[@]}" "$HERE/oracle.h" "$HERE"/../pelephysics_b200/csrc/mech/*.h; do
+for f in "${SRC[@]}" "$HERE/oracle.h" "$HERE"/../pelephysics_b200/csrc/mech/*.h "$HERE"/../pelephysics_b200/csrc/ppb_erk_tables.h; do
   t=$(stat -c %Y "$f"); [ "$t" -gt "$newest" ] && newest=$t
 done
 if [ -f "$OUT" ] && [ "$(stat -c %Y "$OUT")" -ge "$newest" ]; then exit 0; fi

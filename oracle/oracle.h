@@ -78,6 +78,26 @@ typedef struct PPOOptions {
 
 void ppo_default_options(PPOOptions* o);
 
+// ReactorArkode (ReactorArkode.cpp:10-20, :134-398): the whole batch as one
+// explicit embedded RK integration with one adaptive step.
+typedef struct PPOArkOptions {
+  double rtol, atol;
+  int rk_method;      // ode.rk_method (table number), 40
+  int rk_controller;  // ode.rk_controller: 0 PID, 1 PI, 2 I, 3 explicit Gustafsson
+  long max_steps;     // ARKODE's default 500
+  const double* typ_vals_atol; // N+1 absolute tolerances or NULL
+} PPOArkOptions;
+typedef struct PPOArkStats {
+  double t, h;        // time reached (tout on success), last step
+  long nst, nfe, netf;
+  int status;         // 0 ok, -1 too much work, -3 error-test failures, -27 too close
+} PPOArkStats;
+// rY[ncells*(N+1)] YCOrder in/out, rX advanced by the time reached; cells
+// with mask == -1 are left untouched (mask may be NULL).
+int ppo_react_arkode(
+  const PPBMechTables* M, int reactor_type, const PPOArkOptions* opt, double* rY, const double* rYsrc, double* rX,
+  const double* rX_src, const int* mask, double dt, int ncells, int nthreads, PPOArkStats* st);
+
 // Integrate one cell (YCOrder y[N+1], in/out) over dt with the CVODE
 // algorithm; returns the CVODE-style flag.
 int ppo_bdf_cell(

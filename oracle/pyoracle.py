@@ -98,6 +98,8 @@ def lib():
         L.ppo_reactor_rhs.restype = C.c_double
         L.ppo_reactor_jac.argtypes = [C.c_void_p, C.c_int, _DP, _DP]
         L.ppo_default_options.argtypes = [C.POINTER(Options)]
+        L.ppo_react_arkode.argtypes = [C.c_void_p, C.c_int, C.POINTER(ArkOptions), _DP, _DP, _DP, _DP, _IP,
+                                       C.c_double, C.c_int, C.c_int, C.POINTER(ArkStats)]
         L.ppo_bdf_cell.argtypes = [C.c_void_p, C.c_int, C.POINTER(Options), _DP, _DP, C.c_double,
                                    C.c_double, C.c_double, C.POINTER(Stats)]
         L.ppo_rk64_cell.argtypes = [C.c_void_p, C.c_int, C.POINTER(Options), _DP, _DP, C.c_double,
@@ -328,6 +330,35 @@ def react_flat_arrhenius(mech, A, beta, EaR, reactor_type, rY, rYsrc, rX, rX_src
     finally:
         L.ppo_mech_free(M)
     return flag, nfe, st
+
+
+class ArkOptions(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("rk_method", C.c_int), ("rk_controller", C.c_int),
+                ("max_steps", C.c_long), ("typ_vals_atol", _DP)]
+
+
+class ArkStats(C.Structure):
+    _fields_ = [("t", C.c_double), ("h", C.c_double), ("nst", C.c_long), ("nfe", C.c_long), ("netf", C.c_long),
+                ("status", C.c_int)]
+
+
+def react_arkode(mech, reactor_type, rY, rYsrc, rX, rX_src, dt, rtol=1e-6, atol=1e-10, rk_method=40,
+                 rk_controller=0, max_steps=500, mask=None, atolv=None, nthreads=0):
+    """ReactorArkode restatement: the batch as one explicit embedded RK
+    integration (YCOrder arrays modified in place, rX advanced by the time
+    reached).  Returns (status, dict of t, h, nst, nfe, netf)."""
+    L = lib()
+    o = ArkOptions(float(rtol), float(atol), int(rk_method), int(rk_controller), int(max_steps), None)
+    if atolv is not None:
+        atolv = np.ascontiguousarray(atolv, float)
+        o.typ_vals_atol = _p(atolv)
+    ncells = rX.shape[0]
+    mk = None if mask is None else np.ascontiguousarray(mask, np.int32)
+    st = ArkStats()
+    flag = L.ppo_react_arkode(C.c_void_p(Mech(mech).M), reactor_type, C.byref(o), _p(rY), _p(rYsrc), _p(rX),
+                              _p(rX_src), None if mk is None else mk.ctypes.data_as(_IP), float(dt), ncells,
+                              nthreads, C.byref(st))
+    return flag, {"t": st.t, "h": st.h, "nst": st.nst, "nfe": st.nfe, "netf": st.netf}
 
 
 def load_ref(mech):

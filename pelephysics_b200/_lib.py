@@ -45,6 +45,10 @@ class Options(C.Structure):
         ("adjoint_memory_mb", C.c_int),
         ("team_lanes", C.c_int),
         ("register_budget", C.c_int),
+        ("rk_method", C.c_int),
+        ("rk_controller", C.c_int),
+        ("use_erkstep", C.c_int),
+        ("arkode_max_steps", C.c_int),
     ]
 
 

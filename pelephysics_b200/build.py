@@ -43,6 +43,8 @@ def _units():
         units.append((f"ppb_engine_ns{ns}.o", "ppb_engine_ns.cu", [f"-DPPB_NS={ns}"]))
     for ns in SPECIES_COUNTS:
         units.append((f"ppb_adjoint_ns{ns}.o", "ppb_adjoint_ns.cu", [f"-DPPB_NS={ns}"]))
+    for ns in SPECIES_COUNTS:
+        units.append((f"ppb_ark_ns{ns}.o", "ppb_ark_ns.cu", [f"-DPPB_NS={ns}"]))
     return units
 
 

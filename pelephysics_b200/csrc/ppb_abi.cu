@@ -98,6 +98,14 @@ struct ppb_reactor {
   double* atolv = nullptr;
   int *status = nullptr, *nfe = nullptr, *queue = nullptr, *mask = nullptr, *stats = nullptr;
   int last_ncells = 0;
+  // ReactorArkode: cell-major state, stage-0 and FSAL derivatives, sources,
+  // block partial sums, grid barrier, batch result
+  size_t ark_cap = 0;
+  double *ark_y0 = nullptr, *ark_y1 = nullptr, *ark_f0 = nullptr, *ark_f1 = nullptr, *ark_s = nullptr;
+  double* ark_partial = nullptr;
+  unsigned* ark_bar = nullptr;
+  ArkInfo* ark_info = nullptr;
+  ArkInfo ark_last{};
   // graph cache for the device paths; capture runs on a private stream (the
   // legacy default stream cannot be captured) and the graph is launched on
   // the caller's stream
@@ -165,7 +173,19 @@ static void free_scratch(ppb_reactor* r)
   r->cap = 0;
   if (r->gexec) cudaGraphExecDestroy(r->gexec);
   r->gexec = nullptr;
+  for (double** q : {&r->ark_y0, &r->ark_y1, &r->ark_f0, &r->ark_f1, &r->ark_s, &r->ark_partial}) {
+    cudaFree(*q);
+    *q = nullptr;
+  }
+  cudaFree(r->ark_bar);
+  cudaFree(r->ark_info);
+  r->ark_bar = nullptr;
+  r->ark_info = nullptr;
+  r->ark_cap = 0;
 }
+
+// capacity of the ARKODE partial-sum buffer, in blocks (>= SMs x resident blocks)
+static const int ARK_MAX_GRID = 4096;
 
 static int ensure_scratch(ppb_reactor* r, int ncells)
 {
@@ -184,6 +204,86 @@ static int ensure_scratch(ppb_reactor* r, int ncells)
   PPB_CUDA(cudaMalloc(&r->stats, c * 7 * 4), "cudaMalloc");
   PPB_CUDA(cudaMalloc(&r->queue, 16), "cudaMalloc");
   r->cap = c;
+  if (r->method == METHOD_ARK) {
+    const size_t N = r->t->nsp;
+    PPB_CUDA(cudaMalloc(&r->ark_y0, n * c * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&r->ark_y1, n * c * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&r->ark_f0, n * c * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&r->ark_f1, n * c * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&r->ark_s, N * c * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&r->ark_partial, 2 * ARK_MAX_GRID * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&r->ark_bar, 16), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&r->ark_info, sizeof(ArkInfo)), "cudaMalloc");
+    r->ark_cap = c;
+  }
+  return 0;
+}
+
+// The ERK table of a reference ode.rk_method number; unknown numbers select
+// the default, as the reference's switch does (ReactorArkode.cpp:80-83).
+static const ErkTable& erk_table(int id)
+{
+  for (int i = 0; i < ppb_erk_ntables; i++)
+    if (ppb_erk_tables[i].id == id) return ppb_erk_tables[i];
+  return erk_table(40);
+}
+
+static bool erk_fsal(const ErkTable& t)
+{
+  const int s = t.stages;
+  if (t.c[s - 1] != 1.0 || t.b[s - 1] != 0.0) return false;
+  for (int j = 0; j < s - 1; j++)
+    if (t.A[s - 1][j] != t.b[j]) return false;
+  return true;
+}
+
+// ReactorArkode over a species-major device batch: one cooperative launch.
+// box: the box path (rk_method / rk_controller apply); rhoe_out: where the
+// energies advanced by the time reached go (nullable).
+static int run_ark(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st, double* rhoe_out, bool box)
+{
+  ArkParams P{};
+  P.tab = erk_table(box ? r->opt.rk_method : 40);
+  P.rtol = r->opt.rtol;
+  P.atol = r->opt.atol;
+  P.tout = dt;
+  P.reactor_type = r->reactor_type;
+  const int ctl = box ? r->opt.rk_controller : 0;
+  P.controller = (ctl >= 0 && ctl <= 3) ? ctl : 0; // unknown: PID (ReactorArkode.cpp:110-114)
+  P.max_steps = r->opt.arkode_max_steps;
+  P.fsal = erk_fsal(P.tab) ? 1 : 0;
+  ArkBuffers B{};
+  B.ncells = b.ncells;
+  B.ld = b.ld;
+  B.ysoa = b.y;
+  B.srcsoa = b.src;
+  B.rhoe = b.rhoe;
+  B.rhoesrc = b.rhoesrc;
+  B.mask = b.mask;
+  B.atolv = r->atolv;
+  B.rhoe_out = rhoe_out;
+  B.Y0 = r->ark_y0;
+  B.Y1 = r->ark_y1;
+  B.F0 = r->ark_f0;
+  B.F1 = r->ark_f1;
+  B.S = r->ark_s;
+  B.partial = r->ark_partial;
+  B.bar = r->ark_bar;
+  B.info = r->ark_info;
+  B.status = r->status;
+  B.nfe = r->nfe;
+  B.stats = r->stats;
+  PPB_CUDA(cudaMemsetAsync(r->ark_info, 0, sizeof(ArkInfo), st), "cudaMemsetAsync");
+  int grid = ARK_MAX_GRID;
+  return cuda_fail(launch_ark(*r->dm, P, B, &grid, st), "launch_ark");
+}
+
+// Result of the last ReactorArkode launch (synchronises the stream).
+static int ark_result(ppb_reactor* r, cudaStream_t st)
+{
+  PPB_CUDA(cudaMemcpyAsync(&r->ark_last, r->ark_info, sizeof(ArkInfo), cudaMemcpyDeviceToHost, st), "D2H info");
+  PPB_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  if (r->ark_last.barrier_timeout) return fail(PPB_E_CUDA, "ReactorArkode: grid barrier timed out");
   return 0;
 }
 
@@ -390,7 +490,7 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
 // Run the autotuner on this batch unless the stream is being captured.
 static int maybe_autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
 {
-  if (r->opt.engine != PPB_ENGINE_TUNED || r->opt.warps_per_block > 0) return 0;
+  if (r->method == METHOD_ARK || r->opt.engine != PPB_ENGINE_TUNED || r->opt.warps_per_block > 0) return 0;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return 0;
   return autotune(r, b, dt, st);
@@ -444,6 +544,10 @@ void ppb_default_options(ppb_options* o)
   o->adjoint_memory_mb = 16384;
   o->team_lanes = 32;
   o->register_budget = 2;
+  o->rk_method = 40;
+  o->rk_controller = 0;
+  o->use_erkstep = 1;
+  o->arkode_max_steps = 500;
 }
 
 const char* ppb_last_error(void) { return g_err; }
@@ -484,6 +588,8 @@ int ppb_create(const char* mechanism, const char* integrator, ppb_reactor** out)
     method = METHOD_BDF;
   } else if (!strcmp(integrator, "ReactorRK64") || !strcmp(integrator, "ReactorB200RK")) {
     method = METHOD_RK64;
+  } else if (!strcmp(integrator, "ReactorArkode")) {
+    method = METHOD_ARK;
   } else {
     return fail(PPB_E_ARG, std::string("unknown integrator ") + integrator);
   }
@@ -567,12 +673,14 @@ void ppb_destroy(ppb_reactor* r)
 }
 
 // Integrate a species-major batch already on the device (the core call).
-static int run_batch(ppb_reactor* r, Batch b, double dt, cudaStream_t st)
+static int run_batch(ppb_reactor* r, Batch b, double dt, cudaStream_t st, double* rhoe_out = nullptr,
+                     bool box = false)
 {
   b.atolv = r->atolv;
   b.status = r->status;
   b.nfe = r->nfe;
   b.stats = r->stats;
+  if (r->method == METHOD_ARK) return run_ark(r, b, dt, st, rhoe_out, box);
   int te = maybe_autotune(r, b, dt, st);
   if (te) return te;
   const Options o = engine_options(r);
@@ -593,6 +701,11 @@ static int finish(ppb_reactor* r, int ncells, cudaStream_t st, long* cost)
   for (int c = 0; c < ncells; c++) {
     tot += nfe[c];
     if (stat[c] < 0) bad++;
+  }
+  if (r->method == METHOD_ARK) {
+    int ae = ark_result(r, st);
+    if (ae) return ae;
+    tot = r->ark_last.nfe; // one integrator for the batch: its RHS evaluations
   }
   if (cost) *cost = (r->method == METHOD_RK64) ? (ncells ? tot / ncells : 0) : tot;
   if (bad) return fail(PPB_E_INTEGRATE, std::to_string(bad) + " cell(s) failed to integrate");
@@ -633,6 +746,7 @@ int ppb_react_flat(ppb_reactor* r, double* rY, double* rYsrc, double* rX, double
   PPB_CUDA(launch_soa_to_aos(r->soa, ncells, n, r->aos, n, ncells, st), "soa_to_aos");
   PPB_CUDA(cudaMemcpyAsync(rY, r->aos, (size_t)ncells * n * 8, cudaMemcpyDeviceToHost, st), "D2H rY");
   e = finish(r, ncells, st, cost);
+  if (r->method == METHOD_ARK) *dt_react = r->ark_last.t; // the interval integrated
   // ReactorCvode.cpp:1652-1655: rX += dt * rX_src on the host arrays
   for (int i = 0; i < ncells; i++) rX[i] = rX[i] + *dt_react * rX_src[i];
   *time += *dt_react;
@@ -668,14 +782,14 @@ int ppb_react_flat_device(ppb_reactor* r, double* rY, double* rYsrc, double* rX,
     b.rhoesrc = rX_src;
     b.ncells = ncells;
     b.ld = ncells;
-    ee = run_batch(r, b, dt, s);
+    ee = run_batch(r, b, dt, s, rX);
     if (ee) return ee;
     ee = launch_soa_to_aos(r->soa, ncells, n, rY, n, ncells, s);
-    if (!ee) ee = launch_energy_update(rX, rX_src, dt, ncells, s);
+    if (!ee && r->method != METHOD_ARK) ee = launch_energy_update(rX, rX_src, dt, ncells, s);
     if (ee) return cuda_fail(ee, "soa_to_aos");
     return 0;
   };
-  if (r->opt.use_graph) {
+  if (r->opt.use_graph && r->method != METHOD_ARK) {
     if (!r->gexec || !(r->gkey == key)) {
       // tune outside the capture, on the batch converted to species-major
       PPB_CUDA(launch_aos_to_soa(rY, n, r->soa, ncells, n, ncells, st), "aos_to_soa");
@@ -698,7 +812,8 @@ int ppb_react_flat_device(ppb_reactor* r, double* rY, double* rYsrc, double* rX,
     if (e) return e;
   }
   e = finish(r, ncells, st, cost);
-  *time += dt;
+  if (r->method == METHOD_ARK) *dt_react = r->ark_last.t;
+  *time += *dt_react;
   return e;
 }
 
@@ -726,11 +841,12 @@ int ppb_react_soa_device(ppb_reactor* r, double* y, const double* src, double* r
   b.ncells = ncells;
   b.ld = ld;
   auto body = [&](cudaStream_t s) -> int {
-    int ee = run_batch(r, b, dt, s);
-    if (!ee) ee = cuda_fail(launch_energy_update(rX, rX_src, dt, ncells, s), "energy_update");
+    int ee = run_batch(r, b, dt, s, rX);
+    if (!ee && r->method != METHOD_ARK)
+      ee = cuda_fail(launch_energy_update(rX, rX_src, dt, ncells, s), "energy_update");
     return ee;
   };
-  if (r->opt.use_graph) {
+  if (r->opt.use_graph && r->method != METHOD_ARK) {
     if (!r->gexec || !(r->gkey == key)) {
       e = maybe_autotune(r, b, dt, st); // outside the capture
       if (e) return e;
@@ -743,7 +859,8 @@ int ppb_react_soa_device(ppb_reactor* r, double* y, const double* src, double* r
     if (e) return e;
   }
   e = finish(r, ncells, st, cost);
-  *time += dt;
+  if (r->method == METHOD_ARK) *dt_react = r->ark_last.t;
+  *time += *dt_react;
   return e;
 }
 
@@ -816,8 +933,13 @@ int ppb_react_box(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 r
   b.ld = ncells;
   b.nfe = r->nfe;
   PPB_CUDA(launch_box_flatten(*r->dm, r->reactor_type, r->opt.clean_init_massfrac, a, b, st), "box_flatten");
-  e = run_batch(r, b, *dt_react, st);
+  e = run_batch(r, b, *dt_react, st, nullptr, true);
   if (e) return e;
+  if (r->method == METHOD_ARK) {
+    e = ark_result(r, st);
+    if (e) return e;
+    *dt_react = r->ark_last.t; // the interval integrated (ReactorArkode.cpp:223-226)
+  }
   PPB_CUDA(launch_box_unflatten(*r->dm, r->reactor_type, r->opt.clean_init_massfrac, a, b, *dt_react, st),
            "box_unflatten");
   e = finish(r, ncells, st, nullptr);

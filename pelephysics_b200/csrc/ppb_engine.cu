@@ -454,6 +454,23 @@ PPB_DECL(21)
 PPB_DECL(53)
 PPB_DECL(88)
 
+#define PPB_DECL_ARK(NS) int launch_ark_##NS(const DeviceMechanism&, const ArkParams&, const ArkBuffers&, int*, cudaStream_t);
+PPB_DECL_ARK(9)
+PPB_DECL_ARK(21)
+PPB_DECL_ARK(53)
+PPB_DECL_ARK(88)
+
+int launch_ark(const DeviceMechanism& m, const ArkParams& P, const ArkBuffers& B, int* grid, cudaStream_t st)
+{
+  switch (m.host->nsp) {
+  case 9: return launch_ark_9(m, P, B, grid, st);
+  case 21: return launch_ark_21(m, P, B, grid, st);
+  case 53: return launch_ark_53(m, P, B, grid, st);
+  case 88: return launch_ark_88(m, P, B, grid, st);
+  default: return (int)cudaErrorNotSupported;
+  }
+}
+
 int launch_react(const DeviceMechanism& m, const Options& o, int method, const LaunchConfig& lc, Batch b,
                  double dt, int* queue, cudaStream_t st)
 {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "mech/mech_tables.h"
+#include "ppb_erk_tables.h"
 
 namespace ppb {
 struct DevMech;
@@ -41,7 +42,7 @@ struct Batch {
 };
 
 enum Engine { ENGINE_PLAIN = 0, ENGINE_TUNED = 1 };
-enum Method { METHOD_BDF = 0, METHOD_RK64 = 1 };
+enum Method { METHOD_BDF = 0, METHOD_RK64 = 1, METHOD_ARK = 2 };
 
 struct LaunchConfig {
   int engine = ENGINE_TUNED;
@@ -103,6 +104,43 @@ int launch_pyt2re(const DeviceMechanism& m, int eh, const double* P, const doubl
 // FP64 FMA throughput probe: returns GFLOP/s measured with CUDA events.
 int probe_fp64_peak(double* gflops, cudaStream_t st);
 int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells, cudaStream_t st);
+
+enum ArkController { ARK_PID = 0, ARK_PI = 1, ARK_I = 2, ARK_EXPGUS = 3 };
+
+// The ARKODE-style reactor (ppb_ark.cuh): method, tolerances, end time.
+struct ArkParams {
+  ErkTable tab;
+  double rtol, atol, tout;
+  int reactor_type, controller, max_steps, fsal;
+};
+
+// Batch result: time reached, last step, counters, flag.
+struct ArkInfo {
+  double t, h;
+  long long nst, nfe, netf, attempts;
+  int status, barrier_timeout;
+};
+
+// Device buffers of one call.
+struct ArkBuffers {
+  int ncells, ld;
+  double* ysoa;          // in/out, species-major with leading dimension ld
+  const double* srcsoa;  // species sources, species-major
+  const double *rhoe, *rhoesrc;
+  const int* mask;       // -1 skips a cell (nullable)
+  const double* atolv;   // N+1 absolute tolerances (nullable: atol)
+  double* rhoe_out;      // nullable: rhoe + t_reached * rhoesrc
+  double *Y0, *Y1, *F0, *F1, *S; // cell-major scratch
+  double* partial;       // 2 * gridDim.x doubles
+  unsigned* bar;         // [arrivals, generation]
+  ArkInfo* info;
+  int *status, *nfe, *stats;
+};
+
+// Integrate the batch with one cooperative launch; *grid in: the capacity of
+// B.partial / 2 (0: no bound), out: the grid used.
+int launch_ark(const DeviceMechanism& m, const ArkParams& P, const ArkBuffers& B, int* grid, cudaStream_t st);
+
 
 // Store the message ppb_last_error() returns for the calling thread (no
 // allocation).

@@ -47,7 +47,7 @@ def _stream(stream):
 
 
 class Reactor:
-    """A chemistry reactor on the GPU ("ReactorCvode" or "ReactorRK64")."""
+    """A chemistry reactor on the GPU ("ReactorCvode", "ReactorRK64" or "ReactorArkode")."""
 
     def __init__(self, mechanism: str, integrator: str = "ReactorCvode"):
         self.mechanism = mechanism
