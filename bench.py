@@ -624,6 +624,68 @@ def arkode_arm(args):
     return 0
 
 
+def transport_arm(args):
+    """Mixture-averaged transport (ppb_transport, the reference's
+    SimpleTransport) on the drm19 edge^3 field and on edge^3 heptane_lu_88sk
+    cells (edge 64 by default): cells/s, the binary-diffusion pairs per
+    second, the HBM traffic the call needs, the oracle's agreement on a
+    sample and its CPU time."""
+    import torch
+
+    from oracle import pyoracle as po
+    from pelephysics_b200 import transport as tr
+    from pelephysics_b200 import workloads as wl
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    out = {}
+    for mech, cells in (("drm19", wl.drm19_field(args.edge, device=dev)),
+                        ("heptane_lu_88sk", wl.heptane_cells(args.edge ** 3, device=dev))):
+        n = cells.ncells
+        N = cells.rY.shape[1] - 1
+        rho = cells.rY[:, :N].sum(1)
+        Y = cells.rY[:, :N] / rho[:, None]
+        T = cells.rY[:, N]
+        Td = torch.as_tensor(T, device=dev)
+        rd = torch.as_tensor(rho, device=dev)
+        Yd = torch.as_tensor(np.ascontiguousarray(Y.T), device=dev)
+        res = None
+        for _ in range(max(args.warmup, 1)):
+            res = tr.transport(mech, Td, rd, Yd, tr.TR_ALL)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            res = tr.transport(mech, Td, rd, Yd, tr.TR_ALL)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        t_ms = sum(ms) / len(ms)
+        # bytes the call must move: Y, T, rho in; D, chi, mu, xi, lam out
+        hbm = n * 8.0 * (N + 2 + 2 * N + 3)
+        idx = cpu_sample_index(n, 512)
+        D = res["D"].cpu().numpy().T
+        worst = 0.0
+        for c in idx[:64]:
+            Dr, _, mur, _, lamr = po.transport(mech, po.TR_ALL, T[c], rho[c], Y[c])
+            worst = max(worst, float(np.max(np.abs(D[c] - Dr) / np.abs(Dr))),
+                        abs(res["mu"][c].item() - mur) / mur, abs(res["lam"][c].item() - lamr) / lamr)
+        ns = min(n, 20000)
+        t0 = time.perf_counter()
+        po.transport_batch(mech, po.TR_ALL, T[:ns], rho[:ns], Y[:ns])
+        cpu_s = time.perf_counter() - t0
+        out[mech] = {"cells": n, "ms_per_call": t_ms, "cells_per_s": n / (t_ms / 1e3),
+                     "dbin_pairs_per_s": n * N * (N - 1) / 2 / (t_ms / 1e3), "hbm_gb_s": hbm / (t_ms / 1e3) / 1e9,
+                     "max_rel_vs_oracle_64_cells": worst,
+                     "oracle_cpu_cells_per_s": ns / cpu_s, "oracle_cores": os.cpu_count()}
+    print(json.dumps({"config": "transport", "workload": "SimpleTransport (D, chi, mu, xi, lam) on the drm19 "
+                      f"{args.edge}^3 field and {args.edge ** 3} heptane_lu_88sk cells", "results": out,
+                      "dtype": "f64"}),
+          flush=True)
+    return 0
+
+
 def flops_probe():
     """One drm19 cell: reactor RHS and reactor Jacobian pointwise kernels,
     thread per cell (run under ncu to count FP64 operations)."""
@@ -741,7 +803,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-workload measurement")
     ap.add_argument("--adjoint-cells", type=int, default=65536)
-    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane", "arkode"],
+    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane", "arkode", "transport"],
                     help="drm19: the headline line; dodecane / heptane: the larger configurations; arkode: "
                          "the ReactorArkode integrator on the drm19 field")
     ap.add_argument("--sample", type=int, default=256, help="oracle sample cells for --config dodecane/heptane")
@@ -765,6 +827,8 @@ def main():
         return reference_arm(args)
     if args.config == "arkode":
         return arkode_arm(args)
+    if args.config == "transport":
+        return transport_arm(args)
     if args.config != "drm19":
         return config_arm(args)
     return our_arm(args)

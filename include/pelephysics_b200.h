@@ -196,6 +196,28 @@ int ppb_reactor_rhs(const char* mechanism, int reactor_type, double t, const dou
 int ppb_pyt2re(const char* mechanism, int eh, const double* P, const double* T, const double* Y, double* rho,
                double* e, int ncells, void* stream);
 
+/* Mixture-averaged transport coefficients: the reference's SimpleTransport
+ * (Source/Transport/Simple.H) with the ideal-gas EOS and the mechanism's
+ * CEPTR transport fits.  flags select the outputs as SimpleTransport::
+ * transport's wtr_get_* switches do (Simple.H:263-270); xi is computed only
+ * together with mu (else 0), as there. */
+#define PPB_TR_XI 1   /* bulk viscosity xi, g/(cm s) */
+#define PPB_TR_MU 2   /* shear viscosity mu, g/(cm s) */
+#define PPB_TR_LAM 4  /* thermal conductivity lambda, erg/(cm s K) */
+#define PPB_TR_DIAG 8 /* mixture-averaged Ddiag_k (rho D_k W_k / W), g/(cm s) */
+#define PPB_TR_CHI 16 /* thermal diffusion ratios of the light species (others 0) */
+/* SimpleTransport::transport per cell on DEVICE arrays: T, rho [ncells];
+ * Y, D, chi species-major with leading dimension ld >= ncells
+ * (Y[k*ld + c]); outputs not selected by flags may be NULL. */
+int ppb_transport(const char* mechanism, int flags, const double* T, const double* rho, const double* Y, int ld,
+                  double* D, double* chi, double* mu, double* xi, double* lam, int ncells, void* stream);
+/* SimpleTransport::get_transport_coeffs (Simple.H:395-446) on a box of DEVICE
+ * Array4 views: Y, D, chi N components, T, rho, mu, xi, lam one; chi is
+ * written only with use_soret (transport.use_soret), as there. */
+int ppb_transport_box(const char* mechanism, int use_soret, const int lo[3], const int hi[3], ppb_array4 Y,
+                      ppb_array4 T, ppb_array4 rho, ppb_array4 D, ppb_array4 chi, ppb_array4 mu, ppb_array4 xi,
+                      ppb_array4 lam, void* stream);
+
 /* Allocation-free flat react on DEVICE YCOrder arrays (no counterpart in the
  * reference).  For callers that must not have a library allocate GPU memory,
  * e.g. applications whose device memory is owned by an arena allocator

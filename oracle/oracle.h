@@ -9,6 +9,7 @@
 // lines it restates.
 #pragma once
 #include "../pelephysics_b200/csrc/mech/mech_tables.h"
+#include "../pelephysics_b200/csrc/mech/trans_tables.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -77,6 +78,16 @@ typedef struct PPOOptions {
 } PPOOptions;
 
 void ppo_default_options(PPOOptions* o);
+
+// Mixture-averaged transport (Source/Transport/Simple.H, ideal gas) at one
+// point: flags bit 0 bulk viscosity xi, 1 viscosity mu, 2 conductivity lam,
+// 3 Ddiag, 4 thermal diffusion ratios chi (the light species; others 0).
+#define NMAX_TR 96
+const PPBTransTables* ppo_trans(const char* name);
+int ppo_transport(const char* mech, int flags, double T, double rho, const double* Y, double* D, double* chi,
+                  double* mu, double* xi, double* lam);
+int ppo_transport_batch(const char* mech, int flags, int ncells, const double* T, const double* rho, const double* Y,
+                        double* D, double* chi, double* mu, double* xi, double* lam, int nthreads);
 
 // ReactorArkode (ReactorArkode.cpp:10-20, :134-398): the whole batch as one
 // explicit embedded RK integration with one adaptive step.

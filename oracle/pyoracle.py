@@ -491,3 +491,55 @@ class Ref:
         J = np.zeros((self.nsp + 1) ** 2)
         self.L.ref_reactor_jac(reactor_type, _p(np.ascontiguousarray(y, float)), _p(J))
         return J.reshape(self.nsp + 1, self.nsp + 1)
+
+
+# ---------------------------------------------------------------- transport
+TR_XI, TR_MU, TR_LAM, TR_DIAG, TR_CHI = 1, 2, 4, 8, 16
+TR_ALL = TR_XI | TR_MU | TR_LAM | TR_DIAG | TR_CHI
+_reftr = {}
+
+
+def _tr_call(fn, flags, T, rho, Y):
+    N = Y.shape[-1]
+    D, chi = np.zeros(N), np.zeros(N)
+    mu, xi, lam = C.c_double(), C.c_double(), C.c_double()
+    y = np.ascontiguousarray(Y, float)
+    fn(int(flags), float(T), float(rho), _p(y), _p(D), _p(chi), C.byref(mu), C.byref(xi), C.byref(lam))
+    return D, chi, mu.value, xi.value, lam.value
+
+
+def transport(mech, flags, T, rho, Y):
+    """Mixture-averaged transport (Simple.H restatement) at one point:
+    (Ddiag[N], chi[N], mu, xi, lam); see oracle.h for the flags."""
+    L = lib()
+    if not getattr(L, "_tr_set", False):
+        L.ppo_transport.argtypes = [C.c_char_p, C.c_int, C.c_double, C.c_double, _DP, _DP, _DP, _DP, _DP, _DP]
+        L._tr_set = True
+    fn = lambda *a: L.ppo_transport(mech.encode(), *a)  # noqa: E731
+    return _tr_call(fn, flags, T, rho, Y)
+
+
+def reftr_path(mech):
+    return os.path.join(HERE, "_ref", f"libreftr_{mech}.so")
+
+
+def ref_transport(mech, flags, T, rho, Y):
+    """The reference's own compiled SimpleTransport::transport (oracle/_ref)."""
+    if mech not in _reftr:
+        L = C.CDLL(reftr_path(mech))
+        L.reftr_transport.argtypes = [C.c_int, C.c_double, C.c_double, _DP, _DP, _DP, _DP, _DP, _DP]
+        _reftr[mech] = L
+    return _tr_call(_reftr[mech].reftr_transport, flags, T, rho, Y)
+
+
+def transport_batch(mech, flags, T, rho, Y, nthreads=0):
+    """transport() over cells (Y [n, N] cell-major), OpenMP over cells."""
+    L = lib()
+    L.ppo_transport_batch.argtypes = [C.c_char_p, C.c_int, C.c_int, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP, C.c_int]
+    n, N = Y.shape
+    T, rho, Y = (np.ascontiguousarray(a, float) for a in (T, rho, Y))
+    D, chi = np.zeros((n, N)), np.zeros((n, N))
+    mu, xi, lam = np.zeros(n), np.zeros(n), np.zeros(n)
+    L.ppo_transport_batch(mech.encode(), int(flags), n, _p(T), _p(rho), _p(Y), _p(D), _p(chi), _p(mu), _p(xi),
+                          _p(lam), int(nthreads))
+    return D, chi, mu, xi, lam

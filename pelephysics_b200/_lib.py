@@ -125,6 +125,8 @@ def lib():
     L.ppb_tangent_flat_device.argtypes = [vp, dp, dp, dp, dp, C.c_double, C.c_int, dp, dp, dp, dp, dp, vp]
     L.ppb_rhs_exact.argtypes = [C.c_char_p, C.c_int, C.c_double, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp,
                                 C.c_int, vp]
+    L.ppb_transport.argtypes = [C.c_char_p, C.c_int, dp, dp, dp, C.c_int, dp, dp, dp, dp, dp, C.c_int, vp]
+    L.ppb_transport_box.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [Array4] * 8 + [vp]
     _lib = L
     return L
 

@@ -38,6 +38,7 @@ def _units():
         ("ppb_engine.o", "ppb_engine.cu", []),
         ("ppb_abi.o", "ppb_abi.cu", []),
         ("ppb_noalloc.o", "ppb_noalloc.cu", []),
+        ("ppb_transport.o", "ppb_transport.cu", []),
     ]
     for ns in SPECIES_COUNTS:
         units.append((f"ppb_engine_ns{ns}.o", "ppb_engine_ns.cu", [f"-DPPB_NS={ns}"]))

@@ -947,6 +947,85 @@ int ppb_react_box(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 r
   return e;
 }
 
+// ---------------------------------------------------------------- transport
+static int transport_tables(const char* mechanism, DeviceMechanism** dm, DeviceTransport** dt)
+{
+  const PPBMechTables* t = mechanism ? find_mechanism(mechanism) : nullptr;
+  const PPBTransTables* tr = mechanism ? find_transport(mechanism) : nullptr;
+  if (!t || !tr) return fail(PPB_E_MECH, std::string("unknown mechanism ") + (mechanism ? mechanism : "(null)"));
+  int e = device_mechanism(t, dm);
+  if (e) return e;
+  e = device_transport(tr, dt);
+  return e ? cuda_fail(e, "transport tables") : 0;
+}
+
+static BoxView flat_view(const double* p, long nstride)
+{
+  BoxView v{};
+  v.p = const_cast<double*>(p);
+  v.nstride = nstride;
+  return v;
+}
+
+int ppb_transport(const char* mechanism, int flags, const double* T, const double* rho, const double* Y, int ld,
+                  double* D, double* chi, double* mu, double* xi, double* lam, int ncells, void* stream)
+{
+  if (ncells < 0 || ld < ncells || (flags & ~31)) return fail(PPB_E_ARG, "ppb_transport: invalid arguments");
+  if (ncells > 0 && (!T || !Y || ((flags & PPB_TR_DIAG) && !D) || ((flags & PPB_TR_CHI) && !chi) ||
+                     ((flags & PPB_TR_MU) && !mu) || ((flags & PPB_TR_XI) && !xi) || ((flags & PPB_TR_LAM) && !lam)))
+    return fail(PPB_E_ARG, "ppb_transport: null array for a selected output");
+  DeviceMechanism* dm = nullptr;
+  DeviceTransport* dt = nullptr;
+  int e = transport_tables(mechanism, &dm, &dt);
+  if (e || ncells == 0) return e;
+  TrBox b{};
+  b.hi[0] = ncells - 1;
+  b.Y = flat_view(Y, ld);
+  b.T = flat_view(T, 0);
+  b.rho = flat_view(rho, 0);
+  b.D = flat_view(D, ld);
+  b.chi = flat_view(chi, ld);
+  b.mu = flat_view((flags & PPB_TR_MU) ? mu : nullptr, 0);
+  b.xi = flat_view((flags & PPB_TR_XI) ? xi : nullptr, 0);
+  b.lam = flat_view((flags & PPB_TR_LAM) ? lam : nullptr, 0);
+  return cuda_fail(launch_transport(*dm, *dt, flags, b, (cudaStream_t)stream), "launch_transport");
+}
+
+int ppb_transport_box(const char* mechanism, int use_soret, const int lo[3], const int hi[3], ppb_array4 Y,
+                      ppb_array4 T, ppb_array4 rho, ppb_array4 D, ppb_array4 chi, ppb_array4 mu, ppb_array4 xi,
+                      ppb_array4 lam, void* stream)
+{
+  if (!lo || !hi) return fail(PPB_E_ARG, "ppb_transport_box: null box");
+  const PPBMechTables* t = mechanism ? find_mechanism(mechanism) : nullptr;
+  if (!t) return fail(PPB_E_MECH, std::string("unknown mechanism ") + (mechanism ? mechanism : "(null)"));
+  const int N = t->nsp;
+  for (int d = 0; d < 3; d++)
+    if (hi[d] < lo[d]) return fail(PPB_E_ARG, "ppb_transport_box: empty box");
+  if (!covers(Y, lo, hi, N) || !covers(T, lo, hi, 1) || !covers(rho, lo, hi, 1) || !covers(D, lo, hi, N) ||
+      !covers(mu, lo, hi, 1) || !covers(xi, lo, hi, 1) || !covers(lam, lo, hi, 1) ||
+      (use_soret && !covers(chi, lo, hi, N)))
+    return fail(PPB_E_ARG, "ppb_transport_box: an Array4 does not cover the box");
+  DeviceMechanism* dm = nullptr;
+  DeviceTransport* dt = nullptr;
+  int e = transport_tables(mechanism, &dm, &dt);
+  if (e) return e;
+  TrBox b{};
+  for (int d = 0; d < 3; d++) {
+    b.lo[d] = lo[d];
+    b.hi[d] = hi[d];
+  }
+  b.Y = view(Y);
+  b.T = view(T);
+  b.rho = view(rho);
+  b.D = view(D);
+  b.chi = use_soret ? view(chi) : BoxView{};
+  b.mu = view(mu);
+  b.xi = view(xi);
+  b.lam = view(lam);
+  const int flags = PPB_TR_XI | PPB_TR_MU | PPB_TR_LAM | PPB_TR_DIAG | (use_soret ? PPB_TR_CHI : 0);
+  return cuda_fail(launch_transport(*dm, *dt, flags, b, (cudaStream_t)stream), "launch_transport");
+}
+
 int ppb_get_cell_status(ppb_reactor* r, int* status, int* cost, int ncells)
 {
   if (!r || ncells < 0 || ncells > r->last_ncells) return fail(PPB_E_ARG, "ppb_get_cell_status: bad arguments");

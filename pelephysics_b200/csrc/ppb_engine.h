@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include "mech/mech_tables.h"
+#include "mech/trans_tables.h"
 #include "ppb_erk_tables.h"
 
 namespace ppb {
@@ -104,6 +105,26 @@ int launch_pyt2re(const DeviceMechanism& m, int eh, const double* P, const doubl
 // FP64 FMA throughput probe: returns GFLOP/s measured with CUDA events.
 int probe_fp64_peak(double* gflops, cudaStream_t st);
 int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells, cudaStream_t st);
+
+// Mixture-averaged transport (ppb_transport.cu).  A mechanism's transport
+// tables uploaded to one device, and the views of one call: a box lo..hi
+// (a flat batch is the box 0..ncells-1 x 0 x 0) with Y, D, chi holding N
+// components nstride apart.  flags: 1 xi, 2 mu, 4 lam, 8 Ddiag, 16 chi.
+struct DevTrans;
+struct DeviceTransport {
+  const PPBTransTables* host = nullptr;
+  int device = -1;
+  void* blob = nullptr;
+  DevTrans* dt = nullptr;
+};
+struct TrBox {
+  int lo[3], hi[3];
+  BoxView Y, T, rho, D, chi, mu, xi, lam;
+};
+const PPBTransTables* find_transport(const char* name);
+int device_transport(const PPBTransTables* t, DeviceTransport** out);
+int launch_transport(const DeviceMechanism& m, const DeviceTransport& tr, int flags, const TrBox& b,
+                     cudaStream_t st);
 
 enum ArkController { ARK_PID = 0, ARK_PI = 1, ARK_I = 2, ARK_EXPGUS = 3 };
 

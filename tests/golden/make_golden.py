@@ -4,10 +4,13 @@ Runs in a container that has the reference tree: it compiles
 Mechanisms/<mech>/mechanism.H through oracle/build_ref.sh and evaluates the
 reference's generated functions (productionRate, aJacobian in both consP
 modes, CKUBMS/CKHBMS/CKCVBS/CKCPBS, CKUMS/CKHMS, gibbs, GET_T_GIVEN_EY/HY)
-on seeded random states.  The .npz files it writes are the committed
-fixtures the tests compare the CPU oracle and the CUDA kernels against.
+on seeded random states, and the reference's SimpleTransport::transport
+(Source/Transport/Simple.H, compiled by oracle/build_ref.sh with the
+mechanism's transport fits) on seeded (T, rho, Y).  The .npz files it writes
+are the committed fixtures the tests compare the CPU oracle and the CUDA
+kernels against.
 
-Usage: python tests/golden/make_golden.py
+Usage: python tests/golden/make_golden.py [point|transport]   (default both)
 """
 
 import os
@@ -36,8 +39,34 @@ def states(nsp, npts, seed):
     return T, sc, Y
 
 
+TRANSPORT_POINTS = {"LiDryer": 24, "drm19": 24, "dodecane_lu": 12, "heptane_lu_88sk": 8}
+
+
+def transport_main():
+    for seed, (mech, npts) in enumerate(TRANSPORT_POINTS.items()):
+        N = po.Mech(mech).nsp
+        rng = np.random.default_rng(2000 + seed)
+        T = rng.uniform(300.0, 3000.0, npts)
+        rho = 10.0 ** rng.uniform(-5, -1, npts)
+        Y = rng.uniform(0.0, 1.0, (npts, N)) ** 4
+        Y[rng.uniform(size=(npts, N)) < 0.15] = 0.0
+        Y /= Y.sum(axis=1, keepdims=True)
+        res = [po.ref_transport(mech, po.TR_ALL, T[i], rho[i], Y[i]) for i in range(npts)]
+        out = {"T": T, "rho": rho, "Y": Y, "D": np.array([r[0] for r in res]), "chi": np.array([r[1] for r in res]),
+               "mu": np.array([r[2] for r in res]), "xi": np.array([r[3] for r in res]),
+               "lam": np.array([r[4] for r in res])}
+        path = os.path.join(HERE, f"transport_{mech}.npz")
+        np.savez_compressed(path, **out)
+        print(mech, npts, os.path.getsize(path), "bytes")
+
+
 def main():
     po.build()
+    what = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if what in ("all", "transport"):
+        transport_main()
+    if what == "transport":
+        return
     for seed, (mech, npts) in enumerate(POINTS.items()):
         R = po.Ref(mech)
         N = R.nsp
