@@ -147,7 +147,19 @@ __device__ int lu_factor(const Team<TEAM>& tm, LT* A, int n, int* piv)
         bi = i;
       }
     }
-    tm.argmax(best, bi);
+    if constexpr (TEAM <= 32) {
+#pragma unroll
+      for (int o = TEAM / 2; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(tm.mask, best, o, TEAM);
+        const int oi = __shfl_xor_sync(tm.mask, bi, o, TEAM);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+    } else {
+      tm.argmax(best, bi);
+    }
     const int l = bi;
     // a zero column is singular; an all-NaN column selects no row (bi == n)
     if (!(best > 0.0) || l >= n) {

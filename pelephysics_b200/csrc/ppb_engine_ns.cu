@@ -110,13 +110,11 @@ __global__ void __launch_bounds__(128) k_react_plain(DevMech M, Options o, Batch
 // shared-memory workspace, persistent work queue.  MINB is the register
 // budget: at least MINB blocks of 256 threads per SM (2: <= 128 registers a
 // thread, 1: <= 255).
-template <int NS, typename LT, int METHOD, int TEAM, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
-                                                          size_t cell_bytes, int persistent)
+template <int NS, typename LT, int METHOD, int TEAM>
+__device__ __forceinline__ void react_team_body(const Team<TEAM>& tm, const DevMech& M, const Options& o,
+                                                const Batch& b, double dt, int* queue, size_t cell_bytes,
+                                                int persistent, char* smem)
 {
-  extern __shared__ __align__(16) char smem[];
-  __shared__ double red[TEAM > 32 ? 16 : 1]; // reductions of a multi-warp team
-  Team<TEAM> tm(red);
   const int team = threadIdx.x / TEAM;
   Work<LT> w;
   carve<LT>(w, smem + (size_t)team * cell_bytes, M.nsp, M.nrxn);
@@ -132,6 +130,38 @@ __global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, 
   } else {
     const int c = blockIdx.x * tpb + team;
     if (c < b.ncells) react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, c, dt);
+  }
+}
+
+// Warp teams carry no block-shared scratch; a multi-warp team gets 16
+// doubles for its cross-warp reductions.
+template <int NS, typename LT, int METHOD, int TEAM, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
+                                                          size_t cell_bytes, int persistent)
+{
+  extern __shared__ __align__(16) char smem[];
+  if constexpr (TEAM > 32) {
+    __shared__ double red[16];
+    const Team<TEAM> tm(red);
+    react_team_body<NS, LT, METHOD, TEAM>(tm, M, o, b, dt, queue, cell_bytes, persistent, smem);
+  } else {
+    Team<TEAM> tm;
+    const int team = threadIdx.x / TEAM;
+    Work<LT> w;
+    carve<LT>(w, smem + (size_t)team * cell_bytes, M.nsp, M.nrxn);
+    const int tpb = blockDim.x / TEAM;
+    if (persistent) {
+      for (;;) {
+        int c = 0;
+        if (tm.lane == 0) c = atomicAdd(queue, 1);
+        c = __shfl_sync(tm.mask, c, 0, TEAM);
+        if (c >= b.ncells) break;
+        react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, c, dt);
+      }
+    } else {
+      const int c = blockIdx.x * tpb + team;
+      if (c < b.ncells) react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, c, dt);
+    }
   }
 }
 

@@ -167,17 +167,37 @@ struct Team : TeamScratch<TEAM> {
     }
     return x;
   }
+  // warp teams: plain xor butterflies (the multi-warp path adds the
+  // cross-warp step of reduce)
   __device__ __forceinline__ double sum(double x) const
   {
-    return reduce(x, [](double a, double b) { return a + b; });
+    if constexpr (TEAM <= 32) {
+#pragma unroll
+      for (int o = TEAM / 2; o > 0; o >>= 1) x += __shfl_xor_sync(mask, x, o, TEAM);
+      return x;
+    } else {
+      return reduce(x, [](double a, double b) { return a + b; });
+    }
   }
   __device__ __forceinline__ double max(double x) const
   {
-    return reduce(x, [](double a, double b) { return fmax(a, b); });
+    if constexpr (TEAM <= 32) {
+#pragma unroll
+      for (int o = TEAM / 2; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(mask, x, o, TEAM));
+      return x;
+    } else {
+      return reduce(x, [](double a, double b) { return fmax(a, b); });
+    }
   }
   __device__ __forceinline__ int imax(int x) const
   {
-    return reduce(x, [](int a, int b) { return ::max(a, b); });
+    if constexpr (TEAM <= 32) {
+#pragma unroll
+      for (int o = TEAM / 2; o > 0; o >>= 1) x = ::max(x, __shfl_xor_sync(mask, x, o, TEAM));
+      return x;
+    } else {
+      return reduce(x, [](int a, int b) { return ::max(a, b); });
+    }
   }
   // broadcast from team lane src
   __device__ __forceinline__ double bcast(double x, int src) const
