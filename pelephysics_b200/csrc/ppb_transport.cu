@@ -10,10 +10,14 @@
 //     pair list whose coefficients are contiguous, into the cell's matrix E
 //     in shared memory; lane i then forms its row sum in the reference's
 //     order j = 0..N-1, reading E column-wise (conflict-free);
-//   * N <= 96: species blocks of 32; for each block pair (I <= J) lane i of
-//     block I evaluates E_ij for the 32 j of block J, adds X_j E_ij to its
-//     row, and a warp sum of X_i E_ij hands row j its share (no matrix kept;
-//     the row sums' order differs from the reference's in the last bits).
+//   * N <= 96: species blocks of 32.  For a block pair I < J, at rotation
+//     d = 0..31 lane l evaluates E_ij for i = 32 I + l, j = 32 J + (l + d)
+//     mod 32, adds X_j E_ij to its row and passes X_i E_ij by one shuffle to
+//     the lane owning row j; a diagonal block needs rotations 1..16 only.
+//     The coefficients are stored in that (pair of blocks, rotation, lane)
+//     order, so every load is coalesced; padding and duplicate entries carry
+//     a constant term of 1000 (exp = 0).  No matrix is kept; the row sums'
+//     order differs from the reference's in the last bits.
 // Tiles of Y, T and rho are staged through shared memory with loads along
 // the box's x rows, and the outputs leave the same way.  Mixture sums (mean
 // weight, viscosity, conductivity, bulk viscosity, thermal diffusion) are
@@ -43,7 +47,7 @@ const PPBTransTables* find_transport(const char* name)
 // Device copy of one mechanism's transport tables (one allocation).
 struct DevTrans {
   int nsp, nlite, npairs;
-  const double *wt, *iwt, *eps, *zrot, *cvms, *fitmu, *fitlam, *fitdbin, *pairc, *fittdrat;
+  const double *wt, *iwt, *eps, *zrot, *cvms, *fitmu, *fitlam, *tilec, *pairc, *fittdrat;
   const int *nlin, *ktdif, *pairs; // pairs: i | j << 16, i < j
 };
 
@@ -67,12 +71,14 @@ __device__ __forceinline__ double fit3(const double* c, double L0, double L1, do
   return c[0] + c[1] * L0 + c[2] * L1 + c[3] * L2;
 }
 
-// shared memory of a block: Y, D, chi tiles [N][TT]; per warp X, Y [N] and,
-// with NB == 0, the cell's E matrix [N][ld], ld = N rounded up to odd
+// shared memory of a block: Y, D, chi tiles [N][TT]; per warp X, Y [NP]
+// (NP = N, or 32 NB zero-padded) and, with NB == 0, the cell's E matrix
+// [N][ld], ld = N rounded up to odd
 __host__ __device__ inline int e_ld(int N) { return N | 1; }
 __host__ __device__ inline size_t tr_smem_doubles(int N, int tt, int nb)
 {
-  return (size_t)3 * N * tt + (size_t)TR_WARPS * (2 * N + (nb == 0 ? (size_t)N * e_ld(N) : 0));
+  const size_t np = nb ? 32 * (size_t)nb : (size_t)N;
+  return (size_t)3 * N * tt + (size_t)TR_WARPS * (2 * np + (nb == 0 ? (size_t)N * e_ld(N) : 0));
 }
 
 // TT cells per block tile; NB = 0: the E-matrix form (N <= 32), else the
@@ -88,9 +94,10 @@ __global__ void __launch_bounds__(TR_THREADS) k_transport(DevMech M, DevTrans t,
   double* Dt = Yt + (size_t)N * TT;
   double* Ct = Dt + (size_t)N * TT;
   const int team = threadIdx.x / TEAM;
-  double* X = Ct + (size_t)N * TT + (size_t)team * (2 * N + (NB == 0 ? (size_t)N * ld : 0));
-  double* Yw = X + N;
-  double* E = Yw + N;
+  const int NP = NB ? 32 * NB : N;
+  double* X = Ct + (size_t)N * TT + (size_t)team * (2 * NP + (NB == 0 ? (size_t)N * ld : 0));
+  double* Yw = X + NP;
+  double* E = Yw + NP;
   const Team<TEAM> tm;
   const bool get_xi = flags & 1, get_mu = flags & 2, get_lam = flags & 4, get_D = flags & 8, get_chi = flags & 16;
   const int nx = b.hi[0] - b.lo[0] + 1, ny = b.hi[1] - b.lo[1] + 1;
@@ -129,6 +136,7 @@ __global__ void __launch_bounds__(TR_THREADS) k_transport(DevMech M, DevTrans t,
       }
       const double wbar = 1.0 / tm.sum(a);
       for (int s = tm.lane; s < N; s += TEAM) X[s] = Yw[s] * wbar * t.iwt[s];
+      for (int s = N + tm.lane; s < NP; s += TEAM) X[s] = Yw[s] = 0.0;
       tm.sync();
       double mu = 0.0, xi = 0.0, lam = 0.0;
       if (get_mu) {
@@ -174,23 +182,17 @@ __global__ void __launch_bounds__(TR_THREADS) k_transport(DevMech M, DevTrans t,
         double t2[NB > 0 ? NB : 1];
 #pragma unroll
         for (int I = 0; I < NB; I++) t2[I] = 0.0;
+        const double* c = t.tilec + 4 * tm.lane;
 #pragma unroll
         for (int I = 0; I < NB; I++) {
-          const int i = I * 32 + tm.lane;
-          const bool vi = i < N;
-          const double Xi = vi ? X[i] : 0.0;
-          const double* fi = t.fitdbin + 4 * (vi ? i : 0);
-          const int je = min(N, I * 32 + 32);
-          for (int j = I * 32; j < je; j++)
-            if (vi && j != i) t2[I] += X[j] * exp(-fit3(fi + (size_t)4 * N * j, L0, L1, L2));
+          const double Xi = X[I * 32 + tm.lane];
 #pragma unroll
-          for (int J = I + 1; J < NB; J++) {
-            const int je2 = min(N, J * 32 + 32);
-            for (int j = J * 32; j < je2; j++) {
-              const double e = vi ? exp(-fit3(fi + (size_t)4 * N * j, L0, L1, L2)) : 0.0;
-              t2[I] += X[j] * e;
-              const double cs = tm.sum(Xi * e);
-              if (tm.lane == j - J * 32) t2[J] += cs;
+          for (int J = I; J < NB; J++) {
+            const int d0 = I == J ? 1 : 0, d1 = I == J ? 16 : 31;
+            for (int d = d0; d <= d1; d++, c += 128) {
+              const double e = exp(-fit3(c, L0, L1, L2));
+              t2[I] += X[J * 32 + ((tm.lane + d) & 31)] * e;
+              t2[J] += __shfl_sync(0xffffffffu, Xi * e, (tm.lane - d) & 31);
             }
           }
         }
@@ -295,9 +297,22 @@ int upload_transport(const PPBTransTables* t, DeviceTransport* out)
       }
       pr.push_back(i | (j << 16));
     }
+  // species-block form: per block pair I <= J, rotation d, lane l the
+  // coefficients of (32 I + l, 32 J + (l + d) mod 32); padding species and
+  // the duplicate half of rotation 16 of a diagonal block get exp = 0
+  std::vector<double> tc;
+  const int NB = (N + 31) / 32;
+  for (int I = 0; I < NB; I++)
+    for (int J = I; J < NB; J++)
+      for (int dd = (I == J ? 1 : 0); dd <= (I == J ? 16 : 31); dd++)
+        for (int l = 0; l < 32; l++) {
+          const int i = 32 * I + l, j = 32 * J + ((l + dd) & 31);
+          const bool ok = i < N && j < N && !(I == J && dd == 16 && l >= 16);
+          for (int q = 0; q < 4; q++) tc.push_back(ok ? t->fitdbin[4 * (i + N * j) + q] : (q == 0 ? 1000.0 : 0.0));
+        }
   const size_t o_wt = put(t->wt, N), o_iwt = put(iwt.data(), N), o_eps = put(t->eps, N), o_zrot = put(t->zrot, N),
                o_cvms = put(t->cvms, N), o_mu = put(t->fitmu, 4 * N), o_lam = put(t->fitlam, 4 * N),
-               o_full = put(t->fitdbin, (size_t)4 * N * N), o_db = put(pc.data(), pc.size()),
+               o_full = put(tc.data(), tc.size()), o_db = put(pc.data(), pc.size()),
                o_td = put(t->fittdrat, (size_t)4 * N * L);
   const size_t nd = d.size();
   std::vector<int> ii(t->nlin, t->nlin + N);
