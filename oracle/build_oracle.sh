@@ -3,7 +3,7 @@
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/liboracle.so"
-SRC=("$HERE/mech_eval.c" "$HERE/reactor.c" "$HERE/arkode.c" "$HERE/transport.c")
+SRC=("$HERE/mech_eval.c" "$HERE/reactor.c" "$HERE/arkode.c" "$HERE/transport.c" "$HERE/srk.c")
 newest=0
 for f in "${SRC[@]}" "$HERE/oracle.h" "$HERE"/../pelephysics_b200/csrc/mech/*.h "$HERE"/../pelephysics_b200/csrc/ppb_erk_tables.h; do
   t=$(stat -c %Y "$f"); [ "$t" -gt "$newest" ] && newest=$t

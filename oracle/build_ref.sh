@@ -35,3 +35,15 @@ for mech in LiDryer drm19 dodecane_lu heptane_lu_88sk; do
       "$HERE/ref_transport.cpp" -o "$lib.tmp"
   mv "$lib.tmp" "$lib"
 done
+# the reference's SRK equation of state (Source/Eos/SRK.H) per mechanism
+for mech in LiDryer drm19 dodecane_lu heptane_lu_88sk; do
+  src="$REF/Mechanisms/$mech/mechanism.H"
+  lib="$OUT/librefsrk_${mech}.so"
+  if [ -f "$lib" ] && [ "$lib" -nt "$src" ] && [ "$lib" -nt "$HERE/ref_srk.cpp" ]; then
+    continue
+  fi
+  g++ -std=c++17 -O3 -march=x86-64-v3 -fPIC -shared -fvisibility=hidden \
+      -I"$HERE/amrex_stub" -I"$REF/Mechanisms/$mech" -I"$REF/Source" \
+      "$HERE/ref_srk.cpp" -o "$lib.tmp"
+  mv "$lib.tmp" "$lib"
+done

@@ -86,6 +86,18 @@ void ppo_default_options(PPOOptions* o);
 const PPBTransTables* ppo_trans(const char* name);
 int ppo_transport(const char* mech, int flags, double T, double rho, const double* Y, double* D, double* chi,
                   double* mu, double* xi, double* lam);
+// Soave-Redlich-Kwong EOS (Source/Eos/SRK.H) for the e-reactor: the
+// mechanism's GET_CRITPARAMS_SRK values, the EOS functions and the reactor
+// right-hand side over them (reactor type 1).
+const double* ppo_srk(const char* name);
+int ppo_srk_rey2t(const char* mech, double R, double E, const double* Y, double* T);
+double ppo_srk_rty2e(const char* mech, double R, double T, const double* Y);
+void ppo_srk_rty2ei(const char* mech, double R, double T, const double* Y, double* Ei);
+double ppo_srk_rty2cv(const char* mech, double R, double T, const double* Y);
+void ppo_srk_rty2c(const char* mech, double R, double T, const double* Y, double* C);
+void ppo_srk_rty2wdot(const char* mech, double R, double T, const double* Y, double* wdot);
+double ppo_reactor_rhs_srk(const char* mech, double t_rel, const double* y, double* ydot, double rhoe_init,
+                           double rhoesrc, const double* rYsrc);
 int ppo_transport_batch(const char* mech, int flags, int ncells, const double* T, const double* rho, const double* Y,
                         double* D, double* chi, double* mu, double* xi, double* lam, int nthreads);
 

@@ -543,3 +543,89 @@ def transport_batch(mech, flags, T, rho, Y, nthreads=0):
     L.ppo_transport_batch(mech.encode(), int(flags), n, _p(T), _p(rho), _p(Y), _p(D), _p(chi), _p(mu), _p(xi),
                           _p(lam), int(nthreads))
     return D, chi, mu, xi, lam
+
+
+# ---------------------------------------------------------------- SRK EOS
+_refsrk = {}
+
+
+def _srk_lib():
+    L = lib()
+    if not getattr(L, "_srk_set", False):
+        cp = C.c_char_p
+        L.ppo_srk_rey2t.argtypes = [cp, C.c_double, C.c_double, _DP, _DP]
+        for fn in ("ppo_srk_rty2e", "ppo_srk_rty2cv"):
+            getattr(L, fn).argtypes = [cp, C.c_double, C.c_double, _DP]
+            getattr(L, fn).restype = C.c_double
+        for fn in ("ppo_srk_rty2ei", "ppo_srk_rty2c", "ppo_srk_rty2wdot"):
+            getattr(L, fn).argtypes = [cp, C.c_double, C.c_double, _DP, _DP]
+        L.ppo_reactor_rhs_srk.argtypes = [cp, C.c_double, _DP, _DP, C.c_double, C.c_double, _DP]
+        L.ppo_reactor_rhs_srk.restype = C.c_double
+        L._srk_set = True
+    return L
+
+
+class Srk:
+    """The SRK equation of state for the e-reactor: the oracle's restatement
+    (ref=False) or the reference's own compiled Source/Eos/SRK.H (ref=True)."""
+
+    def __init__(self, mech, ref=False):
+        self.mech, self.ref = mech, ref
+        self.N = Mech(mech).nsp
+        if ref:
+            if mech not in _refsrk:
+                L = C.CDLL(os.path.join(HERE, "_ref", f"librefsrk_{mech}.so"))
+                L.refsrk_rey2t.argtypes = [C.c_double, C.c_double, _DP, _DP]
+                for fn in ("refsrk_rty2e", "refsrk_rty2cv"):
+                    getattr(L, fn).argtypes = [C.c_double, C.c_double, _DP]
+                    getattr(L, fn).restype = C.c_double
+                for fn in ("refsrk_rty2ei", "refsrk_rty2c", "refsrk_rty2wdot"):
+                    getattr(L, fn).argtypes = [C.c_double, C.c_double, _DP, _DP]
+                L.refsrk_reactor_rhs.argtypes = [C.c_double, _DP, _DP, C.c_double, C.c_double, _DP]
+                L.refsrk_reactor_rhs.restype = C.c_double
+                _refsrk[mech] = L
+            self.L = _refsrk[mech]
+        else:
+            self.L = _srk_lib()
+
+    def _call(self, name, *a):
+        if self.ref:
+            return getattr(self.L, "refsrk_" + name)(*a)
+        return getattr(self.L, "ppo_srk_" + name)(self.mech.encode(), *a)
+
+    def rey2t(self, R, E, Y, Tguess):
+        T = np.array([float(Tguess)])
+        y = np.ascontiguousarray(Y, float)
+        self._call("rey2t", float(R), float(E), _p(y), _p(T))
+        return T[0]
+
+    def rty2e(self, R, T, Y):
+        return self._call("rty2e", float(R), float(T), _p(np.ascontiguousarray(Y, float)))
+
+    def rty2cv(self, R, T, Y):
+        return self._call("rty2cv", float(R), float(T), _p(np.ascontiguousarray(Y, float)))
+
+    def _vec(self, name, R, T, Y):
+        out = np.zeros(self.N)
+        self._call(name, float(R), float(T), _p(np.ascontiguousarray(Y, float)), _p(out))
+        return out
+
+    def rty2ei(self, R, T, Y):
+        return self._vec("rty2ei", R, T, Y)
+
+    def rty2c(self, R, T, Y):
+        return self._vec("rty2c", R, T, Y)
+
+    def rty2wdot(self, R, T, Y):
+        return self._vec("rty2wdot", R, T, Y)
+
+    def reactor_rhs(self, t_rel, y, rhoe, rhoesrc, src):
+        y = np.ascontiguousarray(y, float)
+        ydot = np.zeros(self.N + 1)
+        s = np.ascontiguousarray(src, float)
+        if self.ref:
+            T = self.L.refsrk_reactor_rhs(float(t_rel), _p(y), _p(ydot), float(rhoe), float(rhoesrc), _p(s))
+        else:
+            T = self.L.ppo_reactor_rhs_srk(self.mech.encode(), float(t_rel), _p(y), _p(ydot), float(rhoe),
+                                           float(rhoesrc), _p(s))
+        return ydot, T

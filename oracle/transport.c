@@ -145,3 +145,13 @@ int ppo_transport_batch(const char* mech, int flags, int ncells, const double* T
                   lam + c);
   return 0;
 }
+
+// SRK parameters of a mechanism: [sqrt(1/Tc) | sqrt(a*) | B | F(omega)], N each.
+const double* ppo_srk(const char* name)
+{
+  if (!strcmp(name, "LiDryer")) return ppbt_LiDryer_srk;
+  if (!strcmp(name, "drm19")) return ppbt_drm19_srk;
+  if (!strcmp(name, "dodecane_lu")) return ppbt_dodecane_lu_srk;
+  if (!strcmp(name, "heptane_lu_88sk")) return ppbt_heptane_lu_88sk_srk;
+  return 0;
+}

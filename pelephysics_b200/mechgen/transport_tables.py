@@ -1,11 +1,13 @@
-"""Transport tables for the mixture-averaged transport kernels.
+"""Transport and SRK tables (mixture-averaged transport, real-gas EOS).
 
 The reference's SimpleTransport (Source/Transport/Simple.H) reads every
 coefficient from the mechanism's generated header: the CEPTR transport fits
 and molecular data behind egtransetWT / EPS / SIG / DIP / POL / ZROT / NLIN /
 COFETA / COFLAM / COFD / NLITE / KTDIF / COFTD (loaded by
 Source/Transport/TransportParams.H:228-258), and, for the bulk viscosity,
-CKCVMS's R / W_k factors.  These are the mechanism's transport data, fitted by
+CKCVMS's R / W_k factors; and the SRK equation of state's per-species
+parameters of GET_CRITPARAMS_SRK (Source/Eos/SRK.H).  These are the
+mechanism's transport and critical-point data, fitted by
 CEPTR from the mechanism's Lennard-Jones parameters; this script reads them
 from Mechanisms/<mech>/mechanism.H (the values only) and writes
 csrc/mech/trans_<mech>.h for the engine and the oracle.
@@ -74,6 +76,10 @@ def build(mech_dir: str, name: str):
     T["ktdif"] = _array(src, "egtransetKTDIF", "KTDIF", int)
     T["fittdrat"] = _array(src, "egtransetCOFTD", "COFTD")
     T["cvms"] = _scaled(src, "CKCVMS", "cvms")
+    # SRK parameters (GET_CRITPARAMS_SRK), used by Source/Eos/SRK.H
+    for key in ("sqrtOneOverTc", "sqrtAsti", "Bi", "Fomega"):
+        T["srk_" + key] = _array(src, "GET_CRITPARAMS_SRK", key)
+        assert len(T["srk_" + key]) == nsp, (name, key)
     for key in ("wt", "eps", "sig", "dip", "pol", "zrot", "nlin", "cvms"):
         assert len(T[key]) == nsp, (name, key)
     assert len(T["fitmu"]) == len(T["fitlam"]) == 4 * nsp
@@ -104,6 +110,10 @@ def emit_header(T, path):
     out.append(f"\nstatic const PPBTransTables ppbt_{name} = {{\n  \"{name}\", {T['nsp']}, {T['nlite']},\n")
     out.append("".join(f"  {P}{k},\n" for k in FIELDS))
     out.append("};\n")
+    # SRK: [sqrtOneOverTc | sqrtAsti | Bi | Fomega], N each
+    srk = T["srk_sqrtOneOverTc"] + T["srk_sqrtAsti"] + T["srk_Bi"] + T["srk_Fomega"]
+    out.append("\n// SRK parameters (GET_CRITPARAMS_SRK): sqrt(1/Tc) | sqrt(a*) | B | F(omega), N each\n")
+    out.append(_carr("double", P + "srk", srk))
     with open(path, "w") as fh:
         fh.write("".join(out))
 

@@ -6,11 +6,12 @@ reference's generated functions (productionRate, aJacobian in both consP
 modes, CKUBMS/CKHBMS/CKCVBS/CKCPBS, CKUMS/CKHMS, gibbs, GET_T_GIVEN_EY/HY)
 on seeded random states, and the reference's SimpleTransport::transport
 (Source/Transport/Simple.H, compiled by oracle/build_ref.sh with the
-mechanism's transport fits) on seeded (T, rho, Y).  The .npz files it writes
+mechanism's transport fits) on seeded (T, rho, Y), and the reference's
+SRK equation of state (Source/Eos/SRK.H) on seeded (rho, T, Y).  The .npz files it writes
 are the committed fixtures the tests compare the CPU oracle and the CUDA
 kernels against.
 
-Usage: python tests/golden/make_golden.py [point|transport]   (default both)
+Usage: python tests/golden/make_golden.py [point|transport|srk]   (default all)
 """
 
 import os
@@ -60,12 +61,47 @@ def transport_main():
         print(mech, npts, os.path.getsize(path), "bytes")
 
 
+SRK_POINTS = {"LiDryer": 16, "drm19": 16, "dodecane_lu": 8, "heptane_lu_88sk": 6}
+
+
+def srk_main():
+    """The reference's compiled Source/Eos/SRK.H on seeded (rho, T, Y):
+    RTY2E, RTY2Cv, RTY2Ei, RTY2C, RTY2WDOT, REY2T (from T + 100 K) and the
+    e-reactor right-hand side over them."""
+    for seed, (mech, npts) in enumerate(SRK_POINTS.items()):
+        R = po.Srk(mech, ref=True)
+        N = R.N
+        rng = np.random.default_rng(3000 + seed)
+        T = rng.uniform(300.0, 2500.0, npts)
+        rho = 10.0 ** rng.uniform(-4, -0.7, npts)
+        Y = rng.uniform(0.0, 1.0, (npts, N)) ** 3
+        Y /= Y.sum(axis=1, keepdims=True)
+        src = rng.normal(size=(npts, N)) * 1e-2
+        rhoesrc = rng.normal(size=npts) * 1e5
+        out = {"T": T, "rho": rho, "Y": Y, "src": src, "rhoesrc": rhoesrc}
+        out["e"] = np.array([R.rty2e(rho[i], T[i], Y[i]) for i in range(npts)])
+        out["cv"] = np.array([R.rty2cv(rho[i], T[i], Y[i]) for i in range(npts)])
+        out["ei"] = np.array([R.rty2ei(rho[i], T[i], Y[i]) for i in range(npts)])
+        out["c"] = np.array([R.rty2c(rho[i], T[i], Y[i]) for i in range(npts)])
+        out["wdot"] = np.array([R.rty2wdot(rho[i], T[i], Y[i]) for i in range(npts)])
+        out["T_ey"] = np.array([R.rey2t(rho[i], out["e"][i], Y[i], T[i] + 100.0) for i in range(npts)])
+        y = np.c_[rho[:, None] * Y, T + 30.0]
+        out["y"] = y
+        rhs = [R.reactor_rhs(2e-7, y[i], rho[i] * out["e"][i], rhoesrc[i], src[i]) for i in range(npts)]
+        out["ydot"] = np.array([r[0] for r in rhs])
+        path = os.path.join(HERE, f"srk_{mech}.npz")
+        np.savez_compressed(path, **out)
+        print(mech, npts, os.path.getsize(path), "bytes")
+
+
 def main():
     po.build()
     what = sys.argv[1] if len(sys.argv) > 1 else "all"
     if what in ("all", "transport"):
         transport_main()
-    if what == "transport":
+    if what in ("all", "srk"):
+        srk_main()
+    if what in ("transport", "srk"):
         return
     for seed, (mech, npts) in enumerate(POINTS.items()):
         R = po.Ref(mech)
