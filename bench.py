@@ -686,6 +686,69 @@ def transport_arm(args):
     return 0
 
 
+def srk_arm(args):
+    """The SRK real-gas e-reactor (ReactorCvode, eos = SRK) on the drm19
+    edge^3 field compressed to 50 atm (rho scaled by 50; rho*e from the SRK
+    EOS): cells/s against the ideal-gas reactor on the same cells, and the
+    oracle's SRK BDF on a 256-cell sample (agreement and CPU time)."""
+    import torch
+
+    from oracle import pyoracle as po
+    from pelephysics_b200 import workloads as wl
+    from pelephysics_b200.reactor import Reactor
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cells = wl.drm19_field(args.edge, device=dev)
+    n = cells.ncells
+    N = cells.rY.shape[1] - 1
+    rY = cells.rY.copy()
+    rY[:, :N] *= 50.0
+    rho = rY[:, :N].sum(1)
+    Y = rY[:, :N] / rho[:, None]
+    s = po.Srk(MECH)
+    rX = np.array([rho[c] * s.rty2e(rho[c], rY[c, N], Y[c]) for c in range(n)])
+    dt, opts = DT, dict(rtol=1e-10, atol=1e-10, max_order=5)
+    y0 = torch.as_tensor(rY, device=dev).contiguous()
+    s0 = torch.as_tensor(cells.rYsrc, device=dev).contiguous()
+    x0 = torch.as_tensor(rX, device=dev)
+    xs = torch.as_tensor(cells.rX_src, device=dev)
+    out = {}
+    for name, eos in (("srk", 1), ("ideal_same_cells", 0)):
+        r = Reactor(MECH)
+        r.init(1, n, **opts, eos=eos)
+        y, x = y0.clone(), x0.clone()
+        r.react(y, s0, x, xs, dt)  # warm-up (and the autotuner for the ideal gas)
+        ms = []
+        for _ in range(args.steps):
+            y.copy_(y0)
+            x.copy_(x0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            r.react(y, s0, x, xs, dt)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        st = r.cell_stats(n).mean(axis=0)
+        out[name] = {"cells_per_s": n * len(ms) / (sum(ms) / 1e3), "ms_per_react": sum(ms) / len(ms),
+                     "mean_steps": float(st[0]), "mean_rhs": float(st[1]), "mean_jac": float(st[2])}
+        if eos == 1:
+            ysrk = y.cpu().numpy()
+        r.close()
+    idx = cpu_sample_index(n, 256)
+    yc = rY[idx].copy()
+    t0 = time.perf_counter()
+    flag, _, _ = po.react_flat(MECH, 1, yc, np.ascontiguousarray(cells.rYsrc[idx]), rX[idx].copy(),
+                               cells.rX_src[idx].copy(), dt, eos=1, **opts)
+    cpu_s = time.perf_counter() - t0
+    dT = np.abs(ysrk[idx, N] - yc[:, N]) / yc[:, N]
+    out["oracle_sample"] = {"cells": 256, "flag": int(flag), "max_rel_T_vs_gpu": float(dT.max()),
+                            "cpu_cells_per_s": 256 / cpu_s, "cores": os.cpu_count()}
+    print(json.dumps({"config": "srk", "workload": f"drm19 {args.edge}^3 field at 50 atm (SRK energies), "
+                      f"dt {dt} s, rtol = atol = 1e-10", "results": out, "dtype": "f64"}), flush=True)
+    return 0
+
+
 def flops_probe():
     """One drm19 cell: reactor RHS and reactor Jacobian pointwise kernels,
     thread per cell (run under ncu to count FP64 operations)."""
@@ -803,7 +866,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-workload measurement")
     ap.add_argument("--adjoint-cells", type=int, default=65536)
-    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane", "arkode", "transport"],
+    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane", "arkode", "transport", "srk"],
                     help="drm19: the headline line; dodecane / heptane: the larger configurations; arkode: "
                          "the ReactorArkode integrator on the drm19 field")
     ap.add_argument("--sample", type=int, default=256, help="oracle sample cells for --config dodecane/heptane")
@@ -829,6 +892,8 @@ def main():
         return arkode_arm(args)
     if args.config == "transport":
         return transport_arm(args)
+    if args.config == "srk":
+        return srk_arm(args)
     if args.config != "drm19":
         return config_arm(args)
     return our_arm(args)

@@ -71,7 +71,13 @@ typedef struct ppb_options {
   int rk_controller;        /* ode.rk_controller, 0 (PID), 1 PI, 2 I, 3 explicit Gustafsson; box path only */
   int use_erkstep;          /* ode.use_erkstep, 1 (ERKStep and an explicit-only ARKStep integrate alike) */
   int arkode_max_steps;     /* internal steps per react call, 500 (the ARKODE default; the reference sets none) */
+  /* equation of state (the reference's build-time EOS choice, Source/Eos/EOS.H:20-27) */
+  int eos;                  /* PPB_EOS_IDEAL (Fuego, default) or PPB_EOS_SRK (ReactorCvode, reactor type 1) */
 } ppb_options;
+
+#define PPB_EOS_IDEAL 0 /* ideal gas: the mechanism's NASA-7 thermo (Source/Eos/Fuego.H) */
+#define PPB_EOS_SRK 1   /* Soave-Redlich-Kwong real gas (Source/Eos/SRK.H): e-reactor only, BDF with a
+                           difference-quotient Jacobian (SRK has no analytical one) */
 
 /* An amrex::Array4<Real>-compatible view: element (i,j,k,n) lives at
  * p[(i-lo[0]) + (j-lo[1])*jstride + (k-lo[2])*kstride + n*nstride]. */

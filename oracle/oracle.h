@@ -75,6 +75,7 @@ typedef struct PPOOptions {
   int use_ref_kernels;// 1: the reference's compiled mechanism kernels; 0: tables
   int rk64_nsubsteps_guess, rk64_nsubsteps_min, rk64_nsubsteps_max;
   const double* typ_vals; // N+1 typical values or NULL
+  int eos;                // 0 ideal gas (Fuego), 1 SRK (reactor type 1, difference-quotient Jacobian)
 } PPOOptions;
 
 void ppo_default_options(PPOOptions* o);

@@ -50,6 +50,7 @@ class Options(C.Structure):
         ("rk64_nsubsteps_min", C.c_int),
         ("rk64_nsubsteps_max", C.c_int),
         ("typ_vals", _DP),
+        ("eos", C.c_int),
     ]
 
 

@@ -133,11 +133,14 @@ typedef struct Sys {
   int reactor_type, ref;
   const double* rYsrc;
   double rhoe_init, rhoesrc;
+  int eos; // 0 ideal gas, 1 SRK (oracle/srk.c; difference-quotient Jacobian)
 } Sys;
 
 static void sys_f(const Sys* s, double t, const double* y, double* f)
 {
-  if (s->ref >= 0) {
+  if (s->eos == 1) {
+    ppo_reactor_rhs_srk(s->M->name, t, y, f, s->rhoe_init, s->rhoesrc, s->rYsrc);
+  } else if (s->ref >= 0) {
     g_ref[s->ref].rhs(s->reactor_type, t, y, f, s->rhoe_init, s->rhoesrc, s->rYsrc);
   } else {
     ppo_reactor_rhs(s->M, s->reactor_type, t, y, f, s->rhoe_init, s->rhoesrc, s->rYsrc);
@@ -169,6 +172,7 @@ void ppo_default_options(PPOOptions* o)
   o->rk64_nsubsteps_min = 5;
   o->rk64_nsubsteps_max = 500;
   o->typ_vals = 0;
+  o->eos = 0;
 }
 
 // ------------------------------------------------------------ dense LU
@@ -438,6 +442,31 @@ static void cv_set(BDF* b)
 }
 
 // cvLsSetup with a matrix-based direct solver
+// CVODE's dense difference-quotient Jacobian (the reference's path when
+// the EOS has no analytical Jacobian, Source/Eos/SRK.H:640-648) at
+// (tn, y) with f(tn, y) in ftemp: column j with inc = max(sqrt(eps)|y_j|,
+// min_inc / ewt_j), min_inc = 1000 |h| eps n ||f||_WRMS (1 if ||f|| = 0).
+// Its evaluations are not counted in nfe.
+static void dq_jac(BDF* b)
+{
+  const int n = b->n;
+  const double fnorm = wrms(b, b->ftemp);
+  const double srur = sqrt(DBL_EPSILON);
+  const double min_inc = (fnorm != 0.0) ? (1000.0 * fabs(b->h) * DBL_EPSILON * n * fnorm) : 1.0;
+  double yp[NMAX];
+  memcpy(yp, b->y, sizeof(double) * n);
+  for (int j = 0; j < n; j++) {
+    const double yj = yp[j];
+    const double inc = fmax(srur * fabs(yj), min_inc / b->ewt[j]);
+    yp[j] = yj + inc;
+    double* col = b->savedJ + (long)j * n;
+    sys_f(b->sys, b->tn, yp, col);
+    const double inc_inv = 1.0 / inc;
+    for (int i = 0; i < n; i++) col[i] = inc_inv * col[i] + (-inc_inv) * b->ftemp[i];
+    yp[j] = yj;
+  }
+}
+
 static int ls_setup(BDF* b, int convfail)
 {
   const int n = b->n;
@@ -451,7 +480,11 @@ static int ls_setup(BDF* b, int convfail)
     b->nje++;
     b->nstlj = b->nst;
     b->jcur = 1;
-    sys_j(b->sys, b->y, b->savedJ);
+    if (b->sys->eos == 1) {
+      dq_jac(b);
+    } else {
+      sys_j(b->sys, b->y, b->savedJ);
+    }
   }
   for (int i = 0; i < n * n; i++) b->A[i] = -b->gamma * b->savedJ[i];
   for (int i = 0; i < n; i++) b->A[i * n + i] += 1.0;
@@ -763,7 +796,7 @@ int ppo_bdf_cell(
   const PPBMechTables* M, int reactor_type, const PPOOptions* opt, double* y,
   const double* rYsrc, double rhoe_init, double rhoesrc, double dt, PPOStats* st)
 {
-  Sys sys = {M, reactor_type, -1, rYsrc, rhoe_init, rhoesrc};
+  Sys sys = {M, reactor_type, -1, rYsrc, rhoe_init, rhoesrc, opt->eos};
   if (opt->use_ref_kernels) sys.ref = find_ref(M->name);
   BDF* b = (BDF*)calloc(1, sizeof(BDF));
   const int n = M->nsp + 1;
@@ -840,7 +873,7 @@ int ppo_rk64_cell(
                                  -1.07992686223881, -0.248664241213447, 0.0};
   static const double err[6] = {-0.0554699315064507, 0.158481845574980, -0.0905918835751907,
                                 -0.219084567203338, 0.164022338959433, 0.0426421977505659};
-  Sys sys = {M, reactor_type, -1, rYsrc, rhoe_init, rhoesrc};
+  Sys sys = {M, reactor_type, -1, rYsrc, rhoe_init, rhoesrc, opt->eos};
   if (opt->use_ref_kernels) sys.ref = find_ref(M->name);
   const int neq = M->nsp + 1;
   double soln[NMAX], carry[NMAX], error[NMAX], ydot[NMAX];

@@ -49,6 +49,7 @@ class Options(C.Structure):
         ("rk_controller", C.c_int),
         ("use_erkstep", C.c_int),
         ("arkode_max_steps", C.c_int),
+        ("eos", C.c_int),
     ]
 
 

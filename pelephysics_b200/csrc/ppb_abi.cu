@@ -351,6 +351,22 @@ static LaunchConfig launch_config(const ppb_reactor* r)
   lc.engine = r->opt.engine;
   lc.lu_fp32 = r->opt.lu_fp32;
   lc.persistent = 1;
+  if (r->opt.eos == PPB_EOS_SRK) {
+    // one compiled SRK kernel: warp teams, <= 128 registers; the block size
+    // the caller gives, else the largest (<= 8 warps) that fits
+    lc.srk = 1;
+    lc.team = 32;
+    lc.minb = 2;
+    if (r->opt.warps_per_block > 0) {
+      lc.warps_per_block = r->opt.warps_per_block;
+    } else {
+      const size_t cb = team_cell_bytes(r->t, 0);
+      int w = 8;
+      while (w > 1 && cb * w > 200 * 1024) w--;
+      lc.warps_per_block = w;
+    }
+    return lc;
+  }
   if (r->opt.warps_per_block > 0) {
     lc.warps_per_block = r->opt.warps_per_block;
     lc.team = (r->opt.team_lanes == 16 || r->opt.team_lanes == 64 || r->opt.team_lanes == 128) ? r->opt.team_lanes : 32;
@@ -490,7 +506,9 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
 // Run the autotuner on this batch unless the stream is being captured.
 static int maybe_autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
 {
-  if (r->method == METHOD_ARK || r->opt.engine != PPB_ENGINE_TUNED || r->opt.warps_per_block > 0) return 0;
+  if (r->method == METHOD_ARK || r->opt.eos == PPB_EOS_SRK || r->opt.engine != PPB_ENGINE_TUNED ||
+      r->opt.warps_per_block > 0)
+    return 0;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return 0;
   return autotune(r, b, dt, st);
@@ -548,6 +566,7 @@ void ppb_default_options(ppb_options* o)
   o->rk_controller = 0;
   o->use_erkstep = 1;
   o->arkode_max_steps = 500;
+  o->eos = PPB_EOS_IDEAL;
 }
 
 const char* ppb_last_error(void) { return g_err; }
@@ -616,6 +635,15 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
     return fail(PPB_E_ARG, "engine must be PPB_ENGINE_PLAIN or PPB_ENGINE_TUNED");
   if (r->opt.engine == PPB_ENGINE_PLAIN && r->opt.lu_fp32)
     return fail(PPB_E_ARG, "the plain engine is FP64 only");
+  if (r->opt.eos != PPB_EOS_IDEAL && r->opt.eos != PPB_EOS_SRK) return fail(PPB_E_ARG, "eos must be 0 or 1");
+  if (r->opt.eos == PPB_EOS_SRK) {
+    // SRK::RHY2T is not supported (Source/Eos/SRK.H:499-507), nor an
+    // analytical Jacobian; this engine runs it on the tuned FP64 BDF
+    if (r->method != METHOD_BDF || reactor_type != PPB_REACTOR_E || r->opt.engine != PPB_ENGINE_TUNED ||
+        r->opt.lu_fp32)
+      return fail(PPB_E_ARG, "the SRK EOS needs ReactorCvode, reactor type 1, the tuned engine and the FP64 LU");
+    if (!find_srk(r->t->name)) return fail(PPB_E_MECH, "the mechanism has no SRK parameters");
+  }
   r->reactor_type = reactor_type;
   int e = 0;
   if (r->own) {
@@ -889,6 +917,7 @@ int ppb_react_box(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 r
 {
   if (!r || !r->inited) return fail(PPB_E_STATE, "react before init");
   if (!lo || !hi || !dt_react || !time) return fail(PPB_E_ARG, "ppb_react_box: null argument");
+  if (r->opt.eos == PPB_EOS_SRK) return fail(PPB_E_ARG, "ppb_react_box: the SRK EOS runs on the flat paths only");
   const int N = r->t->nsp;
   long ncl = 1;
   for (int d = 0; d < 3; d++) {
@@ -1204,6 +1233,7 @@ static int run_adjoint(ppb_reactor* r, int mode, AdjBatch b, double dt, double* 
   if (!r || !r->inited) return fail(PPB_E_ARG, "adjoint: reactor not initialised");
   if (r->method != METHOD_BDF)
     return fail(PPB_E_ARG, "adjoint: only the BDF integrator (ReactorCvode) is differentiated");
+  if (r->opt.eos != PPB_EOS_IDEAL) return fail(PPB_E_ARG, "adjoint: the ideal-gas EOS only");
   if (r->opt.engine != PPB_ENGINE_TUNED) return fail(PPB_E_ARG, "adjoint: runs on the tuned engine only");
   if (b.ncells < 0 || (b.ncells > 0 && (!b.y0 || !b.rhoe))) return fail(PPB_E_ARG, "adjoint: invalid arguments");
   if (mode == ADJ_REVERSE && b.ncells > 0 && !b.lam_y) return fail(PPB_E_ARG, "adjoint: lam_y is required");

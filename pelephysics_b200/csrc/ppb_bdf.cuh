@@ -15,6 +15,7 @@
 // integrator state, vectors are lane-strided over team-shared memory.
 #pragma once
 #include "ppb_mech.cuh"
+#include "ppb_srk.cuh"
 
 namespace ppb {
 
@@ -79,6 +80,64 @@ __device__ double reactor_rhs(
     const double im = __ldg(M.imw + s);
     ei[s] = (EH ? h_RT(M, s, T, invT) : u_RT(M, s, T, invT)) * (RT * im);
     sc[s] = (rho * Y[s] * im) * 1.0e6;
+  }
+  if (tm.lane == 0) sc[N] = 1.0; // padding slot of the packed reaction records
+  tm.sync();
+  RateScratch rs{sc, g, qd};
+  production_rate(tm, M, wdot, sc, T, rs);
+  double acc = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) {
+    const double cd = wdot[s] * 1.0e-6 * __ldg(M.mw + s) + src[s];
+    ydot[s] = cd;
+    acc += cd * ei[s];
+  }
+  const double esrc = rhoesrc - tm.sum(acc);
+  if (tm.lane == 0) ydot[N] = esrc * (rinv / cv);
+  tm.sync();
+  return T;
+}
+
+// The reference's fKernelSpec with the SRK EOS (reactor type 1): REY2T,
+// RTY2Ei, RTY2Cv and the activities of RTY2WDOT (Source/Eos/SRK.H:446-487,
+// 659-688, 413-427, 589-638) in place of the ideal-gas forms.
+template <int TEAM>
+__device__ double reactor_rhs_srk(
+  const Team<TEAM>& tm, const DevMech& M, double t, const double* y, double* ydot, double rhoe, double rhoesrc,
+  const double* src, double* Y, double* sc, double* g, double* qd, double* wdot, double* ei)
+{
+  const int N = M.nsp;
+  double a = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) a += y[s];
+  const double rho = tm.sum(a);
+  const double rinv = 1.0 / rho;
+  for (int s = tm.lane; s < N; s += TEAM) Y[s] = y[s] * rinv;
+  tm.sync();
+  const double nrg = (rhoe + rhoesrc * t) * rinv;
+  double T = y[N];
+  SrkState k;
+  srk_t_from_energy(tm, M, rho, nrg, Y, T, k);
+  srk_sums(tm, M, T, rho, Y, k);
+  const double cv = mix_c(tm, M, 0, T, Y) + T * k.d2AmdT2 * k.K1;
+  const double invT = 1.0 / T, RT = RU * T, sqrtT = sqrt(T);
+  double sy = 0.0;
+  for (int s = tm.lane; s < N; s += TEAM) sy += Y[s] * __ldg(M.imw + s);
+  const double wbar = 1.0 / tm.sum(sy);
+  const double InvBm = 1.0 / k.bm, tau = 1.0 / rho;
+  const double RmT = RU / wbar * T, InvRuT = 1.0 / (RU * T);
+  const double d1 = 1.0 / (tau - k.bm), d3 = 1.0 / (tau + k.bm);
+  const double* P = M.srk;
+  for (int s = tm.lane; s < N; s += TEAM) {
+    const double sOT = __ldg(P + s), sA = __ldg(P + N + s), B = __ldg(P + 2 * N + s), F = __ldg(P + 3 * N + s);
+    const double al = (1.0 + F * (1.0 - sqrtT * sOT)) * sA;
+    const double ad = -0.5 * F * sA * invT * sqrtT * sOT;
+    const double dAmdY = 2.0 * al * k.S1, d2AmdTY = 2.0 * (al * k.S1p + ad * k.S1);
+    const double im = __ldg(M.imw + s);
+    ei[s] = u_RT(M, s, T, invT) * (RT * im) + (T * d2AmdTY - dAmdY) * k.K1 +
+            (T * k.dAmdT - k.am) * B * (d3 - k.K1) * InvBm;
+    const double act = ppb_exp((__ldg(M.mw + s) * InvRuT) *
+                               (RmT * d1 * B - k.K1 * dAmdY + k.am * InvBm * k.K1 * B - k.am * d3 * B * InvBm)) *
+                       Y[s] * im * d1;
+    sc[s] = act * 1.0e6;
   }
   if (tm.lane == 0) sc[N] = 1.0; // padding slot of the packed reaction records
   tm.sync();
@@ -247,7 +306,7 @@ struct NoRec {
   static constexpr bool on = false;
 };
 
-template <int NS, int TEAM, typename LT, typename Rec = NoRec>
+template <int NS, int TEAM, typename LT, typename Rec = NoRec, bool SRK = false>
 struct Bdf {
   static constexpr int n = NS + 1;
   static constexpr int PER = (NS + TEAM - 1) / TEAM;
@@ -287,8 +346,12 @@ struct Bdf {
   __device__ __noinline__ void f(double t, const double* y, double* fy)
   {
     PPB_TIC(PH_RHS);
-    reactor_rhs<TEAM>(tm, M, o.reactor_type, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
-                      w.ei);
+    if constexpr (SRK) {
+      reactor_rhs_srk<TEAM>(tm, M, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot, w.ei);
+    } else {
+      reactor_rhs<TEAM>(tm, M, o.reactor_type, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
+                        w.ei);
+    }
     s.nfe++;
     PPB_TOC(PH_RHS);
   }
@@ -296,11 +359,46 @@ struct Bdf {
   __device__ void jac()
   {
     PPB_TIC(PH_JAC);
-    // the Newton matrix region is free while the Jacobian is formed: it holds
-    // the per-reaction factors of the warp-cooperative evaluation
-    reactor_jac<TEAM, PER>(tm, M, o.reactor_type, w.y, w.J, w.sc, w.g, w.wdot, w.Y, w.ei, w.h1, w.h2,
-                           TEAM > 1 ? w.qd : nullptr, TEAM > 1 ? reinterpret_cast<double*>(w.A) : nullptr);
+    if constexpr (SRK) {
+      jac_dq();
+    } else {
+      // the Newton matrix region is free while the Jacobian is formed: it
+      // holds the per-reaction factors of the warp-cooperative evaluation
+      reactor_jac<TEAM, PER>(tm, M, o.reactor_type, w.y, w.J, w.sc, w.g, w.wdot, w.Y, w.ei, w.h1, w.h2,
+                             TEAM > 1 ? w.qd : nullptr, TEAM > 1 ? reinterpret_cast<double*>(w.A) : nullptr);
+    }
     PPB_TOC(PH_JAC);
+  }
+
+  // Difference-quotient dense Jacobian at (tn, y) with f(tn, y) in ftemp:
+  // the SRK EOS has no analytical Jacobian (SRK::RTY2JAC aborts,
+  // Source/Eos/SRK.H:640-648), so the reference's CVODE forms it by
+  // differences; restated from CVODE's dense difference-quotient Jacobian:
+  // column j uses inc = max(sqrt(eps) |y_j|, min_inc / ewt_j), min_inc =
+  // 1000 |h| eps n ||f||_WRMS (1 when ||f|| = 0).  Its RHS evaluations are
+  // not counted in nfe (CVODE counts them separately).
+  __device__ void jac_dq()
+  {
+    const double fnorm = wrms(w.ftemp);
+    const double eps = 2.220446049250313e-16;
+    const double srur = sqrt(eps);
+    const double min_inc = (fnorm != 0.0) ? (1000.0 * fabs(s.h) * eps * n * fnorm) : 1.0;
+    for (int i = tm.lane; i < n; i += TEAM) w.tempv[i] = w.y[i];
+    tm.sync();
+    for (int j = 0; j < n; j++) {
+      const double yj = w.tempv[j];
+      const double inc = fmax(srur * fabs(yj), min_inc / w.ewt[j]);
+      tm.sync();
+      if (tm.lane == 0) w.tempv[j] = yj + inc;
+      tm.sync();
+      double* col = w.J + (size_t)j * n;
+      reactor_rhs_srk<TEAM>(tm, M, s.tn, w.tempv, col, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
+                            w.ei);
+      const double inc_inv = 1.0 / inc;
+      for (int i = tm.lane; i < n; i += TEAM) col[i] = inc_inv * col[i] + (-inc_inv) * w.ftemp[i];
+      if (tm.lane == 0) w.tempv[j] = yj;
+      tm.sync();
+    }
   }
 
   __device__ int hin(double tout)

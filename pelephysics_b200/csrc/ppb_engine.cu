@@ -377,6 +377,14 @@ static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
   set_off(dm.wg_off, off_goff);
   set_off(dm.wg_rx, off_grx);
   set_off(dm.wg_c, off_gc);
+  // SRK parameters (zeros for a mechanism without them)
+  const double* srk = find_srk(t->name);
+  std::vector<double> nosrk;
+  if (!srk) {
+    nosrk.assign((size_t)4 * N, 0.0);
+    srk = nosrk.data();
+  }
+  set_off(dm.srk, pk.add(srk, (size_t)4 * N));
   return pk.used;
 }
 

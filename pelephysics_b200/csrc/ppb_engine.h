@@ -53,6 +53,7 @@ struct LaunchConfig {
   int team = 32;      // lanes per cell: 32; 16 for <= 21 species; 64 (33..64 species) or 128 (65..128): one
                       // multi-warp team per block
   int minb = 2;       // register budget: >= minb blocks of 256 threads per SM
+  int srk = 0;        // the SRK e-reactor kernel (warp teams, <= 128 registers)
 };
 // Resident cells per SM of the tuned kernel in configuration lc (0: the
 // configuration does not fit or is not compiled).
@@ -122,6 +123,8 @@ struct TrBox {
   BoxView Y, T, rho, D, chi, mu, xi, lam;
 };
 const PPBTransTables* find_transport(const char* name);
+// SRK parameters of a mechanism ([sqrt(1/Tc) | sqrt(a*) | B | F], N each) or nullptr.
+const double* find_srk(const char* name);
 int device_transport(const PPBTransTables* t, DeviceTransport** out);
 int launch_transport(const DeviceMechanism& m, const DeviceTransport& tr, int flags, const TrBox& b,
                      cudaStream_t st);

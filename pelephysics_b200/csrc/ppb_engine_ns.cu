@@ -10,7 +10,7 @@
 namespace ppb {
 
 // ------------------------------------------------------------ react kernels
-template <int NS, int TEAM, typename LT, int METHOD>
+template <int NS, int TEAM, typename LT, int METHOD, bool SRK = false>
 __device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options& o, Work<LT>& w, const Batch& b,
                           int c, double dt)
 {
@@ -33,7 +33,7 @@ __device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options&
   const CellIn cin{b.rhoe[c], b.rhoesrc[c]};
   int flag, cost;
   if (METHOD == METHOD_BDF) {
-    Bdf<NS, TEAM, LT> bdf(tm, M, o, w, cin);
+    Bdf<NS, TEAM, LT, NoRec, SRK> bdf(tm, M, o, w, cin);
     flag = bdf.run(dt);
     cost = bdf.s.nfe;
     if (b.stats && tm.lane == 0) {
@@ -135,7 +135,7 @@ __device__ __forceinline__ void react_team_body(const Team<TEAM>& tm, const DevM
 
 // Warp teams carry no block-shared scratch; a multi-warp team gets 16
 // doubles for its cross-warp reductions.
-template <int NS, typename LT, int METHOD, int TEAM, int MINB>
+template <int NS, typename LT, int METHOD, int TEAM, int MINB, bool SRK = false>
 __global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
                                                           size_t cell_bytes, int persistent)
 {
@@ -156,11 +156,11 @@ __global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, 
         if (tm.lane == 0) c = atomicAdd(queue, 1);
         c = __shfl_sync(tm.mask, c, 0, TEAM);
         if (c >= b.ncells) break;
-        react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, c, dt);
+        react_one<NS, TEAM, LT, METHOD, SRK>(tm, M, o, w, b, c, dt);
       }
     } else {
       const int c = blockIdx.x * tpb + team;
-      if (c < b.ncells) react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, c, dt);
+      if (c < b.ncells) react_one<NS, TEAM, LT, METHOD, SRK>(tm, M, o, w, b, c, dt);
     }
   }
 }
@@ -180,9 +180,13 @@ constexpr int big_team()
 // 21 species, and a multi-warp team (one cell per block, one lane per
 // species) for larger ones.
 template <int NS>
-static TeamKernel team_kernel(int method, bool fp32, int team, int minb)
+static TeamKernel team_kernel(int method, bool fp32, int team, int minb, int srk = 0)
 {
   constexpr bool small = NS <= 21;
+  // the SRK e-reactor: FP64 BDF, one warp per cell, <= 128 registers
+  if (srk) return (method == METHOD_BDF && !fp32 && team == 32 && minb == 2)
+                    ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, true>
+                    : nullptr;
   if (team > 32) {
     if constexpr (big_team<NS>() > 0) {
       constexpr int BT = big_team<NS>();
@@ -230,7 +234,7 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
   const int team = (lc.team == 16 || lc.team > 32) ? lc.team : 32;
   // a multi-warp team is one block
   const int wpb = team > 32 ? team / 32 : (lc.warps_per_block > 0 ? lc.warps_per_block : 4);
-  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb);
+  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.srk);
   if (!kern) return (int)cudaErrorInvalidConfiguration;
   const int tpb = team > 32 ? 1 : wpb * (32 / team); // cells per block
   const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
@@ -263,7 +267,7 @@ static int occupancy_ns(const DevMech& M, int method, const LaunchConfig& lc)
 {
   const bool fp32 = lc.lu_fp32 && method == METHOD_BDF;
   const int team = (lc.team == 16 || lc.team > 32) ? lc.team : 32;
-  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb);
+  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.srk);
   if (!kern) return 0;
   const int wpb = team > 32 ? team / 32 : (lc.warps_per_block > 0 ? lc.warps_per_block : 4);
   const int tpb = team > 32 ? 1 : wpb * (32 / team);

@@ -79,6 +79,8 @@ struct DevMech {
   // species-major gather of the aJacobian net stoichiometry (jn lists)
   const int *jg_off, *jg_rx;
   const double* jg_c;
+  // SRK equation of state: [sqrt(1/Tc) | sqrt(a*) | B | F(omega)], N each
+  const double* srk;
 };
 
 // One reaction in 80 bytes (5 x 16-byte loads).  Species lists are expanded

@@ -44,6 +44,15 @@ const PPBTransTables* find_transport(const char* name)
   return nullptr;
 }
 
+const double* find_srk(const char* name)
+{
+  if (!strcmp(name, "LiDryer")) return ppbt_LiDryer_srk;
+  if (!strcmp(name, "drm19")) return ppbt_drm19_srk;
+  if (!strcmp(name, "dodecane_lu")) return ppbt_dodecane_lu_srk;
+  if (!strcmp(name, "heptane_lu_88sk")) return ppbt_heptane_lu_88sk_srk;
+  return nullptr;
+}
+
 // Device copy of one mechanism's transport tables (one allocation).
 struct DevTrans {
   int nsp, nlite, npairs;

@@ -1,0 +1,68 @@
+"""The SRK real-gas e-reactor (eos = PPB_EOS_SRK) on the GPU against the
+oracle's BDF with the same SRK right-hand side and difference-quotient
+Jacobian, at the integration bar (T 1e-6 relative, Y 1e-8 absolute), and
+the option checks."""
+
+import numpy as np
+import pytest
+
+from pelephysics_b200 import _lib
+from pelephysics_b200.reactor import Reactor
+from tests.helpers import premix_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def srk_cells(oracle, mech, nc, seed, T0, dT, P):
+    """Premixed cells at pressure P with rho*e from the SRK EOS."""
+    rY, src, rX, rXs = premix_oracle(oracle, mech, nc, seed, T0, dT, 0.5, 1.0, P=P)
+    s = oracle.Srk(mech)
+    N = rY.shape[1] - 1
+    rho = rY[:, :N].sum(1)
+    rX = np.array([rho[c] * s.rty2e(rho[c], rY[c, N], rY[c, :N] / rho[c]) for c in range(nc)])
+    return rY, np.ascontiguousarray(src), rX, rXs
+
+
+def compare(y, ref, T_rtol=1e-6, Y_atol=1e-8):
+    N = ref.shape[1] - 1
+    assert np.all(np.isfinite(y))
+    dT = np.max(np.abs(y[:, N] - ref[:, N]) / ref[:, N])
+    Yg = y[:, :N] / y[:, :N].sum(1, keepdims=True)
+    Yr = ref[:, :N] / ref[:, :N].sum(1, keepdims=True)
+    assert dT <= T_rtol, f"max rel T error {dT:.3e}"
+    assert np.abs(Yg - Yr).max() <= Y_atol, f"max abs Y error {np.abs(Yg - Yr).max():.3e}"
+
+
+# dodecane_lu at 40 atm: at tolerances 1e-10 the integration error itself is
+# ~1e-7 in Y (the oracle's 1e-10 and 1e-12 solutions differ by 9e-8), more
+# than the bar, so that case integrates at 1e-12
+@pytest.mark.parametrize("mech,nc,dt,P,tol", [("drm19", 24, 1e-5, 50 * 1013250.0, 1e-10),
+                                              ("dodecane_lu", 6, 2e-6, 40 * 1013250.0, 1e-12)])
+def test_srk_reactor_matches_oracle(cuda, oracle, mech, nc, dt, P, tol):
+    rY, src, rX, rXs = srk_cells(oracle, mech, nc, 4, 1100.0, 500.0, P)
+    opts = dict(rtol=tol, atol=tol, max_order=5)
+    ref, xr = rY.copy(), rX.copy()
+    flag, _, _ = oracle.react_flat(mech, 1, ref, src, xr, rXs, dt, eos=1, **opts)
+    assert flag == 0
+    r = Reactor(mech)
+    r.init(1, nc, **opts, eos=1)
+    y, x = rY.copy(), rX.copy()
+    cost, dtr, t, code = r.react(y, src.copy(), x, rXs.copy(), dt)
+    assert code == 0
+    compare(y, ref)
+    np.testing.assert_allclose(x, xr, rtol=1e-15)
+    # the real-gas energy differs from the ideal one: the ideal reactor on the
+    # same cells ends elsewhere
+    ri = Reactor(mech)
+    ri.init(1, nc, **opts)
+    yi = rY.copy()
+    ri.react(yi, src.copy(), rX.copy(), rXs.copy(), dt)
+    assert np.max(np.abs(yi[:, -1] - y[:, -1])) > 1e-4
+
+
+def test_srk_option_checks(cuda):
+    for integ, rtype, extra in (("ReactorRK64", 1, {}), ("ReactorCvode", 2, {}), ("ReactorCvode", 1, {"lu_fp32": 1}),
+                                ("ReactorCvode", 1, {"engine": 0}), ("ReactorArkode", 1, {})):
+        r = Reactor("drm19", integ)
+        with pytest.raises(_lib.EngineError):
+            r.init(rtype, 4, eos=1, **extra)

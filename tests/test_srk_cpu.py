@@ -47,3 +47,27 @@ def test_srk_tends_to_the_ideal_gas(oracle):
     assert abs(s.rty2e(R, T, Y) - M.ckubms(T, Y)) <= 1e-6 * abs(M.ckubms(T, Y))
     assert abs(s.rty2cv(R, T, Y) - M.ckcvbs(T, Y)) <= 1e-6 * M.ckcvbs(T, Y)
     np.testing.assert_allclose(s.rty2c(R, T, Y), R * Y / M.mw(), rtol=1e-6)
+
+
+def test_oracle_srk_reactor_tends_to_the_ideal_reactor(oracle):
+    """The oracle's BDF with the SRK right-hand side and difference-quotient
+    Jacobian against the ideal-gas BDF: close at 1 atm, apart at 50 atm."""
+    from tests.helpers import premix_oracle
+
+    mech, nc, dt = "drm19", 6, 1e-5
+    out = {}
+    for P in (1013250.0, 50 * 1013250.0):
+        rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 4, 1300.0, 300.0, 0.5, 1.0, P=P)
+        s = oracle.Srk(mech)
+        N = rY.shape[1] - 1
+        rho = rY[:, :N].sum(1)
+        rXs_ = np.array([rho[c] * s.rty2e(rho[c], rY[c, N], rY[c, :N] / rho[c]) for c in range(nc)])
+        ys, yi = rY.copy(), rY.copy()
+        f1, _, _ = oracle.react_flat(mech, 1, ys, np.ascontiguousarray(src), rXs_.copy(), rXs, dt, rtol=1e-10,
+                                     atol=1e-10, max_order=5, eos=1)
+        f2, _, _ = oracle.react_flat(mech, 1, yi, np.ascontiguousarray(src), rX.copy(), rXs, dt, rtol=1e-10,
+                                     atol=1e-10, max_order=5)
+        assert f1 == 0 and f2 == 0
+        out[P] = np.max(np.abs(ys[:, N] - yi[:, N]) / yi[:, N])
+    assert out[1013250.0] < 1e-4
+    assert out[50 * 1013250.0] > 3 * out[1013250.0]
