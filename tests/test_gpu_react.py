@@ -324,3 +324,45 @@ def test_autotuner_choice_is_reproducible(cuda, oracle, mech):
     ref, _, flag, _, _ = oracle_react(oracle, mech, rtype, rY[sub], src[sub], rX[sub], rXs[sub], dt, **opts)
     compare(y.cpu().numpy()[sub], ref)
 
+
+
+def test_ignition_delay_pin_on_gpu(cuda, oracle):
+    """The reference's one integration golden value, through the engine's
+    box path: Testing/Exec/IgnitionDelay (dodecane_lu, 600 K, 5 atm,
+    phi 7.93, enthalpy reactor, rtol = atol = 1e-10, max order 4), reacting
+    in 4000 substeps of 1.1 * 0.0763 s / 4000 with T from the enthalpy
+    around each call (box flatten / unflatten, as the driver's react on a
+    MultiFab does); the first T > T0 + 400 K must fall within 10 substeps
+    of 0.0763 s (check_ignDelay.py:22-29)."""
+    torch = cuda
+    mech = "dodecane_lu"
+    M = oracle.Mech(mech)
+    sp, mw, N = M.species(), M.mw(), M.nsp
+    phi = 7.928571428571429
+    X = np.zeros(N)
+    io2, in2, ifu = sp.index("O2"), sp.index("N2"), sp.index("NC12H26")
+    X[io2] = 1.0 / (phi / 18.5 + 1 + 0.79 / 0.21)  # GPU_misc.H:62-64
+    X[in2] = 0.79 * X[io2] / 0.21
+    X[ifu] = 1 - X[io2] - X[in2]
+    Y = X * mw / np.sum(X * mw)
+    P, T0 = 5066250.0, 600.0
+    rho = M.ckrhoy(P, T0, Y)
+    r = Reactor(mech)
+    r.init(2, 1, rtol=1e-10, atol=1e-10, max_order=4)
+    dev = "cuda"
+    bY = torch.as_tensor((rho * Y).reshape(N, 1, 1, 1), device=dev)
+    bS = torch.zeros((N, 1, 1, 1), dtype=torch.float64, device=dev)
+    bT = torch.full((1, 1, 1, 1), T0, dtype=torch.float64, device=dev)
+    bE = torch.full((1, 1, 1, 1), rho * M.ckhbms(T0, Y), dtype=torch.float64, device=dev)
+    bEs = torch.zeros((1, 1, 1, 1), dtype=torch.float64, device=dev)
+    bFC = torch.zeros((1, 1, 1, 1), dtype=torch.float64, device=dev)
+    ndt = 4000
+    sub = 1.1 * 0.0763 / ndt
+    t_ign = None
+    for i in range(ndt):
+        r.react_box((0, 0, 0), (0, 0, 0), bY, bS, bT, bE, bEs, bFC, dt_react=sub)
+        if bT.item() > T0 + 400:
+            t_ign = (i + 1) * sub
+            break
+    assert t_ign is not None
+    assert abs(t_ign - 0.0763) <= 10 * sub
