@@ -73,6 +73,8 @@ typedef struct ppb_options {
   int arkode_max_steps;     /* internal steps per react call, 500 (the ARKODE default; the reference sets none) */
   /* equation of state (the reference's build-time EOS choice, Source/Eos/EOS.H:20-27) */
   int eos;                  /* PPB_EOS_IDEAL (Fuego, default) or PPB_EOS_SRK (ReactorCvode, reactor type 1) */
+  int cost_order;           /* tuned engine: hand cells to the work queue by descending cost of the previous
+                               call on this reactor (longest first: no tail of a few slow cells), 1 */
 } ppb_options;
 
 #define PPB_EOS_IDEAL 0 /* ideal gas: the mechanism's NASA-7 thermo (Source/Eos/Fuego.H) */

@@ -50,6 +50,7 @@ class Options(C.Structure):
         ("use_erkstep", C.c_int),
         ("arkode_max_steps", C.c_int),
         ("eos", C.c_int),
+        ("cost_order", C.c_int),
     ]
 
 

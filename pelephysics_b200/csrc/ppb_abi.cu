@@ -98,6 +98,10 @@ struct ppb_reactor {
   double* atolv = nullptr;
   int *status = nullptr, *nfe = nullptr, *queue = nullptr, *mask = nullptr, *stats = nullptr;
   int last_ncells = 0;
+  // work-queue order by the previous call's per-cell cost
+  int *order = nullptr, *order_keys = nullptr, *iota = nullptr;
+  void* sort_tmp = nullptr;
+  size_t sort_tmp_bytes = 0;
   // ReactorArkode: cell-major state, stage-0 and FSAL derivatives, sources,
   // block partial sums, grid barrier, batch result
   size_t ark_cap = 0;
@@ -168,6 +172,13 @@ static void free_scratch(ppb_reactor* r)
   cudaFree(r->mask);
   cudaFree(r->stats);
   r->stats = nullptr;
+  cudaFree(r->order);
+  cudaFree(r->order_keys);
+  cudaFree(r->iota);
+  cudaFree(r->sort_tmp);
+  r->order = r->order_keys = r->iota = nullptr;
+  r->sort_tmp = nullptr;
+  r->sort_tmp_bytes = 0;
   r->aos = r->aos_src = r->soa = r->soa_src = r->rhoe = r->rhoesrc = nullptr;
   r->status = r->nfe = r->queue = r->mask = nullptr;
   r->cap = 0;
@@ -203,6 +214,15 @@ static int ensure_scratch(ppb_reactor* r, int ncells)
   PPB_CUDA(cudaMalloc(&r->mask, c * 4), "cudaMalloc");
   PPB_CUDA(cudaMalloc(&r->stats, c * 7 * 4), "cudaMalloc");
   PPB_CUDA(cudaMalloc(&r->queue, 16), "cudaMalloc");
+  // no costs yet: zeros keep the first call in index order (stable sort)
+  PPB_CUDA(cudaMemset(r->nfe, 0, c * 4), "cudaMemset");
+  PPB_CUDA(cudaMalloc(&r->order, c * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->order_keys, c * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&r->iota, c * 4), "cudaMalloc");
+  PPB_CUDA(launch_iota(r->iota, (int)c, nullptr), "iota");
+  r->sort_tmp_bytes = cost_order_tmp_bytes((int)c);
+  PPB_CUDA(cudaMalloc(&r->sort_tmp, r->sort_tmp_bytes > 0 ? r->sort_tmp_bytes : 16), "cudaMalloc");
+  PPB_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
   r->cap = c;
   if (r->method == METHOD_ARK) {
     const size_t N = r->t->nsp;
@@ -567,6 +587,7 @@ void ppb_default_options(ppb_options* o)
   o->use_erkstep = 1;
   o->arkode_max_steps = 500;
   o->eos = PPB_EOS_IDEAL;
+  o->cost_order = 1;
 }
 
 const char* ppb_last_error(void) { return g_err; }
@@ -713,6 +734,14 @@ static int run_batch(ppb_reactor* r, Batch b, double dt, cudaStream_t st, double
   if (te) return te;
   const Options o = engine_options(r);
   const LaunchConfig lc = launch_config(r);
+  if (r->opt.cost_order && lc.engine == ENGINE_TUNED && lc.persistent && b.ncells > 1) {
+    // longest first: the previous call's per-cell cost (r->nfe) sorted
+    // descending; the kernel then overwrites r->nfe with this call's costs
+    int e = launch_cost_order(r->nfe, r->order_keys, r->iota, r->order, r->sort_tmp, r->sort_tmp_bytes, b.ncells,
+                              st);
+    if (e) return cuda_fail(e, "cost order");
+    b.order = r->order;
+  }
   int e = launch_react(*r->dm, o, r->method, lc, b, dt, r->queue, st);
   return cuda_fail(e, "launch_react");
 }

@@ -13,6 +13,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "ppb_work.cuh"
 #include "ppb_engine.h"
 #include "mech/mech_LiDryer.h"
@@ -941,6 +943,36 @@ int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells
 {
   if (ncells <= 0) return 0;
   k_energy_update<<<(ncells + 255) / 256, 256, 0, st>>>(rX, rX_src, dt, ncells);
+  return (int)cudaGetLastError();
+}
+
+size_t cost_order_tmp_bytes(int n)
+{
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, (const int*)nullptr, (int*)nullptr, (const int*)nullptr,
+                                            (int*)nullptr, n);
+  return bytes;
+}
+
+int launch_cost_order(const int* cost, int* keys_tmp, const int* iota, int* order, void* tmp, size_t tmp_bytes,
+                      int n, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  size_t bytes = tmp_bytes;
+  return (int)cub::DeviceRadixSort::SortPairsDescending(tmp, bytes, cost, keys_tmp, iota, order, n, 0,
+                                                        (int)(8 * sizeof(int)), st);
+}
+
+__global__ void k_iota(int* a, int n)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = i;
+}
+
+int launch_iota(int* a, int n, cudaStream_t st)
+{
+  if (n <= 0) return 0;
+  k_iota<<<(n + 255) / 256, 256, 0, st>>>(a, n);
   return (int)cudaGetLastError();
 }
 

@@ -40,6 +40,7 @@ struct Batch {
   int* stats;          // per cell [nsteps, nfe, nje, nsetups, nni, netf, ncfn] (may be nullptr)
   int ncells;
   int ld;
+  const int* order;    // work-queue order of the cells (nullptr: index order)
 };
 
 enum Engine { ENGINE_PLAIN = 0, ENGINE_TUNED = 1 };
@@ -106,6 +107,14 @@ int launch_pyt2re(const DeviceMechanism& m, int eh, const double* P, const doubl
 // FP64 FMA throughput probe: returns GFLOP/s measured with CUDA events.
 int probe_fp64_peak(double* gflops, cudaStream_t st);
 int launch_energy_update(double* rX, const double* rX_src, double dt, int ncells, cudaStream_t st);
+
+// Work-queue order by descending cost: order = cells sorted by cost (the
+// previous call's per-cell RHS evaluations), ties in index order.  keys_tmp
+// (n ints) and tmp (cost_order_tmp_bytes(n)) are scratch; iota holds 0..n-1.
+size_t cost_order_tmp_bytes(int n);
+int launch_cost_order(const int* cost, int* keys_tmp, const int* iota, int* order, void* tmp, size_t tmp_bytes,
+                      int n, cudaStream_t st);
+int launch_iota(int* a, int n, cudaStream_t st);
 
 // Mixture-averaged transport (ppb_transport.cu).  A mechanism's transport
 // tables uploaded to one device, and the views of one call: a box lo..hi

@@ -125,7 +125,7 @@ __device__ __forceinline__ void react_team_body(const Team<TEAM>& tm, const DevM
       if (tm.lane == 0) c = atomicAdd(queue, 1);
       c = tm.bcast_int(c, 0);
       if (c >= b.ncells) break;
-      react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, c, dt);
+      react_one<NS, TEAM, LT, METHOD>(tm, M, o, w, b, b.order ? b.order[c] : c, dt);
     }
   } else {
     const int c = blockIdx.x * tpb + team;
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, 
         if (tm.lane == 0) c = atomicAdd(queue, 1);
         c = __shfl_sync(tm.mask, c, 0, TEAM);
         if (c >= b.ncells) break;
-        react_one<NS, TEAM, LT, METHOD, SRK>(tm, M, o, w, b, c, dt);
+        react_one<NS, TEAM, LT, METHOD, SRK>(tm, M, o, w, b, b.order ? b.order[c] : c, dt);
       }
     } else {
       const int c = blockIdx.x * tpb + team;

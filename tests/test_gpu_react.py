@@ -366,3 +366,25 @@ def test_ignition_delay_pin_on_gpu(cuda, oracle):
             break
     assert t_ign is not None
     assert abs(t_ign - 0.0763) <= 10 * sub
+
+
+def test_cost_ordered_queue_changes_no_bits(cuda, oracle):
+    """cost_order = 1 hands cells to the work queue by the previous call's
+    cost (longest first); every cell is integrated exactly as in index order,
+    so a second call on the same batch gives the same bits as cost_order = 0."""
+    torch = cuda
+    mech, dt, nc = "drm19", 1e-5, 3000
+    rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 8, 1000.0, 1000.0, 0.5, 1.5)
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5, warps_per_block=4)
+    outs = []
+    for co in (0, 1):
+        r = Reactor(mech)
+        r.init(1, nc, **opts, cost_order=co)
+        for _ in range(2):
+            y = torch.as_tensor(rY, device="cuda").contiguous()
+            x = torch.as_tensor(rX, device="cuda")
+            r.react(y, torch.as_tensor(src, device="cuda").contiguous(), x, torch.as_tensor(rXs, device="cuda"), dt)
+        outs.append(y.cpu().numpy())
+        costs = r.cell_status(nc)[1]
+        assert costs.max() > 2 * costs.min()  # the costs differ, so the order does
+    np.testing.assert_array_equal(outs[0], outs[1])
