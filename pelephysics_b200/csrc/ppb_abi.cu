@@ -479,10 +479,14 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
   if (!err) err = cudaMemcpyAsync(re, b.rhoe, nm * 8, cudaMemcpyDeviceToDevice, st);
   if (!err) err = cudaMemcpyAsync(rs, b.rhoesrc, nm * 8, cudaMemcpyDeviceToDevice, st);
   const Options o = engine_options(r);
-  double best = 1e300;
-  LaunchConfig pick = cand[0];
-  for (size_t k = 0; k < cand.size() + 1 && !err; k++) {
-    const LaunchConfig& lc = cand[k == 0 ? 0 : k - 1]; // the first candidate twice: warm-up
+  // Two interleaved passes over the candidates after one warm-up launch;
+  // each candidate keeps its faster time, so a clock ramp or a neighbour's
+  // burst during one pass does not decide the pick.
+  const size_t nc = cand.size();
+  std::vector<double> tbest(nc, 1e300);
+  for (size_t k = 0; k < 2 * nc + 1 && !err; k++) {
+    const size_t ci = k == 0 ? 0 : (k - 1) % nc;
+    const LaunchConfig& lc = cand[ci];
     Batch tb{};
     tb.y = y;
     tb.src = sr;
@@ -500,9 +504,14 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
     if (!err) err = cudaEventSynchronize(e1);
     float ms = 0.f;
     if (!err) err = cudaEventElapsedTime(&ms, e0, e1);
-    if (!err && k > 0 && ms < best) {
-      best = ms;
-      pick = lc;
+    if (!err && k > 0) tbest[ci] = std::min(tbest[ci], (double)ms);
+  }
+  double best = 1e300;
+  LaunchConfig pick = cand[0];
+  for (size_t ci = 0; ci < nc; ci++) {
+    if (tbest[ci] < best) {
+      best = tbest[ci];
+      pick = cand[ci];
     }
   }
   cleanup();
