@@ -313,6 +313,9 @@ def our_arm(args):
         xp = torch.as_tensor(cells.rX[sub], device=dev)
         sp = torch.as_tensor(cells.rYsrc[sub], device=dev).contiguous()
         xsp = torch.as_tensor(cells.rX_src[sub], device=dev)
+        # one untimed call on copies first: module load, scratch and graph
+        # capture stay outside the timed call
+        rp.react(yp.clone(), sp, xp.clone(), xsp, DT)
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
@@ -382,7 +385,7 @@ def our_arm(args):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "tuned_vs_plain": {"plain_value": out["plain_value"], "ratio": value / ws / out["plain_value"],
-                               "plain_sample": "every 8th cell, one react", "max_rel_T_tuned_vs_plain": out["dT_plain"]},
+                               "plain_sample": "every 8th cell, one react after one untimed warm-up react", "max_rel_T_tuned_vs_plain": out["dT_plain"]},
             "accuracy_vs_fp64_oracle": acc,
             "adjoint": out.get("adjoint"),
             "cell_failures": int(np.sum(status < 0)),

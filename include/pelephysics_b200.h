@@ -75,6 +75,10 @@ typedef struct ppb_options {
   int eos;                  /* PPB_EOS_IDEAL (Fuego, default) or PPB_EOS_SRK (ReactorCvode, reactor type 1) */
   int cost_order;           /* tuned engine: hand cells to the work queue by descending cost of the previous
                                call on this reactor (longest first: no tail of a few slow cells), 1 */
+  int rendezvous_cycles;    /* tuned engine, one warp per cell: before each right-hand side a cell's warp waits
+                               up to this many SM clock cycles for the other warps of its block, so that they
+                               run the right-hand side's instruction stream together (0: off; at most 1e8;
+                               results are unchanged either way), 1000000 */
 } ppb_options;
 
 #define PPB_EOS_IDEAL 0 /* ideal gas: the mechanism's NASA-7 thermo (Source/Eos/Fuego.H) */

@@ -51,6 +51,7 @@ class Options(C.Structure):
         ("arkode_max_steps", C.c_int),
         ("eos", C.c_int),
         ("cost_order", C.c_int),
+        ("rendezvous_cycles", C.c_int),
     ]
 
 

@@ -324,6 +324,7 @@ static Options engine_options(const ppb_reactor* r)
   o.rk_min = r->opt.rk64_nsubsteps_min;
   o.rk_max = r->opt.rk64_nsubsteps_max;
   o.use_typ_vals = r->typ_vals.empty() ? 0 : 1;
+  o.rendezvous = r->opt.rendezvous_cycles;
   return o;
 }
 
@@ -430,8 +431,9 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
     for (int minb : {2, 1}) {
       if (minb == 1 && (r->method != METHOD_BDF || r->opt.lu_fp32) && team <= 32) continue;
       if (team > 32 && minb != 1) continue;
-      for (int wpb : {8, 4, 2, 1}) {
+      for (int wpb : {16, 8, 4, 2, 1}) {
         if (team > 32 && wpb != team / 32) continue;
+        if (wpb == 16 && (team != 32 || minb != 2)) continue;
         LaunchConfig lc;
         lc.engine = ENGINE_TUNED;
         lc.lu_fp32 = r->opt.lu_fp32;
@@ -597,6 +599,7 @@ void ppb_default_options(ppb_options* o)
   o->arkode_max_steps = 500;
   o->eos = PPB_EOS_IDEAL;
   o->cost_order = 1;
+  o->rendezvous_cycles = 1000000;
 }
 
 const char* ppb_last_error(void) { return g_err; }
@@ -666,6 +669,9 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
   if (r->opt.engine == PPB_ENGINE_PLAIN && r->opt.lu_fp32)
     return fail(PPB_E_ARG, "the plain engine is FP64 only");
   if (r->opt.eos != PPB_EOS_IDEAL && r->opt.eos != PPB_EOS_SRK) return fail(PPB_E_ARG, "eos must be 0 or 1");
+  if (r->opt.rendezvous_cycles < 0 || r->opt.rendezvous_cycles > 100000000)
+    return fail(PPB_E_ARG, "rendezvous_cycles must be in 0..100000000");
+  if (r->opt.warps_per_block > 16) return fail(PPB_E_ARG, "warps_per_block must be at most 16");
   if (r->opt.eos == PPB_EOS_SRK) {
     // SRK::RHY2T is not supported (Source/Eos/SRK.H:499-507), nor an
     // analytical Jacobian; this engine runs it on the tuned FP64 BDF

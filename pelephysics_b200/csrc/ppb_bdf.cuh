@@ -43,6 +43,7 @@ struct Options {
   int refine_sweeps;     // iterative-refinement sweeps when lu_fp32
   int rk_guess, rk_min, rk_max;
   int use_typ_vals;
+  int rendezvous;        // cycles a warp waits at a right-hand side for its block's other warps (0: off)
 };
 
 // Team-shared per-cell workspace.  LT is the LU storage type.
@@ -55,7 +56,32 @@ struct Work {
   int* piv;
   // rate scratch
   double *Y, *sc, *g, *qd, *wdot, *ei, *h1, *h2, *h3;
+  // block-shared rendezvous counters {arrived, generation, active warps}, or nullptr
+  int* rv = nullptr;
 };
+
+// Soft rendezvous of a block's warp teams before a right-hand side: the
+// team's lane 0 counts itself in and waits (at most `cycles` SM clocks) until
+// every active team of the block has arrived, so that the block's warps run
+// the right-hand side's instruction stream together.  It changes no
+// arithmetic: a team that times out just goes on alone.  Stale or doubled
+// arrivals only release a generation early.
+__device__ __forceinline__ void rendezvous(int* rv, int cycles)
+{
+  if ((threadIdx.x & 31) == 0) {
+    volatile int* v = rv;
+    const int g = v[1];
+    const int old = atomicAdd(&rv[0], 1);
+    if (old + 1 >= v[2]) {
+      atomicExch(&rv[0], 0);
+      atomicAdd(&rv[1], 1);
+    } else {
+      const long long t0 = clock64();
+      while (v[1] == g && clock64() - t0 < cycles) __nanosleep(32);
+    }
+  }
+  __syncwarp();
+}
 
 template <int TEAM>
 __device__ double reactor_rhs(
@@ -345,6 +371,7 @@ struct Bdf {
   // out of line: one copy of the right-hand side in the kernel
   __device__ __noinline__ void f(double t, const double* y, double* fy)
   {
+    if (w.rv) rendezvous(w.rv, o.rendezvous);
     PPB_TIC(PH_RHS);
     if constexpr (SRK) {
       reactor_rhs_srk<TEAM>(tm, M, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot, w.ei);

@@ -134,9 +134,10 @@ __device__ __forceinline__ void react_team_body(const Team<TEAM>& tm, const DevM
 }
 
 // Warp teams carry no block-shared scratch; a multi-warp team gets 16
-// doubles for its cross-warp reductions.
-template <int NS, typename LT, int METHOD, int TEAM, int MINB, bool SRK = false>
-__global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
+// doubles for its cross-warp reductions.  MAXT = 512 is the 16-warp block
+// (one block per SM, <= 128 registers) whose warps share one rendezvous.
+template <int NS, typename LT, int METHOD, int TEAM, int MINB, bool SRK = false, int MAXT = 256>
+__global__ void __launch_bounds__(MAXT, MINB) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
                                                           size_t cell_bytes, int persistent)
 {
   extern __shared__ __align__(16) char smem[];
@@ -151,12 +152,29 @@ __global__ void __launch_bounds__(256, MINB) k_react_team(DevMech M, Options o, 
     carve<LT>(w, smem + (size_t)team * cell_bytes, M.nsp, M.nrxn);
     const int tpb = blockDim.x / TEAM;
     if (persistent) {
+      __shared__ int rv[3];
+      if (TEAM == 32 && o.rendezvous > 0) {
+        if (threadIdx.x == 0) {
+          rv[0] = 0;
+          rv[1] = 0;
+          rv[2] = tpb;
+        }
+        __syncthreads();
+        w.rv = rv;
+      }
       for (;;) {
         int c = 0;
         if (tm.lane == 0) c = atomicAdd(queue, 1);
         c = __shfl_sync(tm.mask, c, 0, TEAM);
         if (c >= b.ncells) break;
         react_one<NS, TEAM, LT, METHOD, SRK>(tm, M, o, w, b, b.order ? b.order[c] : c, dt);
+      }
+      if (w.rv && tm.lane == 0) { // leave: the others stop waiting for this team
+        const int left = atomicSub(&rv[2], 1) - 1;
+        if (left > 0 && atomicAdd(&rv[0], 0) >= left) {
+          atomicExch(&rv[0], 0);
+          atomicAdd(&rv[1], 1);
+        }
       }
     } else {
       const int c = blockIdx.x * tpb + team;
@@ -180,9 +198,14 @@ constexpr int big_team()
 // 21 species, and a multi-warp team (one cell per block, one lane per
 // species) for larger ones.
 template <int NS>
-static TeamKernel team_kernel(int method, bool fp32, int team, int minb, int srk = 0)
+static TeamKernel team_kernel(int method, bool fp32, int team, int minb, int srk, int wpb)
 {
   constexpr bool small = NS <= 21;
+  // 16 warps per block: the FP64 BDF warp-per-cell kernel, <= 128 registers
+  if (wpb > 8)
+    return (wpb == 16 && method == METHOD_BDF && !fp32 && team == 32 && minb == 2 && !srk)
+             ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 512>
+             : nullptr;
   // the SRK e-reactor: FP64 BDF, one warp per cell, <= 128 registers
   if (srk) return (method == METHOD_BDF && !fp32 && team == 32 && minb == 2)
                     ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, true>
@@ -234,7 +257,7 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
   const int team = (lc.team == 16 || lc.team > 32) ? lc.team : 32;
   // a multi-warp team is one block
   const int wpb = team > 32 ? team / 32 : (lc.warps_per_block > 0 ? lc.warps_per_block : 4);
-  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.srk);
+  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.srk, wpb);
   if (!kern) return (int)cudaErrorInvalidConfiguration;
   const int tpb = team > 32 ? 1 : wpb * (32 / team); // cells per block
   const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
@@ -267,9 +290,9 @@ static int occupancy_ns(const DevMech& M, int method, const LaunchConfig& lc)
 {
   const bool fp32 = lc.lu_fp32 && method == METHOD_BDF;
   const int team = (lc.team == 16 || lc.team > 32) ? lc.team : 32;
-  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.srk);
-  if (!kern) return 0;
   const int wpb = team > 32 ? team / 32 : (lc.warps_per_block > 0 ? lc.warps_per_block : 4);
+  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.srk, wpb);
+  if (!kern) return 0;
   const int tpb = team > 32 ? 1 : wpb * (32 / team);
   const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
   const size_t shm = cb * tpb;

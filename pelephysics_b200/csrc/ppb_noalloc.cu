@@ -190,6 +190,9 @@ extern "C" int ppb_react_flat_device_noalloc(const char* mechanism, const char* 
   eo.rk_min = o.rk64_nsubsteps_min;
   eo.rk_max = o.rk64_nsubsteps_max;
   eo.use_typ_vals = 0;
+  if (o.rendezvous_cycles < 0 || o.rendezvous_cycles > 100000000)
+    return nf(PPB_E_ARG, "rendezvous_cycles must be in 0..100000000");
+  eo.rendezvous = o.rendezvous_cycles;
   LaunchConfig lc;
   lc.engine = o.engine;
   lc.lu_fp32 = o.lu_fp32;

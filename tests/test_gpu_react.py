@@ -388,3 +388,32 @@ def test_cost_ordered_queue_changes_no_bits(cuda, oracle):
         costs = r.cell_status(nc)[1]
         assert costs.max() > 2 * costs.min()  # the costs differ, so the order does
     np.testing.assert_array_equal(outs[0], outs[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("wpb", [8, 16])
+def test_block_rendezvous_changes_no_bits(cuda, oracle, wpb):
+    """The rendezvous before each right-hand side only changes when a cell's
+    warp runs, never what it computes: every cell gives the same bits with
+    rendezvous_cycles = 0 and the default, at 8 and 16 warps per block, and
+    the cells still match the CPU oracle."""
+    torch = cuda
+    mech, dt, nc = "drm19", 1e-5, 3000
+    rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 8, 1000.0, 1000.0, 0.5, 1.5)
+    outs, stats = [], []
+    for cyc in (0, 1000000):
+        r = Reactor(mech)
+        r.init(1, nc, rtol=1e-10, atol=1e-10, max_order=5, warps_per_block=wpb, rendezvous_cycles=cyc)
+        y = torch.as_tensor(rY, device="cuda").contiguous()
+        x = torch.as_tensor(rX, device="cuda")
+        r.react(y, torch.as_tensor(src, device="cuda").contiguous(), x, torch.as_tensor(rXs, device="cuda"), dt)
+        outs.append(y.cpu().numpy())
+        stats.append(r.cell_stats(nc))
+        assert r.launch_config()[0] == wpb
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(stats[0], stats[1])
+    idx = np.arange(0, nc, 97)
+    ref, _, flag, _, _ = oracle_react(oracle, mech, 1, rY[idx], src[idx], rX[idx], rXs[idx], dt, rtol=1e-10,
+                                      atol=1e-10, max_order=5)
+    assert flag == 0
+    compare(outs[1][idx], ref)
