@@ -161,6 +161,8 @@ __global__ void __launch_bounds__(256) k_tangent(DevMech M, Options o, AdjBatch 
   char* base = smem + (size_t)warp * L.warp_smem;
   Work<LT> w;
   carve<LT>(w, base, NS, R);
+  __shared__ int rv[3];
+  w.rv = rendezvous_init(rv, blockDim.x / 32, o.rendezvous);
   AdjWork a;
   carve_adj(a, base + team_bytes<LT>(NS, R), NS, R);
   TapeRec* tape = reinterpret_cast<TapeRec*>(L.tape) + gwarp * (size_t)L.cap_rec;
@@ -172,6 +174,7 @@ __global__ void __launch_bounds__(256) k_tangent(DevMech M, Options o, AdjBatch 
     if (c >= b.ncells) break;
     tangent_cell<NS, LT>(tm, M, o, w, a, b, L, tape, ys, c, dt);
   }
+  rendezvous_leave(w.rv);
 }
 
 // Pointwise: f, df/dy, df/dE and, for a weight vector v per cell,
@@ -342,6 +345,8 @@ __global__ void __launch_bounds__(256) k_adj_seg(DevMech M, Options o, AdjBatch 
   const int warp = threadIdx.x / 32;
   Work<LT> w;
   carve<LT>(w, smem + (size_t)warp * warp_smem, NS, R);
+  __shared__ int rv[3];
+  w.rv = rendezvous_init(rv, blockDim.x / 32, o.rendezvous);
   for (;;) {
     int c = 0;
     if (tm.lane == 0) c = atomicAdd(queue, 1);
@@ -451,6 +456,7 @@ __global__ void __launch_bounds__(256) k_adj_seg(DevMech M, Options o, AdjBatch 
     }
     tm.sync();
   }
+  rendezvous_leave(w.rv);
 }
 
 // Every differentiated point of items [i0, i1) of segment seg (item i of

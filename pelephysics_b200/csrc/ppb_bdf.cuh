@@ -83,6 +83,32 @@ __device__ __forceinline__ void rendezvous(int* rv, int cycles)
   __syncwarp();
 }
 
+// The block's counters for a persistent loop of `teams` warp teams; every
+// thread of the block calls it.  nullptr (no rendezvous) when cycles <= 0.
+__device__ __forceinline__ int* rendezvous_init(int* rv, int teams, int cycles)
+{
+  if (cycles <= 0) return nullptr;
+  if (threadIdx.x == 0) {
+    rv[0] = 0;
+    rv[1] = 0;
+    rv[2] = teams;
+  }
+  __syncthreads();
+  return rv;
+}
+
+// A team leaves the persistent loop: the others stop waiting for it.
+__device__ __forceinline__ void rendezvous_leave(int* rv)
+{
+  if (rv && (threadIdx.x & 31) == 0) {
+    const int left = atomicSub(&rv[2], 1) - 1;
+    if (left > 0 && atomicAdd(&rv[0], 0) >= left) {
+      atomicExch(&rv[0], 0);
+      atomicAdd(&rv[1], 1);
+    }
+  }
+}
+
 template <int TEAM>
 __device__ double reactor_rhs(
   const Team<TEAM>& tm, const DevMech& M, int rtype, double t, const double* y, double* ydot, double rhoe,

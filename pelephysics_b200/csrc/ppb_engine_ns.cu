@@ -153,15 +153,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_react_team(DevMech M, Options o,
     const int tpb = blockDim.x / TEAM;
     if (persistent) {
       __shared__ int rv[3];
-      if (TEAM == 32 && o.rendezvous > 0) {
-        if (threadIdx.x == 0) {
-          rv[0] = 0;
-          rv[1] = 0;
-          rv[2] = tpb;
-        }
-        __syncthreads();
-        w.rv = rv;
-      }
+      if (TEAM == 32) w.rv = rendezvous_init(rv, tpb, o.rendezvous);
       for (;;) {
         int c = 0;
         if (tm.lane == 0) c = atomicAdd(queue, 1);
@@ -169,13 +161,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_react_team(DevMech M, Options o,
         if (c >= b.ncells) break;
         react_one<NS, TEAM, LT, METHOD, SRK>(tm, M, o, w, b, b.order ? b.order[c] : c, dt);
       }
-      if (w.rv && tm.lane == 0) { // leave: the others stop waiting for this team
-        const int left = atomicSub(&rv[2], 1) - 1;
-        if (left > 0 && atomicAdd(&rv[0], 0) >= left) {
-          atomicExch(&rv[0], 0);
-          atomicAdd(&rv[1], 1);
-        }
-      }
+      rendezvous_leave(w.rv);
     } else {
       const int c = blockIdx.x * tpb + team;
       if (c < b.ncells) react_one<NS, TEAM, LT, METHOD, SRK>(tm, M, o, w, b, c, dt);
