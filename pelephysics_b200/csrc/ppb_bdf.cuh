@@ -395,7 +395,10 @@ struct Bdf {
   }
 
   // out of line: one copy of the right-hand side in the kernel
-  __device__ __noinline__ void f(double t, const double* y, double* fy)
+#ifndef PPB_RHS_ATTR
+#define PPB_RHS_ATTR __noinline__
+#endif
+  __device__ PPB_RHS_ATTR void f(double t, const double* y, double* fy)
   {
     if (w.rv) rendezvous(w.rv, o.rendezvous);
     PPB_TIC(PH_RHS);
