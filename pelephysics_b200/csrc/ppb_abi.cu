@@ -431,9 +431,9 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
     for (int minb : {2, 1}) {
       if (minb == 1 && (r->method != METHOD_BDF || r->opt.lu_fp32) && team <= 32) continue;
       if (team > 32 && minb != 1) continue;
-      for (int wpb : {16, 8, 4, 2, 1}) {
+      for (int wpb : {16, 12, 8, 4, 2, 1}) {
         if (team > 32 && wpb != team / 32) continue;
-        if (wpb == 16 && (team != 32 || minb != 2)) continue;
+        if (wpb > 8 && (team != 32 || minb != 2)) continue;
         LaunchConfig lc;
         lc.engine = ENGINE_TUNED;
         lc.lu_fp32 = r->opt.lu_fp32;

@@ -134,8 +134,9 @@ __device__ __forceinline__ void react_team_body(const Team<TEAM>& tm, const DevM
 }
 
 // Warp teams carry no block-shared scratch; a multi-warp team gets 16
-// doubles for its cross-warp reductions.  MAXT = 512 is the 16-warp block
-// (one block per SM, <= 128 registers) whose warps share one rendezvous.
+// doubles for its cross-warp reductions.  MAXT = 384 / 512 are the 12- and
+// 16-warp blocks (one block per SM, <= 168 / <= 128 registers) whose warps
+// share one rendezvous.
 template <int NS, typename LT, int METHOD, int TEAM, int MINB, bool SRK = false, int MAXT = 256>
 __global__ void __launch_bounds__(MAXT, MINB) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
                                                           size_t cell_bytes, int persistent)
@@ -187,11 +188,14 @@ template <int NS>
 static TeamKernel team_kernel(int method, bool fp32, int team, int minb, int srk, int wpb)
 {
   constexpr bool small = NS <= 21;
-  // 16 warps per block: the FP64 BDF warp-per-cell kernel, <= 128 registers
-  if (wpb > 8)
-    return (wpb == 16 && method == METHOD_BDF && !fp32 && team == 32 && minb == 2 && !srk)
-             ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 512>
-             : nullptr;
+  // 12 or 16 warps per block (one block per SM: <= 168 or <= 128 registers):
+  // the FP64 BDF warp-per-cell kernel
+  if (wpb > 8) {
+    if (method != METHOD_BDF || fp32 || team != 32 || minb != 2 || srk) return nullptr;
+    if (wpb == 16) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 512>;
+    if (wpb == 12) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 384>;
+    return nullptr;
+  }
   // the SRK e-reactor: FP64 BDF, one warp per cell, <= 128 registers
   if (srk) return (method == METHOD_BDF && !fp32 && team == 32 && minb == 2)
                     ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, true>

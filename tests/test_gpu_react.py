@@ -391,11 +391,11 @@ def test_cost_ordered_queue_changes_no_bits(cuda, oracle):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("wpb", [8, 16])
+@pytest.mark.parametrize("wpb", [8, 12, 16])
 def test_block_rendezvous_changes_no_bits(cuda, oracle, wpb):
     """The rendezvous before each right-hand side only changes when a cell's
     warp runs, never what it computes: every cell gives the same bits with
-    rendezvous_cycles = 0 and the default, at 8 and 16 warps per block, and
+    rendezvous_cycles = 0 and the default, at 8, 12 and 16 warps per block, and
     the cells still match the CPU oracle."""
     torch = cuda
     mech, dt, nc = "drm19", 1e-5, 3000
