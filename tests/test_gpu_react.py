@@ -391,19 +391,20 @@ def test_cost_ordered_queue_changes_no_bits(cuda, oracle):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("wpb", [8, 12, 16])
-def test_block_rendezvous_changes_no_bits(cuda, oracle, wpb):
+@pytest.mark.parametrize("wpb,cyc", [(8, 1000000), (12, 1000000), (16, 1000000), (16, 2000)])
+def test_block_rendezvous_changes_no_bits(cuda, oracle, wpb, cyc):
     """The rendezvous before each right-hand side only changes when a cell's
     warp runs, never what it computes: every cell gives the same bits with
-    rendezvous_cycles = 0 and the default, at 8, 12 and 16 warps per block, and
+    rendezvous_cycles = 0 and with a bound (the default, and a bound short
+    enough that most waits time out), at 8, 12 and 16 warps per block, and
     the cells still match the CPU oracle."""
     torch = cuda
     mech, dt, nc = "drm19", 1e-5, 3000
     rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 8, 1000.0, 1000.0, 0.5, 1.5)
     outs, stats = [], []
-    for cyc in (0, 1000000):
+    for bound in (0, cyc):
         r = Reactor(mech)
-        r.init(1, nc, rtol=1e-10, atol=1e-10, max_order=5, warps_per_block=wpb, rendezvous_cycles=cyc)
+        r.init(1, nc, rtol=1e-10, atol=1e-10, max_order=5, warps_per_block=wpb, rendezvous_cycles=bound)
         y = torch.as_tensor(rY, device="cuda").contiguous()
         x = torch.as_tensor(rX, device="cuda")
         r.react(y, torch.as_tensor(src, device="cuda").contiguous(), x, torch.as_tensor(rXs, device="cuda"), dt)
