@@ -79,15 +79,17 @@ def cpu_sample_index(ncells, n):
 
 
 def run_cpu(po, cells, idx, nthreads=0):
-    """The oracle (reference kernels) on cells[idx]; returns (seconds, rY)."""
+    """The oracle (reference kernels) on cells[idx]; returns (seconds, rY,
+    flag, per-cell counters [steps, RHS, Jacobians, factorisations, Newton
+    iterations, error-test failures, convergence failures])."""
     po.load_ref(MECH)
     rY = cells.rY[idx].copy()
     rX = cells.rX[idx].copy()
     src = np.ascontiguousarray(cells.rYsrc[idx])
     rXs = cells.rX_src[idx].copy()
     t0 = time.perf_counter()
-    flag, nfe, st = po.react_flat(MECH, 1, rY, src, rX, rXs, DT, use_ref_kernels=1, nthreads=nthreads, **OPTS)
-    return time.perf_counter() - t0, rY, flag
+    flag, st, stats = po.react_flat_stats(MECH, 1, rY, src, rX, rXs, DT, use_ref_kernels=1, nthreads=nthreads, **OPTS)
+    return time.perf_counter() - t0, rY, flag, stats
 
 
 def reference_arm(args):
@@ -105,7 +107,7 @@ def reference_arm(args):
         run_cpu(po, cells, idx[:1024])
     times = []
     for _ in range(args.steps):
-        dt, _, flag = run_cpu(po, cells, idx)
+        dt, _, flag, _ = run_cpu(po, cells, idx)
         times.append(dt)
     tot = sum(times)
     value = len(idx) * args.steps / tot
@@ -306,60 +308,107 @@ def our_arm(args):
 
     out = {}
     if rank == 0:
-        # plain engine on a strided sub-field (the full field takes tens of s)
-        sub = np.arange(0, n, 8)
+        # the plain per-cell FP64 engine on the same full field (equal work)
         rp = Reactor(MECH)
-        rp.init(1, sub.size, engine=0, **OPTS)
-        yp = torch.as_tensor(cells.rY[sub], device=dev).contiguous()
-        xp = torch.as_tensor(cells.rX[sub], device=dev)
-        sp = torch.as_tensor(cells.rYsrc[sub], device=dev).contiguous()
-        xsp = torch.as_tensor(cells.rX_src[sub], device=dev)
-        # one untimed call on copies first: module load, scratch and graph
-        # capture stay outside the timed call
-        rp.react(yp.clone(), sp, xp.clone(), xsp, DT)
+        rp.init(1, n, engine=0, **OPTS)
+        yp = y0.clone()
+        xp = x0.clone()
+        # one untimed call first: module load, scratch and graph capture stay
+        # outside the timed call
+        rp.react_soa(yp, s0, xp, xs, DT)
+        yp.copy_(y0)
+        xp.copy_(x0)
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        rp.react(yp, sp, xp, xsp, DT)
-        b.record()
+        a.record(stream)
+        rp.react_soa(yp, s0, xp, xs, DT, stream=stream)
+        b.record(stream)
         torch.cuda.synchronize()
-        plain_value = sub.size / (a.elapsed_time(b) / 1e3)
-        y_plain = yp.cpu().numpy()
-        dT_plain = float(np.max(np.abs(y_plain[:, N] - y_gpu[sub, N]) / y_gpu[sub, N]))
+        plain_value = n / (a.elapsed_time(b) / 1e3)
+        y_plain = yp.cpu().numpy().T
+        dT_plain = float(np.max(np.abs(y_plain[:, N] - y_gpu[:, N]) / y_gpu[:, N]))
         rp.close()
+        # the FP32-factor engine (FP32 LU of I - gamma J, one FP64
+        # refinement sweep) on the same field
+        rf = Reactor(MECH)
+        rf.init(1, n, engine=1, lu_fp32=1, refine_sweeps=1, **OPTS)
+        yf = y0.clone()
+        xf = x0.clone()
+        rf.react_soa(yf, s0, xf, xs, DT)
+        ms_f = []
+        for _ in range(args.steps):
+            yf.copy_(y0)
+            xf.copy_(x0)
+            flush.zero_()
+            a.record(stream)
+            rf.react_soa(yf, s0, xf, xs, DT, stream=stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms_f.append(a.elapsed_time(b))
+        fp32_value = n * len(ms_f) / (sum(ms_f) / 1e3)
+        y_fp32 = yf.cpu().numpy().T.copy()
+        fw, ft, fr, _ = rf.launch_config()
+        rf.close()
         if not args.no_adjoint:
             out["adjoint"] = adjoint_measure(dev, args.adjoint_cells)
         peak = probe_fp64_peak()
-        flops = algorithmic_flops(stats, N + 1)
-        out.update(plain_value=plain_value, dT_plain=dT_plain, fp64_peak_gflops=peak, flops=flops)
+        out.update(plain_value=plain_value, dT_plain=dT_plain, fp64_peak_gflops=peak, fp32_value=fp32_value,
+                   fp32_launch={"warps_per_block": fw, "lanes_per_cell": ft, "register_budget": fr})
 
     cpu = None
     acc = None
+    flops = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         from oracle import pyoracle as po
 
         idx = cpu_sample_index(n, CPU_SAMPLE)
-        secs, y_cpu, flag = run_cpu(po, cells, idx)
+        secs, y_cpu, flag, ostats = run_cpu(po, cells, idx)
         cpu = {"value": len(idx) / secs, "unit": "cells/s", "cores": os.cpu_count(), "kind": "reference",
                "sample": f"{len(idx)} seeded cells of the same 64^3 field, one react; CVODE-algorithm BDF "
                          "(oracle/reactor.c) over the reference's own compiled drm19 kernels (oracle/_ref), "
                          "OpenMP over all host threads (ReactorCvode needs the absent SUNDIALS)"}
-        g = y_gpu[idx]
-        dT = np.abs(g[:, N] - y_cpu[:, N]) / y_cpu[:, N]
-        Yg = g[:, :N] / g[:, :N].sum(1, keepdims=True)
-        Yc = y_cpu[:, :N] / y_cpu[:, :N].sum(1, keepdims=True)
-        acc = {"cells": int(len(idx)), "max_rel_T": float(dT.max()), "max_abs_Y": float(np.abs(Yg - Yc).max())}
+        # algorithmic work per cell from the oracle's counters on the sample
+        # (implementation-independent), times the cells of the field
+        flops = algorithmic_flops(ostats, N + 1) / len(idx) * n
+        inputs = (cells.rY[idx], cells.rYsrc[idx], cells.rX[idx], cells.rX_src[idx])
+        acc = po.compare_to_reference(MECH, 1, *inputs, DT, y_gpu[idx], y_cpu, use_ref_kernels=1, **OPTS)
+        acc["fp32_factor"] = po.compare_to_reference(MECH, 1, *inputs, DT, y_fp32[idx], y_cpu, use_ref_kernels=1,
+                                                     **OPTS)
+        acc["plain"] = po.compare_to_reference(MECH, 1, *inputs, DT, y_plain[idx], y_cpu, use_ref_kernels=1, **OPTS)
+        # against a converged solution (the oracle at rtol = atol = 1e-13):
+        # the error of the GPU and of the oracle itself at 1e-10
+        yconv = cells.rY[idx].copy()
+        po.react_flat(MECH, 1, yconv, np.ascontiguousarray(cells.rYsrc[idx]), cells.rX[idx].copy(),
+                      cells.rX_src[idx].copy(), DT, use_ref_kernels=1, rtol=1e-13, atol=1e-13, max_order=5)
+        Yv = po.mass_fraction_rows(yconv, N)
+        err = lambda yy: {"max_rel_T": float(np.max(np.abs(yy[:, N] - yconv[:, N]) / yconv[:, N])),
+                          "max_abs_Y": float(np.abs(po.mass_fraction_rows(yy, N) - Yv).max())}
+        acc["vs_converged_oracle_1e-13"] = {"gpu_tuned": err(y_gpu[idx]), "gpu_fp32_factor": err(y_fp32[idx]),
+                                            "oracle_1e-10": err(y_cpu)}
+        acc["oracle_counts_per_cell"] = dict(zip(["steps", "rhs", "jac", "lu", "newton", "err_fail", "conv_fail"],
+                                                 [round(float(v), 3) for v in ostats.mean(axis=0)]))
+
+    configs = None
+    if rank == 0 and ws == 1 and not args.no_configs:
+        from oracle import pyoracle as po
+
+        configs = {"lidryer_16cubed": measure_lidryer(po, dev)}
+        for cfg in ("dodecane", "heptane"):
+            configs[cfg] = measure_config(cfg, 1, 256)
 
     if rank == 0:
         t_step = t_dev / args.steps
         roof = None
-        if out.get("flops") is not None:
-            achieved = out["flops"] / t_step / 1e12
+        if flops is not None:
+            achieved = flops / t_step / 1e12
             peak_t = out["fp64_peak_gflops"] / 1e3
             roof = {"bound": "fp64", "achieved": achieved, "peak": peak_t, "unit": "TFLOP/s",
                     "frac": achieved / peak_t, "traffic": TRAFFIC_PER_CELL * n,
-                    "traffic_note": "bytes per launch, scaled from the 16^3 ncu capture by cells",
+                    "work_note": "FP64 work per cell = n_RHS F_rhs + n_Jac F_jac + n_LU ((2/3) n^3 + n^2) + "
+                                 "n_Newton 2 n^2 with the counts of the CPU oracle on the 8192-cell sample "
+                                 "(accuracy_vs_fp64_oracle.oracle_counts_per_cell), times the cells",
+                    "traffic_note": "DRAM bytes per launch, per cell from the 16^3 ncu capture times the cells",
                     "peak_source": "measured FP64 FMA probe on this GPU (ppb_probe_fp64_peak)"}
         line = {
             "metric": METRIC,
@@ -386,9 +435,15 @@ def our_arm(args):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "tuned_vs_plain": {"plain_value": out["plain_value"], "ratio": value / ws / out["plain_value"],
-                               "plain_sample": "every 8th cell, one react after one untimed warm-up react", "max_rel_T_tuned_vs_plain": out["dT_plain"]},
+                               "plain_sample": "the full field, one react after one untimed warm-up react",
+                               "max_rel_T_tuned_vs_plain": out["dT_plain"]},
+            "fp32_factor": {"value": out["fp32_value"], "ratio_vs_plain": out["fp32_value"] / out["plain_value"],
+                            "ratio_vs_fp64_lu": out["fp32_value"] / (value / ws),
+                            "engine": "tuned, FP32 LU of I - gamma J + one FP64 refinement sweep",
+                            "launch": out["fp32_launch"]},
             "accuracy_vs_fp64_oracle": acc,
             "adjoint": out.get("adjoint"),
+            "configs": configs,
             "cell_failures": int(np.sum(status < 0)),
             "per_cell_mean": dict(zip(["steps", "rhs", "jac", "lu", "newton", "err_fail", "conv_fail"],
                                       [round(float(v), 3) for v in stats.mean(axis=0)])),
@@ -461,20 +516,20 @@ def adjoint_measure(dev, ncells):
             "mean_steps": float(fwd_stats[:, 0].mean())}
 
 
-def config_arm(args):
-    """The larger configurations, one JSON line each (not the headline):
-    dodecane_lu 128x128x64 (FP64 LU vs FP32 factor + FP64 refinement) and
-    heptane_lu_88sk 64^3 (the same two, plus RK64), with errors against the
-    FP64 CPU oracle on a seeded sample of cells."""
+def measure_config(config, steps, sample):
+    """One of the larger configurations, as a dict: dodecane_lu 128x128x64
+    (FP64 LU vs FP32 factor + FP64 refinement) or heptane_lu_88sk 64^3 (the
+    same two, plus RK64); per arm cells/s over `steps` timed react calls after
+    one warm-up call, and errors against the FP64 CPU oracle on a seeded
+    sample of `sample` cells."""
     import torch
 
     from oracle import pyoracle as po
     from pelephysics_b200 import workloads as wl
     from pelephysics_b200.reactor import Reactor
 
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(dev)
-    if args.config == "dodecane":
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if config == "dodecane":
         mech = "dodecane_lu"
         cells = wl.dodecane_field(device=dev)
         opts = dict(rtol=1e-10, atol=1e-10, max_order=5)
@@ -495,11 +550,11 @@ def config_arm(args):
     s0 = torch.as_tensor(cells.rYsrc.T.copy(), device=dev)
     x0 = torch.as_tensor(cells.rX, device=dev)
     xs = torch.as_tensor(cells.rX_src, device=dev)
-    idx = np.sort(np.random.default_rng(9).permutation(n)[:args.sample])
+    idx = np.sort(np.random.default_rng(9).permutation(n)[:sample])
     yc = cells.rY[idx].copy()
     t0 = time.perf_counter()
     flag, _, _ = po.react_flat(mech, 1, yc, np.ascontiguousarray(cells.rYsrc[idx]), cells.rX[idx].copy(),
-                               cells.rX_src[idx].copy(), cells.dt, use_ref_kernels=0, **opts)
+                               cells.rX_src[idx].copy(), cells.dt, use_ref_kernels=1, **opts)
     cpu_s = time.perf_counter() - t0
     out = {}
     for name, integ, extra in arms:
@@ -507,9 +562,9 @@ def config_arm(args):
         r.init(1, n, engine=1, **opts, **extra)
         y = y0.clone()
         x = x0.clone()
-        r.react_soa(y, s0, x, xs, cells.dt)  # warm-up (allocations, graph)
+        r.react_soa(y, s0, x, xs, cells.dt)  # warm-up (autotuner, allocations, graph)
         ms = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             y.copy_(y0)
             x.copy_(x0)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -540,7 +595,7 @@ def config_arm(args):
             # the oracle's RK64 on the sample: the explicit scheme's own answer
             yk = cells.rY[idx].copy()
             po.react_flat(mech, 1, yk, np.ascontiguousarray(cells.rYsrc[idx]), cells.rX[idx].copy(),
-                          cells.rX_src[idx].copy(), cells.dt, method=1, use_ref_kernels=0, **opts)
+                          cells.rX_src[idx].copy(), cells.dt, method=1, use_ref_kernels=1, **opts)
             okk = np.all(np.isfinite(yk), axis=1)
             both = okk & ok
             out[name]["oracle_rk64_nonfinite_in_sample"] = int(np.sum(~okk))
@@ -548,9 +603,64 @@ def config_arm(args):
             if both.any():
                 out[name]["max_rel_T_vs_oracle_rk64"] = float(np.max(np.abs(yg[both, N] - yk[both, N]) / yk[both, N]))
         r.close()
-    line = {"config": args.config, "workload": workload, "cells": n, "opts": opts, "arms": out,
+    return {"workload": workload, "cells": n, "opts": opts, "arms": out,
             "oracle_sample": {"cells": int(len(idx)), "seconds": cpu_s, "flag": int(flag),
-                              "kind": "oracle BDF (table-driven FP64 kernels), OpenMP"},
+                              "kind": "oracle BDF over the reference's compiled kernels (oracle/_ref), OpenMP"}}
+
+
+def measure_lidryer(po, dev):
+    """Configuration 1: LiDryer 16^3 = 4096 cells (T 1000 + 400 U, phi 0.5 +
+    1.5 U, seed 0, 1 atm), dt 1e-4 s, rtol = atol = 1e-10, BDF orders <= 5;
+    tuned and plain engines, one timed react each after a warm-up react, and
+    every cell against the oracle over the reference's compiled kernels."""
+    import torch
+
+    from pelephysics_b200 import workloads as wl
+    from pelephysics_b200.reactor import Reactor
+
+    cells = wl.lidryer_16(device=dev)
+    n = cells.ncells
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5)
+    yc = cells.rY.copy()
+    t0 = time.perf_counter()
+    flag, _, _ = po.react_flat("LiDryer", 1, yc, np.ascontiguousarray(cells.rYsrc), cells.rX.copy(),
+                               cells.rX_src.copy(), cells.dt, use_ref_kernels=1, **opts)
+    cpu_s = time.perf_counter() - t0
+    out = {"workload": "LiDryer 16^3 (4096 cells), 1 atm, T 1000+400 U, phi 0.5+1.5 U, dt 1e-4 s, "
+                       "rtol=atol=1e-10, BDF q<=5", "cells": n,
+           "oracle": {"cells_per_s": n / cpu_s, "cores": os.cpu_count(), "flag": int(flag)}}
+    y0 = torch.as_tensor(cells.rY.T.copy(), device=dev)
+    s0 = torch.as_tensor(cells.rYsrc.T.copy(), device=dev)
+    x0 = torch.as_tensor(cells.rX, device=dev)
+    xs = torch.as_tensor(cells.rX_src, device=dev)
+    for name, engine in (("tuned", 1), ("plain", 0)):
+        r = Reactor("LiDryer")
+        r.init(1, n, engine=engine, **opts)
+        y, x = y0.clone(), x0.clone()
+        r.react_soa(y, s0, x, xs, cells.dt)
+        y.copy_(y0)
+        x.copy_(x0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        r.react_soa(y, s0, x, xs, cells.dt)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        yg = y.cpu().numpy().T.copy()
+        acc = po.compare_to_reference("LiDryer", 1, cells.rY, cells.rYsrc, cells.rX, cells.rX_src, cells.dt, yg, yc,
+                                      use_ref_kernels=1, **opts)
+        out[name] = {"cells_per_s": n / (ms / 1e3), "ms_per_react": ms, "accuracy_vs_fp64_oracle": acc}
+        r.close()
+    out["tuned_vs_plain"] = out["tuned"]["cells_per_s"] / out["plain"]["cells_per_s"]
+    return out
+
+
+def config_arm(args):
+    """--config dodecane|heptane: the larger configuration on its own line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    line = {"config": args.config, **measure_config(args.config, args.steps, args.sample),
             "dtype": "f64 state; LU as named"}
     print(json.dumps(line), flush=True)
     return 0
@@ -757,36 +867,12 @@ def srk_arm(args):
     return 0
 
 
-def flops_probe():
-    """One drm19 cell: reactor RHS and reactor Jacobian pointwise kernels,
-    thread per cell (run under ncu to count FP64 operations)."""
-    import torch
-
-    from pelephysics_b200 import _lib, workloads as wl
-
-    cells = wl.premix_cells(MECH, 1, 3, 1500.0, 0.0, 1.0, 0.0, dt=DT)
-    N = cells.rY.shape[1] - 1
-    y = torch.as_tensor(cells.rY, device="cuda")
-    x = torch.as_tensor(cells.rX, device="cuda")
-    xs = torch.as_tensor(cells.rX_src, device="cuda")
-    s = torch.as_tensor(cells.rYsrc, device="cuda")
-    f = torch.zeros_like(y)
-    _lib.check(_lib.lib().ppb_reactor_rhs(MECH.encode(), 1, 0.0, y.data_ptr(), x.data_ptr(), xs.data_ptr(),
-                                          s.data_ptr(), f.data_ptr(), 1, 1, None))
-    rho = y[:, :N].sum()
-    sc = (y[:, :N] / torch.as_tensor(_lib.molecular_weights(MECH), device="cuda")) * 1e6
-    J = torch.zeros(((N + 1) ** 2,), dtype=torch.float64, device="cuda")
-    T = y[:, N].contiguous()
-    _lib.check(_lib.lib().ppb_ajacobian(MECH.encode(), sc.contiguous().data_ptr(), T.data_ptr(), 0, J.data_ptr(), 1,
-                                        1, None))
-    torch.cuda.synchronize()
-    print("flops probe done", float(rho))
-    return 0
-
-
-def kernel_probe(ncells=16384, reps=5):
-    """Device time of the pointwise reactor RHS and Jacobian kernels on the
-    drm19 field's first ncells cells, thread-per-cell and warp-per-cell."""
+def pointwise_arm(args, reps=5):
+    """Device time of the pointwise kernels -- reactor RHS (fKernelSpec),
+    productionRate and aJacobian -- on the drm19 field's first --cells cells,
+    thread-per-cell and warp-per-cell (one JSON line; with --cells 1 the
+    launches are the single-cell ones whose FP64 operations ncu counts)."""
+    ncells = args.cells
     import torch
 
     from pelephysics_b200 import _lib, workloads as wl
@@ -822,46 +908,7 @@ def kernel_probe(ncells=16384, reps=5):
             torch.cuda.synchronize()
             us = a.elapsed_time(b) * 1e3 / reps
             out[f"{name}_team{team}"] = {"us_per_launch": round(us, 2), "ns_per_cell": round(us * 1e3 / n, 3)}
-    print(json.dumps({"kernel_probe": out, "cells": n}), flush=True)
-    return 0
-
-
-def phase_probe(edge=64, engine=1, lu_fp32=0):
-    """Per-phase cycle totals of one react() of the field (needs the profiling
-    build: PPB_LIB=pelephysics_b200/libppb200_phase.so)."""
-    import ctypes as C
-
-    import torch
-
-    from pelephysics_b200 import _lib, workloads as wl
-    from pelephysics_b200.reactor import Reactor
-
-    L = _lib.lib()
-    if not hasattr(L, "ppb_phase_cycles"):
-        raise SystemExit("phase probe needs PPB_LIB=pelephysics_b200/libppb200_phase.so")
-    cells = wl.drm19_field(edge)
-    n = cells.ncells
-    r = Reactor(MECH)
-    r.init(1, n, engine=engine, lu_fp32=lu_fp32, use_graph=0, **OPTS)
-    buf = (C.c_ulonglong * 7)()
-    y = torch.as_tensor(cells.rY.T.copy(), device="cuda")
-    s_ = torch.as_tensor(cells.rYsrc.T.copy(), device="cuda")
-    x = torch.as_tensor(cells.rX, device="cuda")
-    xs = torch.as_tensor(cells.rX_src, device="cuda")
-    r.react_soa(y.clone(), s_, x.clone(), xs, DT)
-    torch.cuda.synchronize()
-    L.ppb_phase_cycles(buf, 1)
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    r.react_soa(y, s_, x, xs, DT)
-    b.record()
-    torch.cuda.synchronize()
-    L.ppb_phase_cycles(buf, 1)
-    names = ["rhs", "jac", "lu", "solve", "newton", "step", "total"]
-    tot = buf[6]
-    res = {k: {"cycles_per_cell": buf[i] / n, "frac_of_total": buf[i] / tot} for i, k in enumerate(names)}
-    print(json.dumps({"phase_probe": res, "cells": n, "ms": a.elapsed_time(b),
-                      "per_cell_mean": r.cell_stats(n).mean(axis=0).round(3).tolist()}), flush=True)
+    print(json.dumps({"config": "pointwise", "mech": MECH, "kernels": out, "cells": n}), flush=True)
     return 0
 
 
@@ -874,26 +921,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-workload measurement")
     ap.add_argument("--adjoint-cells", type=int, default=65536)
-    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane", "arkode", "transport", "srk"],
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (LiDryer 16^3, dodecane_lu, heptane_lu_88sk) in the line")
+    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane", "arkode", "transport", "srk", "pointwise"],
                     help="drm19: the headline line; dodecane / heptane: the larger configurations; arkode: "
                          "the ReactorArkode integrator on the drm19 field")
     ap.add_argument("--sample", type=int, default=256, help="oracle sample cells for --config dodecane/heptane")
     ap.add_argument("--launch", default="", help="W,T,R: fixed warps per block, lanes per cell, register budget "
                                                  "instead of the autotuner (profiling runs)")
     ap.add_argument("--edge", type=int, default=64, help="field edge (profiling runs use a smaller box)")
-    ap.add_argument("--phase-probe", action="store_true",
-                    help="per-phase cycle counters of one react (profiling build, PPB_LIB)")
-    ap.add_argument("--kernel-probe", action="store_true",
-                    help="time the pointwise RHS / Jacobian / rate kernels on the field's cells")
-    ap.add_argument("--flops-probe", action="store_true",
-                    help="launch one single-cell RHS and one Jacobian evaluation (for an ncu FP64 op count)")
+    ap.add_argument("--cells", type=int, default=16384, help="cells of the field for --config pointwise")
     args = ap.parse_args()
-    if args.flops_probe:
-        return flops_probe()
-    if args.kernel_probe:
-        return kernel_probe()
-    if args.phase_probe:
-        return phase_probe(args.edge)
     if args.impl == "reference":
         return reference_arm(args)
     if args.config == "arkode":
@@ -902,6 +940,8 @@ def main():
         return transport_arm(args)
     if args.config == "srk":
         return srk_arm(args)
+    if args.config == "pointwise":
+        return pointwise_arm(args)
     if args.config != "drm19":
         return config_arm(args)
     return our_arm(args)

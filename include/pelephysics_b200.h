@@ -78,8 +78,12 @@ typedef struct ppb_options {
                                call on this reactor (longest first: no tail of a few slow cells), 1 */
   int rendezvous_cycles;    /* tuned engine, one warp per cell: before each right-hand side a cell's warp waits
                                up to this many SM clock cycles for the other warps of its block, so that they
-                               run the right-hand side's instruction stream together (0: off; at most 1e8;
+                               run the right-hand side's instruction stream together (0: off; at most 1e7;
                                results are unchanged either way), 1000000 */
+  int arkode_barrier_us;    /* ReactorArkode: longest wait of a block at the grid barrier of its one cooperative
+                               launch, in microseconds (0..60000000; 0: a block that would have to wait gives up
+                               at once); a wait that runs out ends the call with PPB_E_CUDA and the message
+                               "grid barrier timed out" instead of hanging, 20000000 */
 } ppb_options;
 
 #define PPB_EOS_IDEAL 0 /* ideal gas: the mechanism's NASA-7 thermo (Source/Eos/Fuego.H) */
@@ -169,9 +173,31 @@ int ppb_react_box(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 r
                   ppb_array4 rEner, ppb_array4 rEner_src, ppb_array4 FC, ppb_array4i mask, double* dt_react,
                   double* time, void* stream);
 
+/* ReactorBase::flatten (ReactorBase.H:56-67; FlattenOps::flatten and
+ * box_flatten of ReactorUtils.H:160-220, 302-324) on DEVICE arrays: the box's
+ * cells (i fastest) into component-major vectors -- the reference GPU build's
+ * CYOrder (ReactorCvode.H:65): y_vect[n*ncells + c] for n <= N (T from the
+ * energy with the stored T as the Newton start, in slot N), src_vect[n*ncells
+ * + c], vect_energy[c], src_vect_energy[c], ncells the box's cell count --
+ * with the reactor's reactor type and clean_init_massfrac.  Stream-ordered. */
+int ppb_flatten(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 rhoY, ppb_array4 frcExt,
+                ppb_array4 temperature, ppb_array4 rhoE, ppb_array4 frcEExt, double* y_vect, double* src_vect,
+                double* vect_energy, double* src_vect_energy, void* stream);
+/* ReactorBase::unflatten (ReactorBase.H:69-80; box_unflatten of
+ * ReactorUtils.H:222-291) on DEVICE arrays: rhoY from y_vect (with
+ * clean_init_massfrac the clipped increment is added to the old rhoY),
+ * rhoE = vect_energy + dt * frcEExt, T from the new energy, FC = FCunt[c]. */
+int ppb_unflatten(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 rhoY, ppb_array4 temperature,
+                  ppb_array4 rhoE, ppb_array4 frcEExt, ppb_array4 FC, const double* y_vect,
+                  const double* vect_energy, const long* FCunt, double dt, void* stream);
+
 /* Per-cell integrator flag (0 ok, 1 skipped by mask, <0 CVODE-style failure
  * code) and cost (RHS evaluations or RK steps) of the last react call. */
 int ppb_get_cell_status(ppb_reactor* r, int* status, int* cost, int ncells);
+
+/* Cell count of the calling thread's last react call on r (0 before one;
+ * negative PPB_E_ARG for a null reactor). */
+int ppb_last_ncells(ppb_reactor* r);
 
 /* Per-cell integrator counters of the last react call, 7 ints per cell:
  * steps, RHS evaluations, Jacobian evaluations, matrix factorisations,
@@ -246,7 +272,16 @@ int ppb_transport_box(const char* mechanism, int use_soret, const int lo[3], con
  * on a device shares the array and keeps the last call's contents; calls
  * that overlap on the GPU race and must not be issued.  integrator is
  * "ReactorCvode" or "ReactorRK64"; opt may be NULL (reference defaults); the
- * arrays are as in ppb_react_flat and rX += dt_react * rX_src.  When nfailed
+ * arrays are as in ppb_react_flat and rX += dt_react * rX_src.  Options:
+ * the integrator keys, lu_fp32 / refine_sweeps, eos (SRK as ppb_init allows
+ * it), rendezvous_cycles and a fixed launch (warps_per_block, team_lanes,
+ * register_budget; warps_per_block = 0 takes the largest block of <= 8 warps
+ * of one warp per cell, as there is no autotuner here) are honoured; a value
+ * this path cannot honour returns PPB_E_ARG.  use_graph and cost_order only
+ * schedule work and leave results unchanged; they are not used (no graph,
+ * cells in index order).  There are no typical values (ppb_set_typ_vals
+ * belongs to a reactor handle).  The results are bitwise those of
+ * ppb_react_flat_device with the same launch and cost_order = 0.  When nfailed
  * is not NULL the call waits for the stream and stores the number of cells
  * that failed (returning PPB_E_INTEGRATE if any); with nfailed == NULL it
  * returns once the work is queued. */

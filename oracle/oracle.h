@@ -147,6 +147,14 @@ int ppo_react_flat_tables(
   const PPBMechTables* M, int reactor_type, const PPOOptions* opt, int method,
   double* rY, const double* rYsrc, double* rX, const double* rX_src, double dt,
   int ncells, int nthreads, long* nfe_out, int* status_out);
+// Same as ppo_react_flat with the per-cell counters, 7 longs per cell: steps,
+// RHS evaluations, Jacobian evaluations, factorisations of I - gamma J,
+// Newton iterations, error-test failures, convergence failures (RK64: steps,
+// 6 * steps, zeros).
+int ppo_react_flat_stats(
+  const char* mech, int reactor_type, const PPOOptions* opt, int method,
+  double* rY, const double* rYsrc, double* rX, const double* rX_src, double dt,
+  int ncells, int nthreads, int* status_out, long* stats_out);
 
 // A copy of `name`'s tables with the forward Arrhenius parameters replaced
 // (A in the tables' SI units, beta, Ea/R in K; arrays of R).  Free with

@@ -109,6 +109,8 @@ def lib():
                                      _DP, _DP, C.c_double, C.c_int, C.c_int, _LP, _IP]
         L.ppo_react_flat_tables.argtypes = [C.c_void_p, C.c_int, C.POINTER(Options), C.c_int, _DP, _DP,
                                             _DP, _DP, C.c_double, C.c_int, C.c_int, _LP, _IP]
+        L.ppo_react_flat_stats.argtypes = [C.c_char_p, C.c_int, C.POINTER(Options), C.c_int, _DP, _DP,
+                                           _DP, _DP, C.c_double, C.c_int, C.c_int, _IP, _LP]
         L.ppo_mech_with_arrhenius.argtypes = [C.c_char_p, _DP, _DP, _DP]
         L.ppo_mech_with_arrhenius.restype = C.c_void_p
         L.ppo_mech_free.argtypes = [C.c_void_p]
@@ -118,6 +120,21 @@ def lib():
         L.ppo_mw.argtypes = [C.c_char_p, _DP]
         _lib = L
     return _lib
+
+
+def reference_root():
+    """The PelePhysics tree the reference kernels were built from: the
+    PPB_REFERENCE_ROOT environment variable, else the root oracle/build_ref.sh
+    recorded in _ref/reference_root; None when neither names an existing
+    tree (e.g. on a machine that only has the prebuilt libraries)."""
+    cands = [os.environ.get("PPB_REFERENCE_ROOT")]
+    rec = os.path.join(HERE, "_ref", "reference_root")
+    if os.path.exists(rec):
+        cands.append(open(rec).read().strip())
+    for c in cands:
+        if c and os.path.isdir(os.path.join(c, "Mechanisms")):
+            return c
+    return None
 
 
 def ref_path(mech):
@@ -288,6 +305,23 @@ def react_flat(mech, reactor_type, rY, rYsrc, rX, rX_src, dt, method=0, nthreads
                                 _p(rX), _p(rX_src), float(dt), ncells, nthreads,
                                 nfe.ctypes.data_as(_LP), st.ctypes.data_as(_IP))
     return flag, nfe, st
+
+
+def react_flat_stats(mech, reactor_type, rY, rYsrc, rX, rX_src, dt, method=0, nthreads=0, **kw):
+    """react_flat with the per-cell integrator counters: returns (flag,
+    status[ncells], stats[ncells, 7]) with columns steps, RHS evaluations,
+    Jacobian evaluations, factorisations, Newton iterations, error-test
+    failures, convergence failures."""
+    o = options(**kw)
+    if o.use_ref_kernels:
+        load_ref(mech)
+    ncells = rX.shape[0]
+    st = np.zeros(ncells, dtype=np.int32)
+    stats = np.zeros((ncells, 7), dtype=np.int64)
+    flag = lib().ppo_react_flat_stats(mech.encode(), reactor_type, C.byref(o), method, _p(rY), _p(rYsrc),
+                                      _p(rX), _p(rX_src), float(dt), ncells, nthreads,
+                                      st.ctypes.data_as(_IP), stats.ctypes.data_as(_LP))
+    return flag, st, stats
 
 
 class _MechHead(C.Structure):
@@ -630,3 +664,51 @@ class Srk:
             T = self.L.ppo_reactor_rhs_srk(self.mech.encode(), float(t_rel), _p(y), _p(ydot), float(rhoe),
                                            float(rhoesrc), _p(s))
         return ydot, T
+
+
+def mass_fraction_rows(rY, N):
+    """Y_k = rhoY_k / sum_j rhoY_j per YCOrder row."""
+    return rY[:, :N] / rY[:, :N].sum(1, keepdims=True)
+
+
+def compare_to_reference(mech, reactor_type, rY0, rYsrc, rX, rX_src, dt, y_test, y_ref, Y_atol=1e-8, k=8,
+                         seed=0, nthreads=0, **opts):
+    """Integration parity of y_test against the oracle's y_ref (both YCOrder,
+    integrated from rY0 over dt with the options opts).
+
+    At rtol = atol = 1e-10 the CVODE algorithm is not continuous in its
+    input on some cells: a 1-ulp change of one rhoY_k can flip an
+    accept/reject decision, and the cell then ends on another step sequence
+    whose result differs by up to the integration error (measured on the
+    drm19 64^3 field: 6.5e-8 in Y between the oracle over the reference's
+    compiled kernels and the same oracle on a 1-ulp neighbour of the input).
+    Two implementations whose rates differ in the last bit land on either
+    branch.  So a cell whose mass fractions differ by more than Y_atol is
+    also compared with the oracle integrated from k neighbours of its input,
+    each rhoY_k moved one ulp up or down (seeded signs), and its figure is
+    the distance to the nearest of those k + 1 oracle results.
+
+    Returns max relative T error, max abs Y error against y_ref, the cells
+    above Y_atol, and the max over cells of the nearest-neighbour figure."""
+    N = rY0.shape[1] - 1
+    Yt = mass_fraction_rows(y_test, N)
+    Yr = mass_fraction_rows(y_ref, N)
+    dY = np.abs(Yt - Yr).max(1)
+    dT = np.abs(y_test[:, N] - y_ref[:, N]) / np.abs(y_ref[:, N])
+    over = np.nonzero(dY > Y_atol)[0]
+    nearest = dY.copy()
+    rng = np.random.default_rng(seed)
+    if over.size:
+        reps = np.repeat(over, k)
+        yp = rY0[reps].copy()
+        sgn = rng.choice([-1.0, 1.0], size=(reps.size, N))
+        yp[:, :N] = np.nextafter(yp[:, :N], sgn * np.inf)
+        xp = rX[reps].copy()
+        flag, _, _ = react_flat(mech, reactor_type, yp, np.ascontiguousarray(rYsrc[reps]), xp,
+                                np.ascontiguousarray(rX_src[reps]), dt, nthreads=nthreads, **opts)
+        Yp = mass_fraction_rows(yp, N).reshape(over.size, k, N)
+        dn = np.abs(Yp - Yt[over][:, None, :]).max(2).min(1)
+        nearest[over] = np.minimum(dY[over], dn)
+    return {"cells": int(rY0.shape[0]), "max_rel_T": float(dT.max()), "max_abs_Y": float(dY.max()),
+            "cells_over_Y_atol": int(over.size), "Y_atol": Y_atol,
+            "max_abs_Y_nearest_of_1ulp_neighbours": float(nearest.max()), "neighbours_per_cell": k}

@@ -953,10 +953,10 @@ void ppo_mech_free(PPBMechTables* M)
   free(M);
 }
 
-int ppo_react_flat_tables(
+static int react_flat_impl(
   const PPBMechTables* M, int reactor_type, const PPOOptions* opt, int method,
   double* rY, const double* rYsrc, double* rX, const double* rX_src, double dt,
-  int ncells, int nthreads, long* nfe_out, int* status_out)
+  int ncells, int nthreads, long* nfe_out, int* status_out, long* stats_out)
 {
   if (!M) return -100;
   const int N = M->nsp;
@@ -973,6 +973,16 @@ int ppo_react_flat_tables(
       const int f = ppo_bdf_cell(M, reactor_type, opt, y, src, rX[c], rX_src[c], dt, &st);
       if (nfe_out) nfe_out[c] = st.nfe;
       if (status_out) status_out[c] = f;
+      if (stats_out) {
+        long* o = stats_out + (long)c * 7;
+        o[0] = st.nsteps;
+        o[1] = st.nfe;
+        o[2] = st.nje;
+        o[3] = st.nsetups;
+        o[4] = st.nni;
+        o[5] = st.netf;
+        o[6] = st.ncfn;
+      }
       if (f != 0) {
 #ifdef _OPENMP
 #pragma omp critical
@@ -983,8 +993,32 @@ int ppo_react_flat_tables(
       const int ns = ppo_rk64_cell(M, reactor_type, opt, y, src, rX[c], rX_src[c], dt);
       if (nfe_out) nfe_out[c] = ns;
       if (status_out) status_out[c] = 0;
+      if (stats_out) {
+        long* o = stats_out + (long)c * 7;
+        o[0] = ns;
+        o[1] = 6L * ns;
+        for (int q = 2; q < 7; q++) o[q] = 0;
+      }
     }
     rX[c] = rX[c] + dt * rX_src[c];
   }
   return first_err;
+}
+
+int ppo_react_flat_tables(
+  const PPBMechTables* M, int reactor_type, const PPOOptions* opt, int method,
+  double* rY, const double* rYsrc, double* rX, const double* rX_src, double dt,
+  int ncells, int nthreads, long* nfe_out, int* status_out)
+{
+  return react_flat_impl(M, reactor_type, opt, method, rY, rYsrc, rX, rX_src, dt, ncells, nthreads, nfe_out,
+                         status_out, 0);
+}
+
+int ppo_react_flat_stats(
+  const char* mech, int reactor_type, const PPOOptions* opt, int method,
+  double* rY, const double* rYsrc, double* rX, const double* rX_src, double dt,
+  int ncells, int nthreads, int* status_out, long* stats_out)
+{
+  return react_flat_impl(ppo_mech(mech), reactor_type, opt, method, rY, rYsrc, rX, rX_src, dt, ncells, nthreads,
+                         0, status_out, stats_out);
 }

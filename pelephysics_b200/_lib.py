@@ -11,8 +11,7 @@ import os
 import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-# PPB_LIB selects another build of the engine (e.g. the profiling variant
-# libppb200_phase.so with per-phase cycle counters)
+# PPB_LIB selects another build of the engine library
 LIB_PATH = os.environ.get("PPB_LIB", os.path.join(HERE, "libppb200.so"))
 HEADER = os.path.join(os.path.dirname(HERE), "include", "pelephysics_b200.h")
 
@@ -52,6 +51,7 @@ class Options(C.Structure):
         ("eos", C.c_int),
         ("cost_order", C.c_int),
         ("rendezvous_cycles", C.c_int),
+        ("arkode_barrier_us", C.c_int),
     ]
 
 
@@ -116,6 +116,10 @@ def lib():
     L.ppb_t_from_energy.argtypes = [C.c_char_p, C.c_int, dp, dp, dp, C.c_int, C.c_int, vp]
     L.ppb_reactor_rhs.argtypes = [C.c_char_p, C.c_int, C.c_double, dp, dp, dp, dp, dp, C.c_int, C.c_int, vp]
     L.ppb_get_cell_stats.argtypes = [vp, ip, C.c_int]
+    L.ppb_last_ncells.argtypes = [vp]
+    L.ppb_flatten.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [Array4] * 5 + [dp, dp, dp, dp, vp]
+    L.ppb_unflatten.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)] + [Array4] * 5 + [dp, dp, dp,
+                                                                                              C.c_double, vp]
     L.ppb_probe_fp64_peak.argtypes = [dpp, vp]
     L.ppb_react_flat_device_noalloc.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(Options), dp, dp, dp, dp,
                                                 C.c_double, C.c_int, vp, ip]

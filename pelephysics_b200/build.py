@@ -1,7 +1,8 @@
 """Build the engine's shared library for sm_100a: pelephysics_b200/libppb200.so.
 
 The kernels are compiled once per species count of the shipped mechanisms
-(ppb_engine_ns.cu with -DPPB_NS=<N>), in parallel, then linked with the
+(ppb_engine_ns.cu with -DPPB_NS=<N>, in four kernel groups -DPPB_PART=0..3),
+in parallel, then linked with the
 common kernels and the C-ABI layer.  Objects are rebuilt only when a source
 or header is newer.  Usage: ``python -m pelephysics_b200.build [-j N]``.
 """
@@ -18,9 +19,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libppb200.so")
-# profiling variant: per-phase cycle counters in the BDF kernels
-PHASE_OBJ = os.path.join(HERE, "_build_phase")
-PHASE_LIB = os.path.join(HERE, "libppb200_phase.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 SPECIES_COUNTS = (9, 21, 53, 88)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -41,7 +39,8 @@ def _units():
         ("ppb_transport.o", "ppb_transport.cu", []),
     ]
     for ns in SPECIES_COUNTS:
-        units.append((f"ppb_engine_ns{ns}.o", "ppb_engine_ns.cu", [f"-DPPB_NS={ns}"]))
+        for part in range(4):  # the kernel groups of one species count, compiled in parallel
+            units.append((f"ppb_engine_ns{ns}_p{part}.o", "ppb_engine_ns.cu", [f"-DPPB_NS={ns}", f"-DPPB_PART={part}"]))
     for ns in SPECIES_COUNTS:
         units.append((f"ppb_adjoint_ns{ns}.o", "ppb_adjoint_ns.cu", [f"-DPPB_NS={ns}"]))
     for ns in SPECIES_COUNTS:
@@ -70,12 +69,14 @@ def _compile(unit, extra_flags, objdir=OBJ):
     return obj
 
 
-def build(jobs: int | None = None, verbose: bool = False, extra_flags=(), phase_timers: bool = False) -> str:
+def build(jobs: int | None = None, verbose: bool = False, extra_flags=()) -> str:
     """Compile (incrementally) and link the engine; returns the library path."""
-    objdir, lib = (PHASE_OBJ, PHASE_LIB) if phase_timers else (OBJ, LIB)
-    flags = list(extra_flags) + (["-DPPB_PHASE_TIMERS"] if phase_timers else [])
+    objdir, lib = OBJ, LIB
+    flags = list(extra_flags)
     os.makedirs(objdir, exist_ok=True)
     units = _units()
+    # the per-species kernel groups are the long poles: start them first
+    units.sort(key=lambda u: 0 if "_ns" in u[0] and "engine" in u[0] else 1)
     jobs = jobs or min(len(units), os.cpu_count() or 4)
     with ThreadPoolExecutor(max_workers=jobs) as ex:
         done = list(ex.map(lambda u: _compile(u, flags, objdir), units))
@@ -96,7 +97,7 @@ if __name__ == "__main__":
     if "-j" in sys.argv:
         j = int(sys.argv[sys.argv.index("-j") + 1])
     try:
-        build(j, verbose=True, phase_timers="--phase-timers" in sys.argv)
+        build(j, verbose=True)
     except RuntimeError as e:
         print(e, file=sys.stderr)
         sys.exit(1)

@@ -3,15 +3,24 @@
 // A ppb_reactor plays the role of the reference's ReactorCvode / ReactorRK64
 // object (Source/Reactions/ReactorCvode.{H,cpp}, ReactorRK64.{H,cpp}): it is
 // created by name, initialised once, and then advances batches of cells.
-// Device scratch is owned by the reactor and grown on demand; the device
-// paths can be replayed as a captured CUDA graph.
+// The reference's driver calls one reactor's react() from several OpenMP
+// threads at once (Testing/Exec/ReactEval/main.cpp:478-520), and
+// ReactorCvode survives that because it creates its CVODE memory per call
+// (ReactorCvode.cpp:1307).  Here every host thread that calls a reactor gets
+// its own call context -- device scratch grown on demand, the cost order of
+// its previous call, its captured CUDA graph, its per-cell flags -- so calls
+// from different threads never share mutable state.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pelephysics_b200.h"
@@ -77,25 +86,18 @@ struct GraphKey {
   int ncells, ld;
   double dt;
   cudaStream_t st;
+  unsigned gen, tune_gen; // reactor and autotuner generations at capture
   bool operator==(const GraphKey& o) const
   {
-    return memcmp(p, o.p, sizeof(p)) == 0 && ncells == o.ncells && ld == o.ld && dt == o.dt && st == o.st;
+    return memcmp(p, o.p, sizeof(p)) == 0 && ncells == o.ncells && ld == o.ld && dt == o.dt && st == o.st &&
+           gen == o.gen && tune_gen == o.tune_gen;
   }
 };
 
-struct ppb_reactor {
-  std::string mech;
-  int method = METHOD_BDF;
-  const PPBMechTables* t = nullptr;
-  DeviceMechanism* dm = nullptr;
-  int reactor_type = 0;
-  bool inited = false;
-  ppb_options opt{};
-  std::vector<double> typ_vals;
-  // device scratch
+// Per-thread call context of a reactor: everything a react() call writes.
+struct CallCtx {
   size_t cap = 0;
   double *aos = nullptr, *aos_src = nullptr, *soa = nullptr, *soa_src = nullptr, *rhoe = nullptr, *rhoesrc = nullptr;
-  double* atolv = nullptr;
   int *status = nullptr, *nfe = nullptr, *queue = nullptr, *mask = nullptr, *stats = nullptr;
   int last_ncells = 0;
   // work-queue order by the previous call's per-cell cost
@@ -116,6 +118,27 @@ struct ppb_reactor {
   cudaGraphExec_t gexec = nullptr;
   GraphKey gkey{};
   cudaStream_t cap_stream = nullptr;
+};
+
+struct ppb_reactor {
+  std::string mech;
+  int method = METHOD_BDF;
+  const PPBMechTables* t = nullptr;
+  DeviceMechanism* dm = nullptr;
+  int reactor_type = 0;
+  bool inited = false;
+  ppb_options opt{};
+  std::vector<double> typ_vals;
+  double* atolv = nullptr;
+  // bumped whenever something a captured graph holds changes (typical
+  // values, Arrhenius tables, options): graphs of older generations are
+  // captured again
+  std::atomic<unsigned> gen{0};
+  // call contexts by host thread
+  std::mutex ctx_mu;
+  std::map<std::thread::id, std::unique_ptr<CallCtx>> ctxs;
+  // the adjoint and tangent calls share the adjoint scratch: one at a time
+  std::mutex adj_mu;
   // reactor-private mechanism tables (ppb_set_arrhenius)
   PPBMechTables own_t{};
   std::vector<double> own_A, own_beta, own_EaR;
@@ -129,6 +152,19 @@ struct ppb_reactor {
   size_t adj_yinfo_bytes = 0, adj_cpidx_bytes = 0, adj_ints_bytes = 0, adj_dbl_bytes = 0, adj_lam_bytes = 0,
          adj_items_bytes = 0, adj_ioff_bytes = 0;
 };
+
+// The calling thread's context of reactor r (created on first use).
+static CallCtx* ctx_of(ppb_reactor* r)
+{
+  std::lock_guard<std::mutex> lk(r->ctx_mu);
+  std::unique_ptr<CallCtx>& c = r->ctxs[std::this_thread::get_id()];
+  if (!c) c.reset(new CallCtx());
+  return c.get();
+}
+
+// Generation of the autotuner's picks: a pick that changes makes every
+// reactor capture its graphs again.
+static std::atomic<unsigned> g_tune_gen{0};
 
 static void free_adjoint_scratch(ppb_reactor* r)
 {
@@ -158,83 +194,87 @@ static int grow(void*& p, size_t& cap, size_t bytes)
   return 0;
 }
 
-static void free_scratch(ppb_reactor* r)
+static void free_scratch(CallCtx* c)
 {
-  cudaFree(r->aos);
-  cudaFree(r->aos_src);
-  cudaFree(r->soa);
-  cudaFree(r->soa_src);
-  cudaFree(r->rhoe);
-  cudaFree(r->rhoesrc);
-  cudaFree(r->status);
-  cudaFree(r->nfe);
-  cudaFree(r->queue);
-  cudaFree(r->mask);
-  cudaFree(r->stats);
-  r->stats = nullptr;
-  cudaFree(r->order);
-  cudaFree(r->order_keys);
-  cudaFree(r->iota);
-  cudaFree(r->sort_tmp);
-  r->order = r->order_keys = r->iota = nullptr;
-  r->sort_tmp = nullptr;
-  r->sort_tmp_bytes = 0;
-  r->aos = r->aos_src = r->soa = r->soa_src = r->rhoe = r->rhoesrc = nullptr;
-  r->status = r->nfe = r->queue = r->mask = nullptr;
-  r->cap = 0;
-  if (r->gexec) cudaGraphExecDestroy(r->gexec);
-  r->gexec = nullptr;
-  for (double** q : {&r->ark_y0, &r->ark_y1, &r->ark_f0, &r->ark_f1, &r->ark_s, &r->ark_partial}) {
+  cudaFree(c->aos);
+  cudaFree(c->aos_src);
+  cudaFree(c->soa);
+  cudaFree(c->soa_src);
+  cudaFree(c->rhoe);
+  cudaFree(c->rhoesrc);
+  cudaFree(c->status);
+  cudaFree(c->nfe);
+  cudaFree(c->queue);
+  cudaFree(c->mask);
+  cudaFree(c->stats);
+  c->stats = nullptr;
+  cudaFree(c->order);
+  cudaFree(c->order_keys);
+  cudaFree(c->iota);
+  cudaFree(c->sort_tmp);
+  c->order = c->order_keys = c->iota = nullptr;
+  c->sort_tmp = nullptr;
+  c->sort_tmp_bytes = 0;
+  c->aos = c->aos_src = c->soa = c->soa_src = c->rhoe = c->rhoesrc = nullptr;
+  c->status = c->nfe = c->queue = c->mask = nullptr;
+  c->cap = 0;
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  c->gexec = nullptr;
+  for (double** q : {&c->ark_y0, &c->ark_y1, &c->ark_f0, &c->ark_f1, &c->ark_s, &c->ark_partial}) {
     cudaFree(*q);
     *q = nullptr;
   }
-  cudaFree(r->ark_bar);
-  cudaFree(r->ark_info);
-  r->ark_bar = nullptr;
-  r->ark_info = nullptr;
-  r->ark_cap = 0;
+  cudaFree(c->ark_bar);
+  cudaFree(c->ark_info);
+  c->ark_bar = nullptr;
+  c->ark_info = nullptr;
+  c->ark_cap = 0;
 }
 
 // capacity of the ARKODE partial-sum buffer, in blocks (>= SMs x resident blocks)
 static const int ARK_MAX_GRID = 4096;
 
-static int ensure_scratch(ppb_reactor* r, int ncells)
+static int ensure_scratch(ppb_reactor* r, CallCtx* c, int ncells, cudaStream_t st = nullptr)
 {
-  if ((size_t)ncells <= r->cap && r->queue) return 0;
-  free_scratch(r);
-  const size_t n = r->t->nsp + 1, c = (size_t)ncells;
-  PPB_CUDA(cudaMalloc(&r->aos, n * c * 8), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->aos_src, n * c * 8), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->soa, n * c * 8), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->soa_src, n * c * 8), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->rhoe, c * 8), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->rhoesrc, c * 8), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->status, c * 4), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->nfe, c * 4), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->mask, c * 4), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->stats, c * 7 * 4), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->queue, 16), "cudaMalloc");
+  if ((size_t)ncells <= c->cap && c->queue) return 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (st && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+    return fail(PPB_E_STATE, "react inside a stream capture needs device scratch for at least this many cells: "
+                             "call ppb_init with ncells >= the batch (or react once) on this thread before capturing");
+  free_scratch(c);
+  const size_t n = r->t->nsp + 1, nc = (size_t)ncells;
+  PPB_CUDA(cudaMalloc(&c->aos, n * nc * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->aos_src, n * nc * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->soa, n * nc * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->soa_src, n * nc * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->rhoe, nc * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->rhoesrc, nc * 8), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->status, nc * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->nfe, nc * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->mask, nc * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->stats, nc * 7 * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->queue, 16), "cudaMalloc");
   // no costs yet: zeros keep the first call in index order (stable sort)
-  PPB_CUDA(cudaMemset(r->nfe, 0, c * 4), "cudaMemset");
-  PPB_CUDA(cudaMalloc(&r->order, c * 4), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->order_keys, c * 4), "cudaMalloc");
-  PPB_CUDA(cudaMalloc(&r->iota, c * 4), "cudaMalloc");
-  PPB_CUDA(launch_iota(r->iota, (int)c, nullptr), "iota");
-  r->sort_tmp_bytes = cost_order_tmp_bytes((int)c);
-  PPB_CUDA(cudaMalloc(&r->sort_tmp, r->sort_tmp_bytes > 0 ? r->sort_tmp_bytes : 16), "cudaMalloc");
+  PPB_CUDA(cudaMemset(c->nfe, 0, nc * 4), "cudaMemset");
+  PPB_CUDA(cudaMalloc(&c->order, nc * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->order_keys, nc * 4), "cudaMalloc");
+  PPB_CUDA(cudaMalloc(&c->iota, nc * 4), "cudaMalloc");
+  PPB_CUDA(launch_iota(c->iota, (int)nc, nullptr), "iota");
+  c->sort_tmp_bytes = cost_order_tmp_bytes((int)nc);
+  PPB_CUDA(cudaMalloc(&c->sort_tmp, c->sort_tmp_bytes > 0 ? c->sort_tmp_bytes : 16), "cudaMalloc");
   PPB_CUDA(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
-  r->cap = c;
+  c->cap = nc;
   if (r->method == METHOD_ARK) {
     const size_t N = r->t->nsp;
-    PPB_CUDA(cudaMalloc(&r->ark_y0, n * c * 8), "cudaMalloc");
-    PPB_CUDA(cudaMalloc(&r->ark_y1, n * c * 8), "cudaMalloc");
-    PPB_CUDA(cudaMalloc(&r->ark_f0, n * c * 8), "cudaMalloc");
-    PPB_CUDA(cudaMalloc(&r->ark_f1, n * c * 8), "cudaMalloc");
-    PPB_CUDA(cudaMalloc(&r->ark_s, N * c * 8), "cudaMalloc");
-    PPB_CUDA(cudaMalloc(&r->ark_partial, 2 * ARK_MAX_GRID * 8), "cudaMalloc");
-    PPB_CUDA(cudaMalloc(&r->ark_bar, 16), "cudaMalloc");
-    PPB_CUDA(cudaMalloc(&r->ark_info, sizeof(ArkInfo)), "cudaMalloc");
-    r->ark_cap = c;
+    PPB_CUDA(cudaMalloc(&c->ark_y0, n * nc * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&c->ark_y1, n * nc * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&c->ark_f0, n * nc * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&c->ark_f1, n * nc * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&c->ark_s, N * nc * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&c->ark_partial, 2 * ARK_MAX_GRID * 8), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&c->ark_bar, 16), "cudaMalloc");
+    PPB_CUDA(cudaMalloc(&c->ark_info, sizeof(ArkInfo)), "cudaMalloc");
+    c->ark_cap = nc;
   }
   return 0;
 }
@@ -260,7 +300,8 @@ static bool erk_fsal(const ErkTable& t)
 // ReactorArkode over a species-major device batch: one cooperative launch.
 // box: the box path (rk_method / rk_controller apply); rhoe_out: where the
 // energies advanced by the time reached go (nullable).
-static int run_ark(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st, double* rhoe_out, bool box)
+static int run_ark(ppb_reactor* r, CallCtx* c, const Batch& b, double dt, cudaStream_t st, double* rhoe_out,
+                   bool box)
 {
   ArkParams P{};
   P.tab = erk_table(box ? r->opt.rk_method : 40);
@@ -272,6 +313,7 @@ static int run_ark(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st, d
   P.controller = (ctl >= 0 && ctl <= 3) ? ctl : 0; // unknown: PID (ReactorArkode.cpp:110-114)
   P.max_steps = r->opt.arkode_max_steps;
   P.fsal = erk_fsal(P.tab) ? 1 : 0;
+  P.barrier_ns = 1000ull * (unsigned long long)r->opt.arkode_barrier_us;
   ArkBuffers B{};
   B.ncells = b.ncells;
   B.ld = b.ld;
@@ -282,28 +324,31 @@ static int run_ark(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st, d
   B.mask = b.mask;
   B.atolv = r->atolv;
   B.rhoe_out = rhoe_out;
-  B.Y0 = r->ark_y0;
-  B.Y1 = r->ark_y1;
-  B.F0 = r->ark_f0;
-  B.F1 = r->ark_f1;
-  B.S = r->ark_s;
-  B.partial = r->ark_partial;
-  B.bar = r->ark_bar;
-  B.info = r->ark_info;
-  B.status = r->status;
-  B.nfe = r->nfe;
-  B.stats = r->stats;
-  PPB_CUDA(cudaMemsetAsync(r->ark_info, 0, sizeof(ArkInfo), st), "cudaMemsetAsync");
+  B.Y0 = c->ark_y0;
+  B.Y1 = c->ark_y1;
+  B.F0 = c->ark_f0;
+  B.F1 = c->ark_f1;
+  B.S = c->ark_s;
+  B.partial = c->ark_partial;
+  B.bar = c->ark_bar;
+  B.info = c->ark_info;
+  B.status = c->status;
+  B.nfe = c->nfe;
+  B.stats = c->stats;
+  PPB_CUDA(cudaMemsetAsync(c->ark_info, 0, sizeof(ArkInfo), st), "cudaMemsetAsync");
+  // a call that timed out can leave arrivals counted: every launch starts
+  // from a clear barrier
+  PPB_CUDA(cudaMemsetAsync(c->ark_bar, 0, 16, st), "cudaMemsetAsync");
   int grid = ARK_MAX_GRID;
   return cuda_fail(launch_ark(*r->dm, P, B, &grid, st), "launch_ark");
 }
 
 // Result of the last ReactorArkode launch (synchronises the stream).
-static int ark_result(ppb_reactor* r, cudaStream_t st)
+static int ark_result(CallCtx* c, cudaStream_t st)
 {
-  PPB_CUDA(cudaMemcpyAsync(&r->ark_last, r->ark_info, sizeof(ArkInfo), cudaMemcpyDeviceToHost, st), "D2H info");
+  PPB_CUDA(cudaMemcpyAsync(&c->ark_last, c->ark_info, sizeof(ArkInfo), cudaMemcpyDeviceToHost, st), "D2H info");
   PPB_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
-  if (r->ark_last.barrier_timeout) return fail(PPB_E_CUDA, "ReactorArkode: grid barrier timed out");
+  if (c->ark_last.barrier_timeout) return fail(PPB_E_CUDA, "ReactorArkode: grid barrier timed out");
   return 0;
 }
 
@@ -527,10 +572,7 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
   } else {
     g_tune.push_back(te);
   }
-  if (r->gexec) { // a graph captured with the earlier choice
-    cudaGraphExecDestroy(r->gexec);
-    r->gexec = nullptr;
-  }
+  g_tune_gen++; // graphs captured with the earlier choice are captured again
   return 0;
 }
 
@@ -542,12 +584,15 @@ static int maybe_autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_
     return 0;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return 0;
+  // one tuner at a time: a thread that waited finds the pick made
+  static std::mutex tuner_mu;
+  std::lock_guard<std::mutex> lk(tuner_mu);
   return autotune(r, b, dt, st);
 }
 
 // Capture body() on the reactor's private stream into r->gexec.
 template <typename F>
-static int capture(ppb_reactor* r, const GraphKey& key, F body)
+static int capture(CallCtx* r, const GraphKey& key, F body)
 {
   if (r->gexec && r->gkey == key) return 0;
   if (r->gexec) cudaGraphExecDestroy(r->gexec);
@@ -600,6 +645,7 @@ void ppb_default_options(ppb_options* o)
   o->eos = PPB_EOS_IDEAL;
   o->cost_order = 1;
   o->rendezvous_cycles = 1000000;
+  o->arkode_barrier_us = 20000000;
 }
 
 const char* ppb_last_error(void) { return g_err; }
@@ -669,9 +715,11 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
   if (r->opt.engine == PPB_ENGINE_PLAIN && r->opt.lu_fp32)
     return fail(PPB_E_ARG, "the plain engine is FP64 only");
   if (r->opt.eos != PPB_EOS_IDEAL && r->opt.eos != PPB_EOS_SRK) return fail(PPB_E_ARG, "eos must be 0 or 1");
-  if (r->opt.rendezvous_cycles < 0 || r->opt.rendezvous_cycles > 100000000)
-    return fail(PPB_E_ARG, "rendezvous_cycles must be in 0..100000000");
+  if (r->opt.rendezvous_cycles < 0 || r->opt.rendezvous_cycles > 10000000)
+    return fail(PPB_E_ARG, "rendezvous_cycles must be in 0..10000000");
   if (r->opt.warps_per_block > 16) return fail(PPB_E_ARG, "warps_per_block must be at most 16");
+  if (r->opt.arkode_barrier_us < 0 || r->opt.arkode_barrier_us > 60000000)
+    return fail(PPB_E_ARG, "arkode_barrier_us must be in 0..60000000");
   if (r->opt.eos == PPB_EOS_SRK) {
     // SRK::RHY2T is not supported (Source/Eos/SRK.H:499-507), nor an
     // analytical Jacobian; this engine runs it on the tuned FP64 BDF
@@ -689,9 +737,10 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
     if (e) return e;
   }
   if (ncells > 0) {
-    e = ensure_scratch(r, ncells);
+    e = ensure_scratch(r, ctx_of(r), ncells);
     if (e) return e;
   }
+  r->gen++;
   r->inited = true;
   return 0;
 }
@@ -705,19 +754,21 @@ int ppb_set_typ_vals(ppb_reactor* r, const double* typ_vals, int n)
   std::vector<double> at(n);
   for (int i = 0; i < n; i++) at[i] = typ_vals[i] * r->opt.atol;
   PPB_CUDA(cudaMemcpy(r->atolv, at.data(), n * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
-  if (r->gexec) {
-    cudaGraphExecDestroy(r->gexec);
-    r->gexec = nullptr;
-  }
+  r->gen++;
   return 0;
 }
 
 int ppb_close(ppb_reactor* r)
 {
   if (!r) return fail(PPB_E_ARG, "ppb_close: null reactor");
-  free_scratch(r);
-  if (r->cap_stream) cudaStreamDestroy(r->cap_stream);
-  r->cap_stream = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(r->ctx_mu);
+    for (auto& kv : r->ctxs) {
+      free_scratch(kv.second.get());
+      if (kv.second->cap_stream) cudaStreamDestroy(kv.second->cap_stream);
+    }
+    r->ctxs.clear();
+  }
   cudaFree(r->atolv);
   r->atolv = nullptr;
   free_adjoint_scratch(r);
@@ -737,47 +788,58 @@ void ppb_destroy(ppb_reactor* r)
 }
 
 // Integrate a species-major batch already on the device (the core call).
-static int run_batch(ppb_reactor* r, Batch b, double dt, cudaStream_t st, double* rhoe_out = nullptr,
+static int run_batch(ppb_reactor* r, CallCtx* c, Batch b, double dt, cudaStream_t st, double* rhoe_out = nullptr,
                      bool box = false)
 {
   b.atolv = r->atolv;
-  b.status = r->status;
-  b.nfe = r->nfe;
-  b.stats = r->stats;
-  if (r->method == METHOD_ARK) return run_ark(r, b, dt, st, rhoe_out, box);
+  b.status = c->status;
+  b.nfe = c->nfe;
+  b.stats = c->stats;
+  if (r->method == METHOD_ARK) return run_ark(r, c, b, dt, st, rhoe_out, box);
   int te = maybe_autotune(r, b, dt, st);
   if (te) return te;
   const Options o = engine_options(r);
   const LaunchConfig lc = launch_config(r);
   if (r->opt.cost_order && lc.engine == ENGINE_TUNED && lc.persistent && b.ncells > 1) {
-    // longest first: the previous call's per-cell cost (r->nfe) sorted
-    // descending; the kernel then overwrites r->nfe with this call's costs
-    int e = launch_cost_order(r->nfe, r->order_keys, r->iota, r->order, r->sort_tmp, r->sort_tmp_bytes, b.ncells,
+    // longest first: the previous call's per-cell cost (c->nfe) sorted
+    // descending; the kernel then overwrites c->nfe with this call's costs
+    int e = launch_cost_order(c->nfe, c->order_keys, c->iota, c->order, c->sort_tmp, c->sort_tmp_bytes, b.ncells,
                               st);
     if (e) return cuda_fail(e, "cost order");
-    b.order = r->order;
+    b.order = c->order;
   }
-  int e = launch_react(*r->dm, o, r->method, lc, b, dt, r->queue, st);
+  int e = launch_react(*r->dm, o, r->method, lc, b, dt, c->queue, st);
   return cuda_fail(e, "launch_react");
 }
 
-static int finish(ppb_reactor* r, int ncells, cudaStream_t st, long* cost)
+// True when the caller's stream is being captured into a CUDA graph.
+static bool capturing(cudaStream_t st)
 {
-  r->last_ncells = ncells;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+static int finish(ppb_reactor* r, CallCtx* c, int ncells, cudaStream_t st, long* cost)
+{
+  c->last_ncells = ncells;
+  if (capturing(st)) { // stream-ordered only: flags and costs stay on the device
+    if (cost) *cost = 0;
+    return 0;
+  }
   std::vector<int> stat(ncells), nfe(ncells);
-  PPB_CUDA(cudaMemcpyAsync(stat.data(), r->status, ncells * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
-  PPB_CUDA(cudaMemcpyAsync(nfe.data(), r->nfe, ncells * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  PPB_CUDA(cudaMemcpyAsync(stat.data(), c->status, ncells * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+  PPB_CUDA(cudaMemcpyAsync(nfe.data(), c->nfe, ncells * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
   PPB_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   long tot = 0;
   int bad = 0;
-  for (int c = 0; c < ncells; c++) {
-    tot += nfe[c];
-    if (stat[c] < 0) bad++;
+  for (int i = 0; i < ncells; i++) {
+    tot += nfe[i];
+    if (stat[i] < 0) bad++;
   }
   if (r->method == METHOD_ARK) {
-    int ae = ark_result(r, st);
+    int ae = ark_result(c, st);
     if (ae) return ae;
-    tot = r->ark_last.nfe; // one integrator for the batch: its RHS evaluations
+    tot = c->ark_last.nfe; // one integrator for the batch: its RHS evaluations
   }
   if (cost) *cost = (r->method == METHOD_RK64) ? (ncells ? tot / ncells : 0) : tot;
   if (bad) return fail(PPB_E_INTEGRATE, std::to_string(bad) + " cell(s) failed to integrate");
@@ -796,29 +858,31 @@ int ppb_react_flat(ppb_reactor* r, double* rY, double* rYsrc, double* rX, double
     return 0;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  int e = ensure_scratch(r, ncells);
+  if (capturing(st)) return fail(PPB_E_STATE, "ppb_react_flat copies host arrays and waits: not inside a stream capture");
+  CallCtx* c = ctx_of(r);
+  int e = ensure_scratch(r, c, ncells, st);
   if (e) return e;
   const int N = r->t->nsp, n = N + 1;
-  PPB_CUDA(cudaMemcpyAsync(r->aos, rY, (size_t)ncells * n * 8, cudaMemcpyHostToDevice, st), "H2D rY");
-  PPB_CUDA(cudaMemcpyAsync(r->aos_src, rYsrc, (size_t)ncells * N * 8, cudaMemcpyHostToDevice, st), "H2D rYsrc");
-  PPB_CUDA(cudaMemcpyAsync(r->rhoe, rX, (size_t)ncells * 8, cudaMemcpyHostToDevice, st), "H2D rX");
-  PPB_CUDA(cudaMemcpyAsync(r->rhoesrc, rX_src, (size_t)ncells * 8, cudaMemcpyHostToDevice, st), "H2D rX_src");
-  PPB_CUDA(launch_aos_to_soa(r->aos, n, r->soa, ncells, n, ncells, st), "aos_to_soa");
-  PPB_CUDA(launch_aos_to_soa(r->aos_src, N, r->soa_src, ncells, N, ncells, st), "aos_to_soa");
+  PPB_CUDA(cudaMemcpyAsync(c->aos, rY, (size_t)ncells * n * 8, cudaMemcpyHostToDevice, st), "H2D rY");
+  PPB_CUDA(cudaMemcpyAsync(c->aos_src, rYsrc, (size_t)ncells * N * 8, cudaMemcpyHostToDevice, st), "H2D rYsrc");
+  PPB_CUDA(cudaMemcpyAsync(c->rhoe, rX, (size_t)ncells * 8, cudaMemcpyHostToDevice, st), "H2D rX");
+  PPB_CUDA(cudaMemcpyAsync(c->rhoesrc, rX_src, (size_t)ncells * 8, cudaMemcpyHostToDevice, st), "H2D rX_src");
+  PPB_CUDA(launch_aos_to_soa(c->aos, n, c->soa, ncells, n, ncells, st), "aos_to_soa");
+  PPB_CUDA(launch_aos_to_soa(c->aos_src, N, c->soa_src, ncells, N, ncells, st), "aos_to_soa");
   Batch b{};
-  b.y = r->soa;
-  b.src = r->soa_src;
-  b.rhoe = r->rhoe;
-  b.rhoesrc = r->rhoesrc;
+  b.y = c->soa;
+  b.src = c->soa_src;
+  b.rhoe = c->rhoe;
+  b.rhoesrc = c->rhoesrc;
   b.mask = nullptr;
   b.ncells = ncells;
   b.ld = ncells;
-  e = run_batch(r, b, *dt_react, st);
+  e = run_batch(r, c, b, *dt_react, st);
   if (e) return e;
-  PPB_CUDA(launch_soa_to_aos(r->soa, ncells, n, r->aos, n, ncells, st), "soa_to_aos");
-  PPB_CUDA(cudaMemcpyAsync(rY, r->aos, (size_t)ncells * n * 8, cudaMemcpyDeviceToHost, st), "D2H rY");
-  e = finish(r, ncells, st, cost);
-  if (r->method == METHOD_ARK) *dt_react = r->ark_last.t; // the interval integrated
+  PPB_CUDA(launch_soa_to_aos(c->soa, ncells, n, c->aos, n, ncells, st), "soa_to_aos");
+  PPB_CUDA(cudaMemcpyAsync(rY, c->aos, (size_t)ncells * n * 8, cudaMemcpyDeviceToHost, st), "D2H rY");
+  e = finish(r, c, ncells, st, cost);
+  if (r->method == METHOD_ARK) *dt_react = c->ark_last.t; // the interval integrated
   // ReactorCvode.cpp:1652-1655: rX += dt * rX_src on the host arrays
   for (int i = 0; i < ncells; i++) rX[i] = rX[i] + *dt_react * rX_src[i];
   *time += *dt_react;
@@ -838,37 +902,41 @@ int ppb_react_flat_device(ppb_reactor* r, double* rY, double* rYsrc, double* rX,
     return 0;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  int e = ensure_scratch(r, ncells);
+  const bool cap = capturing(st);
+  if (cap && r->method == METHOD_ARK)
+    return fail(PPB_E_STATE, "ReactorArkode reads its batch result on the host: not inside a stream capture");
+  CallCtx* c = ctx_of(r);
+  int e = ensure_scratch(r, c, ncells, st);
   if (e) return e;
   const int N = r->t->nsp, n = N + 1;
   const double dt = *dt_react;
-  GraphKey key{{rY, rYsrc, rX, rX_src, nullptr, nullptr}, ncells, ncells, dt, st};
+  GraphKey key{{rY, rYsrc, rX, rX_src, nullptr, nullptr}, ncells, ncells, dt, st, r->gen.load(), g_tune_gen.load()};
   auto body = [&](cudaStream_t s) -> int {
-    int ee = launch_aos_to_soa(rY, n, r->soa, ncells, n, ncells, s);
-    if (!ee) ee = launch_aos_to_soa(rYsrc, N, r->soa_src, ncells, N, ncells, s);
+    int ee = launch_aos_to_soa(rY, n, c->soa, ncells, n, ncells, s);
+    if (!ee) ee = launch_aos_to_soa(rYsrc, N, c->soa_src, ncells, N, ncells, s);
     if (ee) return cuda_fail(ee, "aos_to_soa");
     Batch b{};
-    b.y = r->soa;
-    b.src = r->soa_src;
+    b.y = c->soa;
+    b.src = c->soa_src;
     b.rhoe = rX;
     b.rhoesrc = rX_src;
     b.ncells = ncells;
     b.ld = ncells;
-    ee = run_batch(r, b, dt, s, rX);
+    ee = run_batch(r, c, b, dt, s, rX);
     if (ee) return ee;
-    ee = launch_soa_to_aos(r->soa, ncells, n, rY, n, ncells, s);
+    ee = launch_soa_to_aos(c->soa, ncells, n, rY, n, ncells, s);
     if (!ee && r->method != METHOD_ARK) ee = launch_energy_update(rX, rX_src, dt, ncells, s);
     if (ee) return cuda_fail(ee, "soa_to_aos");
     return 0;
   };
-  if (r->opt.use_graph && r->method != METHOD_ARK) {
-    if (!r->gexec || !(r->gkey == key)) {
+  if (r->opt.use_graph && r->method != METHOD_ARK && !cap) {
+    if (!c->gexec || !(c->gkey == key)) {
       // tune outside the capture, on the batch converted to species-major
-      PPB_CUDA(launch_aos_to_soa(rY, n, r->soa, ncells, n, ncells, st), "aos_to_soa");
-      PPB_CUDA(launch_aos_to_soa(rYsrc, N, r->soa_src, ncells, N, ncells, st), "aos_to_soa");
+      PPB_CUDA(launch_aos_to_soa(rY, n, c->soa, ncells, n, ncells, st), "aos_to_soa");
+      PPB_CUDA(launch_aos_to_soa(rYsrc, N, c->soa_src, ncells, N, ncells, st), "aos_to_soa");
       Batch tb{};
-      tb.y = r->soa;
-      tb.src = r->soa_src;
+      tb.y = c->soa;
+      tb.src = c->soa_src;
       tb.rhoe = rX;
       tb.rhoesrc = rX_src;
       tb.ncells = ncells;
@@ -876,15 +944,15 @@ int ppb_react_flat_device(ppb_reactor* r, double* rY, double* rYsrc, double* rX,
       e = maybe_autotune(r, tb, dt, st);
       if (e) return e;
     }
-    e = capture(r, key, body);
+    e = capture(c, key, body);
     if (e) return e;
-    PPB_CUDA(cudaGraphLaunch(r->gexec, st), "cudaGraphLaunch");
+    PPB_CUDA(cudaGraphLaunch(c->gexec, st), "cudaGraphLaunch");
   } else {
     e = body(st);
     if (e) return e;
   }
-  e = finish(r, ncells, st, cost);
-  if (r->method == METHOD_ARK) *dt_react = r->ark_last.t;
+  e = finish(r, c, ncells, st, cost);
+  if (r->method == METHOD_ARK) *dt_react = c->ark_last.t;
   *time += *dt_react;
   return e;
 }
@@ -901,10 +969,14 @@ int ppb_react_soa_device(ppb_reactor* r, double* y, const double* src, double* r
     return 0;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  int e = ensure_scratch(r, ncells);
+  const bool cap = capturing(st);
+  if (cap && r->method == METHOD_ARK)
+    return fail(PPB_E_STATE, "ReactorArkode reads its batch result on the host: not inside a stream capture");
+  CallCtx* c = ctx_of(r);
+  int e = ensure_scratch(r, c, ncells, st);
   if (e) return e;
   const double dt = *dt_react;
-  GraphKey key{{y, src, rX, rX_src, (void*)1, nullptr}, ncells, ld, dt, st};
+  GraphKey key{{y, src, rX, rX_src, (void*)1, nullptr}, ncells, ld, dt, st, r->gen.load(), g_tune_gen.load()};
   Batch b{};
   b.y = y;
   b.src = const_cast<double*>(src);
@@ -913,25 +985,25 @@ int ppb_react_soa_device(ppb_reactor* r, double* y, const double* src, double* r
   b.ncells = ncells;
   b.ld = ld;
   auto body = [&](cudaStream_t s) -> int {
-    int ee = run_batch(r, b, dt, s, rX);
+    int ee = run_batch(r, c, b, dt, s, rX);
     if (!ee && r->method != METHOD_ARK)
       ee = cuda_fail(launch_energy_update(rX, rX_src, dt, ncells, s), "energy_update");
     return ee;
   };
-  if (r->opt.use_graph && r->method != METHOD_ARK) {
-    if (!r->gexec || !(r->gkey == key)) {
+  if (r->opt.use_graph && r->method != METHOD_ARK && !cap) {
+    if (!c->gexec || !(c->gkey == key)) {
       e = maybe_autotune(r, b, dt, st); // outside the capture
       if (e) return e;
     }
-    e = capture(r, key, body);
+    e = capture(c, key, body);
     if (e) return e;
-    PPB_CUDA(cudaGraphLaunch(r->gexec, st), "cudaGraphLaunch");
+    PPB_CUDA(cudaGraphLaunch(c->gexec, st), "cudaGraphLaunch");
   } else {
     e = body(st);
     if (e) return e;
   }
-  e = finish(r, ncells, st, cost);
-  if (r->method == METHOD_ARK) *dt_react = r->ark_last.t;
+  e = finish(r, c, ncells, st, cost);
+  if (r->method == METHOD_ARK) *dt_react = c->ark_last.t;
   *time += *dt_react;
   return e;
 }
@@ -978,7 +1050,11 @@ int ppb_react_box(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 r
   }
   const int ncells = (int)ncl;
   cudaStream_t st = (cudaStream_t)stream;
-  int e = ensure_scratch(r, ncells);
+  const bool cap = capturing(st);
+  if (cap && r->method == METHOD_ARK)
+    return fail(PPB_E_STATE, "ReactorArkode reads its batch result on the host: not inside a stream capture");
+  CallCtx* c = ctx_of(r);
+  int e = ensure_scratch(r, c, ncells, st);
   if (e) return e;
   BoxArgs a{};
   for (int d = 0; d < 3; d++) {
@@ -997,27 +1073,108 @@ int ppb_react_box(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 r
   a.mask.nstride = mask.nstride;
   for (int d = 0; d < 3; d++) a.mask.lo[d] = mask.lo[d];
   Batch b{};
-  b.y = r->soa;
-  b.src = r->soa_src;
-  b.rhoe = r->rhoe;
-  b.rhoesrc = r->rhoesrc;
-  b.mask = r->mask;
+  b.y = c->soa;
+  b.src = c->soa_src;
+  b.rhoe = c->rhoe;
+  b.rhoesrc = c->rhoesrc;
+  b.mask = c->mask;
   b.ncells = ncells;
   b.ld = ncells;
-  b.nfe = r->nfe;
+  b.nfe = c->nfe;
   PPB_CUDA(launch_box_flatten(*r->dm, r->reactor_type, r->opt.clean_init_massfrac, a, b, st), "box_flatten");
-  e = run_batch(r, b, *dt_react, st, nullptr, true);
+  e = run_batch(r, c, b, *dt_react, st, nullptr, true);
   if (e) return e;
   if (r->method == METHOD_ARK) {
-    e = ark_result(r, st);
+    e = ark_result(c, st);
     if (e) return e;
-    *dt_react = r->ark_last.t; // the interval integrated (ReactorArkode.cpp:223-226)
+    *dt_react = c->ark_last.t; // the interval integrated (ReactorArkode.cpp:223-226)
   }
   PPB_CUDA(launch_box_unflatten(*r->dm, r->reactor_type, r->opt.clean_init_massfrac, a, b, *dt_react, st),
            "box_unflatten");
-  e = finish(r, ncells, st, nullptr);
+  e = finish(r, c, ncells, st, nullptr);
   *time += *dt_react;
   return e;
+}
+
+// Box bounds and cell count of a flatten/unflatten call.
+static int box_cells(const int lo[3], const int hi[3], long* ncl)
+{
+  *ncl = 1;
+  for (int d = 0; d < 3; d++) {
+    if (hi[d] < lo[d]) return fail(PPB_E_ARG, "empty box");
+    *ncl *= (hi[d] - lo[d] + 1);
+  }
+  if (*ncl > (1L << 30)) return fail(PPB_E_ARG, "box too large");
+  return 0;
+}
+
+int ppb_flatten(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 rhoY, ppb_array4 frcExt,
+                ppb_array4 temperature, ppb_array4 rhoE, ppb_array4 frcEExt, double* y_vect, double* src_vect,
+                double* vect_energy, double* src_vect_energy, void* stream)
+{
+  if (!r || !r->inited) return fail(PPB_E_STATE, "flatten before init");
+  if (!lo || !hi || !y_vect || !src_vect || !vect_energy || !src_vect_energy)
+    return fail(PPB_E_ARG, "ppb_flatten: null argument");
+  long ncl = 0;
+  if (box_cells(lo, hi, &ncl)) return PPB_E_ARG;
+  const int N = r->t->nsp;
+  if (!covers(rhoY, lo, hi, N) || !covers(frcExt, lo, hi, N) || !covers(temperature, lo, hi, 1) ||
+      !covers(rhoE, lo, hi, 1) || !covers(frcEExt, lo, hi, 1))
+    return fail(PPB_E_ARG, "ppb_flatten: an Array4 does not cover the box");
+  BoxArgs a{};
+  for (int d = 0; d < 3; d++) {
+    a.lo[d] = lo[d];
+    a.hi[d] = hi[d];
+  }
+  a.rY = view(rhoY);
+  a.rYsrc = view(frcExt);
+  a.T = view(temperature);
+  a.rE = view(rhoE);
+  a.rEs = view(frcEExt);
+  Batch b{};
+  b.y = y_vect;
+  b.src = src_vect;
+  b.rhoe = vect_energy;
+  b.rhoesrc = src_vect_energy;
+  b.ncells = (int)ncl;
+  b.ld = (int)ncl;
+  PPB_CUDA(launch_box_flatten(*r->dm, r->reactor_type, r->opt.clean_init_massfrac, a, b, (cudaStream_t)stream),
+           "box_flatten");
+  return 0;
+}
+
+int ppb_unflatten(ppb_reactor* r, const int lo[3], const int hi[3], ppb_array4 rhoY, ppb_array4 temperature,
+                  ppb_array4 rhoE, ppb_array4 frcEExt, ppb_array4 FC, const double* y_vect,
+                  const double* vect_energy, const long* FCunt, double dt, void* stream)
+{
+  if (!r || !r->inited) return fail(PPB_E_STATE, "unflatten before init");
+  if (!lo || !hi || !y_vect || !vect_energy || !FCunt) return fail(PPB_E_ARG, "ppb_unflatten: null argument");
+  long ncl = 0;
+  if (box_cells(lo, hi, &ncl)) return PPB_E_ARG;
+  const int N = r->t->nsp;
+  if (!covers(rhoY, lo, hi, N) || !covers(temperature, lo, hi, 1) || !covers(rhoE, lo, hi, 1) ||
+      !covers(frcEExt, lo, hi, 1) || !covers(FC, lo, hi, 1))
+    return fail(PPB_E_ARG, "ppb_unflatten: an Array4 does not cover the box");
+  BoxArgs a{};
+  for (int d = 0; d < 3; d++) {
+    a.lo[d] = lo[d];
+    a.hi[d] = hi[d];
+  }
+  a.rY = view(rhoY);
+  a.T = view(temperature);
+  a.rE = view(rhoE);
+  a.rEs = view(frcEExt);
+  a.FC = view(FC);
+  a.fcunt = FCunt;
+  Batch b{};
+  b.y = const_cast<double*>(y_vect);
+  b.rhoe = vect_energy;
+  b.ncells = (int)ncl;
+  b.ld = (int)ncl;
+  PPB_CUDA(launch_box_unflatten(*r->dm, r->reactor_type, r->opt.clean_init_massfrac, a, b, dt,
+                                (cudaStream_t)stream),
+           "box_unflatten");
+  return 0;
 }
 
 // ---------------------------------------------------------------- transport
@@ -1101,16 +1258,26 @@ int ppb_transport_box(const char* mechanism, int use_soret, const int lo[3], con
 
 int ppb_get_cell_status(ppb_reactor* r, int* status, int* cost, int ncells)
 {
-  if (!r || ncells < 0 || ncells > r->last_ncells) return fail(PPB_E_ARG, "ppb_get_cell_status: bad arguments");
-  if (status) PPB_CUDA(cudaMemcpy(status, r->status, (size_t)ncells * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
-  if (cost) PPB_CUDA(cudaMemcpy(cost, r->nfe, (size_t)ncells * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  if (!r) return fail(PPB_E_ARG, "ppb_get_cell_status: null reactor");
+  CallCtx* c = ctx_of(r);
+  if (ncells < 0 || ncells > c->last_ncells) return fail(PPB_E_ARG, "ppb_get_cell_status: bad arguments");
+  if (status) PPB_CUDA(cudaMemcpy(status, c->status, (size_t)ncells * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  if (cost) PPB_CUDA(cudaMemcpy(cost, c->nfe, (size_t)ncells * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
   return 0;
+}
+
+int ppb_last_ncells(ppb_reactor* r)
+{
+  if (!r) return fail(PPB_E_ARG, "ppb_last_ncells: null reactor");
+  return ctx_of(r)->last_ncells;
 }
 
 int ppb_get_cell_stats(ppb_reactor* r, int* stats, int ncells)
 {
-  if (!r || !stats || ncells < 0 || ncells > r->last_ncells) return fail(PPB_E_ARG, "ppb_get_cell_stats: bad arguments");
-  PPB_CUDA(cudaMemcpy(stats, r->stats, (size_t)ncells * 7 * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  if (!r || !stats) return fail(PPB_E_ARG, "ppb_get_cell_stats: null argument");
+  CallCtx* c = ctx_of(r);
+  if (ncells < 0 || ncells > c->last_ncells) return fail(PPB_E_ARG, "ppb_get_cell_stats: bad arguments");
+  PPB_CUDA(cudaMemcpy(stats, c->stats, (size_t)ncells * 7 * 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
   return 0;
 }
 
@@ -1170,10 +1337,7 @@ int ppb_set_arrhenius(ppb_reactor* r, const double* A, const double* beta, const
   }
   r->own = m;
   if (r->inited) r->dm = m;
-  if (r->gexec) {
-    cudaGraphExecDestroy(r->gexec);
-    r->gexec = nullptr;
-  }
+  r->gen++;
   return 0;
 }
 
@@ -1188,7 +1352,7 @@ static int grow_items(void* ctx, void** p, size_t bytes)
 
 // The adjoint integration, batched over cells segment by segment (chunks of
 // cells within adjoint_memory_mb).
-static int run_adjoint_batched(ppb_reactor* r, AdjBatch b, double dt, double* grad, cudaStream_t st)
+static int run_adjoint_batched(ppb_reactor* r, CallCtx* cx, AdjBatch b, double dt, double* grad, cudaStream_t st)
 {
   const int N = r->t->nsp, n = N + 1, R = r->t->nrxn;
   const int seg = r->opt.adjoint_checkpoint_interval > 0 ? r->opt.adjoint_checkpoint_interval : 16;
@@ -1238,8 +1402,8 @@ static int run_adjoint_batched(ppb_reactor* r, AdjBatch b, double dt, double* gr
   C.items = (double*)r->adj_items;
   C.item_off = (int*)r->adj_ioff;
   b.atolv = r->atolv;
-  b.status = r->status;
-  b.stats = r->stats;
+  b.status = cx->status;
+  b.stats = cx->stats;
   const Options o = engine_options(r);
   for (long c0 = 0; c0 < b.ncells; c0 += cells) {
     AdjBatch bc = b;
@@ -1255,13 +1419,13 @@ static int run_adjoint_batched(ppb_reactor* r, AdjBatch b, double dt, double* gr
     bc.lam_e = b.lam_e ? b.lam_e + c0 : nullptr;
     bc.status = b.status + c0;
     bc.stats = b.stats + (size_t)c0 * 7;
-    e = launch_adjoint_batched(*r->dm, o, r->opt.lu_fp32, bc, C, dt, r->queue, grad, c0 > 0 ? 1 : 0, grow_items, r,
+    e = launch_adjoint_batched(*r->dm, o, r->opt.lu_fp32, bc, C, dt, cx->queue, grad, c0 > 0 ? 1 : 0, grow_items, r,
                                st);
     if (e) return cuda_fail(e, "launch_adjoint_batched");
   }
-  r->last_ncells = b.ncells;
+  cx->last_ncells = b.ncells;
   std::vector<int> stat(b.ncells);
-  PPB_CUDA(cudaMemcpyAsync(stat.data(), r->status, (size_t)b.ncells * 4, cudaMemcpyDeviceToHost, st),
+  PPB_CUDA(cudaMemcpyAsync(stat.data(), cx->status, (size_t)b.ncells * 4, cudaMemcpyDeviceToHost, st),
            "cudaMemcpyAsync");
   PPB_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   int bad = 0;
@@ -1285,9 +1449,12 @@ static int run_adjoint(ppb_reactor* r, int mode, AdjBatch b, double dt, double* 
     if (grad) PPB_CUDA(cudaMemsetAsync(grad, 0, sizeof(double) * 3 * r->t->nrxn, st), "cudaMemsetAsync");
     return 0;
   }
-  int e = ensure_scratch(r, b.ncells);
+  if (capturing(st)) return fail(PPB_E_STATE, "adjoint: not inside a stream capture");
+  std::lock_guard<std::mutex> lk(r->adj_mu);
+  CallCtx* cx = ctx_of(r);
+  int e = ensure_scratch(r, cx, b.ncells, st);
   if (e) return e;
-  if (mode == ADJ_REVERSE) return run_adjoint_batched(r, b, dt, grad, st);
+  if (mode == ADJ_REVERSE) return run_adjoint_batched(r, cx, b, dt, grad, st);
   const int N = r->t->nsp, n = N + 1, R = r->t->nrxn;
   AdjPlan p;
   e = plan_adjoint(*r->dm, mode, r->opt.lu_fp32, &p);
@@ -1331,8 +1498,8 @@ static int run_adjoint(ppb_reactor* r, int mode, AdjBatch b, double dt, double* 
   L.ys = (double*)r->adj_ys;
   L.gw = mode == ADJ_REVERSE ? (double*)r->adj_gw : nullptr;
   b.atolv = r->atolv;
-  b.status = r->status;
-  b.stats = r->stats;
+  b.status = cx->status;
+  b.stats = cx->stats;
   const Options o = engine_options(r);
   for (int c0 = 0; c0 < b.ncells; c0 += chunk) {
     AdjBatch bc = b;
@@ -1350,12 +1517,12 @@ static int run_adjoint(ppb_reactor* r, int mode, AdjBatch b, double dt, double* 
     bc.lam_e = b.lam_e ? b.lam_e + c0 : nullptr;
     bc.status = b.status + c0;
     bc.stats = b.stats + (size_t)c0 * 7;
-    e = launch_adjoint(*r->dm, o, mode, r->opt.lu_fp32, p, bc, L, dt, r->queue, grad, c0 > 0 ? 1 : 0, st);
+    e = launch_adjoint(*r->dm, o, mode, r->opt.lu_fp32, p, bc, L, dt, cx->queue, grad, c0 > 0 ? 1 : 0, st);
     if (e) return cuda_fail(e, "launch_adjoint");
   }
-  r->last_ncells = b.ncells;
+  cx->last_ncells = b.ncells;
   std::vector<int> stat(b.ncells);
-  PPB_CUDA(cudaMemcpyAsync(stat.data(), r->status, (size_t)b.ncells * 4, cudaMemcpyDeviceToHost, st),
+  PPB_CUDA(cudaMemcpyAsync(stat.data(), cx->status, (size_t)b.ncells * 4, cudaMemcpyDeviceToHost, st),
            "cudaMemcpyAsync");
   PPB_CUDA(cudaStreamSynchronize(st), "cudaStreamSynchronize");
   int bad = 0;

@@ -79,9 +79,9 @@ __host__ __device__ inline double ark_eta(int ctl, int ord, double h, double dsm
 
 // Bounded grid barrier for a co-resident (cooperative) grid: every block
 // arrives once per call; the last one opens the next generation.  A wait
-// gives up after ~20 s of global time and raises *timeout (the kernel then
-// returns), so a lost block can never hang the GPU.
-__device__ inline bool ark_grid_barrier(unsigned* bar, int* timeout)
+// gives up after limit_ns of global time (20 s by default) and raises
+// *timeout (the kernel then returns), so a lost block can never hang the GPU.
+__device__ inline bool ark_grid_barrier(unsigned* bar, int* timeout, unsigned long long limit_ns)
 {
   __shared__ int ok;
   __syncthreads();
@@ -101,7 +101,7 @@ __device__ inline bool ark_grid_barrier(unsigned* bar, int* timeout)
       while (*gen == g) {
         __nanosleep(256);
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-        if (t1 - t0 > 20000000000ull) {
+        if (t1 - t0 > limit_ns) {
           atomicExch(timeout, 1);
           ok = 0;
           break;

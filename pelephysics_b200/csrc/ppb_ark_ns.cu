@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(ARK_THREADS) k_ark(DevMech M, ArkParams P, Ark
       for (int i = 1; i < nwarps; i++) s = mx ? fmax(s, wred[i]) : s + wred[i];
       B.partial[par * gridDim.x + blockIdx.x] = s;
     }
-    if (!ark_grid_barrier(B.bar, tmo)) {
+    if (!ark_grid_barrier(B.bar, tmo, P.barrier_ns)) {
       broken = true;
       return 0.0;
     }

@@ -64,21 +64,34 @@ struct Work {
 // team's lane 0 counts itself in and waits (at most `cycles` SM clocks) until
 // every active team of the block has arrived, so that the block's warps run
 // the right-hand side's instruction stream together.  It changes no
-// arithmetic: a team that times out just goes on alone.  Stale or doubled
-// arrivals only release a generation early.
+// arithmetic: a team that times out just goes on alone.
+//
+// rv[0] packs the generation (high 16 bits) and the arrivals of that
+// generation (low 16 bits), so an arrival learns its generation from the same
+// atomic that counts it; rv[2] is the number of active teams.  A generation
+// is released by one compare-and-swap that bumps the generation and clears
+// the count only if no arrival landed in between, so no arrival is ever
+// erased.  A team that timed out and arrives again early counts twice: that
+// only releases a generation early.
+__device__ __forceinline__ void rendezvous_try_release(int* rv)
+{
+  volatile int* v = rv;
+  for (int i = 0; i < 64; i++) { // bounded: each failed CAS means another arrival landed
+    const int cur = v[0];
+    const int active = v[2];
+    if (active <= 0 || (cur & 0xffff) < active) return;
+    if (atomicCAS(&rv[0], cur, (int)(((unsigned)cur & 0xffff0000u) + 0x10000u)) == cur) return;
+  }
+}
+
 __device__ __forceinline__ void rendezvous(int* rv, int cycles)
 {
   if ((threadIdx.x & 31) == 0) {
     volatile int* v = rv;
-    const int g = v[1];
-    const int old = atomicAdd(&rv[0], 1);
-    if (old + 1 >= v[2]) {
-      atomicExch(&rv[0], 0);
-      atomicAdd(&rv[1], 1);
-    } else {
-      const long long t0 = clock64();
-      while (v[1] == g && clock64() - t0 < cycles) __nanosleep(32);
-    }
+    const unsigned g = (unsigned)atomicAdd(&rv[0], 1) >> 16;
+    rendezvous_try_release(rv);
+    const long long t0 = clock64();
+    while (((unsigned)v[0] >> 16) == g && clock64() - t0 < cycles) __nanosleep(32);
   }
   __syncwarp();
 }
@@ -101,11 +114,8 @@ __device__ __forceinline__ int* rendezvous_init(int* rv, int teams, int cycles)
 __device__ __forceinline__ void rendezvous_leave(int* rv)
 {
   if (rv && (threadIdx.x & 31) == 0) {
-    const int left = atomicSub(&rv[2], 1) - 1;
-    if (left > 0 && atomicAdd(&rv[0], 0) >= left) {
-      atomicExch(&rv[0], 0);
-      atomicAdd(&rv[1], 1);
-    }
+    atomicSub(&rv[2], 1);
+    rendezvous_try_release(rv);
   }
 }
 

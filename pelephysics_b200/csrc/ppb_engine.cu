@@ -829,7 +829,7 @@ __global__ void k_box_flatten(DevMech M, int rtype, int clean, BoxArgs a, Batch 
   const int i = a.lo[0] + c % lx, j = a.lo[1] + (c / lx) % ly, k = a.lo[2] + c / (lx * ly);
   const int N = M.nsp;
   int* mk = const_cast<int*>(b.mask);
-  mk[c] = a.mask.p ? a.mask.p[a4i(a.mask, i, j, k, 0)] : 1;
+  if (mk) mk[c] = a.mask.p ? a.mask.p[a4i(a.mask, i, j, k, 0)] : 1;
   double Y[96];
   double rho_old = 0.0, rho = 0.0;
   if (clean)
@@ -862,7 +862,7 @@ __global__ void k_box_unflatten(DevMech M, int rtype, int clean, BoxArgs a, Batc
   const int lx = a.hi[0] - a.lo[0] + 1, ly = a.hi[1] - a.lo[1] + 1;
   const int i = a.lo[0] + c % lx, j = a.lo[1] + (c / lx) % ly, k = a.lo[2] + c / (lx * ly);
   const int N = M.nsp;
-  if (b.mask[c] == -1) {
+  if (b.mask && b.mask[c] == -1) {
     a.FC.p[a4(a.FC, i, j, k, 0)] = 0.0;
     return;
   }
@@ -892,7 +892,7 @@ __global__ void k_box_unflatten(DevMech M, int rtype, int clean, BoxArgs a, Batc
   Team<1> tm;
   t_from_energy<1>(tm, M, rtype == 2, rE * rinv, Y, T);
   a.T.p[a4(a.T, i, j, k, 0)] = T;
-  a.FC.p[a4(a.FC, i, j, k, 0)] = (double)(b.nfe ? b.nfe[c] : 0);
+  a.FC.p[a4(a.FC, i, j, k, 0)] = a.fcunt ? (double)a.fcunt[c] : (double)(b.nfe ? b.nfe[c] : 0);
 }
 
 int launch_box_flatten(const DeviceMechanism& m, int rtype, int clean, const BoxArgs& a, Batch b, cudaStream_t st)

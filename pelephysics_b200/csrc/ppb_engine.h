@@ -95,9 +95,10 @@ struct BoxArgs {
   int lo[3], hi[3]; // box (inclusive)
   BoxView rY, rYsrc, T, rE, rEs, FC;
   BoxViewI mask;    // p == nullptr: every cell active
+  const long* fcunt = nullptr; // unflatten: per-cell cost as the reference's FCunt (else the batch's nfe)
 };
-// box_flatten / box_unflatten; the batch's mask array receives the Array4
-// mask values and must be writable device memory.
+// box_flatten / box_unflatten; the batch's mask array (when not null)
+// receives the Array4 mask values and must be writable device memory.
 int launch_box_flatten(const DeviceMechanism& m, int rtype, int clean, const BoxArgs& a, Batch b, cudaStream_t st);
 int launch_box_unflatten(const DeviceMechanism& m, int rtype, int clean, const BoxArgs& a, Batch b, double dt,
                          cudaStream_t st);
@@ -145,6 +146,7 @@ struct ArkParams {
   ErkTable tab;
   double rtol, atol, tout;
   int reactor_type, controller, max_steps, fsal;
+  unsigned long long barrier_ns; // longest wait at the grid barrier (global-timer ns)
 };
 
 // Batch result: time reached, last step, counters, flag.

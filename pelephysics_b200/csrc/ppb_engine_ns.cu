@@ -6,6 +6,9 @@
 #ifndef PPB_NS
 #error "compile with -DPPB_NS=<number of species>"
 #endif
+#ifndef PPB_PART
+#error "compile with -DPPB_PART=<0..3> (the kernel group of this object)"
+#endif
 
 namespace ppb {
 
@@ -183,25 +186,38 @@ constexpr int big_team()
 // The compiled variants: 32 lanes per cell with both register budgets for
 // the FP64 BDF kernel; 16 lanes per cell as well for mechanisms of at most
 // 21 species, and a multi-warp team (one cell per block, one lane per
-// species) for larger ones.
+// species) for larger ones.  They are compiled in four parts (PPB_PART 0..3,
+// one object each, built in parallel); each part returns the kernels it holds
+// and nullptr for the others:
+//   0: FP64 BDF, 32 lanes, 8 warps (<= 128 and <= 255 registers)
+//   1: FP64 BDF, 32 lanes, 12 and 16 warps per block (one block per SM)
+//   2: the multi-warp teams (FP64 and FP32 BDF, RK64)
+//   3: FP32 BDF and RK64 with 32 lanes, the 16-lane variants, the SRK kernel
 template <int NS>
-static TeamKernel team_kernel(int method, bool fp32, int team, int minb, int srk, int wpb)
+static TeamKernel team_kernel_part(int method, bool fp32, int team, int minb, int srk, int wpb)
 {
   constexpr bool small = NS <= 21;
+  constexpr int P = PPB_PART;
   // 12 or 16 warps per block (one block per SM: <= 168 or <= 128 registers):
   // the FP64 BDF warp-per-cell kernel
   if (wpb > 8) {
     if (method != METHOD_BDF || fp32 || team != 32 || minb != 2 || srk) return nullptr;
-    if (wpb == 16) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 512>;
-    if (wpb == 12) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 384>;
+    if constexpr (P == 1) {
+      if (wpb == 16) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 512>;
+      if (wpb == 12) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 384>;
+    }
     return nullptr;
   }
   // the SRK e-reactor: FP64 BDF, one warp per cell, <= 128 registers
-  if (srk) return (method == METHOD_BDF && !fp32 && team == 32 && minb == 2)
-                    ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, true>
-                    : nullptr;
+  if (srk) {
+    if constexpr (P == 3)
+      return (method == METHOD_BDF && !fp32 && team == 32 && minb == 2)
+               ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, true>
+               : nullptr;
+    return nullptr;
+  }
   if (team > 32) {
-    if constexpr (big_team<NS>() > 0) {
+    if constexpr (big_team<NS>() > 0 && P == 2) {
       constexpr int BT = big_team<NS>();
       if (team != BT) return nullptr;
       if (method == METHOD_RK64) return (TeamKernel)k_react_team<NS, double, METHOD_RK64, BT, 1>;
@@ -211,22 +227,58 @@ static TeamKernel team_kernel(int method, bool fp32, int team, int minb, int srk
     return nullptr;
   }
   if (team == 16 && !small) return nullptr;
-  if (method == METHOD_RK64) {
-    if (team == 16) return small ? (TeamKernel)k_react_team<NS, double, METHOD_RK64, (small ? 16 : 32), 2> : nullptr;
-    return (TeamKernel)k_react_team<NS, double, METHOD_RK64, 32, 2>;
+  if constexpr (P == 3) {
+    if (method == METHOD_RK64) {
+      if (team == 16) return small ? (TeamKernel)k_react_team<NS, double, METHOD_RK64, (small ? 16 : 32), 2> : nullptr;
+      return (TeamKernel)k_react_team<NS, double, METHOD_RK64, 32, 2>;
+    }
+    if (fp32) {
+      if (team == 16) return small ? (TeamKernel)k_react_team<NS, float, METHOD_BDF, (small ? 16 : 32), 2> : nullptr;
+      return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 2>;
+    }
+    if (team == 16) {
+      if (!small) return nullptr;
+      return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 1>
+                       : (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 2>;
+    }
+    return nullptr;
   }
-  if (fp32) {
-    if (team == 16) return small ? (TeamKernel)k_react_team<NS, float, METHOD_BDF, (small ? 16 : 32), 2> : nullptr;
-    return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 2>;
+  if constexpr (P == 0) {
+    if (method == METHOD_RK64 || fp32 || team == 16) return nullptr;
+    return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1>
+                     : (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2>;
   }
-  if (team == 16) {
-    if (!small) return nullptr;
-    return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 1>
-                     : (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 2>;
-  }
-  return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1>
-                   : (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2>;
+  return nullptr;
 }
+
+#define PPB_CAT2(a, b) a##b
+#define PPB_CAT(a, b) PPB_CAT2(a, b)
+#define PPB_CAT4(a, b, c, d) PPB_CAT(PPB_CAT(a, b), PPB_CAT(c, d))
+// this part's kernels, under a name of its own
+TeamKernel PPB_CAT4(team_kernel_, PPB_NS, _p, PPB_PART)(int method, bool fp32, int team, int minb, int srk, int wpb)
+{
+  return team_kernel_part<PPB_NS>(method, fp32, team, minb, srk, wpb);
+}
+
+#if PPB_PART == 0
+TeamKernel PPB_CAT4(team_kernel_, PPB_NS, _p, 1)(int, bool, int, int, int, int);
+TeamKernel PPB_CAT4(team_kernel_, PPB_NS, _p, 2)(int, bool, int, int, int, int);
+TeamKernel PPB_CAT4(team_kernel_, PPB_NS, _p, 3)(int, bool, int, int, int, int);
+
+template <int NS>
+static TeamKernel team_kernel(int method, bool fp32, int team, int minb, int srk, int wpb)
+{
+  TeamKernel (*parts[4])(int, bool, int, int, int, int) = {
+    PPB_CAT4(team_kernel_, PPB_NS, _p, 0), PPB_CAT4(team_kernel_, PPB_NS, _p, 1),
+    PPB_CAT4(team_kernel_, PPB_NS, _p, 2), PPB_CAT4(team_kernel_, PPB_NS, _p, 3)};
+  for (auto f : parts)
+    if (TeamKernel k = f(method, fp32, team, minb, srk, wpb)) return k;
+  return nullptr;
+}
+
+// the plain engine's kernels (part 3)
+void PPB_CAT4(launch_plain_, PPB_NS, _p, 3)(const DevMech& M, const Options& o, int method, Batch b, double dt,
+                                            cudaStream_t st);
 
 template <int NS>
 static int launch_react_ns(const DeviceMechanism& m, const Options& o, int method, const LaunchConfig& lc,
@@ -235,12 +287,7 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
   const DevMech& M = *m.dm;
   if (b.ncells <= 0) return 0;
   if (lc.engine == ENGINE_PLAIN) {
-    const int threads = 128;
-    const int blocks = (b.ncells + threads - 1) / threads;
-    if (method == METHOD_BDF)
-      k_react_plain<NS, METHOD_BDF><<<blocks, threads, 0, st>>>(M, o, b, dt);
-    else
-      k_react_plain<NS, METHOD_RK64><<<blocks, threads, 0, st>>>(M, o, b, dt);
+    PPB_CAT4(launch_plain_, PPB_NS, _p, 3)(M, o, method, b, dt, st);
     return (int)cudaGetLastError();
   }
   const bool fp32 = lc.lu_fp32 && method == METHOD_BDF;
@@ -347,8 +394,6 @@ static int launch_ajac_ns(const DevMech& M, const double* sc, const double* T, i
 }
 
 
-#define PPB_CAT2(a, b) a##b
-#define PPB_CAT(a, b) PPB_CAT2(a, b)
 int PPB_CAT(launch_react_, PPB_NS)(const DeviceMechanism& m, const Options& o, int method, const LaunchConfig& lc,
                                    Batch b, double dt, int* queue, cudaStream_t st)
 {
@@ -363,7 +408,22 @@ int PPB_CAT(launch_ajacobian_, PPB_NS)(const DevMech& M, const double* sc, const
 {
   return launch_ajac_ns<PPB_NS>(M, sc, T, consP, J, ncells, team, st);
 }
-#ifdef PPB_PHASE_TIMERS
+#endif // PPB_PART == 0
+
+#if PPB_PART == 3
+void PPB_CAT4(launch_plain_, PPB_NS, _p, 3)(const DevMech& M, const Options& o, int method, Batch b, double dt,
+                                            cudaStream_t st)
+{
+  const int threads = 128;
+  const int blocks = (b.ncells + threads - 1) / threads;
+  if (method == METHOD_BDF)
+    k_react_plain<PPB_NS, METHOD_BDF><<<blocks, threads, 0, st>>>(M, o, b, dt);
+  else
+    k_react_plain<PPB_NS, METHOD_RK64><<<blocks, threads, 0, st>>>(M, o, b, dt);
+}
+#endif
+
+#if defined(PPB_PHASE_TIMERS) && PPB_PART == 0
 int PPB_CAT(phase_cycles_, PPB_NS)(unsigned long long* out, int reset)
 {
   cudaError_t e = cudaMemcpyFromSymbol(out, g_phase_cycles, sizeof(unsigned long long) * PH_COUNT);

@@ -152,6 +152,23 @@ extern "C" int ppb_react_flat_device_noalloc(const char* mechanism, const char* 
     return nf(PPB_E_ARG, "invalid integrator options");
   if (o.engine != PPB_ENGINE_TUNED)
     return nf(PPB_E_ARG, "the allocation-free path runs the tuned engine only (engine = PPB_ENGINE_TUNED)");
+  // options this path cannot honour are rejected, never silently dropped
+  if (o.eos != PPB_EOS_IDEAL && o.eos != PPB_EOS_SRK) return nf(PPB_E_ARG, "eos must be 0 or 1");
+  if (o.eos == PPB_EOS_SRK &&
+      (method != METHOD_BDF || reactor_type != PPB_REACTOR_E || o.lu_fp32 || !find_srk(t->name)))
+    return nf(PPB_E_ARG, "the SRK EOS needs ReactorCvode, reactor type 1, the FP64 LU and a mechanism with SRK "
+                         "parameters");
+  if (o.warps_per_block < 0 || o.warps_per_block > 16)
+    return nf(PPB_E_ARG, "warps_per_block must be in 0..16 (0: the largest block of <= 8 warps that fits)");
+  if (o.team_lanes != 0 && o.team_lanes != 16 && o.team_lanes != 32 && o.team_lanes != 64 && o.team_lanes != 128)
+    return nf(PPB_E_ARG, "team_lanes must be 0, 16, 32, 64 or 128");
+  if (o.register_budget != 0 && o.register_budget != 1 && o.register_budget != 2)
+    return nf(PPB_E_ARG, "register_budget must be 0, 1 or 2");
+  if (o.warps_per_block == 0 && ((o.team_lanes != 0 && o.team_lanes != 32) || o.register_budget == 1))
+    return nf(PPB_E_ARG, "the allocation-free path does not autotune: give warps_per_block with team_lanes or "
+                         "register_budget");
+  if (o.eos == PPB_EOS_SRK && ((o.team_lanes != 0 && o.team_lanes != 32) || o.register_budget == 1))
+    return nf(PPB_E_ARG, "the SRK kernel runs one warp per cell with <= 128 registers");
   if (ncells < 0 || (ncells > 0 && (!rY || !rYsrc || !rX || !rX_src)))
     return nf(PPB_E_ARG, "invalid arguments");
   const int N = t->nsp, n = N + 1;
@@ -190,20 +207,31 @@ extern "C" int ppb_react_flat_device_noalloc(const char* mechanism, const char* 
   eo.rk_min = o.rk64_nsubsteps_min;
   eo.rk_max = o.rk64_nsubsteps_max;
   eo.use_typ_vals = 0;
-  if (o.rendezvous_cycles < 0 || o.rendezvous_cycles > 100000000)
-    return nf(PPB_E_ARG, "rendezvous_cycles must be in 0..100000000");
+  if (o.rendezvous_cycles < 0 || o.rendezvous_cycles > 10000000)
+    return nf(PPB_E_ARG, "rendezvous_cycles must be in 0..10000000");
   eo.rendezvous = o.rendezvous_cycles;
+  // the launch the allocating path makes for the same options with a fixed
+  // block size (no autotuner here: it would need scratch of its own)
   LaunchConfig lc;
   lc.engine = o.engine;
   lc.lu_fp32 = o.lu_fp32;
   lc.persistent = 1;
+  lc.srk = o.eos == PPB_EOS_SRK ? 1 : 0;
   lc.warps_per_block = o.warps_per_block;
+  lc.team = (o.team_lanes == 16 || o.team_lanes == 64 || o.team_lanes == 128) ? o.team_lanes : 32;
+  lc.minb = o.register_budget == 1 ? 1 : 2;
+  if (lc.team > 32) { // one cell per block of team / 32 warps, <= 255 registers
+    lc.warps_per_block = lc.team / 32;
+    lc.minb = 1;
+  }
   if (lc.warps_per_block <= 0) {
     const size_t cb = team_cell_bytes(t, o.lu_fp32);
     int w = 8;
     while (w > 1 && cb * w > 200 * 1024) w--;
     lc.warps_per_block = w;
   }
+  if (react_occupancy(dm, method, lc) < 1)
+    return nf(PPB_E_ARG, "this launch configuration is not compiled or does not fit for the mechanism");
   Batch b{};
   b.y = soa;
   b.src = soa_src;

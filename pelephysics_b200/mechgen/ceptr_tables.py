@@ -535,7 +535,9 @@ def emit_header(M, path):
 
 
 def main(argv):
-    ref = argv[1] if len(argv) > 1 else "/root/reference"
+    ref = argv[1] if len(argv) > 1 else os.environ.get("PPB_REFERENCE_ROOT")
+    if not ref:
+        sys.exit(f"usage: python {argv[0]} REFERENCE_ROOT  (or set PPB_REFERENCE_ROOT): the PelePhysics tree")
     here = os.path.dirname(os.path.abspath(__file__))
     outdir = os.path.join(os.path.dirname(here), "csrc", "mech")
     os.makedirs(outdir, exist_ok=True)

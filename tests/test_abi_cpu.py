@@ -33,6 +33,7 @@ def test_default_options_match_reference_defaults():
     assert (o.rk64_nsubsteps_guess, o.rk64_nsubsteps_min, o.rk64_nsubsteps_max) == (10, 5, 500)
     # engine tuning: the block rendezvous before each right-hand side is on
     assert o.rendezvous_cycles == 1000000 and o.cost_order == 1
+    assert o.arkode_barrier_us == 20000000
 
 
 def test_rendezvous_and_block_size_bounds_checked_without_device():
@@ -40,8 +41,10 @@ def test_rendezvous_and_block_size_bounds_checked_without_device():
     h = C.c_void_p()
     assert L.ppb_create(b"drm19", b"ReactorCvode", C.byref(h)) == 0
     for field, bad, msg in (("rendezvous_cycles", -1, b"rendezvous_cycles"),
-                            ("rendezvous_cycles", 100000001, b"rendezvous_cycles"),
-                            ("warps_per_block", 17, b"warps_per_block")):
+                            ("rendezvous_cycles", 10000001, b"rendezvous_cycles"),
+                            ("warps_per_block", 17, b"warps_per_block"),
+                            ("arkode_barrier_us", -1, b"arkode_barrier_us"),
+                            ("arkode_barrier_us", 60000001, b"arkode_barrier_us")):
         o = _lib.default_options()
         setattr(o, field, bad)
         assert L.ppb_init(h, 1, 10, C.byref(o)) == _lib.PPB_E_ARG

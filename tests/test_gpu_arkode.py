@@ -221,3 +221,29 @@ def test_empty_batch_and_all_masked(cuda, oracle):
                                dt_react=1e-6)
     assert code == 0 and dtr == 1e-6
     assert torch.equal(bY, keep) and torch.all(bFC == 0)
+
+
+def test_grid_barrier_bound_runs_out_and_the_next_call_is_clean(cuda, oracle):
+    """The cooperative launch's grid barrier gives up after arkode_barrier_us.
+    With a bound of 0 a block that has to wait gives up at once: the call ends
+    (no hang) with PPB_E_CUDA and the timeout message.  The same reactor, given
+    the default bound again, then reproduces a fresh reactor's result bit for
+    bit (the barrier words are cleared before every launch)."""
+    mech, dt, nc = "drm19", 1e-6, 4096
+    rY, src, rX, rXs = batch(oracle, mech, nc, seed=11)
+    opts = dict(rtol=1e-8, atol=1e-10)
+    r = Reactor(mech, "ReactorArkode")
+    r.init(1, nc, **opts, arkode_barrier_us=0)
+    with pytest.raises(_lib.EngineError, match="grid barrier timed out"):
+        r.react(rY.copy(), src.copy(), rX.copy(), rXs.copy(), dt)
+    r.init(1, nc, **opts)
+    y, x = rY.copy(), rX.copy()
+    _, _, _, code = r.react(y, src.copy(), x, rXs.copy(), dt)
+    assert code == 0
+    fresh = Reactor(mech, "ReactorArkode")
+    fresh.init(1, nc, **opts)
+    yf, xf = rY.copy(), rX.copy()
+    fresh.react(yf, src.copy(), xf, rXs.copy(), dt)
+    assert np.array_equal(y, yf) and np.array_equal(x, xf)
+    with pytest.raises(_lib.EngineError):
+        Reactor(mech, "ReactorArkode").init(1, nc, arkode_barrier_us=-1)

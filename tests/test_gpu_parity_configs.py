@@ -1,0 +1,110 @@
+"""Integration parity on the benchmark configurations themselves, against the
+oracle over the reference's own compiled mechanism kernels (oracle/_ref):
+
+* the drm19 64^3 field (unburnt, igniting and burnt cells; dt 1e-5 s,
+  rtol = atol = 1e-10, BDF orders <= 5), the same seeded 8,192-cell sample
+  the benchmark reports, for the tuned engine (FP64 LU and FP32 factor with
+  FP64 refinement) and the plain per-cell engine;
+* the LiDryer 16^3 = 4,096-cell configuration (dt 1e-4 s, rtol = atol =
+  1e-10), every cell, orders <= 5 and the reference default <= 2.
+
+The bar is T within 1e-6 relative and Y_k within 1e-8 absolute.  A cell whose
+mass fractions differ by more than 1e-8 from the oracle's is held to the
+oracle integrated from 1-ulp neighbours of its input (compare_to_reference
+in oracle/pyoracle.py): at rtol = 1e-10 the CVODE algorithm itself takes a
+different step sequence on some cells when one input component moves by one
+ulp, and those sequences end up to 6.5e-8 apart in Y.  The number of such
+cells is bounded too.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from pelephysics_b200 import workloads as wl
+from pelephysics_b200.reactor import Reactor
+
+pytestmark = pytest.mark.gpu
+
+OPTS = dict(rtol=1e-10, atol=1e-10)
+
+
+def _sample(ncells, n):
+    """The benchmark's oracle sample of the 64^3 field."""
+    return np.sort(np.random.default_rng(7).permutation(ncells)[:n])
+
+
+def _gpu_react(cells, opts, idx=None, integ="ReactorCvode"):
+    rY = cells.rY if idx is None else cells.rY[idx]
+    src = cells.rYsrc if idx is None else cells.rYsrc[idx]
+    rX = cells.rX if idx is None else cells.rX[idx]
+    rXs = cells.rX_src if idx is None else cells.rX_src[idx]
+    r = Reactor(cells.mech, integ)
+    r.init(cells.reactor_type, rX.shape[0], **opts)
+    y = torch.as_tensor(np.ascontiguousarray(rY), device="cuda")
+    s = torch.as_tensor(np.ascontiguousarray(src), device="cuda")
+    x = torch.as_tensor(np.ascontiguousarray(rX), device="cuda")
+    xs = torch.as_tensor(np.ascontiguousarray(rXs), device="cuda")
+    cost, dt, t, code = r.react(y, s, x, xs, cells.dt)
+    torch.cuda.synchronize()
+    status, _ = r.cell_status(rX.shape[0])
+    r.close()
+    assert code == 0 and (status == 0).all()
+    return y.cpu().numpy()
+
+
+def _oracle(oracle, cells, idx, opts):
+    y = np.ascontiguousarray(cells.rY[idx])
+    flag, _, st = oracle.react_flat(cells.mech, cells.reactor_type, y, np.ascontiguousarray(cells.rYsrc[idx]),
+                                    cells.rX[idx].copy(), cells.rX_src[idx].copy(), cells.dt, use_ref_kernels=1,
+                                    **opts)
+    assert flag == 0
+    return y
+
+
+def _check(oracle, cells, idx, y_gpu, y_ref, opts, max_over_frac=0.005):
+    r = oracle.compare_to_reference(cells.mech, cells.reactor_type, cells.rY[idx], cells.rYsrc[idx], cells.rX[idx],
+                                    cells.rX_src[idx], cells.dt, y_gpu, y_ref, use_ref_kernels=1, **opts)
+    assert r["max_rel_T"] <= 1e-6, r
+    assert r["max_abs_Y_nearest_of_1ulp_neighbours"] <= 1e-8, r
+    assert r["cells_over_Y_atol"] <= max_over_frac * r["cells"], r
+    return r
+
+
+@pytest.fixture(scope="module")
+def drm19_field():
+    return wl.drm19_field(64, device="cuda")
+
+
+@pytest.fixture(scope="module")
+def drm19_oracle(oracle, drm19_field):
+    idx = _sample(drm19_field.ncells, 8192)
+    return idx, _oracle(oracle, drm19_field, idx, dict(max_order=5, **OPTS))
+
+
+@pytest.mark.parametrize("extra", [dict(), dict(lu_fp32=1, refine_sweeps=1)], ids=["fp64_lu", "fp32_factor"])
+def test_drm19_field_tuned_vs_reference_kernels(cuda, oracle, drm19_field, drm19_oracle, extra):
+    idx, y_ref = drm19_oracle
+    assert drm19_field.meta["burnt"][idx].any() and (~drm19_field.meta["burnt"][idx]).any()
+    opts = dict(max_order=5, **OPTS)
+    y = _gpu_react(drm19_field, dict(engine=1, **opts, **extra))
+    _check(oracle, drm19_field, idx, y[idx], y_ref, opts)
+
+
+def test_drm19_field_plain_vs_reference_kernels(cuda, oracle, drm19_field, drm19_oracle):
+    idx, y_ref = drm19_oracle
+    opts = dict(max_order=5, **OPTS)
+    y = _gpu_react(drm19_field, dict(engine=0, **opts), idx=idx)
+    _check(oracle, drm19_field, idx, y, y_ref, opts)
+
+
+@pytest.mark.parametrize("engine", [1, 0], ids=["tuned", "plain"])
+@pytest.mark.parametrize("max_order", [5, 2])
+def test_lidryer_16cubed_vs_reference_kernels(cuda, oracle, engine, max_order):
+    cells = wl.lidryer_16(device="cuda")
+    assert cells.ncells == 4096 and cells.dt == 1e-4
+    idx = np.arange(cells.ncells)
+    opts = dict(max_order=max_order, **OPTS)
+    y_ref = _oracle(oracle, cells, idx, opts)
+    y = _gpu_react(cells, dict(engine=engine, **opts))
+    _check(oracle, cells, idx, y, y_ref, opts)

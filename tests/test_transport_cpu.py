@@ -8,6 +8,8 @@ import os
 import numpy as np
 import pytest
 
+from oracle import pyoracle as po
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk"]
 
@@ -61,12 +63,12 @@ def test_binary_diffusion_fits_are_symmetric():
         np.testing.assert_array_equal(c, c.transpose(1, 0, 2))
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/Mechanisms"), reason="needs the reference tree")
+@pytest.mark.skipif(po.reference_root() is None, reason="needs the reference tree")
 def test_tables_regenerate_identically(tmp_path):
     from pelephysics_b200.mechgen import transport_tables as tt
 
     for mech in MECHS:
-        T = tt.build(os.path.join("/root/reference/Mechanisms", mech), mech)
+        T = tt.build(os.path.join(po.reference_root(), "Mechanisms", mech), mech)
         out = tmp_path / f"trans_{mech}.h"
         tt.emit_header(T, str(out))
         ship = os.path.join(os.path.dirname(HERE), "pelephysics_b200", "csrc", "mech", f"trans_{mech}.h")
