@@ -76,6 +76,10 @@ typedef struct PPOOptions {
   int rk64_nsubsteps_guess, rk64_nsubsteps_min, rk64_nsubsteps_max;
   const double* typ_vals; // N+1 typical values or NULL
   int eos;                // 0 ideal gas (Fuego), 1 SRK (reactor type 1, difference-quotient Jacobian)
+  // nonzero: every right-hand-side value is moved by at most one ulp (up,
+  // down or not at all, from a per-cell stream of this seed): the algorithm
+  // as an implementation whose arithmetic differs in the last bit runs it
+  unsigned long long rhs_noise_seed;
 } PPOOptions;
 
 void ppo_default_options(PPOOptions* o);

@@ -134,7 +134,18 @@ typedef struct Sys {
   const double* rYsrc;
   double rhoe_init, rhoesrc;
   int eos; // 0 ideal gas, 1 SRK (oracle/srk.c; difference-quotient Jacobian)
+  unsigned long long* noise; // right-hand-side noise stream (rhs_noise_seed), or NULL
 } Sys;
+
+// splitmix64 (Steele, Lea, Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014)
+static unsigned long long mix64(unsigned long long* x)
+{
+  unsigned long long z = (*x += 0x9e3779b97f4a7c15ull);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
 
 static void sys_f(const Sys* s, double t, const double* y, double* f)
 {
@@ -144,6 +155,13 @@ static void sys_f(const Sys* s, double t, const double* y, double* f)
     g_ref[s->ref].rhs(s->reactor_type, t, y, f, s->rhoe_init, s->rhoesrc, s->rYsrc);
   } else {
     ppo_reactor_rhs(s->M, s->reactor_type, t, y, f, s->rhoe_init, s->rhoesrc, s->rYsrc);
+  }
+  if (s->noise) {
+    for (int i = 0; i <= s->M->nsp; i++) {
+      const unsigned long long r = mix64(s->noise) % 3;
+      if (r == 1) f[i] = nextafter(f[i], INFINITY);
+      if (r == 2) f[i] = nextafter(f[i], -INFINITY);
+    }
   }
 }
 
@@ -168,6 +186,7 @@ void ppo_default_options(PPOOptions* o)
   o->max_err_fails = 100;
   o->jac_eval_freq = 100;
   o->use_ref_kernels = 0;
+  o->rhs_noise_seed = 0;
   o->rk64_nsubsteps_guess = 10;
   o->rk64_nsubsteps_min = 5;
   o->rk64_nsubsteps_max = 500;
@@ -796,8 +815,18 @@ int ppo_bdf_cell(
   const PPBMechTables* M, int reactor_type, const PPOOptions* opt, double* y,
   const double* rYsrc, double rhoe_init, double rhoesrc, double dt, PPOStats* st)
 {
-  Sys sys = {M, reactor_type, -1, rYsrc, rhoe_init, rhoesrc, opt->eos};
+  Sys sys = {M, reactor_type, -1, rYsrc, rhoe_init, rhoesrc, opt->eos, NULL};
   if (opt->use_ref_kernels) sys.ref = find_ref(M->name);
+  unsigned long long noise = 0;
+  if (opt->rhs_noise_seed) { // a stream per cell: the seed mixed with the cell's input bits
+    noise = opt->rhs_noise_seed;
+    for (int i = 0; i <= M->nsp; i++) {
+      unsigned long long u;
+      memcpy(&u, &y[i], sizeof(u));
+      noise ^= u + 0x9e3779b97f4a7c15ull + (noise << 6) + (noise >> 2);
+    }
+    sys.noise = &noise;
+  }
   BDF* b = (BDF*)calloc(1, sizeof(BDF));
   const int n = M->nsp + 1;
   double atolv[NMAX];

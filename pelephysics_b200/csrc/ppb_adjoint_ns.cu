@@ -29,11 +29,11 @@
 
 namespace ppb {
 
-// checkpoint layout: [BdfScalars | nstloc][zn 6n][ewt n][J n*n][A n*n LT][piv n]
+// checkpoint layout: [BdfScalars | BdfArrays | nstloc][zn 6n][ewt n][J n*n][A n*n LT][piv n]
 template <typename LT>
 __host__ __device__ inline size_t cp_head_bytes()
 {
-  return (sizeof(BdfScalars) + 16 + 15) & ~size_t(15);
+  return (sizeof(BdfScalars) + sizeof(BdfArrays) + 16 + 15) & ~size_t(15);
 }
 
 template <typename LT>
@@ -50,7 +50,8 @@ __device__ void save_cp(const Team<32>& tm, char* dst, const B& bdf, const Work<
   constexpr int n = NS + 1;
   if (tm.lane == 0) {
     *reinterpret_cast<BdfScalars*>(dst) = bdf.s;
-    *reinterpret_cast<int*>(dst + sizeof(BdfScalars)) = nstloc;
+    *reinterpret_cast<BdfArrays*>(dst + sizeof(BdfScalars)) = bdf.ar;
+    *reinterpret_cast<int*>(dst + sizeof(BdfScalars) + sizeof(BdfArrays)) = nstloc;
   }
   double* z = reinterpret_cast<double*>(dst + cp_head_bytes<LT>());
   for (int j = 0; j < 6; j++)
@@ -70,7 +71,12 @@ __device__ void restore_cp(const Team<32>& tm, const char* src, B& bdf, Work<LT>
 {
   constexpr int n = NS + 1;
   bdf.s = *reinterpret_cast<const BdfScalars*>(src);
-  nstloc = *reinterpret_cast<const int*>(src + sizeof(BdfScalars));
+  {
+    const double* a = reinterpret_cast<const double*>(src + sizeof(BdfScalars));
+    for (int i = tm.lane; i < (int)(sizeof(BdfArrays) / sizeof(double)); i += 32)
+      reinterpret_cast<double*>(&bdf.ar)[i] = a[i];
+  }
+  nstloc = *reinterpret_cast<const int*>(src + sizeof(BdfScalars) + sizeof(BdfArrays));
   const double* z = reinterpret_cast<const double*>(src + cp_head_bytes<LT>());
   for (int j = 0; j < 6; j++)
     for (int i = tm.lane; i < n; i += 32) w.zn[j][i] = z[j * n + i];
@@ -82,6 +88,7 @@ __device__ void restore_cp(const Team<32>& tm, const char* src, B& bdf, Work<LT>
   const int* piv = reinterpret_cast<const int*>(A + n * n);
   for (int i = tm.lane; i < n; i += 32) w.piv[i] = piv[i];
   tm.sync();
+  perm_from_piv(tm, w.piv, w.perm, n);
 }
 
 // Tangent-linear integration of one cell: each segment's tape is swept
@@ -151,7 +158,9 @@ __device__ void tangent_cell(const Team<32>& tm, const DevMech& M, const Options
 }
 
 template <int NS, typename LT>
-__global__ void __launch_bounds__(256) k_tangent(DevMech M, Options o, AdjBatch b, AdjLayout L, double dt, int* queue)
+__global__ void __launch_bounds__(256) k_tangent(const __grid_constant__ DevMech M, const __grid_constant__ Options o,
+                                                 const __grid_constant__ AdjBatch b, const __grid_constant__ AdjLayout L,
+                                                 double dt, int* queue)
 {
   extern __shared__ __align__(16) char smem[];
   Team<32> tm;
@@ -335,7 +344,9 @@ static int launch_rhs_exact_ns(const DevMech& M, int rtype, double t, const doub
 // recomputation repeats the forward bit for bit; it is checked against the
 // next checkpoint.
 template <int NS, typename LT>
-__global__ void __launch_bounds__(256) k_adj_seg(DevMech M, Options o, AdjBatch b, AdjCells C, double dt, int* queue,
+__global__ void __launch_bounds__(256) k_adj_seg(const __grid_constant__ DevMech M, const __grid_constant__ Options o,
+                                                 const __grid_constant__ AdjBatch b, const __grid_constant__ AdjCells C,
+                                                 double dt, int* queue,
                                                  int seg, int replay, size_t warp_smem)
 {
   extern __shared__ __align__(16) char smem[];

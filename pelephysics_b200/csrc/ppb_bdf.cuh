@@ -54,6 +54,8 @@ struct Work {
   double *J, *src, *atolv;
   LT* A;
   int* piv;
+  int* perm;  // row order of the factored matrix: row i of PA is row perm[i] of A
+  struct BdfArrays* ba; // the integrator's coefficient arrays (team-shared)
   // rate scratch
   double *Y, *sc, *g, *qd, *wdot, *ei, *h1, *h2, *h3;
   // block-shared rendezvous counters {arrived, generation, active warps}, or nullptr
@@ -135,18 +137,46 @@ __device__ double reactor_rhs(
   double T = y[N];
   const int EH = (rtype == 2);
   t_from_energy(tm, M, EH, nrg, Y, T);
-  const double cv = mix_c(tm, M, EH, T, Y);
   const double invT = 1.0 / T;
   const double RT = RU * T;
-  for (int s = tm.lane; s < N; s += TEAM) {
-    const double im = __ldg(M.imw + s);
-    ei[s] = (EH ? h_RT(M, s, T, invT) : u_RT(M, s, T, invT)) * (RT * im);
-    sc[s] = (rho * Y[s] * im) * 1.0e6;
-  }
-  if (tm.lane == 0) sc[N] = 1.0; // padding slot of the packed reaction records
-  tm.sync();
   RateScratch rs{sc, g, qd};
-  production_rate(tm, M, wdot, sc, T, rs);
+  double cv;
+  if constexpr (TEAM > 1) {
+    // one pass over the species at the final T: the heat capacity (as
+    // mix_c), the energies, the concentrations, their sum and g/RT (as
+    // productionRate forms them), then the two sums together
+    const double logT = ppb_log(T);
+    const double refC = 101325 / 8.31446 * invT;
+    const double refCinv = 1 / refC;
+    double cvs = 0.0, mix = 0.0;
+    for (int s = tm.lane; s < N; s += TEAM) {
+      const double im = __ldg(M.imw + s);
+      cvs += Y[s] * (EH ? cp_R(M, s, T) : cv_R(M, s, T)) * __ldg(M.imw + s);
+      ei[s] = (EH ? h_RT(M, s, T, invT) : u_RT(M, s, T, invT)) * (RT * im);
+      const double scs = (rho * Y[s] * im) * 1.0e6;
+      sc[s] = scs;
+      mix += scs;
+      g[s] = g_RT(M, s, T, invT, logT);
+    }
+    cv = tm.sum(cvs) * RU;
+    const double mixture = tm.sum(mix);
+    if (tm.lane == 0) {
+      sc[N] = 1.0; // padding slots of the packed reaction records
+      g[N] = 0.0;
+    }
+    tm.sync();
+    production_rate_core(tm, M, wdot, sc, T, invT, logT, refC, refCinv, mixture, rs);
+  } else {
+    cv = mix_c(tm, M, EH, T, Y);
+    for (int s = tm.lane; s < N; s += TEAM) {
+      const double im = __ldg(M.imw + s);
+      ei[s] = (EH ? h_RT(M, s, T, invT) : u_RT(M, s, T, invT)) * (RT * im);
+      sc[s] = (rho * Y[s] * im) * 1.0e6;
+    }
+    if (tm.lane == 0) sc[N] = 1.0; // padding slot of the packed reaction records
+    tm.sync();
+    production_rate(tm, M, wdot, sc, T, rs);
+  }
   double acc = 0.0;
   for (int s = tm.lane; s < N; s += TEAM) {
     const double cd = wdot[s] * 1.0e-6 * __ldg(M.mw + s) + src[s];
@@ -344,9 +374,70 @@ __device__ void lu_solve(const Team<TEAM>& tm, const LT* A, int n, const int* pi
   tm.sync();
 }
 
+// Row order of a factored matrix from its LAPACK-style pivots: the
+// interchanges k <-> piv[k], in order, applied to the identity, so that the
+// pivoted right-hand side is b[perm[0..n-1]].  A pivot outside [0, n) (pivots
+// of no factorisation yet, e.g. a checkpoint taken before the first step) is
+// skipped, so perm is always a permutation of 0..n-1.
+template <int TEAM>
+__device__ __forceinline__ void perm_from_piv(const Team<TEAM>& tm, const int* piv, int* perm, int n)
+{
+  if (tm.lane == 0) {
+    for (int i = 0; i < n; i++) perm[i] = i;
+    for (int k = 0; k < n; k++) {
+      const int p = piv[k];
+      if (p != k && p >= 0 && p < n) {
+        const int t = perm[k];
+        perm[k] = perm[p];
+        perm[p] = t;
+      }
+    }
+  }
+  tm.sync();
+}
+
+// lu_solve for a team of 16 or 32 lanes and n <= TEAM with the solution in
+// registers, lane i holding entry i: the pivoted gather, then the two
+// triangular sweeps with the running entry k broadcast by a shuffle instead of
+// a shared-memory round trip and a team barrier per column.  Every entry is
+// updated by the same operations in the same order as in lu_solve.
+template <int TEAM, typename LT, int NN>
+__device__ __forceinline__ void lu_solve_reg(const Team<TEAM>& tm, const LT* A, const int* perm, double* b)
+{
+  static_assert((TEAM == 16 || TEAM == 32) && NN <= TEAM, "one entry per lane");
+  const int i = tm.lane;
+  double x = (i < NN) ? b[perm[i]] : 0.0;
+#pragma unroll
+  for (int k = 0; k < NN - 1; k++) {
+    const double bk = __shfl_sync(tm.mask, x, k, TEAM);
+    if (i > k && i < NN) x -= (double)A[k * NN + i] * bk;
+  }
+#pragma unroll
+  for (int k = NN - 1; k > 0; k--) {
+    const double bk = __shfl_sync(tm.mask, x, k, TEAM) / (double)A[k * NN + k];
+    if (i == k) {
+      x = bk;
+    } else if (i < k) {
+      x -= (double)A[k * NN + i] * bk;
+    }
+  }
+  if (i == 0) x /= (double)A[0];
+  tm.sync(); // every lane has gathered its entry before any writes
+  if (i < NN) b[i] = x;
+  tm.sync();
+}
+
 // ---------------------------------------------------------------- BDF
-struct BdfScalars {
+// The integrator's coefficient arrays, indexed by order at run time: one
+// team-shared copy per cell (in registers they would force the integrator's
+// whole state to local memory).
+struct BdfArrays {
   double tau[7], tq[6], l[6];
+};
+
+// The scalar integrator state: every lane of the team holds the same values
+// (in registers).
+struct BdfScalars {
   double h, hprime, hscale, eta, etamax, tn, rl1, gamma, gammap, gamrat, crate, delp, acnrm, saved_tq5, hu;
   double gamma_lu; // gamma of the factored matrix I - gamma J
   int q, qprime, qwait, L, qmax, indx_acor, jcur;
@@ -359,6 +450,26 @@ struct BdfScalars {
 struct CellIn {
   double rhoe, rhoesrc;
 };
+
+// The integrator's right-hand side at (t, y) into fy: the block rendezvous
+// (when on), then fKernelSpec.  Out of line, so that the kernel holds one
+// copy of the right-hand side; a free function taking what it reads, so that
+// no caller's state has to live in memory for the call.
+#ifndef PPB_RHS_ATTR
+#define PPB_RHS_ATTR __noinline__
+#endif
+template <int TEAM, bool SRK>
+__device__ PPB_RHS_ATTR void bdf_rhs(Team<TEAM> tm, const DevMech& M, int rtype, int* rv, int rcycles, double t,
+                                     const double* y, double* fy, double rhoe, double rhoesrc, const double* src,
+                                     double* Y, double* sc, double* g, double* qd, double* wdot, double* ei)
+{
+  if (rv) rendezvous(rv, rcycles);
+  if constexpr (SRK) {
+    reactor_rhs_srk<TEAM>(tm, M, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei);
+  } else {
+    reactor_rhs<TEAM>(tm, M, rtype, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei);
+  }
+}
 
 // Recorder interface of the integrator: every operation that changes the
 // Nordsieck history, with the coefficients it used, in execution order (the
@@ -378,14 +489,15 @@ struct Bdf {
   Work<LT>& w;
   CellIn cin;
   BdfScalars s;
+  BdfArrays& ar;
   Rec rec;
 
   __device__ Bdf(const Team<TEAM>& t, const DevMech& m, const Options& op, Work<LT>& wk, CellIn ci)
-    : tm(t), M(m), o(op), w(wk), cin(ci)
+    : tm(t), M(m), o(op), w(wk), cin(ci), ar(*wk.ba)
   {
   }
 
-  __device__ double wrms(const double* v) const
+  __device__ __forceinline__ double wrms(const double* v) const
   {
     double a = 0.0;
     for (int i = tm.lane; i < n; i += TEAM) {
@@ -395,7 +507,7 @@ struct Bdf {
     return sqrt(tm.sum(a) / n);
   }
 
-  __device__ void set_ewt(const double* y)
+  __device__ __forceinline__ void set_ewt(const double* y)
   {
     for (int i = tm.lane; i < n; i += TEAM) {
       const double at = o.use_typ_vals ? w.atolv[i] : o.atol;
@@ -404,25 +516,16 @@ struct Bdf {
     tm.sync();
   }
 
-  // out of line: one copy of the right-hand side in the kernel
-#ifndef PPB_RHS_ATTR
-#define PPB_RHS_ATTR __noinline__
-#endif
-  __device__ PPB_RHS_ATTR void f(double t, const double* y, double* fy)
+  __device__ __forceinline__ void f(double t, const double* y, double* fy)
   {
-    if (w.rv) rendezvous(w.rv, o.rendezvous);
     PPB_TIC(PH_RHS);
-    if constexpr (SRK) {
-      reactor_rhs_srk<TEAM>(tm, M, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot, w.ei);
-    } else {
-      reactor_rhs<TEAM>(tm, M, o.reactor_type, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
-                        w.ei);
-    }
+    bdf_rhs<TEAM, SRK>(tm, M, o.reactor_type, w.rv, o.rendezvous, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc,
+                       w.g, w.qd, w.wdot, w.ei);
     s.nfe++;
     PPB_TOC(PH_RHS);
   }
 
-  __device__ void jac()
+  __device__ __forceinline__ void jac()
   {
     PPB_TIC(PH_JAC);
     if constexpr (SRK) {
@@ -443,7 +546,7 @@ struct Bdf {
   // column j uses inc = max(sqrt(eps) |y_j|, min_inc / ewt_j), min_inc =
   // 1000 |h| eps n ||f||_WRMS (1 when ||f|| = 0).  Its RHS evaluations are
   // not counted in nfe (CVODE counts them separately).
-  __device__ void jac_dq()
+  __device__ __forceinline__ void jac_dq()
   {
     const double fnorm = wrms(w.ftemp);
     const double eps = 2.220446049250313e-16;
@@ -467,7 +570,7 @@ struct Bdf {
     }
   }
 
-  __device__ int hin(double tout)
+  __device__ __forceinline__ int hin(double tout)
   {
     const double tdiff = tout - s.tn;
     if (tdiff == 0.0) return ST_TOO_CLOSE;
@@ -513,7 +616,7 @@ struct Bdf {
     return ST_OK;
   }
 
-  __device__ void rescale()
+  __device__ __forceinline__ void rescale()
   {
     if constexpr (Rec::on) rec.rescale(tm, s.q, s.eta);
     double factor = s.eta;
@@ -526,7 +629,7 @@ struct Bdf {
     s.hscale = s.h;
   }
 
-  __device__ void predict()
+  __device__ __forceinline__ void predict()
   {
     s.tn += s.h;
     for (int i = tm.lane; i < n; i += TEAM) {
@@ -536,7 +639,7 @@ struct Bdf {
     tm.sync();
   }
 
-  __device__ void restore(double saved_t)
+  __device__ __forceinline__ void restore(double saved_t)
   {
     s.tn = saved_t;
     for (int i = tm.lane; i < n; i += TEAM) {
@@ -546,63 +649,63 @@ struct Bdf {
     tm.sync();
   }
 
-  __device__ void set_bdf()
+  __device__ __forceinline__ void set_bdf()
   {
     double alpha0, alpha0_hat, xi_inv, xistar_inv, hsum;
     const int q = s.q;
-    s.l[0] = s.l[1] = xi_inv = xistar_inv = 1.0;
-    for (int i = 2; i <= q; i++) s.l[i] = 0.0;
+    ar.l[0] = ar.l[1] = xi_inv = xistar_inv = 1.0;
+    for (int i = 2; i <= q; i++) ar.l[i] = 0.0;
     alpha0 = alpha0_hat = -1.0;
     hsum = s.h;
     if (q > 1) {
       for (int j = 2; j < q; j++) {
-        hsum += s.tau[j - 1];
+        hsum += ar.tau[j - 1];
         xi_inv = s.h / hsum;
         alpha0 -= 1.0 / j;
-        for (int i = j; i >= 1; i--) s.l[i] += s.l[i - 1] * xi_inv;
+        for (int i = j; i >= 1; i--) ar.l[i] += ar.l[i - 1] * xi_inv;
       }
       alpha0 -= 1.0 / q;
-      xistar_inv = -s.l[1] - alpha0;
-      hsum += s.tau[q - 1];
+      xistar_inv = -ar.l[1] - alpha0;
+      hsum += ar.tau[q - 1];
       xi_inv = s.h / hsum;
-      alpha0_hat = -s.l[1] - xi_inv;
-      for (int i = q; i >= 1; i--) s.l[i] += s.l[i - 1] * xistar_inv;
+      alpha0_hat = -ar.l[1] - xi_inv;
+      for (int i = q; i >= 1; i--) ar.l[i] += ar.l[i - 1] * xistar_inv;
     }
     const double A1 = 1.0 - alpha0_hat + alpha0;
     const double A2 = 1.0 + q * A1;
-    s.tq[2] = fabs(A1 / (alpha0 * A2));
-    s.tq[5] = fabs(A2 * xistar_inv / (s.l[q] * xi_inv));
+    ar.tq[2] = fabs(A1 / (alpha0 * A2));
+    ar.tq[5] = fabs(A2 * xistar_inv / (ar.l[q] * xi_inv));
     if (s.qwait == 1) {
       if (q > 1) {
-        const double C = xistar_inv / s.l[q];
+        const double C = xistar_inv / ar.l[q];
         const double A3 = alpha0 + 1.0 / q;
         const double A4 = alpha0_hat + xi_inv;
         const double Cpinv = (1.0 - A4 + A3) / A3;
-        s.tq[1] = fabs(C * Cpinv);
+        ar.tq[1] = fabs(C * Cpinv);
       } else {
-        s.tq[1] = 1.0;
+        ar.tq[1] = 1.0;
       }
-      hsum += s.tau[q];
+      hsum += ar.tau[q];
       xi_inv = s.h / hsum;
       const double A5 = alpha0 - (1.0 / (q + 1));
       const double A6 = alpha0_hat - xi_inv;
       const double Cppinv = (1.0 - A6 + A5) / A2;
-      s.tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
+      ar.tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
     }
-    s.tq[4] = 0.1 / s.tq[2];
+    ar.tq[4] = 0.1 / ar.tq[2];
   }
 
-  __device__ void set()
+  __device__ __forceinline__ void set()
   {
     set_bdf();
-    s.rl1 = 1.0 / s.l[1];
+    s.rl1 = 1.0 / ar.l[1];
     s.gamma = s.h * s.rl1;
     if (s.nst == 0) s.gammap = s.gamma;
     s.gamrat = (s.nst > 0) ? s.gamma / s.gammap : 1.0;
   }
 
   // cvLsSetup: (re)use J, form I - gamma J, factor
-  __device__ int ls_setup(int convfail)
+  __device__ __forceinline__ int ls_setup(int convfail)
   {
     const double dgamma = fabs((s.gamma / s.gammap) - 1.0);
     const bool jbad = (s.nst == 0) || (s.nst >= s.nstlj + o.jac_eval_freq) || ((convfail == 1) && (dgamma < 0.2)) ||
@@ -626,30 +729,43 @@ struct Bdf {
     }
     tm.sync();
     const int ier = lu_factor<TEAM, LT>(tm, w.A, n, w.piv) ? 1 : 0;
+    if constexpr ((TEAM == 16 || TEAM == 32) && n <= TEAM) {
+      if (!ier) perm_from_piv(tm, w.piv, w.perm, n);
+    }
     PPB_TOC(PH_LU);
     return ier;
   }
 
+  // (LU) x = b in place with the current factor
+  __device__ __forceinline__ void lsolve(double* b)
+  {
+    if constexpr ((TEAM == 16 || TEAM == 32) && n <= TEAM) {
+      lu_solve_reg<TEAM, LT, n>(tm, w.A, w.perm, b);
+    } else {
+      lu_solve<TEAM, LT>(tm, w.A, n, w.piv, b);
+    }
+  }
+
   // x := (I - gamma J)^{-1} b, with FP64 iterative refinement when the
   // factor is FP32.  b and x are w.delta; w.tempv is scratch.
-  __device__ void ls_solve()
+  __device__ __forceinline__ void ls_solve()
   {
     PPB_TIC(PH_SOLVE);
     ls_solve_impl();
     PPB_TOC(PH_SOLVE);
   }
 
-  __device__ void ls_solve_impl()
+  __device__ __forceinline__ void ls_solve_impl()
   {
     if (sizeof(LT) == sizeof(double) || o.refine_sweeps <= 0) {
-      lu_solve<TEAM, LT>(tm, w.A, n, w.piv, w.delta);
+      lsolve(w.delta);
       return;
     }
     // keep b in ftemp-sized scratch: w.h3 (length >= n)
     double* b = w.h3;
     for (int i = tm.lane; i < n; i += TEAM) b[i] = w.delta[i];
     tm.sync();
-    lu_solve<TEAM, LT>(tm, w.A, n, w.piv, w.delta);
+    lsolve(w.delta);
     for (int sweep = 0; sweep < o.refine_sweeps; sweep++) {
       // r = b - (I - gamma_lu J) x in FP64, against the matrix that was
       // factored (CVODE corrects a stale gamma afterwards, in nls)
@@ -661,13 +777,13 @@ struct Bdf {
         w.tempv[i] = b[i] - ax;
       }
       tm.sync();
-      lu_solve<TEAM, LT>(tm, w.A, n, w.piv, w.tempv);
+      lsolve(w.tempv);
       for (int i = tm.lane; i < n; i += TEAM) w.delta[i] += w.tempv[i];
       tm.sync();
     }
   }
 
-  __device__ void nls_residual()
+  __device__ __forceinline__ void nls_residual()
   {
     for (int i = tm.lane; i < n; i += TEAM) w.y[i] = w.zn[0][i] + w.acor[i];
     tm.sync();
@@ -679,7 +795,7 @@ struct Bdf {
     tm.sync();
   }
 
-  __device__ int nls(int nflag)
+  __device__ __forceinline__ int nls(int nflag)
   {
     PPB_TIC(PH_NEWTON);
     const int r = nls_impl(nflag);
@@ -687,7 +803,7 @@ struct Bdf {
     return r;
   }
 
-  __device__ int nls_impl(int nflag)
+  __device__ __forceinline__ int nls_impl(int nflag)
   {
     const int convfail = ((nflag == 0) || (nflag == 2)) ? 0 : 2;
     bool callSetup = (nflag == 1) || (nflag == 2) || (s.nst == 0) || (s.nst >= s.nstlp + 20) ||
@@ -721,7 +837,7 @@ struct Bdf {
         tm.sync();
         const double del = wrms(w.delta);
         if (m > 0) s.crate = fmax(0.3 * s.crate, del / s.delp);
-        const double dcon = del * fmin(1.0, s.crate) / s.tq[4];
+        const double dcon = del * fmin(1.0, s.crate) / ar.tq[4];
         if (dcon <= 1.0) {
           s.acnrm = (m == 0) ? del : wrms(w.acor);
           s.jcur = 0;
@@ -751,21 +867,21 @@ struct Bdf {
     return retval;
   }
 
-  __device__ void increase_bdf()
+  __device__ __forceinline__ void increase_bdf()
   {
     double alpha0, alpha1, prod, xi, xiold, hsum, A1;
-    for (int i = 0; i <= s.qmax; i++) s.l[i] = 0.0;
-    s.l[2] = alpha1 = prod = xiold = 1.0;
+    for (int i = 0; i <= s.qmax; i++) ar.l[i] = 0.0;
+    ar.l[2] = alpha1 = prod = xiold = 1.0;
     alpha0 = -1.0;
     hsum = s.hscale;
     if (s.q > 1) {
       for (int j = 1; j < s.q; j++) {
-        hsum += s.tau[j + 1];
+        hsum += ar.tau[j + 1];
         xi = hsum / s.hscale;
         prod *= xi;
         alpha0 -= 1.0 / (j + 1);
         alpha1 += 1.0 / xi;
-        for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xiold + s.l[i - 1];
+        for (int i = j + 2; i >= 2; i--) ar.l[i] = ar.l[i] * xiold + ar.l[i - 1];
         xiold = xi;
       }
     }
@@ -773,37 +889,37 @@ struct Bdf {
     for (int i = tm.lane; i < n; i += TEAM) {
       const double zL = A1 * w.zn[s.indx_acor][i];
       w.zn[s.L][i] = zL;
-      for (int j = 2; j <= s.q; j++) w.zn[j][i] += s.l[j] * zL;
+      for (int j = 2; j <= s.q; j++) w.zn[j][i] += ar.l[j] * zL;
     }
     tm.sync();
-    if constexpr (Rec::on) rec.increase(tm, s.q, s.L, s.indx_acor, A1, s.l);
+    if constexpr (Rec::on) rec.increase(tm, s.q, s.L, s.indx_acor, A1, ar.l);
   }
 
-  __device__ void decrease_bdf()
+  __device__ __forceinline__ void decrease_bdf()
   {
     double hsum, xi;
-    for (int i = 0; i <= s.qmax; i++) s.l[i] = 0.0;
-    s.l[2] = 1.0;
+    for (int i = 0; i <= s.qmax; i++) ar.l[i] = 0.0;
+    ar.l[2] = 1.0;
     hsum = 0.0;
     for (int j = 1; j <= s.q - 2; j++) {
-      hsum += s.tau[j];
+      hsum += ar.tau[j];
       xi = hsum / s.hscale;
-      for (int i = j + 2; i >= 2; i--) s.l[i] = s.l[i] * xi + s.l[i - 1];
+      for (int i = j + 2; i >= 2; i--) ar.l[i] = ar.l[i] * xi + ar.l[i - 1];
     }
     for (int i = tm.lane; i < n; i += TEAM)
-      for (int j = 2; j < s.q; j++) w.zn[j][i] -= s.l[j] * w.zn[s.q][i];
+      for (int j = 2; j < s.q; j++) w.zn[j][i] -= ar.l[j] * w.zn[s.q][i];
     tm.sync();
-    if constexpr (Rec::on) rec.decrease(tm, s.q, s.l);
+    if constexpr (Rec::on) rec.decrease(tm, s.q, ar.l);
   }
 
-  __device__ void adjust_order(int deltaq)
+  __device__ __forceinline__ void adjust_order(int deltaq)
   {
     if ((s.q == 2) && (deltaq != 1)) return;
     if (deltaq == 1) increase_bdf();
     else if (deltaq == -1) decrease_bdf();
   }
 
-  __device__ int handle_nflag(int& nflag, double saved_t, int& ncf)
+  __device__ __forceinline__ int handle_nflag(int& nflag, double saved_t, int& ncf)
   {
     if (nflag == 0) return 2; // DO_ERROR_TEST
     s.ncfn++;
@@ -818,9 +934,9 @@ struct Bdf {
     return 3; // PREDICT_AGAIN
   }
 
-  __device__ int do_error_test(int& nflag, double saved_t, int& nef, double& dsm)
+  __device__ __forceinline__ int do_error_test(int& nflag, double saved_t, int& nef, double& dsm)
   {
-    dsm = s.acnrm * s.tq[2];
+    dsm = s.acnrm * ar.tq[2];
     if (dsm <= 1.0) return ST_OK;
     nef++;
     s.netf++;
@@ -855,32 +971,32 @@ struct Bdf {
     return 5;
   }
 
-  __device__ void complete_step()
+  __device__ __forceinline__ void complete_step()
   {
     s.nst++;
     s.hu = s.h;
-    for (int i = s.q; i >= 2; i--) s.tau[i] = s.tau[i - 1];
-    if ((s.q == 1) && (s.nst > 1)) s.tau[2] = s.tau[1];
-    s.tau[1] = s.h;
+    for (int i = s.q; i >= 2; i--) ar.tau[i] = ar.tau[i - 1];
+    if ((s.q == 1) && (s.nst > 1)) ar.tau[2] = ar.tau[1];
+    ar.tau[1] = s.h;
     const bool save = ((s.qwait - 1) == 1) && (s.q != s.qmax);
     if constexpr (Rec::on) {
       rec.predict(tm, s.q);
-      rec.correct(tm, s.q, save, s.tn, s.gamma, s.rl1, s.l, w.zn[0], w.acor);
+      rec.correct(tm, s.q, save, s.tn, s.gamma, s.rl1, ar.l, w.zn[0], w.acor);
     }
     for (int i = tm.lane; i < n; i += TEAM) {
       const double a = w.acor[i];
-      for (int j = 0; j <= s.q; j++) w.zn[j][i] += s.l[j] * a;
+      for (int j = 0; j <= s.q; j++) w.zn[j][i] += ar.l[j] * a;
       if (save) w.zn[s.qmax][i] = a;
     }
     tm.sync();
     s.qwait--;
     if (save) {
-      s.saved_tq5 = s.tq[5];
+      s.saved_tq5 = ar.tq[5];
       s.indx_acor = s.qmax;
     }
   }
 
-  __device__ void set_eta()
+  __device__ __forceinline__ void set_eta()
   {
     if ((s.eta > 0.0) && (s.eta < 1.5)) {
       s.eta = 1.0;
@@ -891,7 +1007,7 @@ struct Bdf {
     }
   }
 
-  __device__ void prepare_next_step(double dsm)
+  __device__ __forceinline__ void prepare_next_step(double dsm)
   {
     if (s.etamax == 1.0) {
       s.qwait = s.qwait > 2 ? s.qwait : 2;
@@ -910,15 +1026,15 @@ struct Bdf {
     s.qwait = 2;
     double etaqm1 = 0.0;
     if (s.q > 1) {
-      const double ddn = wrms(w.zn[s.q]) * s.tq[1];
+      const double ddn = wrms(w.zn[s.q]) * ar.tq[1];
       etaqm1 = 1.0 / (pow(6.0 * ddn, 1.0 / s.q) + 1.0e-6);
     }
     double etaqp1 = 0.0;
     if (s.q != s.qmax && s.saved_tq5 != 0.0) {
-      const double cquot = (s.tq[5] / s.saved_tq5) * pow(s.h / s.tau[2], (double)s.L);
+      const double cquot = (ar.tq[5] / s.saved_tq5) * pow(s.h / ar.tau[2], (double)s.L);
       for (int i = tm.lane; i < n; i += TEAM) w.tempv[i] = -cquot * w.zn[s.qmax][i] + w.acor[i];
       tm.sync();
-      const double dup = wrms(w.tempv) * s.tq[3];
+      const double dup = wrms(w.tempv) * ar.tq[3];
       etaqp1 = 1.0 / (pow(10.0 * dup, 1.0 / (s.L + 1)) + 1.0e-6);
     }
     const double etam = fmax(etaqm1, fmax(etaq, etaqp1));
@@ -941,7 +1057,7 @@ struct Bdf {
     set_eta();
   }
 
-  __device__ void adjust_params()
+  __device__ __forceinline__ void adjust_params()
   {
     if (s.qprime != s.q) {
       adjust_order(s.qprime - s.q);
@@ -952,7 +1068,7 @@ struct Bdf {
     rescale();
   }
 
-  __device__ int step()
+  __device__ __forceinline__ int step()
   {
     PPB_TIC(PH_STEP);
     const int r = step_impl();
@@ -960,7 +1076,7 @@ struct Bdf {
     return r;
   }
 
-  __device__ int step_impl()
+  __device__ __forceinline__ int step_impl()
   {
     const double saved_t = s.tn;
     int ncf = 0, nef = 0, nflag = 0;
@@ -986,9 +1102,18 @@ struct Bdf {
 
   // Start of an integration of w.zn[0] (initial y, team-shared) towards
   // tout: history, error weights, initial step (cvInitialSetup, cvHin).
-  __device__ int start(double tout)
+  __device__ __forceinline__ int start(double tout)
   {
     s = BdfScalars{};
+    for (int i = tm.lane; i < (int)(sizeof(BdfArrays) / sizeof(double)); i += TEAM)
+      reinterpret_cast<double*>(&ar)[i] = 0.0;
+    // no factorisation yet: identity pivots and row order (a checkpoint taken
+    // before the first step holds valid ones)
+    for (int i = tm.lane; i < n; i += TEAM) {
+      w.piv[i] = i;
+      w.perm[i] = i;
+    }
+    tm.sync();
     s.qmax = o.max_order;
     s.q = 1;
     s.L = 2;
@@ -1011,7 +1136,7 @@ struct Bdf {
   // Step until tout is passed (then interpolate to tout into w.y and set
   // done) or, with a recorder, until the recorder closes its segment.
   // nstloc counts the steps of this call to react.
-  __device__ int advance(double tout, int& nstloc, bool& done)
+  __device__ __forceinline__ int advance(double tout, int& nstloc, bool& done)
   {
     done = false;
     for (;;) {
@@ -1039,7 +1164,7 @@ struct Bdf {
   }
 
   // Integrate w.zn[0] (initial y, team-shared) over [0, tout]; result in w.y.
-  __device__ int run(double tout)
+  __device__ __forceinline__ int run(double tout)
   {
     PPB_TIC(PH_TOTAL);
     int flag = start(tout);

@@ -69,14 +69,17 @@ __device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options&
 
 // plain: one thread per cell, FP64, per-cell arrays in thread-local memory
 template <int NS, int METHOD>
-__global__ void __launch_bounds__(128) k_react_plain(DevMech M, Options o, Batch b, double dt)
+__global__ void __launch_bounds__(128) k_react_plain(const __grid_constant__ DevMech M,
+                                                     const __grid_constant__ Options o,
+                                                     const __grid_constant__ Batch b, double dt)
 {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= b.ncells) return;
   constexpr int n = NS + 1;
   double buf[n * n + 22 * n];
   double A[n * n];
-  int piv[n];
+  int piv[n], perm[n];
+  BdfArrays ba;
   Work<double> w;
   {
     double* p = buf;
@@ -104,6 +107,8 @@ __global__ void __launch_bounds__(128) k_react_plain(DevMech M, Options o, Batch
     w.qd = nullptr;
     w.A = A;
     w.piv = piv;
+    w.perm = perm;
+    w.ba = &ba;
   }
   Team<1> tm;
   react_one<NS, 1, double, METHOD>(tm, M, o, w, b, c, dt);
@@ -120,7 +125,7 @@ __device__ __forceinline__ void react_team_body(const Team<TEAM>& tm, const DevM
 {
   const int team = threadIdx.x / TEAM;
   Work<LT> w;
-  carve<LT>(w, smem + (size_t)team * cell_bytes, M.nsp, M.nrxn);
+  carve<LT>(w, smem + (size_t)team * cell_bytes, NS, M.nrxn);
   const int tpb = blockDim.x / TEAM;
   if (persistent) {
     for (;;) {
@@ -141,7 +146,9 @@ __device__ __forceinline__ void react_team_body(const Team<TEAM>& tm, const DevM
 // 16-warp blocks (one block per SM, <= 168 / <= 128 registers) whose warps
 // share one rendezvous.
 template <int NS, typename LT, int METHOD, int TEAM, int MINB, bool SRK = false, int MAXT = 256>
-__global__ void __launch_bounds__(MAXT, MINB) k_react_team(DevMech M, Options o, Batch b, double dt, int* queue,
+__global__ void __launch_bounds__(MAXT, MINB) k_react_team(const __grid_constant__ DevMech M,
+                                                          const __grid_constant__ Options o,
+                                                          const __grid_constant__ Batch b, double dt, int* queue,
                                                           size_t cell_bytes, int persistent)
 {
   extern __shared__ __align__(16) char smem[];
@@ -153,7 +160,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_react_team(DevMech M, Options o,
     Team<TEAM> tm;
     const int team = threadIdx.x / TEAM;
     Work<LT> w;
-    carve<LT>(w, smem + (size_t)team * cell_bytes, M.nsp, M.nrxn);
+    carve<LT>(w, smem + (size_t)team * cell_bytes, NS, M.nrxn);
     const int tpb = blockDim.x / TEAM;
     if (persistent) {
       __shared__ int rv[3];

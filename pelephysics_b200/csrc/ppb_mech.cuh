@@ -367,13 +367,41 @@ __device__ __forceinline__ double mix_c(const Team<TEAM>& tm, const DevMech& M, 
 
 // mechanism.H GET_T_GIVEN_EY / GET_T_GIVEN_HY: Newton from the supplied T,
 // |step| <= 100 K, stop at |dT| < 1e-6 K, <= 200 iterations, linear
-// extrapolation outside [90, 4000] K (returns 1 there).
+// extrapolation outside [90, 4000] K (returns 1 there).  When the supplied T
+// lies in [90, 4000] K (the integrator's case: it is the previous T), the
+// bounds' energies and the first Newton iterate's energy and heat capacity
+// are summed in one pass over the species; every sum is formed in the order
+// mix_e / mix_e_c form it.
 template <int TEAM>
 __device__ int t_from_energy(const Team<TEAM>& tm, const DevMech& M, int EH, double e, const double* Y, double& t)
 {
   const double tmin = 90, tmax = 4000;
-  const double emin = mix_e(tm, M, EH, tmin, Y);
-  const double emax = mix_e(tm, M, EH, tmax, Y);
+  double t1 = t;
+  double emin, emax, e1 = 0.0, cv1 = 0.0;
+  const bool fused = !(t1 < tmin || t1 > tmax);
+  if (fused) {
+    const double imin = 1.0 / tmin, imax = 1.0 / tmax, i1 = 1.0 / t1;
+    double smin = 0.0, smax = 0.0, se = 0.0, sc = 0.0;
+    for (int s = tm.lane; s < M.nsp; s += TEAM) {
+      const double im = __ldg(M.imw + s);
+      const double ys = Y[s];
+      smin += Y[s] * (EH ? h_RT(M, s, tmin, imin) : u_RT(M, s, tmin, imin)) * im;
+      smax += Y[s] * (EH ? h_RT(M, s, tmax, imax) : u_RT(M, s, tmax, imax)) * im;
+      se += ys * (EH ? h_RT(M, s, t1, i1) : u_RT(M, s, t1, i1)) * im;
+      sc += ys * (EH ? cp_R(M, s, t1) : cv_R(M, s, t1)) * im;
+    }
+    smin = tm.sum(smin);
+    smax = tm.sum(smax);
+    se = tm.sum(se);
+    sc = tm.sum(sc);
+    emin = smin * (RU * tmin);
+    emax = smax * (RU * tmax);
+    e1 = se * (RU * t1);
+    cv1 = sc * RU;
+  } else {
+    emin = mix_e(tm, M, EH, tmin, Y);
+    emax = mix_e(tm, M, EH, tmax, Y);
+  }
   if (e < emin) {
     t = tmin - (emin - e) / mix_c(tm, M, EH, tmin, Y);
     return 1;
@@ -382,12 +410,16 @@ __device__ int t_from_energy(const Team<TEAM>& tm, const DevMech& M, int EH, dou
     t = tmax - (emax - e) / mix_c(tm, M, EH, tmax, Y);
     return 1;
   }
-  double t1 = t;
-  if (t1 < tmin || t1 > tmax) t1 = tmin + (tmax - tmin) / (emax - emin) * (e - emin);
+  if (!fused) t1 = tmin + (tmax - tmin) / (emax - emin) * (e - emin);
   for (int i = 0; i < 200; ++i) {
-    double e1, cv;
-    mix_e_c(tm, M, EH, t1, Y, e1, cv);
-    double dt = (e - e1) / cv;
+    double ec, cv;
+    if (i == 0 && fused) {
+      ec = e1;
+      cv = cv1;
+    } else {
+      mix_e_c(tm, M, EH, t1, Y, ec, cv);
+    }
+    double dt = (e - ec) / cv;
     if (dt > 100.) {
       dt = 100.;
     } else if (dt < -100.) {
@@ -499,41 +531,46 @@ __device__ __forceinline__ FoPack load_fo(const DevMech& M, int f)
 
 // Slot lists are sorted by species with repeats adjacent (a species of
 // order o fills o slots); the helpers walk them run by run so that each
-// product is formed exactly as from the (species, order) lists.
+// product is formed exactly as from the (species, order) lists.  Every slot
+// index is a compile-time constant (the loops unroll), so a packed record
+// stays in registers.
 
 // Phase space: product over runs of x^o, as phase_space() forms it.
 template <int K>
 __device__ __forceinline__ double slots_product(const unsigned char (&sp)[K], const double* sc)
 {
-  double p = 1.0;
-  int j = 0;
+  double p = 1.0, t = 1.0;
 #pragma unroll
   for (int i = 0; i < K; i++) {
-    if (i != j) continue;
-    int c = 1;
-    while (j + c < K && sp[j + c] == sp[j]) c++;
-    const double x = sc[sp[j]];
-    double t = x;
-    for (int q = 1; q < c; q++) t *= x;
-    p *= t;
-    j += c;
+    const double x = sc[sp[i]];
+    if (i == 0) {
+      t = x;
+    } else if (sp[i] != sp[i - 1]) {
+      p *= t;
+      t = x;
+    } else {
+      t *= x;
+    }
   }
-  return p;
+  return p * t;
 }
 
-// d(phase space)/d sc[k], as dphase() forms it (jacobian.py:1398-1515).
+// d(phase space)/d sc[k], as dphase() forms it (jacobian.py:1398-1515): a run
+// of species k of order o multiplies by o and then o-1 times by x (nothing
+// for o = 1), another run by x^o.
 template <int K>
 __device__ __forceinline__ double slots_dproduct(const unsigned char (&sp)[K], const double* sc, int k)
 {
   double p = 1.0;
-  int j = 0;
 #pragma unroll
   for (int i = 0; i < K; i++) {
-    if (i != j) continue;
+    if (i > 0 && sp[i] == sp[i - 1]) continue; // not the start of a run
     int c = 1;
-    while (j + c < K && sp[j + c] == sp[j]) c++;
-    const double x = sc[sp[j]];
-    if (sp[j] == k) {
+#pragma unroll
+    for (int q = i + 1; q < K; q++)
+      if (q == i + c && sp[q] == sp[i]) c++;
+    const double x = sc[sp[i]];
+    if (sp[i] == k) {
       if (c > 1) {
         p *= (double)c;
         for (int q = 1; q < c; q++) p *= x;
@@ -543,7 +580,6 @@ __device__ __forceinline__ double slots_dproduct(const unsigned char (&sp)[K], c
       for (int q = 1; q < c; q++) t *= x;
       p *= t;
     }
-    j += c;
   }
   return p;
 }
@@ -552,18 +588,20 @@ __device__ __forceinline__ double slots_dproduct(const unsigned char (&sp)[K], c
 template <int K>
 __device__ __forceinline__ double slots_hsum(const unsigned char (&sp)[K], const double* h)
 {
-  double s = 0.0;
-  int j = 0;
+  double s = 0.0, v = 0.0;
+  int c = 0;
 #pragma unroll
   for (int i = 0; i < K; i++) {
-    if (i != j) continue;
-    int c = 1;
-    while (j + c < K && sp[j + c] == sp[j]) c++;
-    const double v = h[sp[j]];
-    s += (c == 1) ? v : (double)c * v;
-    j += c;
+    const bool start = (i == 0) || (sp[i] != sp[i - 1]);
+    if (start) {
+      if (i > 0) s += (c == 1) ? v : (double)c * v;
+      v = h[sp[i]];
+      c = 1;
+    } else {
+      c++;
+    }
   }
-  return s;
+  return s + ((c == 1) ? v : (double)c * v);
 }
 
 template <int K>
@@ -632,6 +670,28 @@ struct RateScratch {
   double* jx = nullptr; // [4 nrxn] per-reaction Jacobian factors (TEAM > 1)
 };
 
+// The reactions and the species gather of productionRate for a team of
+// lanes (TEAM > 1), given g/RT in rs.g (0 in the padding slot), sc with 1 in
+// its padding slot, and the temperature terms and mixture concentration.
+template <int TEAM>
+__device__ __forceinline__ void production_rate_core(const Team<TEAM>& tm, const DevMech& M, double* wdot,
+                                                     const double* sc_in, double T, double invT, double logT,
+                                                     double refC, double refCinv, double mixture, RateScratch& rs)
+{
+  for (int r = tm.lane; r < M.nrxn; r += TEAM) {
+    const RxPack p = load_rx(M, r);
+    rs.qd[r] = rx_qdot_packed(M, p, T, invT, logT, refC, refCinv, mixture, sc_in, rs.g);
+  }
+  tm.sync();
+  for (int s = tm.lane; s < M.nsp; s += TEAM) {
+    double w = 0.0;
+    const int g1 = __ldg(M.wg_off + s + 1);
+    for (int gi = __ldg(M.wg_off + s); gi < g1; gi++) w += __ldg(M.wg_c + gi) * rs.qd[__ldg(M.wg_rx + gi)];
+    wdot[s] = w;
+  }
+  tm.sync();
+}
+
 // productionRate (SI): wdot[s] for s owned by the lane (team-shared wdot).
 template <int TEAM>
 __device__ void production_rate(
@@ -672,17 +732,8 @@ __device__ void production_rate(
     // g[nsp] = 0
     if (tm.lane == 0) rs.g[M.nsp] = 0.0;
     tm.sync();
-    for (int r = tm.lane; r < M.nrxn; r += TEAM) {
-      const RxPack p = load_rx(M, r);
-      rs.qd[r] = rx_qdot_packed(M, p, T, invT, logT, refC, refCinv, mixture, sc_in, rs.g);
-    }
-    tm.sync();
-    for (int s = tm.lane; s < M.nsp; s += TEAM) {
-      double w = 0.0;
-      const int g1 = __ldg(M.wg_off + s + 1);
-      for (int gi = __ldg(M.wg_off + s); gi < g1; gi++) w += __ldg(M.wg_c + gi) * rs.qd[__ldg(M.wg_rx + gi)];
-      wdot[s] = w;
-    }
+    production_rate_core(tm, M, wdot, sc_in, T, invT, logT, refC, refCinv, mixture, rs);
+    return;
   }
   tm.sync();
 }

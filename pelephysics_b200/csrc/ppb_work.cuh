@@ -18,12 +18,13 @@ __host__ __device__ inline size_t a_region_bytes(int N, int R)
   return (a + 15) & ~size_t(15);
 }
 
+// pivots and row permutation (2n ints), then the coefficient arrays
 template <typename LT>
 __host__ __device__ inline size_t team_bytes(int N, int R)
 {
   const int n = N + 1;
   size_t d = (size_t)n * n + 22 * (size_t)n + (size_t)R;
-  size_t b = d * 8 + a_region_bytes<LT>(N, R) + 4 * (size_t)n;
+  size_t b = d * 8 + a_region_bytes<LT>(N, R) + ((8 * (size_t)n + 7) & ~size_t(7)) + sizeof(BdfArrays);
   return (b + 15) & ~size_t(15);
 }
 
@@ -57,6 +58,8 @@ __device__ inline void carve(Work<LT>& w, char* base, int N, int R)
   w.qd = p; p += R;
   w.A = (LT*)p;
   w.piv = (int*)((char*)p + a_region_bytes<LT>(N, R));
+  w.perm = w.piv + n;
+  w.ba = (BdfArrays*)((char*)w.piv + ((8 * (size_t)n + 7) & ~size_t(7)));
 }
 
 

@@ -9,12 +9,16 @@ oracle over the reference's own compiled mechanism kernels (oracle/_ref):
   1e-10), every cell, orders <= 5 and the reference default <= 2.
 
 The bar is T within 1e-6 relative and Y_k within 1e-8 absolute.  A cell whose
-mass fractions differ by more than 1e-8 from the oracle's is held to the
-oracle integrated from 1-ulp neighbours of its input (compare_to_reference
-in oracle/pyoracle.py): at rtol = 1e-10 the CVODE algorithm itself takes a
-different step sequence on some cells when one input component moves by one
-ulp, and those sequences end up to 6.5e-8 apart in Y.  The number of such
-cells is bounded too.
+mass fractions differ by more than 1e-8 from the oracle's is held to 16
+replicas of the oracle whose right-hand-side values are moved by at most one
+ulp (compare_to_reference in oracle/pyoracle.py): at rtol = 1e-10 the CVODE
+algorithm takes a different step sequence on some cells when its arithmetic
+changes in the last bit, and those sequences end up to 6.5e-8 apart in Y
+(the oracle over a table-driven restatement of the reference's kernels is
+that far from the oracle over the kernels themselves, on the same cells).
+Such a cell passes when it lies within 1e-8 of a replica or within the
+replicas' spread around the reference; at most 0.5 % of the cells may need
+that, and none may be further than 1e-7 from the reference.
 """
 
 import numpy as np
@@ -66,8 +70,9 @@ def _check(oracle, cells, idx, y_gpu, y_ref, opts, max_over_frac=0.005):
     r = oracle.compare_to_reference(cells.mech, cells.reactor_type, cells.rY[idx], cells.rYsrc[idx], cells.rX[idx],
                                     cells.rX_src[idx], cells.dt, y_gpu, y_ref, use_ref_kernels=1, **opts)
     assert r["max_rel_T"] <= 1e-6, r
-    assert r["max_abs_Y_nearest_of_1ulp_neighbours"] <= 1e-8, r
+    assert r["cells_failing"] == 0, r
     assert r["cells_over_Y_atol"] <= max_over_frac * r["cells"], r
+    assert r["max_abs_Y"] <= 1e-7, r
     return r
 
 

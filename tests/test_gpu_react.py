@@ -312,7 +312,7 @@ def test_autotuner_choice_is_reproducible(cuda, oracle, mech):
     xs = torch.as_tensor(rXs, device="cuda")
     ra.react(y, s, x, xs, dt)
     wpb, team, regs, ms = ra.launch_config()
-    assert ms > 0 and wpb in (1, 2, 4, 8) and team in (16, 32) and regs in (1, 2)
+    assert ms > 0 and wpb in (1, 2, 4, 8, 12, 16) and team in (16, 32) and regs in (1, 2)
     rb = Reactor(mech)
     rb.init(rtype, nc, **opts, warps_per_block=wpb, team_lanes=team, register_budget=regs)
     assert rb.launch_config()[:3] == (wpb, team, regs)
@@ -418,3 +418,45 @@ def test_block_rendezvous_changes_no_bits(cuda, oracle, wpb, cyc):
                                       atol=1e-10, max_order=5)
     assert flag == 0
     compare(outs[1][idx], ref)
+
+
+def test_react_inside_a_callers_graph_capture(cuda, oracle):
+    """A react on device arrays issued inside the caller's own stream capture
+    only enqueues its kernels (no internal graph, no wait): the caller's graph
+    replays it, and every replay gives the bits of a direct call.  Scratch
+    comes from init (ncells), the launch is fixed (no autotuner in a capture);
+    the host-array path refuses the capture."""
+    torch = cuda
+    mech, nc, dt = "drm19", 256, 1e-5
+    rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 31, 1100.0, 1000.0, 0.6, 0.8)
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5, warps_per_block=8, team_lanes=32, register_budget=2)
+    y0 = torch.as_tensor(rY.T.copy(), device="cuda")
+    s0 = torch.as_tensor(src.T.copy(), device="cuda")
+    x0 = torch.as_tensor(rX, device="cuda")
+    xs = torch.as_tensor(rXs, device="cuda")
+    rd = Reactor(mech)
+    rd.init(1, nc, **opts)
+    yd, xd = y0.clone(), x0.clone()
+    rd.react_soa(yd, s0, xd, xs, dt)
+    torch.cuda.synchronize()
+    r = Reactor(mech)
+    r.init(1, nc, **opts)
+    y, x = y0.clone(), x0.clone()
+    stream = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        cost, _, _, code = r.react_soa(y, s0, x, xs, dt, stream=stream)
+    assert code == 0 and cost == 0  # nothing read back inside the capture
+    for _ in range(2):
+        y.copy_(y0)
+        x.copy_(x0)
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(y, yd) and torch.equal(x, xd)
+    status, costs = r.cell_status(nc)
+    assert np.all(status == 0) and np.all(costs > 0)
+    # the host-array path copies and waits: refused inside a capture
+    g2 = torch.cuda.CUDAGraph()
+    with pytest.raises(_lib.EngineError, match="stream capture"):
+        with torch.cuda.graph(g2, stream=stream):
+            r.react(rY.copy(), src.copy(), rX.copy(), rXs.copy(), dt, stream=stream)
