@@ -295,7 +295,9 @@ __device__ AdjPoint rhs_exact_jacobian(const Team<TEAM>& tm, const DevMech& M, i
         const double d = __ldg(ed + k) * fac;
         if (d == 0.0) continue;
         double* Jk = a.Jc + k * n;
-        for (int j = 0; j < p.njn; j++) {
+        #pragma unroll
+        for (int j = 0; j < 6; j++) { // static slot index: the record stays in registers
+          if (j >= p.njn) break;
           const double nu = (double)p.jnc[j];
           if (nu != 0) Jk[p.jns[j]] += nu * d;
         }
@@ -318,7 +320,9 @@ __device__ AdjPoint rhs_exact_jacobian(const Team<TEAM>& tm, const DevMech& M, i
       double d = 0.0;
       if (inr) d += a.jxa[5 * r + 0] * slots_dproduct(p.fsp, w.sc, k);
       if (inp) d -= a.jxa[5 * r + 1] * slots_dproduct(p.rsp, w.sc, k);
-      for (int j = 0; j < p.njn; j++) {
+      #pragma unroll
+        for (int j = 0; j < 6; j++) { // static slot index: the record stays in registers
+          if (j >= p.njn) break;
         const double nu = (double)p.jnc[j];
         if (nu != 0) Jk[p.jns[j]] += nu * d;
       }

@@ -82,7 +82,7 @@ __device__ void restore_cp(const Team<32>& tm, const char* src, B& bdf, Work<LT>
     for (int i = tm.lane; i < n; i += 32) w.zn[j][i] = z[j * n + i];
   for (int i = tm.lane; i < n; i += 32) w.ewt[i] = z[6 * n + i];
   const double* J = z + 7 * n;
-  for (int i = tm.lane; i < n * n; i += 32) w.J[i] = J[i];
+  for (int i = tm.lane; i < n * n; i += 32) w.J[i] = (LT)J[i];
   const LT* A = reinterpret_cast<const LT*>(J + n * n);
   for (int i = tm.lane; i < n * n; i += 32) w.A[i] = A[i];
   const int* piv = reinterpret_cast<const int*>(A + n * n);

@@ -51,7 +51,10 @@ template <typename LT>
 struct Work {
   double* zn[6];
   double *ewt, *acor, *y, *tempv, *ftemp, *delta;
-  double *J, *src, *atolv;
+  double *src, *atolv;
+  LT* J;        // saved Jacobian (the factor's precision)
+  double* jtmp; // where the Jacobian is evaluated in FP64 (J itself for FP64)
+  double* jx;   // per-reaction factors of the Jacobian evaluation
   LT* A;
   int* piv;
   int* perm;  // row order of the factored matrix: row i of PA is row perm[i] of A
@@ -428,9 +431,11 @@ __device__ __forceinline__ void lu_solve_reg(const Team<TEAM>& tm, const LT* A, 
 }
 
 // ---------------------------------------------------------------- BDF
-// The integrator's coefficient arrays, indexed by order at run time: one
-// team-shared copy per cell (in registers they would force the integrator's
-// whole state to local memory).
+// The integrator's coefficient arrays, indexed by order at run time (in
+// registers they would force the integrator's whole state to local memory):
+// one shared copy per warp of a cell's team.  The first lane of the warp
+// writes them and the warp synchronises before they are read, so their
+// read-modify-write updates never race.
 struct BdfArrays {
   double tau[7], tq[6], l[6];
 };
@@ -451,19 +456,20 @@ struct CellIn {
   double rhoe, rhoesrc;
 };
 
-// The integrator's right-hand side at (t, y) into fy: the block rendezvous
-// (when on), then fKernelSpec.  Out of line, so that the kernel holds one
-// copy of the right-hand side; a free function taking what it reads, so that
-// no caller's state has to live in memory for the call.
+// The integrator's right-hand side at (t, y) into fy (fKernelSpec).  A free
+// function taking what it reads, so that no caller's state has to live in
+// memory for the call.  Inlined at its call sites by default (drm19 64^3:
+// 909k against 837k cells/s out of line, which keeps one copy of the
+// right-hand side in the kernel; build with -DPPB_RHS_ATTR=__noinline__ for
+// that form).
 #ifndef PPB_RHS_ATTR
-#define PPB_RHS_ATTR __noinline__
+#define PPB_RHS_ATTR __forceinline__
 #endif
 template <int TEAM, bool SRK>
-__device__ PPB_RHS_ATTR void bdf_rhs(Team<TEAM> tm, const DevMech& M, int rtype, int* rv, int rcycles, double t,
-                                     const double* y, double* fy, double rhoe, double rhoesrc, const double* src,
-                                     double* Y, double* sc, double* g, double* qd, double* wdot, double* ei)
+__device__ PPB_RHS_ATTR void bdf_rhs(Team<TEAM> tm, const DevMech& M, int rtype, double t, const double* y,
+                                     double* fy, double rhoe, double rhoesrc, const double* src, double* Y,
+                                     double* sc, double* g, double* qd, double* wdot, double* ei)
 {
-  if (rv) rendezvous(rv, rcycles);
   if constexpr (SRK) {
     reactor_rhs_srk<TEAM>(tm, M, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei);
   } else {
@@ -493,8 +499,20 @@ struct Bdf {
   Rec rec;
 
   __device__ Bdf(const Team<TEAM>& t, const DevMech& m, const Options& op, Work<LT>& wk, CellIn ci)
-    : tm(t), M(m), o(op), w(wk), cin(ci), ar(*wk.ba)
+    : tm(t), M(m), o(op), w(wk), cin(ci), ar(wk.ba[TEAM > 32 ? (t.lane >> 5) : 0])
   {
+  }
+
+  // the lane that writes this warp's copy of the coefficient arrays
+  __device__ __forceinline__ bool lead() const { return (tm.lane % Team<TEAM>::W) == 0; }
+  // the warp (or the team's part of it) sees the copy's latest writes
+  __device__ __forceinline__ void wsync() const
+  {
+    if constexpr (TEAM > 32) {
+      __syncwarp();
+    } else if constexpr (TEAM > 1) {
+      __syncwarp(tm.mask);
+    }
   }
 
   __device__ __forceinline__ double wrms(const double* v) const
@@ -516,11 +534,13 @@ struct Bdf {
     tm.sync();
   }
 
+  // the block rendezvous (when on), then the right-hand side
   __device__ __forceinline__ void f(double t, const double* y, double* fy)
   {
+    if (w.rv) rendezvous(w.rv, o.rendezvous);
     PPB_TIC(PH_RHS);
-    bdf_rhs<TEAM, SRK>(tm, M, o.reactor_type, w.rv, o.rendezvous, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc,
-                       w.g, w.qd, w.wdot, w.ei);
+    bdf_rhs<TEAM, SRK>(tm, M, o.reactor_type, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
+                       w.ei);
     s.nfe++;
     PPB_TOC(PH_RHS);
   }
@@ -533,10 +553,36 @@ struct Bdf {
     } else {
       // the Newton matrix region is free while the Jacobian is formed: it
       // holds the per-reaction factors of the warp-cooperative evaluation
-      reactor_jac<TEAM, PER>(tm, M, o.reactor_type, w.y, w.J, w.sc, w.g, w.wdot, w.Y, w.ei, w.h1, w.h2,
-                             TEAM > 1 ? w.qd : nullptr, TEAM > 1 ? reinterpret_cast<double*>(w.A) : nullptr);
+      reactor_jac<TEAM, PER>(tm, M, o.reactor_type, w.y, w.jtmp, w.sc, w.g, w.wdot, w.Y, w.ei, w.h1, w.h2,
+                             TEAM > 1 ? w.qd : nullptr, TEAM > 1 ? w.jx : nullptr);
+      if constexpr (sizeof(LT) != sizeof(double)) jac_to_lt();
     }
     PPB_TOC(PH_JAC);
+  }
+
+  // The FP64 Jacobian in w.jtmp, rounded to the factor's precision in
+  // place: chunk by chunk, every lane holds its entries of a chunk in
+  // registers before any lane writes, and an entry's FP32 slot lies at or
+  // below the FP64 entries already read.
+  __device__ __forceinline__ void jac_to_lt()
+  {
+    constexpr int CH = 8;
+    const int nn = n * n;
+    for (int base = 0; base < nn; base += CH * TEAM) {
+      double v[CH];
+#pragma unroll
+      for (int q = 0; q < CH; q++) {
+        const int i = base + q * TEAM + tm.lane;
+        v[q] = (i < nn) ? w.jtmp[i] : 0.0;
+      }
+      tm.sync();
+#pragma unroll
+      for (int q = 0; q < CH; q++) {
+        const int i = base + q * TEAM + tm.lane;
+        if (i < nn) w.J[i] = (LT)v[q];
+      }
+      tm.sync();
+    }
   }
 
   // Difference-quotient dense Jacobian at (tn, y) with f(tn, y) in ftemp:
@@ -649,7 +695,14 @@ struct Bdf {
     tm.sync();
   }
 
+  // the coefficients of order q: written by the lead lane only
   __device__ __forceinline__ void set_bdf()
+  {
+    if (lead()) set_bdf_lead();
+    wsync();
+  }
+
+  __device__ __forceinline__ void set_bdf_lead()
   {
     double alpha0, alpha0_hat, xi_inv, xistar_inv, hsum;
     const int q = s.q;
@@ -722,7 +775,7 @@ struct Bdf {
     PPB_TIC(PH_LU);
     for (int i = tm.lane; i < n; i += TEAM) {
       for (int j = 0; j < n; j++) {
-        double v = -s.gamma * w.J[j * n + i];
+        double v = -s.gamma * (double)w.J[j * n + i];
         if (i == j) v += 1.0;
         w.A[j * n + i] = (LT)v;
       }
@@ -772,7 +825,7 @@ struct Bdf {
       for (int i = tm.lane; i < n; i += TEAM) {
         double ax = w.delta[i];
         double jx = 0.0;
-        for (int j = 0; j < n; j++) jx += w.J[j * n + i] * w.delta[j];
+        for (int j = 0; j < n; j++) jx += (double)w.J[j * n + i] * w.delta[j];
         ax -= s.gamma_lu * jx;
         w.tempv[i] = b[i] - ax;
       }
@@ -870,8 +923,12 @@ struct Bdf {
   __device__ __forceinline__ void increase_bdf()
   {
     double alpha0, alpha1, prod, xi, xiold, hsum, A1;
-    for (int i = 0; i <= s.qmax; i++) ar.l[i] = 0.0;
-    ar.l[2] = alpha1 = prod = xiold = 1.0;
+    const bool ld = lead();
+    if (ld) {
+      for (int i = 0; i <= s.qmax; i++) ar.l[i] = 0.0;
+      ar.l[2] = 1.0;
+    }
+    alpha1 = prod = xiold = 1.0;
     alpha0 = -1.0;
     hsum = s.hscale;
     if (s.q > 1) {
@@ -881,10 +938,12 @@ struct Bdf {
         prod *= xi;
         alpha0 -= 1.0 / (j + 1);
         alpha1 += 1.0 / xi;
-        for (int i = j + 2; i >= 2; i--) ar.l[i] = ar.l[i] * xiold + ar.l[i - 1];
+        if (ld)
+          for (int i = j + 2; i >= 2; i--) ar.l[i] = ar.l[i] * xiold + ar.l[i - 1];
         xiold = xi;
       }
     }
+    wsync();
     A1 = (-alpha0 - alpha1) / prod;
     for (int i = tm.lane; i < n; i += TEAM) {
       const double zL = A1 * w.zn[s.indx_acor][i];
@@ -897,15 +956,17 @@ struct Bdf {
 
   __device__ __forceinline__ void decrease_bdf()
   {
-    double hsum, xi;
-    for (int i = 0; i <= s.qmax; i++) ar.l[i] = 0.0;
-    ar.l[2] = 1.0;
-    hsum = 0.0;
-    for (int j = 1; j <= s.q - 2; j++) {
-      hsum += ar.tau[j];
-      xi = hsum / s.hscale;
-      for (int i = j + 2; i >= 2; i--) ar.l[i] = ar.l[i] * xi + ar.l[i - 1];
+    if (lead()) {
+      for (int i = 0; i <= s.qmax; i++) ar.l[i] = 0.0;
+      ar.l[2] = 1.0;
+      double hsum = 0.0;
+      for (int j = 1; j <= s.q - 2; j++) {
+        hsum += ar.tau[j];
+        const double xi = hsum / s.hscale;
+        for (int i = j + 2; i >= 2; i--) ar.l[i] = ar.l[i] * xi + ar.l[i - 1];
+      }
     }
+    wsync();
     for (int i = tm.lane; i < n; i += TEAM)
       for (int j = 2; j < s.q; j++) w.zn[j][i] -= ar.l[j] * w.zn[s.q][i];
     tm.sync();
@@ -975,9 +1036,12 @@ struct Bdf {
   {
     s.nst++;
     s.hu = s.h;
-    for (int i = s.q; i >= 2; i--) ar.tau[i] = ar.tau[i - 1];
-    if ((s.q == 1) && (s.nst > 1)) ar.tau[2] = ar.tau[1];
-    ar.tau[1] = s.h;
+    if (lead()) {
+      for (int i = s.q; i >= 2; i--) ar.tau[i] = ar.tau[i - 1];
+      if ((s.q == 1) && (s.nst > 1)) ar.tau[2] = ar.tau[1];
+      ar.tau[1] = s.h;
+    }
+    wsync();
     const bool save = ((s.qwait - 1) == 1) && (s.q != s.qmax);
     if constexpr (Rec::on) {
       rec.predict(tm, s.q);
@@ -1105,8 +1169,7 @@ struct Bdf {
   __device__ __forceinline__ int start(double tout)
   {
     s = BdfScalars{};
-    for (int i = tm.lane; i < (int)(sizeof(BdfArrays) / sizeof(double)); i += TEAM)
-      reinterpret_cast<double*>(&ar)[i] = 0.0;
+    if (lead()) ar = BdfArrays{};
     // no factorisation yet: identity pivots and row order (a checkpoint taken
     // before the first step holds valid ones)
     for (int i = tm.lane; i < n; i += TEAM) {

@@ -93,7 +93,10 @@ __global__ void __launch_bounds__(128) k_react_plain(const __grid_constant__ Dev
     w.tempv = p; p += n;
     w.ftemp = p; p += n;
     w.delta = p; p += n;
-    w.J = p; p += n * n;
+    w.J = p;
+    w.jtmp = p;
+    w.jx = nullptr;
+    p += n * n;
     w.src = p; p += n;
     w.atolv = p; p += n;
     w.Y = p; p += n;
@@ -121,11 +124,12 @@ __global__ void __launch_bounds__(128) k_react_plain(const __grid_constant__ Dev
 template <int NS, typename LT, int METHOD, int TEAM>
 __device__ __forceinline__ void react_team_body(const Team<TEAM>& tm, const DevMech& M, const Options& o,
                                                 const Batch& b, double dt, int* queue, size_t cell_bytes,
-                                                int persistent, char* smem)
+                                                int persistent, char* smem, BdfArrays* warp_arrays)
 {
   const int team = threadIdx.x / TEAM;
   Work<LT> w;
   carve<LT>(w, smem + (size_t)team * cell_bytes, NS, M.nrxn);
+  w.ba = warp_arrays; // one copy of the coefficient arrays per warp of the team
   const int tpb = blockDim.x / TEAM;
   if (persistent) {
     for (;;) {
@@ -154,8 +158,9 @@ __global__ void __launch_bounds__(MAXT, MINB) k_react_team(const __grid_constant
   extern __shared__ __align__(16) char smem[];
   if constexpr (TEAM > 32) {
     __shared__ double red[16];
+    __shared__ BdfArrays warp_arrays[TEAM / 32];
     const Team<TEAM> tm(red);
-    react_team_body<NS, LT, METHOD, TEAM>(tm, M, o, b, dt, queue, cell_bytes, persistent, smem);
+    react_team_body<NS, LT, METHOD, TEAM>(tm, M, o, b, dt, queue, cell_bytes, persistent, smem, warp_arrays);
   } else {
     Team<TEAM> tm;
     const int team = threadIdx.x / TEAM;

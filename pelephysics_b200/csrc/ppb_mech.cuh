@@ -1067,7 +1067,9 @@ __device__ void ajacobian_packed(
         apply = inr || inp;
       }
       if (apply) {
-        for (int j = 0; j < p.njn; j++) {
+        #pragma unroll
+        for (int j = 0; j < 6; j++) { // static slot index: the record stays in registers
+          if (j >= p.njn) break;
           const double nu = (double)p.jnc[j];
           if (nu != 0) Jk[p.jns[j]] += nu * d;
         }
