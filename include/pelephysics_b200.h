@@ -58,8 +58,8 @@ typedef struct ppb_options {
   int engine;               /* PPB_ENGINE_TUNED */
   int lu_fp32;              /* factor I - gamma J in FP32 + FP64 refinement, 0 */
   int refine_sweeps;        /* refinement sweeps with lu_fp32, 1 */
-  int warps_per_block;      /* tuned engine block size in warps (1, 2, 4, 8; 12 or 16 for the FP64 BDF with
-                               32 lanes per cell and budget 2: one block per SM); 0 = autotune the block
+  int warps_per_block;      /* tuned engine block size in warps (1, 2, 4, 8; 12 or 16 for the BDF, either LU
+                               precision, with 32 lanes per cell and budget 2: one block per SM); 0 = autotune the block
                                size, lanes per cell and register budget on the first call */
   int use_graph;            /* replay react() as a captured CUDA graph, 1 */
   int adjoint_checkpoint_interval; /* accepted BDF steps between adjoint checkpoints, 16 */

@@ -1,7 +1,7 @@
 """Build the engine's shared library for sm_100a: pelephysics_b200/libppb200.so.
 
 The kernels are compiled once per species count of the shipped mechanisms
-(ppb_engine_ns.cu with -DPPB_NS=<N>, in four kernel groups -DPPB_PART=0..3),
+(ppb_engine_ns.cu with -DPPB_NS=<N>, in five kernel groups -DPPB_PART=0..4),
 in parallel, then linked with the
 common kernels and the C-ABI layer.  Objects are rebuilt only when a source
 or header is newer.  Usage: ``python -m pelephysics_b200.build [-j N]``.
@@ -39,7 +39,7 @@ def _units():
         ("ppb_transport.o", "ppb_transport.cu", []),
     ]
     for ns in SPECIES_COUNTS:
-        for part in range(4):  # the kernel groups of one species count, compiled in parallel
+        for part in range(5):  # the kernel groups of one species count, compiled in parallel
             units.append((f"ppb_engine_ns{ns}_p{part}.o", "ppb_engine_ns.cu", [f"-DPPB_NS={ns}", f"-DPPB_PART={part}"]))
     for ns in SPECIES_COUNTS:
         units.append((f"ppb_adjoint_ns{ns}.o", "ppb_adjoint_ns.cu", [f"-DPPB_NS={ns}"]))

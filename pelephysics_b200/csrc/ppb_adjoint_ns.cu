@@ -14,8 +14,12 @@
 //      once, the exact Jacobian, df/dE, the rate derivatives and the FP64
 //      factor of (I - gamma Jc)^T; k_adj_sweep applies the transposed
 //      operations in reverse order with those stored factors.
-// Tangent (k_tangent): each segment's tape is swept forward right after it
-// is recorded, one warp per cell.
+// Tangent (k_adj_seg, tangent mode): each segment's tape (per warp) is swept
+// forward right after it is recorded, one warp per cell.  The adjoint's
+// forward run, its recomputations and the tangent all integrate through the
+// one call site of the integrator in k_adj_seg: two kernels holding their own
+// inlined copies of the integrator may contract multiply-adds differently,
+// and the stiff cells' step sequences then part in the last bit.
 #include <algorithm>
 #include <vector>
 
@@ -91,101 +95,6 @@ __device__ void restore_cp(const Team<32>& tm, const char* src, B& bdf, Work<LT>
   perm_from_piv(tm, w.piv, w.perm, n);
 }
 
-// Tangent-linear integration of one cell: each segment's tape is swept
-// forward right after it is recorded.
-template <int NS, typename LT>
-__device__ void tangent_cell(const Team<32>& tm, const DevMech& M, const Options& o, Work<LT>& w, AdjWork& a,
-                             const AdjBatch& b, const AdjLayout& L, TapeRec* tape, double* ys, int c, double dt)
-{
-  constexpr int n = NS + 1;
-  constexpr int PER = (NS + 31) / 32;
-  const double* y0 = b.y0 + (size_t)c * n;
-  for (int i = tm.lane; i < n; i += 32) {
-    w.zn[0][i] = y0[i];
-    w.y[i] = y0[i];
-    w.src[i] = (i < NS && b.src) ? b.src[(size_t)c * NS + i] : 0.0;
-    if (o.use_typ_vals) w.atolv[i] = b.atolv[i];
-  }
-  tm.sync();
-  const CellIn cin{b.rhoe[c], b.rhoesrc ? b.rhoesrc[c] : 0.0};
-  Bdf<NS, 32, LT, AdjRec<32>> bdf(tm, M, o, w, cin);
-  bdf.rec.tape = tape;
-  bdf.rec.ys = ys;
-  bdf.rec.n = n;
-  bdf.rec.seg_steps = L.seg_steps;
-  bdf.rec.close_rec = L.close_rec;
-  bdf.rec.close_y = L.close_y;
-  bdf.rec.begin();
-  AdjSweep<32, PER, LT> sw{tm, M, o, w, a, cin, n, o.max_order};
-  int flag = bdf.start(dt);
-  int nstloc = 0;
-  bool done = false;
-  for (int i = tm.lane; i < 6 * n; i += 32) a.lam[i] = 0.0;
-  for (int i = tm.lane; i < n; i += 32) a.pend[i] = 0.0;
-  tm.sync();
-  const double dE = b.dE ? b.dE[c] : 0.0;
-  if (flag == ST_OK) {
-    // z_0 = y0, z_1 = h0 f(0, y0)
-    for (int i = tm.lane; i < n; i += 32) a.lam[i] = b.dy0 ? b.dy0[(size_t)c * n + i] : 0.0;
-    tm.sync();
-    sw.fwd_freset(0.0, bdf.rec.h0, y0, dE, b.dp);
-    for (;;) {
-      flag = bdf.advance(dt, nstloc, done);
-      if (flag != ST_OK) break;
-      flag = sw.forward(tape, bdf.rec.nrec, ys, dE, b.dp, a.tmp);
-      if (flag != ST_OK || done) break;
-      bdf.rec.begin();
-    }
-  }
-  if (b.lam_y0)
-    for (int i = tm.lane; i < n; i += 32) b.lam_y0[(size_t)c * n + i] = (flag == ST_OK) ? a.tmp[i] : 0.0;
-  if (b.y_out)
-    for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = (flag == ST_OK) ? w.y[i] : w.zn[0][i];
-  if (tm.lane == 0) {
-    if (b.status) b.status[c] = flag;
-    if (b.stats) {
-      int* st = b.stats + (size_t)c * 7;
-      st[0] = bdf.s.nst;
-      st[1] = bdf.s.nfe;
-      st[2] = bdf.s.nje;
-      st[3] = bdf.s.nsetups;
-      st[4] = bdf.s.nni;
-      st[5] = bdf.s.netf;
-      st[6] = bdf.s.ncfn;
-    }
-  }
-  tm.sync();
-}
-
-template <int NS, typename LT>
-__global__ void __launch_bounds__(256) k_tangent(const __grid_constant__ DevMech M, const __grid_constant__ Options o,
-                                                 const __grid_constant__ AdjBatch b, const __grid_constant__ AdjLayout L,
-                                                 double dt, int* queue)
-{
-  extern __shared__ __align__(16) char smem[];
-  Team<32> tm;
-  const int R = M.nrxn;
-  const int warp = threadIdx.x / 32;
-  const size_t gwarp = (size_t)blockIdx.x * (blockDim.x / 32) + warp;
-  char* base = smem + (size_t)warp * L.warp_smem;
-  Work<LT> w;
-  carve<LT>(w, base, NS, R);
-  __shared__ int rv[3];
-  w.rv = rendezvous_init(rv, blockDim.x / 32, o.rendezvous);
-  AdjWork a;
-  carve_adj(a, base + team_bytes<LT>(NS, R), NS, R);
-  TapeRec* tape = reinterpret_cast<TapeRec*>(L.tape) + gwarp * (size_t)L.cap_rec;
-  double* ys = L.ys + gwarp * (size_t)L.cap_y * (NS + 1);
-  for (;;) {
-    int c = 0;
-    if (tm.lane == 0) c = atomicAdd(queue, 1);
-    c = __shfl_sync(0xffffffffu, c, 0);
-    if (c >= b.ncells) break;
-    tangent_cell<NS, LT>(tm, M, o, w, a, b, L, tape, ys, c, dt);
-  }
-  rendezvous_leave(w.rv);
-}
-
 // Pointwise: f, df/dy, df/dE and, for a weight vector v per cell,
 // v^T df/dy, v^T df/dE and v^T df/dp (per cell) of the reactor RHS.
 template <int NS>
@@ -251,6 +160,195 @@ static __global__ void k_sum_cells(const double* gw, int nc, int np, double* out
   out[p] = s;
 }
 
+template <int NS>
+static int launch_rhs_exact_ns(const DevMech& M, int rtype, double t, const double* y, const double* rhoe,
+                               const double* rhoesrc, const double* src, const double* v, double* f_out,
+                               double* J_out, double* fE_out, double* vy_out, double* vE_out, double* vp_out,
+                               int ncells, cudaStream_t st)
+{
+  if (ncells <= 0) return 0;
+  const size_t wb = team_bytes<double>(NS, M.nrxn) + adj_bytes(NS, M.nrxn);
+  int wpb = 4;
+  while (wpb > 1 && wb * wpb > 200 * 1024) wpb--;
+  const size_t shm = wb * wpb;
+  cudaError_t e =
+    cudaFuncSetAttribute((const void*)k_rhs_exact<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  if (e != cudaSuccess) return (int)e;
+  k_rhs_exact<NS><<<(ncells + wpb - 1) / wpb, wpb * 32, shm, st>>>(M, rtype, t, y, rhoe, rhoesrc, src, v, f_out,
+                                                                   J_out, fE_out, vy_out, vE_out, vp_out, ncells, wb);
+  return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- batched
+// The modes of k_adj_seg.
+enum : int { SEG_FORWARD = 0, SEG_REPLAY = 1, SEG_TANGENT = 2 };
+
+// SEG_FORWARD: every cell from its initial state, a checkpoint at the start
+// of each segment, the last segment's tape left in place (tapes per cell).
+// SEG_REPLAY: recomputation of segment seg of every cell that has an earlier
+// segment; it must end where the forward run did (checked against the next
+// checkpoint).
+// SEG_TANGENT: every cell from its initial state, each segment's tape (per
+// warp) swept forward by the tangent-linear model as soon as it is recorded;
+// dy(t_end) goes to b.lam_y0.  Needs the adjoint workspace after the
+// integrator's in each warp's shared memory.
+// All modes share the one call site of start() and of advance(), so every
+// mode integrates with the same compiled arithmetic and their trajectories
+// agree bit for bit.
+template <int NS, typename LT>
+__global__ void __launch_bounds__(256) k_adj_seg(const __grid_constant__ DevMech M, const __grid_constant__ Options o,
+                                                 const __grid_constant__ AdjBatch b, const __grid_constant__ AdjCells C,
+                                                 double dt, int* queue, int seg, int mode, size_t warp_smem)
+{
+  extern __shared__ __align__(16) char smem[];
+  Team<32> tm;
+  constexpr int n = NS + 1;
+  const int R = M.nrxn;
+  const int warp = threadIdx.x / 32;
+  const bool replay = (mode == SEG_REPLAY);
+  const bool tangent = (mode == SEG_TANGENT);
+  const size_t gwarp = (size_t)blockIdx.x * (blockDim.x / 32) + warp;
+  char* base = smem + (size_t)warp * warp_smem;
+  Work<LT> w;
+  carve<LT>(w, base, NS, R);
+  AdjWork a;
+  if (tangent) carve_adj(a, base + team_bytes<LT>(NS, R), NS, R);
+  __shared__ int rv[3];
+  w.rv = rendezvous_init(rv, blockDim.x / 32, o.rendezvous);
+  for (;;) {
+    int c = 0;
+    if (tm.lane == 0) c = atomicAdd(queue, 1);
+    c = __shfl_sync(0xffffffffu, c, 0);
+    if (c >= b.ncells) break;
+    if (replay) {
+      // cells without a segment seg are idle; for a cell whose last segment
+      // is seg, the forward run left the tape (and its counts) in place
+      const int ns = C.nseg[c];
+      if (seg >= ns - 1) continue;
+    }
+    const double* y0 = b.y0 + (size_t)c * n;
+    for (int i = tm.lane; i < n; i += 32) {
+      w.src[i] = (i < NS && b.src) ? b.src[(size_t)c * NS + i] : 0.0;
+      if (o.use_typ_vals) w.atolv[i] = b.atolv[i];
+      if (!replay) {
+        w.zn[0][i] = y0[i];
+        w.y[i] = y0[i];
+      }
+    }
+    tm.sync();
+    const CellIn cin{b.rhoe[c], b.rhoesrc ? b.rhoesrc[c] : 0.0};
+    Bdf<NS, 32, LT, AdjRec<32>> bdf(tm, M, o, w, cin);
+    const size_t slot_t = tangent ? gwarp : (size_t)c; // the tape's owner
+    TapeRec* tape = reinterpret_cast<TapeRec*>(C.tape) + slot_t * C.cap_rec;
+    double* ys = C.ys + slot_t * C.cap_y * n;
+    bdf.rec.tape = tape;
+    bdf.rec.ys = ys;
+    bdf.rec.yinfo = (tangent || !C.yinfo) ? nullptr : C.yinfo + (size_t)c * C.cap_y * 2;
+    bdf.rec.n = n;
+    bdf.rec.seg_steps = C.seg_steps;
+    bdf.rec.close_rec = C.close_rec;
+    bdf.rec.close_y = C.close_y;
+    bdf.rec.begin();
+    AdjSweep<32, (NS + 31) / 32, LT> sw{tm, M, o, w, a, cin, n, o.max_order};
+    const double dE = (tangent && b.dE) ? b.dE[c] : 0.0;
+    int nstloc = 0, ncp = 0, flag = ST_OK;
+    bool done = false;
+    int* cpi = C.cp_idx + (size_t)c * C.max_seg;
+    if (!replay) {
+      flag = bdf.start(dt);
+      if (tangent) {
+        for (int i = tm.lane; i < 6 * n; i += 32) a.lam[i] = 0.0;
+        for (int i = tm.lane; i < n; i += 32) a.pend[i] = 0.0;
+        tm.sync();
+        if (flag == ST_OK) {
+          // z_0 = y0, z_1 = h0 f(0, y0)
+          for (int i = tm.lane; i < n; i += 32) a.lam[i] = b.dy0 ? b.dy0[(size_t)c * n + i] : 0.0;
+          tm.sync();
+          sw.fwd_freset(0.0, bdf.rec.h0, y0, dE, b.dp);
+        }
+      } else {
+        for (int i = tm.lane; i < 7 * n; i += 32) C.lam[(size_t)c * 7 * n + i] = 0.0;
+        for (int r = tm.lane; r < 3 * R; r += 32) C.gw[(size_t)c * 3 * R + r] = 0.0;
+        if (b.lam_y0)
+          for (int i = tm.lane; i < n; i += 32) b.lam_y0[(size_t)c * n + i] = 0.0;
+        if (tm.lane == 0) {
+          C.lamE[c] = 0.0;
+          if (b.lam_e) b.lam_e[c] = 0.0;
+        }
+      }
+    }
+    for (;;) {
+      if (flag != ST_OK) break;
+      if (mode == SEG_FORWARD) {
+        if (ncp >= C.max_seg) {
+          flag = ST_ADJ_CAPACITY;
+          break;
+        }
+        int slot = 0;
+        if (tm.lane == 0) slot = atomicAdd(C.pool_next, 1);
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (slot >= C.pool_cap) {
+          flag = ST_ADJ_CAPACITY;
+          break;
+        }
+        if (tm.lane == 0) cpi[ncp] = slot;
+        save_cp<NS, LT>(tm, C.cp_pool + (size_t)slot * C.cp_stride, bdf, w, nstloc);
+        ncp++;
+      } else if (replay) {
+        restore_cp<NS, LT>(tm, C.cp_pool + (size_t)cpi[seg] * C.cp_stride, bdf, w, nstloc);
+      }
+      bdf.rec.begin();
+      flag = bdf.advance(dt, nstloc, done);
+      if (tangent && flag == ST_OK) flag = sw.forward(tape, bdf.rec.nrec, ys, dE, b.dp, a.tmp);
+      if (flag != ST_OK || done || replay) break;
+    }
+    if (!replay) {
+      if (b.y_out)
+        for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = (flag == ST_OK) ? w.y[i] : w.zn[0][i];
+      if (tangent && b.lam_y0)
+        for (int i = tm.lane; i < n; i += 32) b.lam_y0[(size_t)c * n + i] = (flag == ST_OK) ? a.tmp[i] : 0.0;
+      if (tm.lane == 0) {
+        if (b.status) b.status[c] = flag;
+        if (b.stats) {
+          int* st = b.stats + (size_t)c * 7;
+          st[0] = bdf.s.nst;
+          st[1] = bdf.s.nfe;
+          st[2] = bdf.ar.nje;
+          st[3] = bdf.ar.nsetups;
+          st[4] = bdf.ar.nni;
+          st[5] = bdf.ar.netf;
+          st[6] = bdf.ar.ncfn;
+        }
+        if (!tangent) {
+          C.nseg[c] = (flag == ST_OK) ? ncp : 0;
+          C.h0[c] = bdf.rec.h0;
+          C.nrec[c] = bdf.rec.nrec;
+          C.ny[c] = bdf.rec.ny;
+        }
+      }
+    } else {
+      if (flag == ST_OK) {
+        // the recomputed segment must end where the forward run did
+        const BdfScalars* nx = reinterpret_cast<const BdfScalars*>(C.cp_pool + (size_t)cpi[seg + 1] * C.cp_stride);
+        if (nx->tn != bdf.s.tn || nx->nst != bdf.s.nst || nx->h != bdf.s.h) flag = ST_ADJ_REPLAY;
+      }
+      if (tm.lane == 0) {
+        if (flag != ST_OK) {
+          if (b.status) b.status[c] = flag;
+          C.nseg[c] = 0;
+          C.nrec[c] = 0;
+          C.ny[c] = 0;
+        } else {
+          C.nrec[c] = bdf.rec.nrec;
+          C.ny[c] = bdf.rec.ny;
+        }
+      }
+    }
+    tm.sync();
+  }
+  rendezvous_leave(w.rv);
+}
+
 template <int NS, typename LT>
 static size_t adj_warp_smem(const DevMech& M)
 {
@@ -262,7 +360,7 @@ template <int NS, typename LT>
 static int plan_ns_t(const DevMech& M, AdjPlan* p)
 {
   const size_t wb = adj_warp_smem<NS, LT>(M);
-  auto kern = k_tangent<NS, LT>;
+  auto kern = k_adj_seg<NS, LT>;
   int dev = 0, nsm = 0, smem_max = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -303,171 +401,29 @@ static int launch_ns(const DevMech& M, const Options& o, int mode, int lu_fp32, 
                      const AdjLayout& L, double dt, int* queue, double* grad, int accumulate, cudaStream_t st)
 {
   if (b.ncells <= 0) return 0;
+  if (mode != ADJ_TANGENT) return (int)cudaErrorNotSupported;
   cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), st);
   if (e != cudaSuccess) return (int)e;
   const size_t shm = p.warp_smem * p.wpb;
-  typedef void (*KT)(DevMech, Options, AdjBatch, AdjLayout, double, int*);
-  if (mode != ADJ_TANGENT) return (int)cudaErrorNotSupported;
-  KT kern = lu_fp32 ? (KT)k_tangent<NS, float> : (KT)k_tangent<NS, double>;
+  // per-warp tapes; no checkpoints
+  AdjCells C{};
+  C.tape = L.tape;
+  C.cap_rec = L.cap_rec;
+  C.close_rec = L.close_rec;
+  C.ys = L.ys;
+  C.cap_y = L.cap_y;
+  C.close_y = L.close_y;
+  C.seg_steps = L.seg_steps;
+  // the warps spend whole segments in the tangent sweep between right-hand
+  // sides, so a block rendezvous would only wait out its bound
+  Options ot = o;
+  ot.rendezvous = 0;
+  typedef void (*KT)(DevMech, Options, AdjBatch, AdjCells, double, int*, int, int, size_t);
+  KT kern = lu_fp32 ? (KT)k_adj_seg<NS, float> : (KT)k_adj_seg<NS, double>;
   e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   if (e != cudaSuccess) return (int)e;
-  kern<<<p.blocks, p.wpb * 32, shm, st>>>(M, o, b, L, dt, queue);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return (int)e;
-  return (int)e;
-}
-
-template <int NS>
-static int launch_rhs_exact_ns(const DevMech& M, int rtype, double t, const double* y, const double* rhoe,
-                               const double* rhoesrc, const double* src, const double* v, double* f_out,
-                               double* J_out, double* fE_out, double* vy_out, double* vE_out, double* vp_out,
-                               int ncells, cudaStream_t st)
-{
-  if (ncells <= 0) return 0;
-  const size_t wb = team_bytes<double>(NS, M.nrxn) + adj_bytes(NS, M.nrxn);
-  int wpb = 4;
-  while (wpb > 1 && wb * wpb > 200 * 1024) wpb--;
-  const size_t shm = wb * wpb;
-  cudaError_t e =
-    cudaFuncSetAttribute((const void*)k_rhs_exact<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  if (e != cudaSuccess) return (int)e;
-  k_rhs_exact<NS><<<(ncells + wpb - 1) / wpb, wpb * 32, shm, st>>>(M, rtype, t, y, rhoe, rhoesrc, src, v, f_out,
-                                                                   J_out, fE_out, vy_out, vE_out, vp_out, ncells, wb);
+  kern<<<p.blocks, p.wpb * 32, shm, st>>>(M, ot, b, C, dt, queue, 0, SEG_TANGENT, p.warp_smem);
   return (int)cudaGetLastError();
-}
-
-// ---------------------------------------------------------------- batched
-// Forward (replay = 0: every cell from its initial state, a checkpoint at
-// the start of each segment, the last segment's tape left in place) or
-// recomputation of segment seg of every cell that has an earlier segment
-// (replay = 1).  One call site of the integrator serves both, so the
-// recomputation repeats the forward bit for bit; it is checked against the
-// next checkpoint.
-template <int NS, typename LT>
-__global__ void __launch_bounds__(256) k_adj_seg(const __grid_constant__ DevMech M, const __grid_constant__ Options o,
-                                                 const __grid_constant__ AdjBatch b, const __grid_constant__ AdjCells C,
-                                                 double dt, int* queue,
-                                                 int seg, int replay, size_t warp_smem)
-{
-  extern __shared__ __align__(16) char smem[];
-  Team<32> tm;
-  constexpr int n = NS + 1;
-  const int R = M.nrxn;
-  const int warp = threadIdx.x / 32;
-  Work<LT> w;
-  carve<LT>(w, smem + (size_t)warp * warp_smem, NS, R);
-  __shared__ int rv[3];
-  w.rv = rendezvous_init(rv, blockDim.x / 32, o.rendezvous);
-  for (;;) {
-    int c = 0;
-    if (tm.lane == 0) c = atomicAdd(queue, 1);
-    c = __shfl_sync(0xffffffffu, c, 0);
-    if (c >= b.ncells) break;
-    if (replay) {
-      // cells without a segment seg are idle; for a cell whose last segment
-      // is seg, the forward run left the tape (and its counts) in place
-      const int ns = C.nseg[c];
-      if (seg >= ns - 1) continue;
-    }
-    const double* y0 = b.y0 + (size_t)c * n;
-    for (int i = tm.lane; i < n; i += 32) {
-      w.src[i] = (i < NS && b.src) ? b.src[(size_t)c * NS + i] : 0.0;
-      if (o.use_typ_vals) w.atolv[i] = b.atolv[i];
-      if (!replay) {
-        w.zn[0][i] = y0[i];
-        w.y[i] = y0[i];
-      }
-    }
-    tm.sync();
-    const CellIn cin{b.rhoe[c], b.rhoesrc ? b.rhoesrc[c] : 0.0};
-    Bdf<NS, 32, LT, AdjRec<32>> bdf(tm, M, o, w, cin);
-    bdf.rec.tape = reinterpret_cast<TapeRec*>(C.tape) + (size_t)c * C.cap_rec;
-    bdf.rec.ys = C.ys + (size_t)c * C.cap_y * n;
-    bdf.rec.yinfo = C.yinfo + (size_t)c * C.cap_y * 2;
-    bdf.rec.n = n;
-    bdf.rec.seg_steps = C.seg_steps;
-    bdf.rec.close_rec = C.close_rec;
-    bdf.rec.close_y = C.close_y;
-    bdf.rec.begin();
-    int nstloc = 0, ncp = 0, flag = ST_OK;
-    bool done = false;
-    int* cpi = C.cp_idx + (size_t)c * C.max_seg;
-    if (!replay) {
-      flag = bdf.start(dt);
-      for (int i = tm.lane; i < 7 * n; i += 32) C.lam[(size_t)c * 7 * n + i] = 0.0;
-      for (int r = tm.lane; r < 3 * R; r += 32) C.gw[(size_t)c * 3 * R + r] = 0.0;
-      if (b.lam_y0)
-        for (int i = tm.lane; i < n; i += 32) b.lam_y0[(size_t)c * n + i] = 0.0;
-      if (tm.lane == 0) {
-        C.lamE[c] = 0.0;
-        if (b.lam_e) b.lam_e[c] = 0.0;
-      }
-    }
-    for (;;) {
-      if (flag != ST_OK) break;
-      if (!replay) {
-        if (ncp >= C.max_seg) {
-          flag = ST_ADJ_CAPACITY;
-          break;
-        }
-        int slot = 0;
-        if (tm.lane == 0) slot = atomicAdd(C.pool_next, 1);
-        slot = __shfl_sync(0xffffffffu, slot, 0);
-        if (slot >= C.pool_cap) {
-          flag = ST_ADJ_CAPACITY;
-          break;
-        }
-        if (tm.lane == 0) cpi[ncp] = slot;
-        save_cp<NS, LT>(tm, C.cp_pool + (size_t)slot * C.cp_stride, bdf, w, nstloc);
-        ncp++;
-      } else {
-        restore_cp<NS, LT>(tm, C.cp_pool + (size_t)cpi[seg] * C.cp_stride, bdf, w, nstloc);
-      }
-      bdf.rec.begin();
-      flag = bdf.advance(dt, nstloc, done);
-      if (flag != ST_OK || done || replay) break;
-    }
-    if (!replay) {
-      if (b.y_out)
-        for (int i = tm.lane; i < n; i += 32) b.y_out[(size_t)c * n + i] = (flag == ST_OK) ? w.y[i] : w.zn[0][i];
-      if (tm.lane == 0) {
-        if (b.status) b.status[c] = flag;
-        if (b.stats) {
-          int* st = b.stats + (size_t)c * 7;
-          st[0] = bdf.s.nst;
-          st[1] = bdf.s.nfe;
-          st[2] = bdf.s.nje;
-          st[3] = bdf.s.nsetups;
-          st[4] = bdf.s.nni;
-          st[5] = bdf.s.netf;
-          st[6] = bdf.s.ncfn;
-        }
-        C.nseg[c] = (flag == ST_OK) ? ncp : 0;
-        C.h0[c] = bdf.rec.h0;
-        C.nrec[c] = bdf.rec.nrec;
-        C.ny[c] = bdf.rec.ny;
-      }
-    } else {
-      if (flag == ST_OK) {
-        // the recomputed segment must end where the forward run did
-        const BdfScalars* nx = reinterpret_cast<const BdfScalars*>(C.cp_pool + (size_t)cpi[seg + 1] * C.cp_stride);
-        if (nx->tn != bdf.s.tn || nx->nst != bdf.s.nst || nx->h != bdf.s.h) flag = ST_ADJ_REPLAY;
-      }
-      if (tm.lane == 0) {
-        if (flag != ST_OK) {
-          if (b.status) b.status[c] = flag;
-          C.nseg[c] = 0;
-          C.nrec[c] = 0;
-          C.ny[c] = 0;
-        } else {
-          C.nrec[c] = bdf.rec.nrec;
-          C.ny[c] = bdf.rec.ny;
-        }
-      }
-    }
-    tm.sync();
-  }
-  rendezvous_leave(w.rv);
 }
 
 // Every differentiated point of items [i0, i1) of segment seg (item i of
@@ -615,7 +571,7 @@ static int batched_ns_t(const DevMech& M, const Options& o, const AdjBatch& b, A
   // forward with checkpoints
   if ((e = cudaMemsetAsync(C.pool_next, 0, sizeof(int), st)) || (e = cudaMemsetAsync(queue, 0, sizeof(int), st)))
     return (int)e;
-  k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, o, b, C, dt, queue, 0, 0, seg_wb);
+  k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, o, b, C, dt, queue, 0, SEG_FORWARD, seg_wb);
   if ((e = cudaGetLastError())) return (int)e;
   std::vector<int> nseg(nc), ny(nc), off(nc + 1);
   if ((e = cudaMemcpyAsync(nseg.data(), C.nseg, nc * sizeof(int), cudaMemcpyDeviceToHost, st)) ||
@@ -625,7 +581,7 @@ static int batched_ns_t(const DevMech& M, const Options& o, const AdjBatch& b, A
   for (int c = 0; c < nc; c++) maxseg = std::max(maxseg, nseg[c]);
   for (int s = maxseg - 1; s >= 0; s--) {
     if ((e = cudaMemsetAsync(queue, 0, sizeof(int), st))) return (int)e;
-    k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, o, b, C, dt, queue, s, 1, seg_wb);
+    k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, o, b, C, dt, queue, s, SEG_REPLAY, seg_wb);
     if ((e = cudaGetLastError())) return (int)e;
     if ((e = cudaMemcpyAsync(nseg.data(), C.nseg, nc * sizeof(int), cudaMemcpyDeviceToHost, st)) ||
         (e = cudaMemcpyAsync(ny.data(), C.ny, nc * sizeof(int), cudaMemcpyDeviceToHost, st)) ||

@@ -438,15 +438,19 @@ __device__ __forceinline__ void lu_solve_reg(const Team<TEAM>& tm, const LT* A, 
 // read-modify-write updates never race.
 struct BdfArrays {
   double tau[7], tq[6], l[6];
+  // cold state, out of the registers: the last step size and the error
+  // constant saved for an order increase; the statistics counters
+  double hu, saved_tq5;
+  int nje, nsetups, nni, ncfn, netf, pad;
 };
 
 // The scalar integrator state: every lane of the team holds the same values
 // (in registers).
 struct BdfScalars {
-  double h, hprime, hscale, eta, etamax, tn, rl1, gamma, gammap, gamrat, crate, delp, acnrm, saved_tq5, hu;
+  double h, hprime, hscale, eta, etamax, tn, rl1, gamma, gammap, gamrat, crate, delp, acnrm;
   double gamma_lu; // gamma of the factored matrix I - gamma J
   int q, qprime, qwait, L, qmax, indx_acor, jcur;
-  int nst, nstlp, nstlj, nfe, nje, nsetups, nni, ncfn, netf;
+  int nst, nstlp, nstlj, nfe;
 #ifdef PPB_PHASE_TIMERS
   long long phase[PH_COUNT];
 #endif
@@ -766,7 +770,7 @@ struct Bdf {
     if (!jbad) {
       s.jcur = 0;
     } else {
-      s.nje++;
+      if (lead()) ar.nje++;
       s.nstlj = s.nst;
       s.jcur = 1;
       jac();
@@ -869,7 +873,7 @@ struct Bdf {
       nls_residual();
       if (callSetup) {
         const int ier = ls_setup(jbad ? 1 : convfail);
-        s.nsetups++;
+        if (lead()) ar.nsetups++;
         s.gamrat = 1.0;
         s.gammap = s.gamma;
         s.crate = 1.0;
@@ -878,7 +882,7 @@ struct Bdf {
       }
       int m = 0;
       for (;;) {
-        s.nni++;
+        if (lead()) ar.nni++;
         for (int i = tm.lane; i < n; i += TEAM) w.delta[i] = -w.delta[i];
         tm.sync();
         ls_solve();
@@ -983,7 +987,7 @@ struct Bdf {
   __device__ __forceinline__ int handle_nflag(int& nflag, double saved_t, int& ncf)
   {
     if (nflag == 0) return 2; // DO_ERROR_TEST
-    s.ncfn++;
+    if (lead()) ar.ncfn++;
     restore(saved_t);
     if (nflag < 0) return ST_LSETUP_FAIL;
     ncf++;
@@ -1000,7 +1004,7 @@ struct Bdf {
     dsm = s.acnrm * ar.tq[2];
     if (dsm <= 1.0) return ST_OK;
     nef++;
-    s.netf++;
+    if (lead()) ar.netf++;
     nflag = 2;
     restore(saved_t);
     if (nef == o.max_err_fails) return ST_ERR_FAILURE;
@@ -1035,14 +1039,15 @@ struct Bdf {
   __device__ __forceinline__ void complete_step()
   {
     s.nst++;
-    s.hu = s.h;
+    const bool save = ((s.qwait - 1) == 1) && (s.q != s.qmax);
     if (lead()) {
+      ar.hu = s.h;
       for (int i = s.q; i >= 2; i--) ar.tau[i] = ar.tau[i - 1];
       if ((s.q == 1) && (s.nst > 1)) ar.tau[2] = ar.tau[1];
       ar.tau[1] = s.h;
+      if (save) ar.saved_tq5 = ar.tq[5];
     }
     wsync();
-    const bool save = ((s.qwait - 1) == 1) && (s.q != s.qmax);
     if constexpr (Rec::on) {
       rec.predict(tm, s.q);
       rec.correct(tm, s.q, save, s.tn, s.gamma, s.rl1, ar.l, w.zn[0], w.acor);
@@ -1054,10 +1059,7 @@ struct Bdf {
     }
     tm.sync();
     s.qwait--;
-    if (save) {
-      s.saved_tq5 = ar.tq[5];
-      s.indx_acor = s.qmax;
-    }
+    if (save) s.indx_acor = s.qmax;
   }
 
   __device__ __forceinline__ void set_eta()
@@ -1094,8 +1096,8 @@ struct Bdf {
       etaqm1 = 1.0 / (pow(6.0 * ddn, 1.0 / s.q) + 1.0e-6);
     }
     double etaqp1 = 0.0;
-    if (s.q != s.qmax && s.saved_tq5 != 0.0) {
-      const double cquot = (ar.tq[5] / s.saved_tq5) * pow(s.h / ar.tau[2], (double)s.L);
+    if (s.q != s.qmax && ar.saved_tq5 != 0.0) {
+      const double cquot = (ar.tq[5] / ar.saved_tq5) * pow(s.h / ar.tau[2], (double)s.L);
       for (int i = tm.lane; i < n; i += TEAM) w.tempv[i] = -cquot * w.zn[s.qmax][i] + w.acor[i];
       tm.sync();
       const double dup = wrms(w.tempv) * ar.tq[3];

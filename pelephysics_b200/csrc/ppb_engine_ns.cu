@@ -7,7 +7,7 @@
 #error "compile with -DPPB_NS=<number of species>"
 #endif
 #ifndef PPB_PART
-#error "compile with -DPPB_PART=<0..3> (the kernel group of this object)"
+#error "compile with -DPPB_PART=<0..4> (the kernel group of this object)"
 #endif
 
 namespace ppb {
@@ -43,11 +43,11 @@ __device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options&
       int* st = b.stats + (size_t)c * 7;
       st[0] = bdf.s.nst;
       st[1] = bdf.s.nfe;
-      st[2] = bdf.s.nje;
-      st[3] = bdf.s.nsetups;
-      st[4] = bdf.s.nni;
-      st[5] = bdf.s.netf;
-      st[6] = bdf.s.ncfn;
+      st[2] = bdf.ar.nje;
+      st[3] = bdf.ar.nsetups;
+      st[4] = bdf.ar.nni;
+      st[5] = bdf.ar.netf;
+      st[6] = bdf.ar.ncfn;
     }
   } else {
     cost = rk64_cell<TEAM, LT>(tm, M, o, w, cin, dt);
@@ -198,13 +198,14 @@ constexpr int big_team()
 // The compiled variants: 32 lanes per cell with both register budgets for
 // the FP64 BDF kernel; 16 lanes per cell as well for mechanisms of at most
 // 21 species, and a multi-warp team (one cell per block, one lane per
-// species) for larger ones.  They are compiled in four parts (PPB_PART 0..3,
+// species) for larger ones.  They are compiled in five parts (PPB_PART 0..4,
 // one object each, built in parallel); each part returns the kernels it holds
 // and nullptr for the others:
 //   0: FP64 BDF, 32 lanes, 8 warps (<= 128 and <= 255 registers)
 //   1: FP64 BDF, 32 lanes, 12 and 16 warps per block (one block per SM)
 //   2: the multi-warp teams (FP64 and FP32 BDF, RK64)
 //   3: FP32 BDF and RK64 with 32 lanes, the 16-lane variants, the SRK kernel
+//   4: FP32 BDF, 32 lanes, 12 and 16 warps per block
 template <int NS>
 static TeamKernel team_kernel_part(int method, bool fp32, int team, int minb, int srk, int wpb)
 {
@@ -213,10 +214,16 @@ static TeamKernel team_kernel_part(int method, bool fp32, int team, int minb, in
   // 12 or 16 warps per block (one block per SM: <= 168 or <= 128 registers):
   // the FP64 BDF warp-per-cell kernel
   if (wpb > 8) {
-    if (method != METHOD_BDF || fp32 || team != 32 || minb != 2 || srk) return nullptr;
+    if (method != METHOD_BDF || team != 32 || minb != 2 || srk) return nullptr;
     if constexpr (P == 1) {
+      if (fp32) return nullptr;
       if (wpb == 16) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 512>;
       if (wpb == 12) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 384>;
+    }
+    if constexpr (P == 4) {
+      if (!fp32) return nullptr;
+      if (wpb == 16) return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 1, false, 512>;
+      if (wpb == 12) return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 1, false, 384>;
     }
     return nullptr;
   }
@@ -276,13 +283,15 @@ TeamKernel PPB_CAT4(team_kernel_, PPB_NS, _p, PPB_PART)(int method, bool fp32, i
 TeamKernel PPB_CAT4(team_kernel_, PPB_NS, _p, 1)(int, bool, int, int, int, int);
 TeamKernel PPB_CAT4(team_kernel_, PPB_NS, _p, 2)(int, bool, int, int, int, int);
 TeamKernel PPB_CAT4(team_kernel_, PPB_NS, _p, 3)(int, bool, int, int, int, int);
+TeamKernel PPB_CAT4(team_kernel_, PPB_NS, _p, 4)(int, bool, int, int, int, int);
 
 template <int NS>
 static TeamKernel team_kernel(int method, bool fp32, int team, int minb, int srk, int wpb)
 {
-  TeamKernel (*parts[4])(int, bool, int, int, int, int) = {
+  TeamKernel (*parts[5])(int, bool, int, int, int, int) = {
     PPB_CAT4(team_kernel_, PPB_NS, _p, 0), PPB_CAT4(team_kernel_, PPB_NS, _p, 1),
-    PPB_CAT4(team_kernel_, PPB_NS, _p, 2), PPB_CAT4(team_kernel_, PPB_NS, _p, 3)};
+    PPB_CAT4(team_kernel_, PPB_NS, _p, 2), PPB_CAT4(team_kernel_, PPB_NS, _p, 3),
+    PPB_CAT4(team_kernel_, PPB_NS, _p, 4)};
   for (auto f : parts)
     if (TeamKernel k = f(method, fp32, team, minb, srk, wpb)) return k;
   return nullptr;
