@@ -84,6 +84,10 @@ typedef struct ppb_options {
                                launch, in microseconds (0..60000000; 0: a block that would have to wait gives up
                                at once); a wait that runs out ends the call with PPB_E_CUDA and the message
                                "grid barrier timed out" instead of hanging, 20000000 */
+  int adjoint_keep_segments; /* adjoint: keep a copy of every recorded segment that fits in a third of what
+                               adjoint_memory_mb leaves after the per-cell arrays, so that the reverse sweep
+                               recomputes from a checkpoint only those that did not fit (0: recompute every
+                               segment; the gradient is the same either way, bit for bit), 1 */
 } ppb_options;
 
 #define PPB_EOS_IDEAL 0 /* ideal gas: the mechanism's NASA-7 thermo (Source/Eos/Fuego.H) */

@@ -52,6 +52,7 @@ class Options(C.Structure):
         ("cost_order", C.c_int),
         ("rendezvous_cycles", C.c_int),
         ("arkode_barrier_us", C.c_int),
+        ("adjoint_keep_segments", C.c_int),
     ]
 
 

@@ -148,9 +148,9 @@ struct ppb_reactor {
   size_t adj_cp_bytes = 0, adj_tape_bytes = 0, adj_ys_bytes = 0, adj_gw_bytes = 0;
   // batched reverse sweep
   void *adj_yinfo = nullptr, *adj_cpidx = nullptr, *adj_ints = nullptr, *adj_dbl = nullptr, *adj_lam = nullptr,
-       *adj_items = nullptr, *adj_ioff = nullptr;
+       *adj_items = nullptr, *adj_ioff = nullptr, *adj_tpool = nullptr;
   size_t adj_yinfo_bytes = 0, adj_cpidx_bytes = 0, adj_ints_bytes = 0, adj_dbl_bytes = 0, adj_lam_bytes = 0,
-         adj_items_bytes = 0, adj_ioff_bytes = 0;
+         adj_items_bytes = 0, adj_ioff_bytes = 0, adj_tpool_bytes = 0;
 };
 
 // The calling thread's context of reactor r (created on first use).
@@ -174,12 +174,13 @@ static void free_adjoint_scratch(ppb_reactor* r)
   cudaFree(r->adj_gw);
   r->adj_cp = r->adj_tape = r->adj_ys = r->adj_gw = nullptr;
   r->adj_cp_bytes = r->adj_tape_bytes = r->adj_ys_bytes = r->adj_gw_bytes = 0;
-  for (void** q : {&r->adj_yinfo, &r->adj_cpidx, &r->adj_ints, &r->adj_dbl, &r->adj_lam, &r->adj_items, &r->adj_ioff}) {
+  for (void** q : {&r->adj_yinfo, &r->adj_cpidx, &r->adj_ints, &r->adj_dbl, &r->adj_lam, &r->adj_items, &r->adj_ioff,
+                   &r->adj_tpool}) {
     cudaFree(*q);
     *q = nullptr;
   }
   r->adj_yinfo_bytes = r->adj_cpidx_bytes = r->adj_ints_bytes = r->adj_dbl_bytes = r->adj_lam_bytes = 0;
-  r->adj_items_bytes = r->adj_ioff_bytes = 0;
+  r->adj_items_bytes = r->adj_ioff_bytes = r->adj_tpool_bytes = 0;
 }
 
 static int grow(void*& p, size_t& cap, size_t bytes)
@@ -646,6 +647,7 @@ void ppb_default_options(ppb_options* o)
   o->cost_order = 1;
   o->rendezvous_cycles = 1000000;
   o->arkode_barrier_us = 20000000;
+  o->adjoint_keep_segments = 1;
 }
 
 const char* ppb_last_error(void) { return g_err; }
@@ -720,6 +722,8 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
   if (r->opt.warps_per_block > 16) return fail(PPB_E_ARG, "warps_per_block must be at most 16");
   if (r->opt.arkode_barrier_us < 0 || r->opt.arkode_barrier_us > 60000000)
     return fail(PPB_E_ARG, "arkode_barrier_us must be in 0..60000000");
+  if (r->opt.adjoint_keep_segments != 0 && r->opt.adjoint_keep_segments != 1)
+    return fail(PPB_E_ARG, "adjoint_keep_segments must be 0 or 1");
   if (r->opt.eos == PPB_EOS_SRK) {
     // SRK::RHY2T is not supported (Source/Eos/SRK.H:499-507), nor an
     // analytical Jacobian; this engine runs it on the tuned FP64 BDF
@@ -1367,11 +1371,19 @@ static int run_adjoint_batched(ppb_reactor* r, CallCtx* cx, AdjBatch b, double d
   const size_t item_b = adj_item_bytes(N, R);
   const size_t budget = (size_t)(r->opt.adjoint_memory_mb > 0 ? r->opt.adjoint_memory_mb : 16384) << 20;
   const size_t per_cell = (size_t)C.max_seg * 4 + (size_t)C.cap_rec * ADJ_TAPE_BYTES + (size_t)C.cap_y * (8 * n + 16) +
-                          3 * 4 + 8 + (size_t)7 * n * 8 + 8 + (size_t)3 * R * 8 + 4;
+                          3 * 4 + 3 * 8 + (size_t)7 * n * 8 + (size_t)3 * R * 8 + 4;
+  // the budget: the per-cell arrays of the cells of one chunk (all cells when
+  // they take at most two fifths), then the rest in equal parts for the
+  // checkpoints, the segment copies (a segment whose copy fits is not
+  // recomputed in the reverse sweep; without copies the checkpoints get
+  // their part) and the evaluated points of one segment
   const long cells = std::max<long>(1, std::min<long>(b.ncells, (long)(budget * 2 / 5 / per_cell)));
-  const size_t pool_bytes = budget * 7 / 20;
+  const size_t rest = budget - std::min(budget, (size_t)cells * per_cell);
+  const bool keep = r->opt.adjoint_keep_segments != 0;
+  const size_t pool_bytes = keep ? rest / 3 : rest / 3 * 2;
   C.pool_cap = (int)std::min<size_t>(pool_bytes / C.cp_stride, 1u << 30);
-  C.items_cap = std::max<long>((long)(budget / 4 / item_b), C.cap_y + 1);
+  C.tpool_bytes = keep ? (rest / 3) & ~size_t(15) : 0;
+  C.items_cap = std::max<long>((long)(rest / 3 / item_b), C.cap_y + 1);
   if (C.pool_cap < 2) return fail(PPB_E_ARG, "adjoint: adjoint_memory_mb too small for the checkpoints");
   const size_t nc = (size_t)cells;
   int e;
@@ -1381,7 +1393,8 @@ static int run_adjoint_batched(ppb_reactor* r, CallCtx* cx, AdjBatch b, double d
       (e = grow(r->adj_ys, r->adj_ys_bytes, nc * C.cap_y * n * 8)) ||
       (e = grow(r->adj_yinfo, r->adj_yinfo_bytes, nc * C.cap_y * 16)) ||
       (e = grow(r->adj_ints, r->adj_ints_bytes, nc * 3 * 4 + 16)) ||
-      (e = grow(r->adj_dbl, r->adj_dbl_bytes, nc * 2 * 8)) || (e = grow(r->adj_lam, r->adj_lam_bytes, nc * 7 * n * 8)) ||
+      (e = grow(r->adj_dbl, r->adj_dbl_bytes, nc * 3 * 8)) || (e = grow(r->adj_lam, r->adj_lam_bytes, nc * 7 * n * 8)) ||
+      (e = grow(r->adj_tpool, r->adj_tpool_bytes, C.tpool_bytes ? C.tpool_bytes + 16 : 0)) ||
       (e = grow(r->adj_gw, r->adj_gw_bytes, nc * 3 * R * 8)) ||
       (e = grow(r->adj_items, r->adj_items_bytes, (size_t)C.items_cap * item_b)) ||
       (e = grow(r->adj_ioff, r->adj_ioff_bytes, (nc + 1) * 4)))
@@ -1397,6 +1410,9 @@ static int run_adjoint_batched(ppb_reactor* r, CallCtx* cx, AdjBatch b, double d
   C.nseg = C.ny + nc;
   C.h0 = (double*)r->adj_dbl;
   C.lamE = C.h0 + nc;
+  C.toff = (long long*)(C.lamE + nc);
+  C.tpool = C.tpool_bytes ? (char*)r->adj_tpool : nullptr;
+  C.tpool_next = C.tpool ? (unsigned long long*)(C.tpool + C.tpool_bytes) : nullptr;
   C.lam = (double*)r->adj_lam;
   C.gw = (double*)r->adj_gw;
   C.items = (double*)r->adj_items;

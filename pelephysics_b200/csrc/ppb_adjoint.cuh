@@ -575,7 +575,7 @@ struct AdjSweep {
     tm.sync();
   }
 
-  __device__ void fwd_freset(double t, double h, const double* yg, double dE, const double* dp)
+  __device__ __noinline__ void fwd_freset(double t, double h, const double* yg, double dE, const double* dp)
   {
     const AdjPoint pt = point(t, yg);
     tangent_rhs(pt, a.lam, dE, dp, a.mu);
@@ -583,7 +583,8 @@ struct AdjSweep {
     tm.sync();
   }
 
-  __device__ int forward(const TapeRec* tape, int nrec, const double* ys, double dE, const double* dp, double* dy_out)
+  __device__ __noinline__ int forward(const TapeRec* tape, int nrec, const double* ys, double dE, const double* dp,
+                                     double* dy_out)
   {
     for (int k = 0; k < nrec; k++) {
       const TapeRec R = tape[k];

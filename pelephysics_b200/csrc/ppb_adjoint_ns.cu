@@ -33,11 +33,18 @@
 
 namespace ppb {
 
-// checkpoint layout: [BdfScalars | BdfArrays | nstloc][zn 6n][ewt n][J n*n][A n*n LT][piv n]
+// checkpoint layout: [BdfScalars | BdfArrays | CpTail][zn 6n][ewt n][J n*n][A n*n LT][piv n]
+// The tail: the step count of the call at the checkpoint and where the
+// compact copy of the segment that starts there lies (toff < 0: none).
+struct CpTail {
+  int nstloc, nrec, ny, pad;
+  long long toff;
+};
+
 template <typename LT>
 __host__ __device__ inline size_t cp_head_bytes()
 {
-  return (sizeof(BdfScalars) + sizeof(BdfArrays) + 16 + 15) & ~size_t(15);
+  return (sizeof(BdfScalars) + sizeof(BdfArrays) + sizeof(CpTail) + 15) & ~size_t(15);
 }
 
 template <typename LT>
@@ -48,14 +55,56 @@ __host__ __device__ inline size_t cp_bytes(int N)
   return (b + 15) & ~size_t(15);
 }
 
+__device__ __forceinline__ CpTail* cp_tail(char* cp)
+{
+  return reinterpret_cast<CpTail*>(cp + sizeof(BdfScalars) + sizeof(BdfArrays));
+}
+__device__ __forceinline__ const CpTail* cp_tail(const char* cp)
+{
+  return reinterpret_cast<const CpTail*>(cp + sizeof(BdfScalars) + sizeof(BdfArrays));
+}
+
+// Bytes of the compact copy of a segment: its records, then the states and
+// their (t, gamma), each part 16-byte aligned.
+__host__ __device__ inline size_t seg_copy_parts(int nrec, int ny, int n, size_t* ys_off, size_t* yi_off)
+{
+  const size_t tb = (size_t)nrec * sizeof(TapeRec);
+  const size_t yb = ((size_t)ny * n * 8 + 15) & ~size_t(15);
+  const size_t ib = ((size_t)ny * 16 + 15) & ~size_t(15);
+  *ys_off = tb;
+  *yi_off = tb + yb;
+  return tb + yb + ib;
+}
+
+// The tape of cell c's current segment: its compact copy, or the cell's own
+// recording area.
+struct SegTape {
+  const TapeRec* tape;
+  const double* ys;
+  const double* yinfo;
+};
+__device__ __forceinline__ SegTape seg_tape(const AdjCells& C, int c, int n)
+{
+  const long long to = C.toff ? C.toff[c] : -1;
+  if (to >= 0) {
+    size_t yo, io;
+    seg_copy_parts(C.nrec[c], C.ny[c], n, &yo, &io);
+    const char* p = C.tpool + to;
+    return {reinterpret_cast<const TapeRec*>(p), reinterpret_cast<const double*>(p + yo),
+            reinterpret_cast<const double*>(p + io)};
+  }
+  return {reinterpret_cast<const TapeRec*>(C.tape) + (size_t)c * C.cap_rec, C.ys + (size_t)c * C.cap_y * n,
+          C.yinfo + (size_t)c * C.cap_y * 2};
+}
+
 template <int NS, typename LT, typename B>
-__device__ void save_cp(const Team<32>& tm, char* dst, const B& bdf, const Work<LT>& w, int nstloc)
+__device__ __noinline__ void save_cp(const Team<32>& tm, char* dst, const B& bdf, const Work<LT>& w, int nstloc)
 {
   constexpr int n = NS + 1;
   if (tm.lane == 0) {
     *reinterpret_cast<BdfScalars*>(dst) = bdf.s;
     *reinterpret_cast<BdfArrays*>(dst + sizeof(BdfScalars)) = bdf.ar;
-    *reinterpret_cast<int*>(dst + sizeof(BdfScalars) + sizeof(BdfArrays)) = nstloc;
+    *cp_tail(dst) = CpTail{nstloc, 0, 0, 0, -1};
   }
   double* z = reinterpret_cast<double*>(dst + cp_head_bytes<LT>());
   for (int j = 0; j < 6; j++)
@@ -71,7 +120,7 @@ __device__ void save_cp(const Team<32>& tm, char* dst, const B& bdf, const Work<
 }
 
 template <int NS, typename LT, typename B>
-__device__ void restore_cp(const Team<32>& tm, const char* src, B& bdf, Work<LT>& w, int& nstloc)
+__device__ __noinline__ void restore_cp(const Team<32>& tm, const char* src, B& bdf, Work<LT>& w, int& nstloc)
 {
   constexpr int n = NS + 1;
   bdf.s = *reinterpret_cast<const BdfScalars*>(src);
@@ -80,7 +129,7 @@ __device__ void restore_cp(const Team<32>& tm, const char* src, B& bdf, Work<LT>
     for (int i = tm.lane; i < (int)(sizeof(BdfArrays) / sizeof(double)); i += 32)
       reinterpret_cast<double*>(&bdf.ar)[i] = a[i];
   }
-  nstloc = *reinterpret_cast<const int*>(src + sizeof(BdfScalars) + sizeof(BdfArrays));
+  nstloc = cp_tail(src)->nstloc;
   const double* z = reinterpret_cast<const double*>(src + cp_head_bytes<LT>());
   for (int j = 0; j < 6; j++)
     for (int i = tm.lane; i < n; i += 32) w.zn[j][i] = z[j * n + i];
@@ -179,6 +228,38 @@ static int launch_rhs_exact_ns(const DevMech& M, int rtype, double t, const doub
   return (int)cudaGetLastError();
 }
 
+// Copy a just-recorded segment (records, states, their (t, gamma)) into the
+// next free bytes of the tape pool and note where in its checkpoint's tail;
+// when the pool is full the segment is recomputed in the reverse sweep.
+static __device__ __noinline__ void copy_segment(const Team<32>& tm, const AdjCells& C, char* cp, const TapeRec* tape,
+                                                 const double* ys, const double* yinfo, int nrec, int ny, int n)
+{
+  size_t yo, io;
+  const size_t bytes = seg_copy_parts(nrec, ny, n, &yo, &io);
+  unsigned long long off = 0;
+  if (tm.lane == 0) off = atomicAdd(C.tpool_next, (unsigned long long)bytes);
+  off = __shfl_sync(0xffffffffu, off, 0);
+  const bool fits = off + bytes <= C.tpool_bytes;
+  __syncwarp(); // the records (lane 0) and states (all lanes) are visible
+  if (fits) {
+    char* p = C.tpool + off;
+    const int4* ts = reinterpret_cast<const int4*>(tape);
+    int4* td = reinterpret_cast<int4*>(p);
+    for (int i = tm.lane; i < nrec * (int)(sizeof(TapeRec) / 16); i += 32) td[i] = ts[i];
+    double* yd = reinterpret_cast<double*>(p + yo);
+    for (int i = tm.lane; i < ny * n; i += 32) yd[i] = ys[i];
+    double* id = reinterpret_cast<double*>(p + io);
+    for (int i = tm.lane; i < 2 * ny; i += 32) id[i] = yinfo[i];
+  }
+  if (tm.lane == 0) {
+    CpTail* tl = cp_tail(cp);
+    tl->nrec = nrec;
+    tl->ny = ny;
+    tl->toff = fits ? (long long)off : -1;
+  }
+  __syncwarp();
+}
+
 // ---------------------------------------------------------------- batched
 // The modes of k_adj_seg.
 enum : int { SEG_FORWARD = 0, SEG_REPLAY = 1, SEG_TANGENT = 2 };
@@ -196,7 +277,7 @@ enum : int { SEG_FORWARD = 0, SEG_REPLAY = 1, SEG_TANGENT = 2 };
 // mode integrates with the same compiled arithmetic and their trajectories
 // agree bit for bit.
 template <int NS, typename LT>
-__global__ void __launch_bounds__(256) k_adj_seg(const __grid_constant__ DevMech M, const __grid_constant__ Options o,
+__global__ void __launch_bounds__(512, 1) k_adj_seg(const __grid_constant__ DevMech M, const __grid_constant__ Options o,
                                                  const __grid_constant__ AdjBatch b, const __grid_constant__ AdjCells C,
                                                  double dt, int* queue, int seg, int mode, size_t warp_smem)
 {
@@ -225,6 +306,16 @@ __global__ void __launch_bounds__(256) k_adj_seg(const __grid_constant__ DevMech
       // is seg, the forward run left the tape (and its counts) in place
       const int ns = C.nseg[c];
       if (seg >= ns - 1) continue;
+      // a segment the forward run copied needs no recomputation
+      const CpTail* tl = cp_tail(C.cp_pool + (size_t)C.cp_idx[(size_t)c * C.max_seg + seg] * C.cp_stride);
+      if (tl->toff >= 0) {
+        if (tm.lane == 0) {
+          C.nrec[c] = tl->nrec;
+          C.ny[c] = tl->ny;
+          C.toff[c] = tl->toff;
+        }
+        continue;
+      }
     }
     const double* y0 = b.y0 + (size_t)c * n;
     for (int i = tm.lane; i < n; i += 32) {
@@ -300,6 +391,9 @@ __global__ void __launch_bounds__(256) k_adj_seg(const __grid_constant__ DevMech
       bdf.rec.begin();
       flag = bdf.advance(dt, nstloc, done);
       if (tangent && flag == ST_OK) flag = sw.forward(tape, bdf.rec.nrec, ys, dE, b.dp, a.tmp);
+      if (mode == SEG_FORWARD && flag == ST_OK && !done && C.tpool)
+        copy_segment(tm, C, C.cp_pool + (size_t)cpi[ncp - 1] * C.cp_stride, tape, ys, bdf.rec.yinfo, bdf.rec.nrec,
+                     bdf.rec.ny, n);
       if (flag != ST_OK || done || replay) break;
     }
     if (!replay) {
@@ -324,6 +418,7 @@ __global__ void __launch_bounds__(256) k_adj_seg(const __grid_constant__ DevMech
           C.h0[c] = bdf.rec.h0;
           C.nrec[c] = bdf.rec.nrec;
           C.ny[c] = bdf.rec.ny;
+          if (C.toff) C.toff[c] = -1; // the last segment stays in the cell's own area
         }
       }
     } else {
@@ -341,6 +436,7 @@ __global__ void __launch_bounds__(256) k_adj_seg(const __grid_constant__ DevMech
         } else {
           C.nrec[c] = bdf.rec.nrec;
           C.ny[c] = bdf.rec.ny;
+          if (C.toff) C.toff[c] = -1;
         }
       }
     }
@@ -456,10 +552,10 @@ __global__ void __launch_bounds__(256) k_adj_items(DevMech M, int rtype, AdjBatc
     t = 0.0;
     gamma = 0.0;
   } else {
-    const size_t k = (size_t)c * C.cap_y + slot;
-    yg = C.ys + k * n;
-    t = C.yinfo[2 * k];
-    gamma = C.yinfo[2 * k + 1];
+    const SegTape sg = seg_tape(C, c, n);
+    yg = sg.ys + (size_t)slot * n;
+    t = sg.yinfo[2 * slot];
+    gamma = sg.yinfo[2 * slot + 1];
   }
   const ItemLayout IL(NS, M.nrxn);
   eval_item<32, PER>(tm, M, rtype, t, gamma, yg, b.rhoe[c], b.rhoesrc ? b.rhoesrc[c] : 0.0,
@@ -496,7 +592,7 @@ __global__ void __launch_bounds__(256) k_adj_sweep(DevMech M, Options o, AdjBatc
   tm.sync();
   const ItemLayout IL(NS, R);
   const double* items = C.items + (size_t)(C.item_off[c] - i0) * IL.stride;
-  const TapeRec* tape = reinterpret_cast<const TapeRec*>(C.tape) + (size_t)c * C.cap_rec;
+  const TapeRec* tape = seg_tape(C, c, n).tape;
   int flag = sweep_items<32>(tm, M, n, o.max_order, a, tape, C.nrec[c], items, IL, b.lam_y + (size_t)c * n, lamE);
   if (flag == ST_OK && seg == 0) {
     // z_0 = y0, z_1 = h0 f(0, y0)
@@ -519,13 +615,13 @@ __global__ void __launch_bounds__(256) k_adj_sweep(DevMech M, Options o, AdjBatc
 
 // Block size (warps) with the most resident warps per SM for a kernel with
 // wb bytes of shared memory per warp.
-static int best_blocks(const void* kern, size_t wb, int* wpb_out, int* per_sm_out)
+static int best_blocks(const void* kern, size_t wb, int max_wpb, int* wpb_out, int* per_sm_out)
 {
   int dev = 0, smem_max = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   int best_w = 0, best_b = 0, best = 0;
-  for (int wpb = 8; wpb >= 1; wpb--) {
+  for (int wpb = max_wpb; wpb >= 1; wpb--) {
     const size_t shm = wb * wpb;
     if (shm > (size_t)smem_max) continue;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -560,17 +656,18 @@ static int batched_ns_t(const DevMech& M, const Options& o, const AdjBatch& b, A
   // launch shapes
   const size_t seg_wb = team_bytes<LT>(NS, R);
   int seg_w = 0, seg_b = 0, it_w = 0, it_b = 0, sw_w = 0, sw_b = 0;
-  int err = best_blocks((const void*)k_adj_seg<NS, LT>, seg_wb, &seg_w, &seg_b);
+  int err = best_blocks((const void*)k_adj_seg<NS, LT>, seg_wb, 16, &seg_w, &seg_b);
   if (err) return err;
   const size_t it_wb = item_bytes(NS, R);
-  if ((err = best_blocks((const void*)k_adj_items<NS>, it_wb, &it_w, &it_b))) return err;
+  if ((err = best_blocks((const void*)k_adj_items<NS>, it_wb, 8, &it_w, &it_b))) return err;
   const size_t sw_wb = ((8 * (9 * (size_t)n + 1 + (size_t)n * n) + 4 * n) + 15) & ~size_t(15);
-  if ((err = best_blocks((const void*)k_adj_sweep<NS>, sw_wb, &sw_w, &sw_b))) return err;
+  if ((err = best_blocks((const void*)k_adj_sweep<NS>, sw_wb, 8, &sw_w, &sw_b))) return err;
   const int seg_grid = std::min(nsm * seg_b, (nc + seg_w - 1) / seg_w);
   const ItemLayout IL(NS, R);
   // forward with checkpoints
   if ((e = cudaMemsetAsync(C.pool_next, 0, sizeof(int), st)) || (e = cudaMemsetAsync(queue, 0, sizeof(int), st)))
     return (int)e;
+  if (C.tpool && (e = cudaMemsetAsync(C.tpool_next, 0, sizeof(unsigned long long), st))) return (int)e;
   k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, o, b, C, dt, queue, 0, SEG_FORWARD, seg_wb);
   if ((e = cudaGetLastError())) return (int)e;
   std::vector<int> nseg(nc), ny(nc), off(nc + 1);

@@ -248,6 +248,12 @@ struct AdjCells {
   int* item_cell;       // [items]
   long items_cap;       // items the buffer holds
   int seg_steps;
+  // compact copies of the recorded segments (all but each cell's last), so
+  // that the reverse sweep needs no recomputation while they fit; or nullptr
+  char* tpool;
+  unsigned long long tpool_bytes;
+  unsigned long long* tpool_next; // bytes handed out (device)
+  long long* toff;                // [cells] the current segment's copy: byte offset in tpool, or -1
 };
 // Host callback growing a device buffer (returns a cudaError_t).
 typedef int (*AdjGrow)(void* ctx, void** p, size_t bytes);

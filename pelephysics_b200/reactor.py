@@ -64,8 +64,12 @@ class Reactor:
 
     def init(self, reactor_type: int, ncells: int = 0, **opts):
         o = _lib.default_options()
+        fields = {f[0] for f in _lib.Options._fields_}
         for k, v in opts.items():
-            setattr(o, _KEYS.get(k, k), v)
+            key = _KEYS.get(k, k)
+            if key not in fields:
+                raise TypeError(f"unknown reactor option {k!r}")
+            setattr(o, key, v)
         check(lib().ppb_init(self._h, int(reactor_type), int(ncells), C.byref(o)))
         self.reactor_type = reactor_type
         self.options = o

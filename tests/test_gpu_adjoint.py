@@ -7,9 +7,11 @@ counterpart; the derivatives are checked against the CPU oracle).
   (oracle production rates and thermo, T solved to 1e-14; relative step
   1e-4): 1e-5 relative per column and row block.
 * Integration: the discrete adjoint against the tangent-linear model on the
-  same cells (dot-product identity to 1e-9 relative); the adjoint gradient
-  independent of the checkpoint interval (bit for bit: the reverse sweep
-  recomputes each segment exactly); the loss gradient against central
+  same cells (dot-product identity to 1e-9 relative; both integrate
+  through one compiled call site, so their trajectories agree bit for bit);
+  the adjoint gradient independent of the checkpoint interval and of
+  whether the reverse sweep reads the forward run's copy of a segment or
+  recomputes it (bit for bit); the loss gradient against central
   finite differences (step 1e-6 relative) of the CPU oracle integrator at
   rtol = atol = 1e-13, 1e-2 relative on the dominant components.
 """
@@ -205,6 +207,39 @@ def test_adjoint_checkpoint_interval_invariance(cuda, oracle):
         ya, ly0, le, gr = r.adjoint(g(rY), g(src), g(rX), g(rXs), dt, g(lam))
         out.append([t.cpu().numpy() for t in (ya, ly0, le, gr)])
         r.close()
+    for o in out[1:]:
+        for a, b in zip(out[0], o):
+            np.testing.assert_array_equal(a, b)
+
+
+def test_adjoint_segment_copies_change_no_bits(cuda, oracle):
+    """The reverse sweep reads each segment from the forward run's copy, or,
+    when the copies do not fit (a small adjoint_memory_mb) or are off
+    (adjoint_keep_segments = 0), recomputes it from its checkpoint: the same
+    records either way, so the same bits.  The small budgets leave room for
+    some of the copies only (a budget too small for the checkpoints ends the
+    call with an error, which is allowed here)."""
+    from pelephysics_b200._lib import EngineError
+
+    torch = cuda
+    mech, rtype, dt, nc = "drm19", 2, 2e-4, 24
+    g = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    out = []
+    for keep, mb in ((1, 16384), (0, 16384), (1, 12), (1, 8), (1, 6)):
+        r, rY, src, rX, rXs = adjoint_setup(oracle, mech, rtype, nc, dt, interval=64, adjoint_keep_segments=keep,
+                                            adjoint_memory_mb=mb)
+        lam = np.random.default_rng(3).normal(size=rY.shape)
+        try:
+            ya, ly0, le, gr = r.adjoint(g(rY), g(src), g(rX), g(rXs), dt, g(lam))
+        except EngineError:
+            assert mb < 100
+            r.close()
+            continue
+        st, _ = r.cell_status(nc)
+        assert np.all(st == 0)
+        out.append([t.cpu().numpy() for t in (ya, ly0, le, gr)])
+        r.close()
+    assert len(out) >= 3
     for o in out[1:]:
         for a, b in zip(out[0], o):
             np.testing.assert_array_equal(a, b)
