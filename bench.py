@@ -867,6 +867,59 @@ def srk_arm(args):
     return 0
 
 
+def layout_arm(args, reps=5):
+    """Device time of ReactorBase::flatten and unflatten (ppb_flatten /
+    ppb_unflatten) on the drm19 --edge^3 box, with their algorithmic HBM
+    bytes: flatten reads rhoY, frcExt (N each), T, rhoE, frcEExt and writes
+    y_vect (N+1), src_vect (N), the energy and its source; unflatten reads
+    y_vect (N+1), the energy, frcEExt, FCunt (int64) and writes rhoY (N), T,
+    rhoE, FC (int32).  flatten also solves T from the energy per cell."""
+    import torch
+
+    from pelephysics_b200 import workloads as wl
+    from pelephysics_b200.reactor import Reactor
+
+    e = args.edge
+    cells = wl.drm19_field(e)
+    nc = cells.ncells
+    N = cells.rY.shape[1] - 1
+    box = lambda a, k: torch.as_tensor(np.ascontiguousarray(a.T.reshape(k, e, e, e)), device="cuda")
+    rY = box(cells.rY[:, :N], N)
+    rYs = box(cells.rYsrc, N)
+    T = box(cells.rY[:, N:], 1)
+    rE = box(cells.rX[:, None], 1)
+    rEs = box(cells.rX_src[:, None], 1)
+    FC = torch.zeros((1, e, e, e), dtype=torch.int32, device="cuda")
+    yv = torch.empty((N + 1) * nc, dtype=torch.float64, device="cuda")
+    sv = torch.empty(N * nc, dtype=torch.float64, device="cuda")
+    ev = torch.empty(nc, dtype=torch.float64, device="cuda")
+    esv = torch.empty(nc, dtype=torch.float64, device="cuda")
+    fcu = torch.ones(nc, dtype=torch.int64, device="cuda")
+    r = Reactor(MECH)
+    r.init(cells.reactor_type, nc)
+    lo, hi = (0, 0, 0), (e - 1, e - 1, e - 1)
+    ops = {"flatten": (lambda: r.flatten(lo, hi, rY, rYs, T, rE, rEs, yv, sv, ev, esv), 8 * (2 * N + 3) + 8 * (2 * N + 3)),
+           "unflatten": (lambda: r.unflatten(lo, hi, rY, T, rE, rEs, FC, yv, ev, fcu, cells.dt),
+                         8 * (N + 1) + 8 + 8 + 8 + 8 * N + 8 + 8 + 4)}
+    out = {}
+    for name, (fn, bpc) in ops.items():
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        s_ = a.elapsed_time(b) / 1e3 / reps
+        out[name] = {"ms": round(1e3 * s_, 4), "bytes_per_cell": bpc, "GB_per_s": round(bpc * nc / s_ / 1e9, 1)}
+    r.close()
+    print(json.dumps({"config": "layout", "mech": MECH, "cells": nc, "kernels": out,
+                      "note": "inputs (83 MB per array set at 64^3) larger than L2 only in total; "
+                              "repeated launches on the same arrays"}), flush=True)
+    return 0
+
+
 def pointwise_arm(args, reps=5):
     """Device time of the pointwise kernels -- reactor RHS (fKernelSpec),
     productionRate and aJacobian -- on the drm19 field's first --cells cells,
@@ -923,7 +976,7 @@ def main():
     ap.add_argument("--adjoint-cells", type=int, default=65536)
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other configurations (LiDryer 16^3, dodecane_lu, heptane_lu_88sk) in the line")
-    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane", "arkode", "transport", "srk", "pointwise"],
+    ap.add_argument("--config", default="drm19", choices=["drm19", "dodecane", "heptane", "arkode", "transport", "srk", "pointwise", "layout"],
                     help="drm19: the headline line; dodecane / heptane: the larger configurations; arkode: "
                          "the ReactorArkode integrator on the drm19 field")
     ap.add_argument("--sample", type=int, default=256, help="oracle sample cells for --config dodecane/heptane")
@@ -942,6 +995,8 @@ def main():
         return srk_arm(args)
     if args.config == "pointwise":
         return pointwise_arm(args)
+    if args.config == "layout":
+        return layout_arm(args)
     if args.config != "drm19":
         return config_arm(args)
     return our_arm(args)

@@ -11,6 +11,7 @@
 #include "../pelephysics_b200/csrc/mech/mech_drm19.h"
 #include "../pelephysics_b200/csrc/mech/mech_dodecane_lu.h"
 #include "../pelephysics_b200/csrc/mech/mech_heptane_lu_88sk.h"
+#include "../pelephysics_b200/csrc/mech/mech_CH4_lean_qss.h"
 
 const PPBMechTables* ppo_mech(const char* name)
 {
@@ -18,7 +19,14 @@ const PPBMechTables* ppo_mech(const char* name)
   if (!strcmp(name, "drm19")) return &ppbm_drm19;
   if (!strcmp(name, "dodecane_lu")) return &ppbm_dodecane_lu;
   if (!strcmp(name, "heptane_lu_88sk")) return &ppbm_heptane_lu_88sk;
+  if (!strcmp(name, "CH4_lean_qss")) return &ppbm_CH4_lean_qss;
   return 0;
+}
+
+int ppo_nqss(const char* name)
+{
+  const PPBMechTables* M = ppo_mech(name);
+  return M ? M->nqss : -1;
 }
 
 const char* ppo_species_name(const char* name, int k)
@@ -253,24 +261,22 @@ static inline double refc_pow(int p, double refC, double refCinv)
   return r;
 }
 
-// production.py:991-1435 (productionRate, SI units).  When absterm is not
-// NULL it also receives, per species, sum over reactions of
-// |nu| (|q_f| + |q_r|): the magnitude against which the rounding error of
-// the (cancelling) sum wdot is measured.
-static void production_rate_impl(const PPBMechTables* M, double* wdot, const double* sc,
-                                 double T, double* absterm)
+// g/RT of thermo entry s (gibbs_nasa7 of thermo.py:572-595; for a QSS
+// mechanism the QSS species' entries are those of gibbs_qss)
+static double gibbs_one(const PPBMechTables* M, int s, double T, double invT, double logT)
 {
-  const int N = M->nsp;
-  const double invT = 1.0 / T;
-  const double logT = log(T);
-  const double refC = 101325 / 8.31446 * invT;
-  const double refCinv = 1 / refC;
-  double g_RT[128];
-  for (int i = 0; i < N; i++) wdot[i] = 0.0;
-  double mixture = 0.0;
-  for (int i = 0; i < N; i++) mixture += sc[i];
-  ppo_gibbs(M, T, g_RT);
-  for (int r = 0; r < M->nrxn; r++) {
+  const double* c = M->th_g + (2 * s + rng(M, s, T)) * 7;
+  return c[0] * invT + c[1] + c[2] * logT + c[3] * T + c[4] * (T * T) + c[5] * (T * T * T) +
+         c[6] * (T * T * T * T);
+}
+
+// Rates of progress q_f, q_r of reaction r (production.py:991-1435) over
+// the concentration slots sc and g/RT slots g.
+static void rxn_rates(const PPBMechTables* M, int r, double T, double invT, double logT, double refC,
+                      double refCinv, double mixture, const double* sc, const double* g_RT, double* qf_out,
+                      double* qr_out)
+{
+  {
     const int kind = M->rx_kind[r];
     const double k_f =
       M->rx_A[r] * exp(M->rx_beta[r] * logT - M->rx_EaR[r] * invT);
@@ -322,6 +328,123 @@ static void production_rate_impl(const PPBMechTables* M, double* wdot, const dou
       const double conv = refc_pow(M->rx_kcpow[r], refC, refCinv);
       qr = (corr ? Corr * k_f : k_f) * exp(-arg) * conv * phr;
     }
+    *qf_out = qf;
+    *qr_out = qr;
+  }
+}
+
+// The QSS concentrations (comp_qss_coeff, comp_sc_qss of the reference's
+// generated QSS mechanism.H): with the QSS slots of sc at 1, the
+// coefficients q_f,k and q_r,k of the QSS reactions; per QSS species i the
+// production P_i = eps + sum, the loss D_i = eps - sum (of the loss
+// coefficients, so negative) and the couplings C_ij = (eps + sum) / D_i, all
+// summed in k order, eps = 1e-12 as the generated code adds it; then the
+// linear balance x_i + sum_j C_ij x_j = -P_i / D_i, solved by Gaussian
+// elimination in species order without pivoting (the generated code
+// eliminates symbolically in an order of its own: the same system, solved to
+// rounding).  No pivoting: the loss of species i includes every reaction
+// that turns it into another QSS species, so the balance matrix is
+// column-diagonally dominant and elimination on its unit diagonal is
+// stable, while a row swap can mix a species of concentration 1e-17 with one
+// of 1e-2 and lose the small one to cancellation.
+static void qss_concentrations(const PPBMechTables* M, double T, double invT, double logT, double refC,
+                               double refCinv, double mixture, double* sc, const double* g_RT)
+{
+  const int N = M->nsp, Q = M->nqss, K = M->nrq;
+  const double eps = 1e-12;
+  double co[2 * 512];
+  double A[32 * 33];
+  for (int q = 0; q < Q; q++) sc[N + 1 + q] = 1.0;
+  for (int k = 0; k < K; k++) rxn_rates(M, M->q_rx[k], T, invT, logT, refC, refCinv, mixture, sc, g_RT, &co[2 * k], &co[2 * k + 1]);
+  for (int i = 0; i < Q; i++) {
+    double* row = A + i * (Q + 1);
+    unsigned char has[32];
+    for (int j = 0; j < Q; j++) {
+      row[j] = 0.0;
+      has[j] = 0;
+    }
+    double P = eps, D = eps;
+    for (int t = M->q_off[i]; t < M->q_off[i + 1]; t++) {
+      const double v = co[M->q_term[t]];
+      const int role = M->q_role[t];
+      if (role == -1) {
+        P += v;
+      } else if (role == -2) {
+        D -= v;
+      } else {
+        if (!has[role]) {
+          row[role] = eps;
+          has[role] = 1;
+        }
+        row[role] += v;
+      }
+    }
+    for (int j = 0; j < Q; j++)
+      if (has[j]) row[j] = row[j] / D;
+    row[i] = 1.0;
+    row[Q] = -P / D;
+  }
+  // forward elimination, then back substitution
+  for (int c = 0; c < Q; c++) {
+    for (int i = c + 1; i < Q; i++) {
+      const double f = A[i * (Q + 1) + c] / A[c * (Q + 1) + c];
+      if (f == 0.0) continue;
+      for (int j = c; j <= Q; j++) A[i * (Q + 1) + j] -= f * A[c * (Q + 1) + j];
+    }
+  }
+  for (int i = Q - 1; i >= 0; i--) {
+    double x = A[i * (Q + 1) + Q];
+    for (int j = i + 1; j < Q; j++) x -= A[i * (Q + 1) + j] * sc[N + 1 + j];
+    sc[N + 1 + i] = x / A[i * (Q + 1) + i];
+  }
+}
+
+// The QSS concentrations (SI) productionRate uses at (sc, T): out[nqss].
+void ppo_qss_concentrations(const PPBMechTables* M, const double* sc_in, double T, double* out)
+{
+  const int N = M->nsp, Q = M->nqss;
+  const double invT = 1.0 / T, logT = log(T);
+  const double refC = 101325 / 8.31446 * invT, refCinv = 1 / refC;
+  double g_RT[160], sc[160];
+  double mixture = 0.0;
+  for (int i = 0; i < N; i++) mixture += sc_in[i];
+  ppo_gibbs(M, T, g_RT);
+  for (int i = 0; i < N; i++) sc[i] = sc_in[i];
+  sc[N] = 1.0;
+  g_RT[N] = 0.0;
+  for (int q = 0; q < Q; q++) g_RT[N + 1 + q] = gibbs_one(M, N + 1 + q, T, invT, logT);
+  qss_concentrations(M, T, invT, logT, refC, refCinv, mixture, sc, g_RT);
+  for (int q = 0; q < Q; q++) out[q] = sc[N + 1 + q];
+}
+
+// production.py:991-1435 (productionRate, SI units).  When absterm is not
+// NULL it also receives, per species, sum over reactions of
+// |nu| (|q_f| + |q_r|): the magnitude against which the rounding error of
+// the (cancelling) sum wdot is measured.  For a QSS mechanism the QSS
+// concentrations are solved first (qss_concentrations).
+static void production_rate_impl(const PPBMechTables* M, double* wdot, const double* sc_in,
+                                 double T, double* absterm)
+{
+  const int N = M->nsp, Q = M->nqss;
+  const double invT = 1.0 / T;
+  const double logT = log(T);
+  const double refC = 101325 / 8.31446 * invT;
+  const double refCinv = 1 / refC;
+  double g_RT[160], sc[160];
+  for (int i = 0; i < N; i++) wdot[i] = 0.0;
+  double mixture = 0.0;
+  for (int i = 0; i < N; i++) mixture += sc_in[i];
+  ppo_gibbs(M, T, g_RT);
+  for (int i = 0; i < N; i++) sc[i] = sc_in[i];
+  sc[N] = 1.0;
+  g_RT[N] = 0.0;
+  if (Q > 0) {
+    for (int q = 0; q < Q; q++) g_RT[N + 1 + q] = gibbs_one(M, N + 1 + q, T, invT, logT);
+    qss_concentrations(M, T, invT, logT, refC, refCinv, mixture, sc, g_RT);
+  }
+  for (int r = 0; r < M->nrxn; r++) {
+    double qf, qr;
+    rxn_rates(M, r, T, invT, logT, refC, refCinv, mixture, sc, g_RT, &qf, &qr);
     const double qdot = qf - qr;
     for (int j = 0; j < M->rx_wup_n[r]; j++) {
       const int s = M->rx_wup_sp[r * PPB_MAXW + j];

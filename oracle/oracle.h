@@ -19,6 +19,7 @@ extern "C" {
 
 const PPBMechTables* ppo_mech(const char* name);
 int ppo_nsp(const char* name);
+int ppo_nqss(const char* name); // QSS species of the mechanism (0: none)
 const char* ppo_species_name(const char* name, int k);
 void ppo_mw(const char* name, double* mw);
 
@@ -43,6 +44,7 @@ int ppo_get_t_given_ey(const PPBMechTables* M, double e, const double* y, double
 int ppo_get_t_given_hy(const PPBMechTables* M, double h, const double* y, double* T);
 // rates and Jacobian (mechanism.H productionRate / aJacobian / DWDOT / CKWC)
 void ppo_production_rate(const PPBMechTables* M, double* wdot, const double* sc, double T);
+void ppo_qss_concentrations(const PPBMechTables* M, const double* sc, double T, double* out);
 // per species sum |nu| (|q_f| + |q_r|): the scale of wdot's rounding error
 void ppo_production_rate_abs(const PPBMechTables* M, double* absterm, const double* sc, double T);
 void ppo_ckwc(const PPBMechTables* M, double T, const double* C, double* wdot);

@@ -80,6 +80,8 @@ def lib():
         L.ppo_mech.restype = C.c_void_p
         L.ppo_mech.argtypes = [C.c_char_p]
         L.ppo_nsp.argtypes = [C.c_char_p]
+        L.ppo_nqss.argtypes = [C.c_char_p]
+        L.ppo_qss_concentrations.argtypes = [C.c_void_p, _DP, C.c_double, _DP]
         for fn in ("ppo_cv_R", "ppo_cp_R", "ppo_dcvpRdT", "ppo_species_internal_energy",
                    "ppo_species_enthalpy", "ppo_gibbs", "ppo_ckums", "ppo_ckhms"):
             getattr(L, fn).argtypes = [C.c_void_p, C.c_double, _DP]
@@ -156,6 +158,12 @@ class Mech:
         if not self.M:
             raise KeyError(name)
         self.nsp = self.L.ppo_nsp(name.encode())
+        self.nqss = self.L.ppo_nqss(name.encode())
+
+    def qss_concentrations(self, sc, T):
+        out = np.zeros(self.nqss)
+        self.L.ppo_qss_concentrations(self.M, _p(np.ascontiguousarray(sc, float)), float(T), _p(out))
+        return out
 
     def species(self):
         return [self.L.ppo_species_name(self.name.encode(), k).decode() for k in range(self.nsp)]
@@ -454,6 +462,13 @@ class Ref:
         w = np.zeros(self.nsp)
         self.L.ref_productionRate(_p(w), _p(sc), float(T))
         return w
+
+    def qss_concentrations(self, sc, T, nqss):
+        """A QSS mechanism's steady-state concentrations (SI) at (sc, T)."""
+        self.L.ref_sc_qss.argtypes = [_DP, _DP, C.c_double]
+        out = np.zeros(64)
+        self.L.ref_sc_qss(_p(out), _p(np.ascontiguousarray(sc, float)), float(T))
+        return out[:nqss]
 
     def ajacobian(self, sc, T, consP):
         sc = np.ascontiguousarray(sc, float)

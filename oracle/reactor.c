@@ -499,7 +499,9 @@ static int ls_setup(BDF* b, int convfail)
     b->nje++;
     b->nstlj = b->nst;
     b->jcur = 1;
-    if (b->sys->eos == 1) {
+    if (b->sys->eos == 1 || b->sys->M->nqss > 0) {
+      // SRK, or a QSS mechanism (its analytical Jacobian needs CEPTR's
+      // symbolic build; the reference's dense_direct solve differences f)
       dq_jac(b);
     } else {
       sys_j(b->sys, b->y, b->savedJ);

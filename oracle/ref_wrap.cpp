@@ -32,6 +32,27 @@ REF_API void ref_productionRate(double* wdot, const double* sc, double T)
 {
   productionRate(wdot, sc, T);
 }
+#ifdef NUM_QSSA_GAS_SPECIES
+// QSS mechanisms: the QSS concentrations productionRate solves first
+// (SI; the first lines of productionRate in a QSS mechanism.H)
+REF_API void ref_sc_qss(double* out, const double* sc_in, double T)
+{
+  const amrex::Real invT = 1.0 / T;
+  const amrex::Real logT = log(T);
+  amrex::Real sc[NUM_SPECIES];
+  std::memcpy(sc, sc_in, sizeof(sc));
+  amrex::Real g_RT[NUM_SPECIES];
+  gibbs(g_RT, T);
+  amrex::Real g_RT_qss[64], sc_qss[64];
+  amrex::Real kf_qss[2048], qf_qss[2048], qr_qss[2048];
+  gibbs_qss(g_RT_qss, T);
+  comp_k_f_qss(T, invT, logT, kf_qss);
+  comp_qss_coeff(kf_qss, qf_qss, qr_qss, sc, T, g_RT, g_RT_qss);
+  comp_sc_qss(sc_qss, qf_qss, qr_qss);
+  for (int q = 0; q < 64; q++) out[q] = sc_qss[q];
+}
+#endif
+
 // mechanism.H: CKWC (CGS wrapper, mol/cm^3 in, mol/cm^3/s out)
 REF_API void ref_CKWC(double T, const double* C, double* wdot)
 {
@@ -42,7 +63,10 @@ REF_API void ref_CKWC(double T, const double* C, double* wdot)
 // mechanism.H: aJacobian (SI concentrations)
 REF_API void ref_aJacobian(double* J, const double* sc, double T, int consP)
 {
-  aJacobian(J, sc, T, consP);
+  // a copy: the QSS mechanisms' aJacobian takes a non-const sc
+  double c[NUM_SPECIES];
+  std::memcpy(c, sc, sizeof(c));
+  aJacobian(J, c, T, consP);
 }
 // mechanism.H: DWDOT (CGS concentrations, rescaled T row/column)
 REF_API void ref_DWDOT(double* J, const double* sc, double T, int consP)

@@ -110,6 +110,21 @@ typedef struct PPBMechTables {
   const double* eff_m1; // efficiency - 1 (productionRate)
   const double* fo_d;   // PPB_NFOD per reaction
   const int* fo_i;      // PPB_NFOI per reaction
+  // QSS mechanisms (the reference's QSSA mechanisms; zero / null otherwise).
+  // The nqss species in steady state have no state entry and no rate: their
+  // concentrations are solved per evaluation from their linear balance
+  // (comp_sc_qss of the reference's generated mechanism.H).  Species slots of
+  // the reaction lists: 0..nsp-1 transported species, nsp the unit slot
+  // (concentration 1, g/RT 0), nsp+1+q the QSS species q; the thermo arrays
+  // and tmid have an entry per slot (the unit slot's is empty), mw and imw
+  // the transported species only.
+  int nqss;
+  int nrq;                          // reactions with a QSS species (k = 0..nrq-1)
+  const char* const* qss_species;
+  const int* q_rx;                  // [nrq] the reaction (evaluation order) of QSS reaction k
+  const int* q_off;                 // [nqss + 1] each QSS species' balance terms, in k order:
+  const int* q_term;                //   2 k + 0 (forward coefficient of k) or 2 k + 1 (reverse)
+  const int* q_role;                //   -1 production, -2 loss, j >= 0 production from QSS species j
 } PPBMechTables;
 
 #ifdef __cplusplus

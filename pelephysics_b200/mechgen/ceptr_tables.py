@@ -46,7 +46,7 @@ from collections import Counter, OrderedDict
 import numpy as np
 import yaml
 
-MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk"]
+MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "CH4_lean_qss"]
 
 RC = 1.98721558317399615845  # cal/mol/K
 ATOMIC_WEIGHTS = {
@@ -243,22 +243,65 @@ def sorted_by_species(d, idx):
     return sorted(d.items(), key=lambda kv: idx[kv[0]])
 
 
-def build(mech_dir, name):
-    y = yaml.safe_load(open(os.path.join(mech_dir, "mechanism.yaml")))
-    phase = y["phases"][0]
-    species = list(phase["species"])
-    idx = {s: i for i, s in enumerate(species)}
-    spdata = {s["name"]: s for s in y["species"]}
-    nsp = len(species)
+def mechanism_file(mech_dir):
+    """The mechanism's YAML: mechanism.yaml, or for a QSS mechanism of the
+    reference (CEPTR's QSSA input) qssa.yaml, whose phase lists the species
+    in steady state under ``qssa_species``."""
+    for f in ("mechanism.yaml", "qssa.yaml"):
+        path = os.path.join(mech_dir, f)
+        if os.path.exists(path):
+            return path
+    raise FileNotFoundError(f"no mechanism.yaml or qssa.yaml in {mech_dir}")
 
-    # --- species data
+
+def build(mech_dir, name):
+    y = yaml.safe_load(open(mechanism_file(mech_dir)))
+    # rate units: the Chemkin-converted mechanisms declare cm / mol / cal/mol;
+    # a file without a units entry (Cantera's writer, e.g. qssa.yaml) is in
+    # Cantera's own m / kmol / J/kmol, the units CEPTR converts from
+    units = y.get("units", {})
+    si_kmol = units.get("length", "m") == "m" and units.get("quantity", "kmol") == "kmol"
+    if si_kmol:
+        assert units.get("activation-energy", "J/kmol") == "J/kmol", units
+    else:
+        assert (units.get("length"), units.get("quantity"), units.get("activation-energy")) == (
+            "cm", "mol", "cal/mol"), units
+    phase = y["phases"][0]
+    all_species = list(phase["species"])
+    qss_set = set(phase.get("qssa_species", []))
+    # transported species keep the mechanism's order; the QSS species (in the
+    # mechanism's order too) take the slots after the unit slot nsp
+    species = [s for s in all_species if s not in qss_set]
+    qss = [s for s in all_species if s in qss_set]
+    nsp = len(species)
+    idx = {s: i for i, s in enumerate(species)}
+    idx.update({s: nsp + 1 + q for q, s in enumerate(qss)})
+    spdata = {s["name"]: s for s in y["species"]}
+    nonq = os.path.join(mech_dir, "non_qssa_list.yaml")
+    if qss and os.path.exists(nonq):
+        listed = yaml.safe_load(open(nonq))["species"]
+        assert listed == species, (listed, species)
+
+    # --- species data (mw, imw: transported species; thermo: transported,
+    # then for a QSS mechanism an empty entry for the unit slot and the QSS
+    # species, so that thermo entry == concentration slot)
     mw, imw, tmid, tlo, thi = [], [], [], [], []
     sets_lo, sets_hi = [], []
-    for s in species:
+    thermo_species = species + ([None] + qss if qss else [])
+    for s in thermo_species:
+        if s is None:
+            zero = {k: [0.0] * len(v) for k, v in thermo_sets([0.0] * 7).items()}
+            tmid.append(None)
+            tlo.append(0.0)
+            thi.append(0.0)
+            sets_lo.append(zero)
+            sets_hi.append(zero)
+            continue
         d = spdata[s]
-        w = species_weight(d["composition"])
-        mw.append(fmt(w, "f"))
-        imw.append(fmt(1.0 / w, ".16f"))
+        if s in idx and idx[s] < nsp:
+            w = species_weight(d["composition"])
+            mw.append(fmt(w, "f"))
+            imw.append(fmt(1.0 / w, ".16f"))
         th = d["thermo"]
         assert th["model"] == "NASA7", th["model"]
         rng = th["temperature-ranges"]
@@ -302,7 +345,13 @@ def build(mech_dir, name):
         A = float(r.rate["A"])
         beta = float(r.rate["b"])
         Ea = float(r.rate["Ea"])
-        if r.kind in (K_SIMPLE,):
+        if si_kmol:
+            # Cantera's values as they are: k in (m^3/kmol)^(order-1)/s to
+            # (m^3/mol)^(order-1)/s, Ea from J/kmol to cal/mol
+            korder = dim + 1 if r.kind in (K_THIRD, K_COLLIDER) else dim
+            pef = A * 1000.0 ** (1 - korder)
+            Ea = Ea / 4184.0
+        elif r.kind in (K_SIMPLE,):
             pef = A * 1e-6 ** (dim - 1)
         elif r.kind in (K_THIRD, K_COLLIDER):
             pef = A * 1e-6 ** dim
@@ -317,12 +366,13 @@ def build(mech_dir, name):
             # Cantera keeps the low-pressure factor in kmol units with one
             # more order than k_inf; CEPTR converts it with the k_inf factor
             # and rescales by 10**(-6 dim) * 10**(3**dim).
-            A0_cantera = A0 * 1e-3 ** dim
+            A0_cantera = A0 if si_kmol else A0 * 1e-3 ** dim
             low_pef = A0_cantera * 1000.0 ** (1 - dim)
             rec["P0"] = fmt(10 ** (-dim * 6) * low_pef * 10 ** 3 ** dim, ".15g")
             rec["k0"] = fmt(low_pef * 10 ** 3 ** dim, ".15g")
             rec["beta0"] = fmt(float(L["b"]), ".15g")
-            rec["EaR0"] = fmt(float(L["Ea"]) / RC, ".15g")
+            Ea0 = float(L["Ea"]) / 4184.0 if si_kmol else float(L["Ea"])
+            rec["EaR0"] = fmt(Ea0 / RC, ".15g")
             rec["prdim"] = float(f"1e-{int(dim * 6)}")
             if r.falloff == "Troe":
                 t = r.troe
@@ -347,6 +397,8 @@ def build(mech_dir, name):
                 rec["sri_n"] = len(s)
         # efficiencies (production.py:1504-1582; jacobian enhancement)
         eff = []
+        if r.third and any(s_ in qss_set for s_ in r.third):
+            raise NotImplementedError("a QSS species as third body")
         if r.kind in (K_THIRD, K_TROE, K_LINDEMANN, K_SRI):
             for s, e in sorted_by_species(r.third, idx):
                 eff.append((idx[s], fmt(e, ".15g"), fmt(e - 1.0, ".15g")))
@@ -359,7 +411,7 @@ def build(mech_dir, name):
         # Gibbs terms of the equilibrium exponent (utilities.py:293-388):
         # per species in index order, reactant term (+) then product term (-)
         terms = []
-        for s in species:
+        for s in species + qss:
             if s in r.reactants:
                 terms.append((idx[s], float(r.reactants[s])))
             if s in r.products:
@@ -375,6 +427,8 @@ def build(mech_dir, name):
         )
         wup = []
         for s, c in agents:
+            if s in qss_set:
+                continue  # no rate for a species in steady state
             if s in r.reactants and r.reactants[s] == c:
                 wup.append((idx[s], -float(c)))
             if s in r.products and r.products[s] == c:
@@ -386,7 +440,7 @@ def build(mech_dir, name):
         rea = dict(fwd) if r.is_collider else dict(r.reactants)
         pro = dict(rev) if r.is_collider else dict(r.products)
         jn = []
-        for k, s in enumerate(species):
+        for k, s in enumerate(species):  # transported species only
             if s in rea and s in pro:
                 nu = pro[s] - rea[s]
             elif s in rea:
@@ -403,8 +457,11 @@ def build(mech_dir, name):
         rec["hp"] = [(idx[s], float(v)) for s, v in sorted_by_species(pro, idx)]
         R.append(rec)
 
+    qss_info = qss_structure(order, qss, qss_set) if qss else None
     return {
         "name": name,
+        "qss": qss,
+        "qss_info": qss_info,
         "species": species,
         "mw": mw,
         "imw": imw,
@@ -415,6 +472,54 @@ def build(mech_dir, name):
         "hi": sets_hi,
         "rxns": R,
     }
+
+
+def qss_structure(order, qss, qss_set):
+    """The steady-state balance of each QSS species, as the reference's
+    generated comp_qss_coeff / comp_sc_qss form it
+    (Support/ceptr/ceptr/qssa_converter.py: qssa_coeff_functions,
+    qssa_component_functions): the reactions that involve a QSS species
+    (in evaluation order, k = 0 ..) give coefficients q_f,k and q_r,k, the
+    rates with the QSS concentration left out.  For QSS species i, in k order:
+    a reaction consuming i adds its coefficient to the loss (role -2); one
+    producing i from transported species only adds to the production
+    (role -1); one producing i from QSS species j adds to the coupling
+    with j (role j).  A reaction with more than one QSS species on a side,
+    or a QSS species of order above one, would make the balance nonlinear:
+    rejected, as the reference's converter rejects it."""
+    q_rx, terms = [], [[] for _ in qss]
+    qi = {s: q for q, s in enumerate(qss)}
+    for pos, r in enumerate(order):
+        rq = [s for s in r.reactants if s in qss_set]
+        pq = [s for s in r.products if s in qss_set]
+        if not rq and not pq:
+            continue
+        if len(rq) > 1 or len(pq) > 1 or any(r.reactants[s] != 1 for s in rq) or any(r.products[s] != 1 for s in pq):
+            raise NotImplementedError(f"nonlinear QSS reaction {r.eq}")
+        if rq and pq and rq[0] == pq[0]:
+            raise NotImplementedError(f"QSS species on both sides of {r.eq}")
+        k = len(q_rx)
+        q_rx.append(pos)
+        if rq:
+            i = qi[rq[0]]
+            terms[i].append((2 * k, -2))  # forward consumes i
+            if r.reversible:
+                terms[i].append((2 * k + 1, qi[pq[0]] if pq else -1))  # reverse produces i
+        if pq:
+            i = qi[pq[0]]
+            terms[i].append((2 * k, qi[rq[0]] if rq else -1))  # forward produces i
+            if r.reversible:
+                terms[i].append((2 * k + 1, -2))  # reverse consumes i
+    off, term, role = [0], [], []
+    for lst in terms:
+        for t, ro in lst:
+            term.append(t)
+            role.append(ro)
+        off.append(len(term))
+    for q, lst in enumerate(terms):
+        if not any(ro == -2 for _, ro in lst) or not any(ro != -2 for _, ro in lst):
+            raise ValueError(f"QSS species {qss[q]} is not both produced and consumed")
+    return {"q_rx": q_rx, "q_off": off, "q_term": term, "q_role": role}
 
 
 def _carr(ctype, name, vals, per_line=4):
@@ -438,7 +543,8 @@ def emit_header(M, path):
     P = f"ppbm_{name}_"
     out = []
     out.append(f"// Generated by pelephysics_b200/mechgen/ceptr_tables.py from\n")
-    out.append(f"// Mechanisms/{name}/mechanism.yaml of the reference. Do not edit.\n")
+    src = "qssa.yaml" if M["qss"] else "mechanism.yaml"
+    out.append(f"// Mechanisms/{name}/{src} of the reference. Do not edit.\n")
     out.append(f"#pragma once\n#include \"mech_tables.h\"\n\n")
     sp = ", ".join(f'"{s}"' for s in M["species"])
     out.append(f"static const char* const {P}species[] = {{{sp}}};\n")
@@ -447,7 +553,7 @@ def emit_header(M, path):
     out.append(_carr("double", P + "tmid", [t if t is not None else -1.0 for t in M["tmid"]]))
     for key, w in (("cv", 5), ("cp", 5), ("dcp", 4), ("u", 6), ("h", 6), ("g", 7)):
         vals = []
-        for s in range(nsp):
+        for s in range(len(M["lo"])):
             vals += M["lo"][s][key] + M["hi"][s][key]
         out.append(_carr("double", P + "th_" + key, vals, w))
     rx = M["rxns"]
@@ -519,6 +625,14 @@ def emit_header(M, path):
         fi += i
     out.append(_carr("double", P + "fo_d", fd, 17))
     out.append(_carr("int", P + "fo_i", fi, 8))
+    if M["qss"]:
+        qi = M["qss_info"]
+        qs = ", ".join(f'"{q}"' for q in M["qss"])
+        out.append(f"static const char* const {P}qss_species[] = {{{qs}}};\n")
+        out.append(_carr("int", P + "q_rx", qi["q_rx"], 16))
+        out.append(_carr("int", P + "q_off", qi["q_off"], 16))
+        out.append(_carr("int", P + "q_term", qi["q_term"], 16))
+        out.append(_carr("int", P + "q_role", qi["q_role"], 16))
     out.append(f"\nstatic const PPBMechTables ppbm_{name} = {{\n")
     out.append(f'  "{name}", {nsp}, {nr},\n')
     fields = [
@@ -529,6 +643,10 @@ def emit_header(M, path):
         fields += [f"rx_{key}_n", f"rx_{key}_sp", f"rx_{key}_c"]
     fields += ["eff_off", "eff_sp", "eff_e", "eff_m1", "fo_d", "fo_i"]
     out.append("".join(f"  {P}{f},\n" for f in fields))
+    if M["qss"]:
+        qi = M["qss_info"]
+        out.append(f"  {len(M['qss'])}, {len(qi['q_rx'])},\n")
+        out.append("".join(f"  {P}{f},\n" for f in ("qss_species", "q_rx", "q_off", "q_term", "q_role")))
     out.append("};\n")
     with open(path, "w") as fh:
         fh.write("".join(out))

@@ -172,23 +172,45 @@ class Reactor:
             check(code)
         return cost.value, dt.value, t.value, code
 
+    @staticmethod
+    def _array4(t, lo, hi, cls=_lib.Array4):
+        """Array4 view of a contiguous torch tensor [ncomp, nz, ny, nx]
+        covering exactly lo..hi."""
+        v = cls()
+        v.p = t.data_ptr()
+        nc, nz, ny, nx = t.shape
+        v.jstride, v.kstride, v.nstride = nx, nx * ny, nx * ny * nz
+        v.lo[:] = list(lo)
+        v.hi[:] = list(hi)
+        v.ncomp = nc
+        return v
+
+    def flatten(self, lo, hi, rY, rYsrc, T, rEner, rEner_src, y_vect, src_vect, vect_energy, src_vect_energy,
+                stream=None):
+        """ReactorBase::flatten on torch CUDA tensors: box arrays shaped
+        [ncomp, nz, ny, nx] into the component-major vectors y_vect[(N+1)
+        ncells], src_vect[N ncells], vect_energy[ncells],
+        src_vect_energy[ncells]."""
+        a4 = lambda t: self._array4(t, lo, hi)
+        check(lib().ppb_flatten(self._h, (C.c_int * 3)(*lo), (C.c_int * 3)(*hi), a4(rY), a4(rYsrc), a4(T), a4(rEner),
+                                a4(rEner_src), _ptr(y_vect), _ptr(src_vect), _ptr(vect_energy),
+                                _ptr(src_vect_energy), _stream(stream)))
+
+    def unflatten(self, lo, hi, rY, T, rEner, rEner_src, FC, y_vect, vect_energy, FCunt, dt_react, stream=None):
+        """ReactorBase::unflatten on torch CUDA tensors (FCunt: int64 per
+        cell)."""
+        a4 = lambda t: self._array4(t, lo, hi)
+        check(lib().ppb_unflatten(self._h, (C.c_int * 3)(*lo), (C.c_int * 3)(*hi), a4(rY), a4(T), a4(rEner),
+                                  a4(rEner_src), self._array4(FC, lo, hi, _lib.Array4i), _ptr(y_vect),
+                                  _ptr(vect_energy), _ptr(FCunt), float(dt_react), _stream(stream)))
+
     def react_box(self, lo, hi, rY, rYsrc, T, rEner, rEner_src, FC, mask=None, dt_react=0.0, time=0.0,
                   stream=None, raise_on_fail=True):
         """Box react on torch CUDA tensors shaped [ncomp, nz, ny, nx] that
         cover exactly the box lo..hi (inclusive)."""
         lo3 = (C.c_int * 3)(*lo)
         hi3 = (C.c_int * 3)(*hi)
-
-        def a4(t, cls=_lib.Array4):
-            v = cls()
-            v.p = t.data_ptr()
-            nc, nz, ny, nx = t.shape
-            v.jstride, v.kstride, v.nstride = nx, nx * ny, nx * ny * nz
-            v.lo[:] = list(lo)
-            v.hi[:] = list(hi)
-            v.ncomp = nc
-            return v
-
+        a4 = lambda t, cls=_lib.Array4: self._array4(t, lo, hi, cls)
         m = _lib.Array4i()
         if mask is not None:
             m = a4(mask, _lib.Array4i)

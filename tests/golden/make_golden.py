@@ -7,11 +7,12 @@ modes, CKUBMS/CKHBMS/CKCVBS/CKCPBS, CKUMS/CKHMS, gibbs, GET_T_GIVEN_EY/HY)
 on seeded random states, and the reference's SimpleTransport::transport
 (Source/Transport/Simple.H, compiled by oracle/build_ref.sh with the
 mechanism's transport fits) on seeded (T, rho, Y), and the reference's
-SRK equation of state (Source/Eos/SRK.H) on seeded (rho, T, Y).  The .npz files it writes
+SRK equation of state (Source/Eos/SRK.H) on seeded (rho, T, Y), and a QSS
+mechanism's productionRate with the QSS concentrations it solves.  The .npz files it writes
 are the committed fixtures the tests compare the CPU oracle and the CUDA
 kernels against.
 
-Usage: python tests/golden/make_golden.py [point|transport|srk]   (default all)
+Usage: python tests/golden/make_golden.py [point|transport|srk|qss]   (default all)
 """
 
 import os
@@ -94,6 +95,52 @@ def srk_main():
         print(mech, npts, os.path.getsize(path), "bytes")
 
 
+QSS_POINTS = {"CH4_lean_qss": 32}
+
+
+def qss_main():
+    """A QSS mechanism's compiled mechanism.H on seeded states: its
+    productionRate (with the QSS concentrations it solves, comp_sc_qss),
+    thermo, GET_T_GIVEN_EY/HY and the reactor right-hand side of both
+    reactor types over them (its aJacobian needs CEPTR's symbolic build and
+    is not used: the engine differences the right-hand side, as the
+    reference's dense_direct solve does)."""
+    for seed, (mech, npts) in enumerate(QSS_POINTS.items()):
+        R = po.Ref(mech)
+        N = R.nsp
+        nq = po.Mech(mech).nqss
+        T, sc, Y = states(N, npts, 4000 + seed)
+        out = {"T": T, "sc": sc, "Y": Y, "mw": R.mw(), "imw": R.imw()}
+        out["wdot"] = np.array([R.production_rate(sc[i], T[i]) for i in range(npts)])
+        out["sc_qss"] = np.array([R.qss_concentrations(sc[i], T[i], nq) for i in range(npts)])
+        out["gibbs"] = np.array([R.gibbs(t) for t in T])
+        out["ums"] = np.array([R.ckums(t) for t in T])
+        out["hms"] = np.array([R.ckhms(t) for t in T])
+        out["ubms"] = np.array([R.ckubms(T[i], Y[i]) for i in range(npts)])
+        out["hbms"] = np.array([R.ckhbms(T[i], Y[i]) for i in range(npts)])
+        out["cvbs"] = np.array([R.ckcvbs(T[i], Y[i]) for i in range(npts)])
+        out["cpbs"] = np.array([R.ckcpbs(T[i], Y[i]) for i in range(npts)])
+        Tguess = T + np.where(T > 1900.0, -150.0, 150.0)
+        out["Tguess"] = Tguess
+        out["T_ey"] = np.array([R.t_given_ey(out["ubms"][i], Y[i], Tguess[i])[0] for i in range(npts)])
+        out["T_hy"] = np.array([R.t_given_hy(out["hbms"][i], Y[i], Tguess[i])[0] for i in range(npts)])
+        # reactor right-hand side (SI-free CGS state rho Y, T) with sources
+        rng = np.random.default_rng(5000 + seed)
+        rho = 10.0 ** rng.uniform(-4, -2, npts)
+        y = np.c_[rho[:, None] * Y, T + 20.0]
+        src = rng.normal(size=(npts, N)) * 1e-3
+        rhoesrc = rng.normal(size=npts) * 1e4
+        out.update({"rho": rho, "y": y, "src": src, "rhoesrc": rhoesrc})
+        for rt, key in ((1, "ubms"), (2, "hbms")):
+            rhoe = rho * out[key]
+            out[f"rhoe{rt}"] = rhoe
+            res = [R.reactor_rhs(rt, 1e-7, y[i], rhoe[i], rhoesrc[i], src[i]) for i in range(npts)]
+            out[f"ydot{rt}"] = np.array([r[0] for r in res])
+        path = os.path.join(HERE, f"point_{mech}.npz")
+        np.savez_compressed(path, **out)
+        print(mech, npts, os.path.getsize(path), "bytes")
+
+
 def main():
     po.build()
     what = sys.argv[1] if len(sys.argv) > 1 else "all"
@@ -101,7 +148,9 @@ def main():
         transport_main()
     if what in ("all", "srk"):
         srk_main()
-    if what in ("transport", "srk"):
+    if what in ("all", "qss"):
+        qss_main()
+    if what in ("transport", "srk", "qss"):
         return
     for seed, (mech, npts) in enumerate(POINTS.items()):
         R = po.Ref(mech)
