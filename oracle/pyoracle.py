@@ -688,7 +688,7 @@ def mass_fraction_rows(rY, N):
 
 
 def compare_to_reference(mech, reactor_type, rY0, rYsrc, rX, rX_src, dt, y_test, y_ref, Y_atol=1e-8, k=16,
-                         k_more=256, nthreads=0, **opts):
+                         k_more=256, nthreads=0, T_rtol=1e-6, **opts):
     """Integration parity of y_test against the oracle's y_ref (both YCOrder,
     integrated from rY0 over dt with the options opts).
 
@@ -711,17 +711,21 @@ def compare_to_reference(mech, reactor_type, rY0, rYsrc, rX, rX_src, dt, y_test,
     y_ref (the reference's own rounding-level sensitivity at that cell).  A
     cell that passes neither way after k replicas gets k_more further ones.
 
+    The temperature is judged the same way against T_rtol (relative).
+
     Returns max relative T error, max abs Y error against y_ref, the cells
-    above Y_atol, the worst nearest-replica distance, and the cells that pass
-    neither way ("cells_failing")."""
+    above Y_atol, the worst nearest-replica distances, and the cells that pass
+    neither way in Y or in T ("cells_failing")."""
     N = rY0.shape[1] - 1
     Yt = mass_fraction_rows(y_test, N)
     Yr = mass_fraction_rows(y_ref, N)
     dY = np.abs(Yt - Yr).max(1)
     dT = np.abs(y_test[:, N] - y_ref[:, N]) / np.abs(y_ref[:, N])
-    over = np.nonzero(dY > Y_atol)[0]
+    over = np.nonzero((dY > Y_atol) | (dT > T_rtol))[0]
     nearest = dY.copy()
     spread = np.zeros_like(dY)
+    nearest_T = dT.copy()
+    spread_T = np.zeros_like(dT)
     replicas = np.zeros(dY.size, dtype=int)
 
     def replicate(cells, seeds):
@@ -732,10 +736,15 @@ def compare_to_reference(mech, reactor_type, rY0, rYsrc, rX, rX_src, dt, y_test,
             Yp = mass_fraction_rows(yp, N)
             nearest[cells] = np.minimum(nearest[cells], np.abs(Yp - Yt[cells]).max(1))
             spread[cells] = np.maximum(spread[cells], np.abs(Yp - Yr[cells]).max(1))
+            Tr = np.abs(y_ref[cells, N])
+            nearest_T[cells] = np.minimum(nearest_T[cells], np.abs(yp[:, N] - y_test[cells, N]) / Tr)
+            spread_T[cells] = np.maximum(spread_T[cells], np.abs(yp[:, N] - y_ref[cells, N]) / Tr)
             replicas[cells] += 1
 
     def failing_cells(cells):
-        return cells[~((nearest[cells] <= Y_atol) | (dY[cells] <= spread[cells]))]
+        ok_Y = (nearest[cells] <= Y_atol) | (dY[cells] <= spread[cells])
+        ok_T = (nearest_T[cells] <= T_rtol) | (dT[cells] <= spread_T[cells])
+        return cells[~(ok_Y & ok_T)]
 
     if over.size:
         replicate(over, range(1, k + 1))
@@ -747,5 +756,6 @@ def compare_to_reference(mech, reactor_type, rY0, rYsrc, rX, rX_src, dt, y_test,
         fail = over
     return {"cells": int(rY0.shape[0]), "max_rel_T": float(dT.max()), "max_abs_Y": float(dY.max()),
             "cells_over_Y_atol": int(over.size), "Y_atol": Y_atol,
-            "max_abs_Y_nearest_replica": float(nearest.max()), "max_replicas_per_cell": int(replicas.max()),
+            "max_abs_Y_nearest_replica": float(nearest.max()), "max_rel_T_nearest_replica": float(nearest_T.max()),
+            "max_replicas_per_cell": int(replicas.max()),
             "cells_failing": int(fail.size), "failing_cells": [int(c) for c in fail[:16]]}

@@ -20,7 +20,10 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libppb200.so")
 NVCC = os.environ.get("NVCC", "nvcc")
-SPECIES_COUNTS = (9, 21, 53, 88)
+SPECIES_COUNTS = (9, 13, 21, 53, 88)
+# species counts of the QSS mechanisms, compiled for their QSS kernel only
+# (no adjoint, no ReactorArkode)
+QSS_ONLY_COUNTS = (13,)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-diag-suppress", "177,550"]
 
@@ -42,9 +45,11 @@ def _units():
         for part in range(5):  # the kernel groups of one species count, compiled in parallel
             units.append((f"ppb_engine_ns{ns}_p{part}.o", "ppb_engine_ns.cu", [f"-DPPB_NS={ns}", f"-DPPB_PART={part}"]))
     for ns in SPECIES_COUNTS:
-        units.append((f"ppb_adjoint_ns{ns}.o", "ppb_adjoint_ns.cu", [f"-DPPB_NS={ns}"]))
+        if ns not in QSS_ONLY_COUNTS:
+            units.append((f"ppb_adjoint_ns{ns}.o", "ppb_adjoint_ns.cu", [f"-DPPB_NS={ns}"]))
     for ns in SPECIES_COUNTS:
-        units.append((f"ppb_ark_ns{ns}.o", "ppb_ark_ns.cu", [f"-DPPB_NS={ns}"]))
+        if ns not in QSS_ONLY_COUNTS:
+            units.append((f"ppb_ark_ns{ns}.o", "ppb_ark_ns.cu", [f"-DPPB_NS={ns}"]))
     return units
 
 

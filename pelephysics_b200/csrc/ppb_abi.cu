@@ -418,10 +418,10 @@ static LaunchConfig launch_config(const ppb_reactor* r)
   lc.engine = r->opt.engine;
   lc.lu_fp32 = r->opt.lu_fp32;
   lc.persistent = 1;
-  if (r->opt.eos == PPB_EOS_SRK) {
-    // one compiled SRK kernel: warp teams, <= 128 registers; the block size
-    // the caller gives, else the largest (<= 8 warps) that fits
-    lc.srk = 1;
+  if (r->opt.eos == PPB_EOS_SRK || r->t->nqss > 0) {
+    // one compiled SRK or QSS kernel: warp teams, <= 128 registers; the
+    // block size the caller gives, else the largest (<= 8 warps) that fits
+    lc.rhsv = r->opt.eos == PPB_EOS_SRK ? 1 : 2;
     lc.team = 32;
     lc.minb = 2;
     if (r->opt.warps_per_block > 0) {
@@ -580,7 +580,7 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
 // Run the autotuner on this batch unless the stream is being captured.
 static int maybe_autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
 {
-  if (r->method == METHOD_ARK || r->opt.eos == PPB_EOS_SRK || r->opt.engine != PPB_ENGINE_TUNED ||
+  if (r->method == METHOD_ARK || r->opt.eos == PPB_EOS_SRK || r->t->nqss > 0 || r->opt.engine != PPB_ENGINE_TUNED ||
       r->opt.warps_per_block > 0)
     return 0;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -731,6 +731,16 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
         r->opt.lu_fp32)
       return fail(PPB_E_ARG, "the SRK EOS needs ReactorCvode, reactor type 1, the tuned engine and the FP64 LU");
     if (!find_srk(r->t->name)) return fail(PPB_E_MECH, "the mechanism has no SRK parameters");
+  }
+  if (r->t->nqss > 0) {
+    // a QSS mechanism: the QSS species solved in every right-hand side, the
+    // Jacobian by differences (the reference's dense_direct solve; its
+    // analytical QSS Jacobian needs CEPTR's symbolic build); one compiled
+    // kernel, the tuned FP64 BDF
+    if (r->method != METHOD_BDF || r->opt.engine != PPB_ENGINE_TUNED || r->opt.lu_fp32 ||
+        r->opt.eos != PPB_EOS_IDEAL)
+      return fail(PPB_E_ARG, "a QSS mechanism needs ReactorCvode, the tuned engine, the FP64 LU and the ideal-gas EOS");
+    if (r->opt.warps_per_block > 8) return fail(PPB_E_ARG, "a QSS mechanism runs at most 8 warps per block");
   }
   r->reactor_type = reactor_type;
   int e = 0;
@@ -1458,6 +1468,7 @@ static int run_adjoint(ppb_reactor* r, int mode, AdjBatch b, double dt, double* 
   if (r->method != METHOD_BDF)
     return fail(PPB_E_ARG, "adjoint: only the BDF integrator (ReactorCvode) is differentiated");
   if (r->opt.eos != PPB_EOS_IDEAL) return fail(PPB_E_ARG, "adjoint: the ideal-gas EOS only");
+  if (r->t->nqss > 0) return fail(PPB_E_ARG, "adjoint: not for QSS mechanisms");
   if (r->opt.engine != PPB_ENGINE_TUNED) return fail(PPB_E_ARG, "adjoint: runs on the tuned engine only");
   if (b.ncells < 0 || (b.ncells > 0 && (!b.y0 || !b.rhoe))) return fail(PPB_E_ARG, "adjoint: invalid arguments");
   if (mode == ADJ_REVERSE && b.ncells > 0 && !b.lam_y) return fail(PPB_E_ARG, "adjoint: lam_y is required");

@@ -61,6 +61,7 @@ struct Work {
   struct BdfArrays* ba; // the integrator's coefficient arrays (team-shared)
   // rate scratch
   double *Y, *sc, *g, *qd, *wdot, *ei, *h1, *h2, *h3;
+  double* qco = nullptr; // QSS solve scratch (QSS mechanisms)
   // block-shared rendezvous counters {arrived, generation, active warps}, or nullptr
   int* rv = nullptr;
 };
@@ -124,10 +125,14 @@ __device__ __forceinline__ void rendezvous_leave(int* rv)
   }
 }
 
-template <int TEAM>
+// QSS: a QSS mechanism (sc and g then have its QSS slots, qco the QSS
+// solve's scratch; the team path solves the QSS concentrations only when
+// QSS is set, the one-lane path whenever the mechanism has QSS species).
+template <int TEAM, bool QSS = false>
 __device__ double reactor_rhs(
   const Team<TEAM>& tm, const DevMech& M, int rtype, double t, const double* y, double* ydot, double rhoe,
-  double rhoesrc, const double* src, double* Y, double* sc, double* g, double* qd, double* wdot, double* ei)
+  double rhoesrc, const double* src, double* Y, double* sc, double* g, double* qd, double* wdot, double* ei,
+  double* qco = nullptr)
 {
   const int N = M.nsp;
   double a = 0.0;
@@ -142,7 +147,7 @@ __device__ double reactor_rhs(
   t_from_energy(tm, M, EH, nrg, Y, T);
   const double invT = 1.0 / T;
   const double RT = RU * T;
-  RateScratch rs{sc, g, qd};
+  RateScratch rs{sc, g, qd, nullptr, qco};
   double cv;
   if constexpr (TEAM > 1) {
     // one pass over the species at the final T: the heat capacity (as
@@ -168,6 +173,7 @@ __device__ double reactor_rhs(
       g[N] = 0.0;
     }
     tm.sync();
+    if constexpr (QSS) qss_solve<TEAM>(tm, M, sc, g, T, invT, logT, refC, refCinv, mixture, qco, qco + 2 * M.nrq);
     production_rate_core(tm, M, wdot, sc, T, invT, logT, refC, refCinv, mixture, rs);
   } else {
     cv = mix_c(tm, M, EH, T, Y);
@@ -469,15 +475,20 @@ struct CellIn {
 #ifndef PPB_RHS_ATTR
 #define PPB_RHS_ATTR __forceinline__
 #endif
-template <int TEAM, bool SRK>
+// The right-hand side variants of the integrator (the RHSV template
+// argument): the ideal-gas reactor, the SRK e-reactor, the ideal-gas reactor
+// of a QSS mechanism.  The last two have no analytical Jacobian.
+enum : int { RHS_IDEAL = 0, RHS_SRK = 1, RHS_QSS = 2 };
+
+template <int TEAM, int RHSV>
 __device__ PPB_RHS_ATTR void bdf_rhs(Team<TEAM> tm, const DevMech& M, int rtype, double t, const double* y,
                                      double* fy, double rhoe, double rhoesrc, const double* src, double* Y,
-                                     double* sc, double* g, double* qd, double* wdot, double* ei)
+                                     double* sc, double* g, double* qd, double* wdot, double* ei, double* qco)
 {
-  if constexpr (SRK) {
+  if constexpr (RHSV == RHS_SRK) {
     reactor_rhs_srk<TEAM>(tm, M, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei);
   } else {
-    reactor_rhs<TEAM>(tm, M, rtype, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei);
+    reactor_rhs<TEAM, RHSV == RHS_QSS>(tm, M, rtype, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei, qco);
   }
 }
 
@@ -489,7 +500,7 @@ struct NoRec {
   static constexpr bool on = false;
 };
 
-template <int NS, int TEAM, typename LT, typename Rec = NoRec, bool SRK = false>
+template <int NS, int TEAM, typename LT, typename Rec = NoRec, int RHSV = RHS_IDEAL>
 struct Bdf {
   static constexpr int n = NS + 1;
   static constexpr int PER = (NS + TEAM - 1) / TEAM;
@@ -543,8 +554,8 @@ struct Bdf {
   {
     if (w.rv) rendezvous(w.rv, o.rendezvous);
     PPB_TIC(PH_RHS);
-    bdf_rhs<TEAM, SRK>(tm, M, o.reactor_type, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
-                       w.ei);
+    bdf_rhs<TEAM, RHSV>(tm, M, o.reactor_type, t, y, fy, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
+                        w.ei, w.qco);
     s.nfe++;
     PPB_TOC(PH_RHS);
   }
@@ -552,7 +563,7 @@ struct Bdf {
   __device__ __forceinline__ void jac()
   {
     PPB_TIC(PH_JAC);
-    if constexpr (SRK) {
+    if constexpr (RHSV != RHS_IDEAL) {
       jac_dq();
     } else {
       // the Newton matrix region is free while the Jacobian is formed: it
@@ -591,8 +602,10 @@ struct Bdf {
 
   // Difference-quotient dense Jacobian at (tn, y) with f(tn, y) in ftemp:
   // the SRK EOS has no analytical Jacobian (SRK::RTY2JAC aborts,
-  // Source/Eos/SRK.H:640-648), so the reference's CVODE forms it by
-  // differences; restated from CVODE's dense difference-quotient Jacobian:
+  // Source/Eos/SRK.H:640-648), nor a QSS mechanism without CEPTR's symbolic
+  // build (aJacobian_precond aborts in its mechanism.H), so the reference's
+  // CVODE forms it by differences (cvode.solve_type = dense_direct);
+  // restated from CVODE's dense difference-quotient Jacobian:
   // column j uses inc = max(sqrt(eps) |y_j|, min_inc / ewt_j), min_inc =
   // 1000 |h| eps n ||f||_WRMS (1 when ||f|| = 0).  Its RHS evaluations are
   // not counted in nfe (CVODE counts them separately).
@@ -611,8 +624,8 @@ struct Bdf {
       if (tm.lane == 0) w.tempv[j] = yj + inc;
       tm.sync();
       double* col = w.J + (size_t)j * n;
-      reactor_rhs_srk<TEAM>(tm, M, s.tn, w.tempv, col, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g, w.qd, w.wdot,
-                            w.ei);
+      bdf_rhs<TEAM, RHSV>(tm, M, o.reactor_type, s.tn, w.tempv, col, cin.rhoe, cin.rhoesrc, w.src, w.Y, w.sc, w.g,
+                          w.qd, w.wdot, w.ei, w.qco);
       const double inc_inv = 1.0 / inc;
       for (int i = tm.lane; i < n; i += TEAM) col[i] = inc_inv * col[i] + (-inc_inv) * w.ftemp[i];
       if (tm.lane == 0) w.tempv[j] = yj;

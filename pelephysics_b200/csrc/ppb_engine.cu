@@ -21,6 +21,7 @@
 #include "mech/mech_drm19.h"
 #include "mech/mech_dodecane_lu.h"
 #include "mech/mech_heptane_lu_88sk.h"
+#include "mech/mech_CH4_lean_qss.h"
 
 namespace ppb {
 
@@ -30,6 +31,7 @@ const PPBMechTables* find_mechanism(const char* name)
   if (!strcmp(name, "drm19")) return &ppbm_drm19;
   if (!strcmp(name, "dodecane_lu")) return &ppbm_dodecane_lu;
   if (!strcmp(name, "heptane_lu_88sk")) return &ppbm_heptane_lu_88sk;
+  if (!strcmp(name, "CH4_lean_qss")) return &ppbm_CH4_lean_qss;
   return nullptr;
 }
 
@@ -83,16 +85,20 @@ static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
   dm = DevMech{};
   dm.nsp = N;
   dm.nrxn = R;
+  dm.nqss = t->nqss;
+  dm.nrq = t->nrq;
+  // thermo entries: one per concentration slot for a QSS mechanism
+  const int NT = t->nqss > 0 ? N + 1 + t->nqss : N;
 #define PPB_ADD(field, ptr, count) set_off(dm.field, pk.add(ptr, count))
   PPB_ADD(mw, t->mw, N);
   PPB_ADD(imw, t->imw, N);
-  PPB_ADD(tmid, t->tmid, N);
-  PPB_ADD(th_cv, t->th_cv, N * 10);
-  PPB_ADD(th_cp, t->th_cp, N * 10);
-  PPB_ADD(th_dcp, t->th_dcp, N * 8);
-  PPB_ADD(th_u, t->th_u, N * 12);
-  PPB_ADD(th_h, t->th_h, N * 12);
-  PPB_ADD(th_g, t->th_g, N * 14);
+  PPB_ADD(tmid, t->tmid, NT);
+  PPB_ADD(th_cv, t->th_cv, NT * 10);
+  PPB_ADD(th_cp, t->th_cp, NT * 10);
+  PPB_ADD(th_dcp, t->th_dcp, NT * 8);
+  PPB_ADD(th_u, t->th_u, NT * 12);
+  PPB_ADD(th_h, t->th_h, NT * 12);
+  PPB_ADD(th_g, t->th_g, NT * 14);
   PPB_ADD(rx_kind, t->rx_kind, R);
   PPB_ADD(rx_rev, t->rx_rev, R);
   PPB_ADD(rx_kcpow, t->rx_kcpow, R);
@@ -127,6 +133,19 @@ static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
   PPB_ADD(eff_m1, t->eff_m1, t->eff_off[R]);
   PPB_ADD(fo_d, t->fo_d, R * PPB_NFOD);
   PPB_ADD(fo_i, t->fo_i, R * PPB_NFOI);
+  if (t->nqss > 0) {
+    PPB_ADD(q_rx, t->q_rx, t->nrq);
+    PPB_ADD(q_off, t->q_off, t->nqss + 1);
+    PPB_ADD(q_term, t->q_term, t->q_off[t->nqss]);
+    PPB_ADD(q_role, t->q_role, t->q_off[t->nqss]);
+    // the balance solve keeps a 32-bit coupling mask; slots are bytes
+    if (t->nqss > 32 || N + 1 + t->nqss > 255) pk.overflow = true;
+  } else {
+    PPB_ADD(q_rx, t->rx_kind, 0);
+    PPB_ADD(q_off, t->rx_kind, 0);
+    PPB_ADD(q_term, t->rx_kind, 0);
+    PPB_ADD(q_role, t->rx_kind, 0);
+  }
 #undef PPB_ADD
   // gather lists, written entry by entry at exact offsets (no temporary
   // containers, so packing itself allocates nothing)
@@ -451,7 +470,8 @@ void free_mechanism(DeviceMechanism* m)
 
 size_t team_cell_bytes(const PPBMechTables* t, int lu_fp32)
 {
-  return lu_fp32 ? team_bytes<float>(t->nsp, t->nrxn) : team_bytes<double>(t->nsp, t->nrxn);
+  return lu_fp32 ? team_bytes<float>(t->nsp, t->nrxn, t->nqss, t->nrq)
+                 : team_bytes<double>(t->nsp, t->nrxn, t->nqss, t->nrq);
 }
 
 #define PPB_DECL(NS)                                                                                              \
@@ -460,6 +480,7 @@ size_t team_cell_bytes(const PPBMechTables* t, int lu_fp32)
   int launch_ajacobian_##NS(const DevMech&, const double*, const double*, int, double*, int, int, cudaStream_t);      \
   int react_occupancy_##NS(const DevMech&, int, const LaunchConfig&);
 PPB_DECL(9)
+PPB_DECL(13)
 PPB_DECL(21)
 PPB_DECL(53)
 PPB_DECL(88)
@@ -487,6 +508,8 @@ int launch_react(const DeviceMechanism& m, const Options& o, int method, const L
   switch (m.host->nsp) {
   case 9:
     return launch_react_9(m, o, method, lc, b, dt, queue, st);
+  case 13:
+    return launch_react_13(m, o, method, lc, b, dt, queue, st);
   case 21:
     return launch_react_21(m, o, method, lc, b, dt, queue, st);
   case 53:
@@ -503,6 +526,7 @@ int react_occupancy(const DeviceMechanism& m, int method, const LaunchConfig& lc
   const DevMech& M = *m.dm;
   switch (M.nsp) {
   case 9: return react_occupancy_9(M, method, lc);
+  case 13: return react_occupancy_13(M, method, lc);
   case 21: return react_occupancy_21(M, method, lc);
   case 53: return react_occupancy_53(M, method, lc);
   case 88: return react_occupancy_88(M, method, lc);
@@ -563,6 +587,10 @@ int launch_soa_to_aos(const double* soa, int ld, int ncomp, double* aos, int nc_
 
 // ------------------------------------------------------------ pointwise
 
+// One thread per cell touches only sc, g and wdot of the point layout (the
+// net-rate scratch serves the teams): the extent of its local buffer.
+__host__ __device__ inline size_t point1_doubles(int N) { return 3 * ((size_t)N + 1); }
+
 template <int TEAM>
 __global__ void k_production_rate(DevMech M, const double* sc, const double* T, double* wdot, int ncells)
 {
@@ -573,17 +601,24 @@ __global__ void k_production_rate(DevMech M, const double* sc, const double* T, 
   const int slot = threadIdx.x / TEAM;
   const int c = blockIdx.x * per_block + slot;
   double local[8 * 96];
-  double* base = (TEAM == 1) ? local : psm + (size_t)slot * point_doubles(N, M.nrxn, false);
+  const size_t pd = point_doubles(N, M.nrxn, false);
+  double* base = (TEAM == 1) ? local : psm + (size_t)slot * (pd + point_qss_doubles(N, M.nqss, M.nrq));
   if (TEAM == 1 && c >= ncells) return;
   const int cc = c < ncells ? c : ncells - 1;
   double* s_sc = base;
   double* s_g = base + (N + 1);
   double* s_w = base + 2 * (N + 1);
   double* s_qd = base + 8 * (N + 1);
+  double* qco = nullptr;
+  if (M.nqss > 0) { // the QSS tail: sc and g over all slots, the solve's scratch
+    s_sc = base + (TEAM == 1 ? point1_doubles(N) : pd);
+    s_g = s_sc + (N + 1 + M.nqss);
+    qco = s_g + (N + 1 + M.nqss);
+  }
   for (int s = tm.lane; s < N; s += TEAM) s_sc[s] = sc[(size_t)cc * N + s];
   if (tm.lane == 0) s_sc[N] = 1.0; // padding slot of the packed reaction records
   tm.sync();
-  RateScratch rs{s_sc, s_g, s_qd};
+  RateScratch rs{s_sc, s_g, s_qd, nullptr, qco};
   production_rate<TEAM>(tm, M, s_w, s_sc, T[cc], rs);
   if (c < ncells)
     for (int s = tm.lane; s < N; s += TEAM) wdot[(size_t)c * N + s] = s_w[s];
@@ -602,7 +637,16 @@ __global__ void k_t_from_energy(DevMech M, int eh, const double* e, const double
   if (c < ncells && tm.lane == 0) T[c] = t;
 }
 
-template <int TEAM>
+// doubles of one cell of k_reactor_rhs (with the QSS tail of a QSS
+// mechanism); one thread per cell uses the first 8 (N + 1) and the tail
+// (its rates need no net-rate scratch), placed there
+__host__ __device__ inline size_t rhs_point_doubles(const DevMech& M, bool one_thread)
+{
+  const size_t n = M.nsp + 1;
+  return (one_thread ? 8 * n : 10 * n + M.nrxn) + point_qss_doubles(M.nsp, M.nqss, M.nrq);
+}
+
+template <int TEAM, bool QSS>
 __global__ void k_reactor_rhs(DevMech M, int rtype, double t, const double* y, const double* rhoe,
                               const double* rhoesrc, const double* src, double* ydot, int ncells)
 {
@@ -615,7 +659,7 @@ __global__ void k_reactor_rhs(DevMech M, int rtype, double t, const double* y, c
   double local[10 * 96];
   if (TEAM == 1 && c >= ncells) return;
   const int cc = c < ncells ? c : ncells - 1;
-  double* base = (TEAM == 1) ? local : psm + (size_t)slot * (10 * (size_t)n + M.nrxn);
+  double* base = (TEAM == 1) ? local : psm + (size_t)slot * rhs_point_doubles(M, false);
   double* s_y = base;
   double* s_f = base + n;
   double* s_src = base + 2 * n;
@@ -625,12 +669,18 @@ __global__ void k_reactor_rhs(DevMech M, int rtype, double t, const double* y, c
   double* wb = base + 6 * n;
   double* eb = base + 7 * n;
   double* qd = base + 10 * n;
+  double* qco = nullptr;
+  if (M.nqss > 0) { // the QSS tail: sc and g over all slots, the solve's scratch
+    scb = base + (TEAM == 1 ? 8 * n : 10 * n + M.nrxn);
+    gb = scb + (n + M.nqss);
+    qco = gb + (n + M.nqss);
+  }
   for (int i = tm.lane; i < n; i += TEAM) {
     s_y[i] = y[(size_t)cc * n + i];
     s_src[i] = (i < N) ? src[(size_t)cc * N + i] : 0.0;
   }
   tm.sync();
-  reactor_rhs<TEAM>(tm, M, rtype, t, s_y, s_f, rhoe[cc], rhoesrc[cc], s_src, Yb, scb, gb, qd, wb, eb);
+  reactor_rhs<TEAM, QSS>(tm, M, rtype, t, s_y, s_f, rhoe[cc], rhoesrc[cc], s_src, Yb, scb, gb, qd, wb, eb, qco);
   if (c < ncells)
     for (int i = tm.lane; i < n; i += TEAM) ydot[(size_t)c * n + i] = s_f[i];
 }
@@ -641,10 +691,13 @@ int launch_production_rate(const DeviceMechanism& m, const double* sc, const dou
   const DevMech& M = *m.dm;
   if (ncells <= 0) return 0;
   if (team == 1) {
+    // one thread per cell: the cell's arrays in an 8 x 96-double local buffer
+    if (point1_doubles(M.nsp) + point_qss_doubles(M.nsp, M.nqss, M.nrq) > 8 * 96) return (int)cudaErrorNotSupported;
     k_production_rate<1><<<(ncells + 63) / 64, 64, 0, st>>>(M, sc, T, wdot, ncells);
   } else {
     const int cells_per_block = 4;
-    const size_t shm = point_doubles(M.nsp, M.nrxn, false) * 8 * cells_per_block;
+    const size_t shm =
+      (point_doubles(M.nsp, M.nrxn, false) + point_qss_doubles(M.nsp, M.nqss, M.nrq)) * 8 * cells_per_block;
     cudaFuncSetAttribute((const void*)k_production_rate<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     k_production_rate<32><<<(ncells + cells_per_block - 1) / cells_per_block, 32 * cells_per_block, shm, st>>>(
       M, sc, T, wdot, ncells);
@@ -765,6 +818,8 @@ int launch_ajacobian(const DeviceMechanism& m, const double* sc, const double* T
   switch (M.nsp) {
   case 9:
     return launch_ajacobian_9(M, sc, T, consP, J, ncells, team, st);
+  case 13:
+    return launch_ajacobian_13(M, sc, T, consP, J, ncells, team, st);
   case 21:
     return launch_ajacobian_21(M, sc, T, consP, J, ncells, team, st);
   case 53:
@@ -796,12 +851,16 @@ int launch_reactor_rhs(const DeviceMechanism& m, int reactor_type, double t, con
   if (ncells <= 0) return 0;
   const DevMech& M = *m.dm;
   if (team == 1) {
-    k_reactor_rhs<1><<<(ncells + 63) / 64, 64, 0, st>>>(M, reactor_type, t, y, rhoe, rhoesrc, src, ydot, ncells);
+    // one thread per cell: the cell's arrays in a 10 x 96-double local buffer
+    if (rhs_point_doubles(M, true) > 10 * 96) return (int)cudaErrorNotSupported;
+    k_reactor_rhs<1, false><<<(ncells + 63) / 64, 64, 0, st>>>(M, reactor_type, t, y, rhoe, rhoesrc, src, ydot,
+                                                                 ncells);
   } else {
     const int cells_per_block = 4;
-    const size_t shm = (10 * (size_t)(M.nsp + 1) + M.nrxn) * 8 * cells_per_block;
-    cudaFuncSetAttribute((const void*)k_reactor_rhs<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-    k_reactor_rhs<32><<<(ncells + cells_per_block - 1) / cells_per_block, 32 * cells_per_block, shm, st>>>(
+    const size_t shm = rhs_point_doubles(M, false) * 8 * cells_per_block;
+    auto k = M.nqss > 0 ? k_reactor_rhs<32, true> : k_reactor_rhs<32, false>;
+    cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    k<<<(ncells + cells_per_block - 1) / cells_per_block, 32 * cells_per_block, shm, st>>>(
       M, reactor_type, t, y, rhoe, rhoesrc, src, ydot, ncells);
   }
   return (int)cudaGetLastError();

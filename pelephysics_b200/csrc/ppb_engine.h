@@ -54,7 +54,8 @@ struct LaunchConfig {
   int team = 32;      // lanes per cell: 32; 16 for <= 21 species; 64 (33..64 species) or 128 (65..128): one
                       // multi-warp team per block
   int minb = 2;       // register budget: >= minb blocks of 256 threads per SM
-  int srk = 0;        // the SRK e-reactor kernel (warp teams, <= 128 registers)
+  int rhsv = 0;       // right-hand side: 0 ideal gas, 1 the SRK e-reactor, 2 a QSS mechanism (the last two:
+                      // warp teams, <= 128 registers, difference-quotient Jacobian)
 };
 // Resident cells per SM of the tuned kernel in configuration lc (0: the
 // configuration does not fit or is not compiled).

@@ -13,7 +13,7 @@
 namespace ppb {
 
 // ------------------------------------------------------------ react kernels
-template <int NS, int TEAM, typename LT, int METHOD, bool SRK = false>
+template <int NS, int TEAM, typename LT, int METHOD, int RHSV = RHS_IDEAL>
 __device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options& o, Work<LT>& w, const Batch& b,
                           int c, double dt)
 {
@@ -36,7 +36,7 @@ __device__ void react_one(const Team<TEAM>& tm, const DevMech& M, const Options&
   const CellIn cin{b.rhoe[c], b.rhoesrc[c]};
   int flag, cost;
   if (METHOD == METHOD_BDF) {
-    Bdf<NS, TEAM, LT, NoRec, SRK> bdf(tm, M, o, w, cin);
+    Bdf<NS, TEAM, LT, NoRec, RHSV> bdf(tm, M, o, w, cin);
     flag = bdf.run(dt);
     cost = bdf.s.nfe;
     if (b.stats && tm.lane == 0) {
@@ -149,7 +149,7 @@ __device__ __forceinline__ void react_team_body(const Team<TEAM>& tm, const DevM
 // doubles for its cross-warp reductions.  MAXT = 384 / 512 are the 12- and
 // 16-warp blocks (one block per SM, <= 168 / <= 128 registers) whose warps
 // share one rendezvous.
-template <int NS, typename LT, int METHOD, int TEAM, int MINB, bool SRK = false, int MAXT = 256>
+template <int NS, typename LT, int METHOD, int TEAM, int MINB, int RHSV = RHS_IDEAL, int MAXT = 256>
 __global__ void __launch_bounds__(MAXT, MINB) k_react_team(const __grid_constant__ DevMech M,
                                                           const __grid_constant__ Options o,
                                                           const __grid_constant__ Batch b, double dt, int* queue,
@@ -165,7 +165,11 @@ __global__ void __launch_bounds__(MAXT, MINB) k_react_team(const __grid_constant
     Team<TEAM> tm;
     const int team = threadIdx.x / TEAM;
     Work<LT> w;
-    carve<LT>(w, smem + (size_t)team * cell_bytes, NS, M.nrxn);
+    if constexpr (RHSV == RHS_QSS) {
+      carve<LT>(w, smem + (size_t)team * cell_bytes, NS, M.nrxn, M.nqss, M.nrq);
+    } else {
+      carve<LT>(w, smem + (size_t)team * cell_bytes, NS, M.nrxn);
+    }
     const int tpb = blockDim.x / TEAM;
     if (persistent) {
       __shared__ int rv[3];
@@ -175,12 +179,12 @@ __global__ void __launch_bounds__(MAXT, MINB) k_react_team(const __grid_constant
         if (tm.lane == 0) c = atomicAdd(queue, 1);
         c = __shfl_sync(tm.mask, c, 0, TEAM);
         if (c >= b.ncells) break;
-        react_one<NS, TEAM, LT, METHOD, SRK>(tm, M, o, w, b, b.order ? b.order[c] : c, dt);
+        react_one<NS, TEAM, LT, METHOD, RHSV>(tm, M, o, w, b, b.order ? b.order[c] : c, dt);
       }
       rendezvous_leave(w.rv);
     } else {
       const int c = blockIdx.x * tpb + team;
-      if (c < b.ncells) react_one<NS, TEAM, LT, METHOD, SRK>(tm, M, o, w, b, c, dt);
+      if (c < b.ncells) react_one<NS, TEAM, LT, METHOD, RHSV>(tm, M, o, w, b, c, dt);
     }
   }
 }
@@ -206,68 +210,87 @@ constexpr int big_team()
 //   2: the multi-warp teams (FP64 and FP32 BDF, RK64)
 //   3: FP32 BDF and RK64 with 32 lanes, the 16-lane variants, the SRK kernel
 //   4: FP32 BDF, 32 lanes, 12 and 16 warps per block
+// Species counts compiled for a QSS mechanism only (CH4_lean_qss: 13
+// transported species): the one QSS kernel, no other variant.
+template <int NS>
+constexpr bool qss_only()
+{
+  return NS == 13;
+}
+
 template <int NS>
 static TeamKernel team_kernel_part(int method, bool fp32, int team, int minb, int srk, int wpb)
 {
   constexpr bool small = NS <= 21;
   constexpr int P = PPB_PART;
-  // 12 or 16 warps per block (one block per SM: <= 168 or <= 128 registers):
-  // the FP64 BDF warp-per-cell kernel
-  if (wpb > 8) {
-    if (method != METHOD_BDF || team != 32 || minb != 2 || srk) return nullptr;
-    if constexpr (P == 1) {
-      if (fp32) return nullptr;
-      if (wpb == 16) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 512>;
-      if (wpb == 12) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, false, 384>;
-    }
-    if constexpr (P == 4) {
-      if (!fp32) return nullptr;
-      if (wpb == 16) return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 1, false, 512>;
-      if (wpb == 12) return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 1, false, 384>;
-    }
-    return nullptr;
-  }
-  // the SRK e-reactor: FP64 BDF, one warp per cell, <= 128 registers
-  if (srk) {
+  // the QSS reactor (srk == RHS_QSS): FP64 BDF, one warp per cell, <= 128
+  // registers, difference-quotient Jacobian
+  if constexpr (qss_only<NS>()) {
     if constexpr (P == 3)
-      return (method == METHOD_BDF && !fp32 && team == 32 && minb == 2)
-               ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, true>
+      return (srk == RHS_QSS && method == METHOD_BDF && !fp32 && team == 32 && minb == 2 && wpb <= 8)
+               ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, RHS_QSS>
                : nullptr;
     return nullptr;
-  }
-  if (team > 32) {
-    if constexpr (big_team<NS>() > 0 && P == 2) {
-      constexpr int BT = big_team<NS>();
-      if (team != BT) return nullptr;
-      if (method == METHOD_RK64) return (TeamKernel)k_react_team<NS, double, METHOD_RK64, BT, 1>;
-      if (fp32) return (TeamKernel)k_react_team<NS, float, METHOD_BDF, BT, 1>;
-      return (TeamKernel)k_react_team<NS, double, METHOD_BDF, BT, 1>;
+  } else {
+    if (srk == RHS_QSS) return nullptr;
+    // 12 or 16 warps per block (one block per SM: <= 168 or <= 128 registers):
+    // the FP64 BDF warp-per-cell kernel
+    if (wpb > 8) {
+      if (method != METHOD_BDF || team != 32 || minb != 2 || srk) return nullptr;
+      if constexpr (P == 1) {
+        if (fp32) return nullptr;
+        if (wpb == 16) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, RHS_IDEAL, 512>;
+        if (wpb == 12) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, RHS_IDEAL, 384>;
+      }
+      if constexpr (P == 4) {
+        if (!fp32) return nullptr;
+        if (wpb == 16) return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 1, RHS_IDEAL, 512>;
+        if (wpb == 12) return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 1, RHS_IDEAL, 384>;
+      }
+      return nullptr;
+    }
+    // the SRK e-reactor: FP64 BDF, one warp per cell, <= 128 registers
+    if (srk) {
+      if constexpr (P == 3)
+        return (method == METHOD_BDF && !fp32 && team == 32 && minb == 2)
+                 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, RHS_SRK>
+                 : nullptr;
+      return nullptr;
+    }
+    if (team > 32) {
+      if constexpr (big_team<NS>() > 0 && P == 2) {
+        constexpr int BT = big_team<NS>();
+        if (team != BT) return nullptr;
+        if (method == METHOD_RK64) return (TeamKernel)k_react_team<NS, double, METHOD_RK64, BT, 1>;
+        if (fp32) return (TeamKernel)k_react_team<NS, float, METHOD_BDF, BT, 1>;
+        return (TeamKernel)k_react_team<NS, double, METHOD_BDF, BT, 1>;
+      }
+      return nullptr;
+    }
+    if (team == 16 && !small) return nullptr;
+    if constexpr (P == 3) {
+      if (method == METHOD_RK64) {
+        if (team == 16) return small ? (TeamKernel)k_react_team<NS, double, METHOD_RK64, (small ? 16 : 32), 2> : nullptr;
+        return (TeamKernel)k_react_team<NS, double, METHOD_RK64, 32, 2>;
+      }
+      if (fp32) {
+        if (team == 16) return small ? (TeamKernel)k_react_team<NS, float, METHOD_BDF, (small ? 16 : 32), 2> : nullptr;
+        return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 2>;
+      }
+      if (team == 16) {
+        if (!small) return nullptr;
+        return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 1>
+                         : (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 2>;
+      }
+      return nullptr;
+    }
+    if constexpr (P == 0) {
+      if (method == METHOD_RK64 || fp32 || team == 16) return nullptr;
+      return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1>
+                       : (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2>;
     }
     return nullptr;
   }
-  if (team == 16 && !small) return nullptr;
-  if constexpr (P == 3) {
-    if (method == METHOD_RK64) {
-      if (team == 16) return small ? (TeamKernel)k_react_team<NS, double, METHOD_RK64, (small ? 16 : 32), 2> : nullptr;
-      return (TeamKernel)k_react_team<NS, double, METHOD_RK64, 32, 2>;
-    }
-    if (fp32) {
-      if (team == 16) return small ? (TeamKernel)k_react_team<NS, float, METHOD_BDF, (small ? 16 : 32), 2> : nullptr;
-      return (TeamKernel)k_react_team<NS, float, METHOD_BDF, 32, 2>;
-    }
-    if (team == 16) {
-      if (!small) return nullptr;
-      return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 1>
-                       : (TeamKernel)k_react_team<NS, double, METHOD_BDF, (small ? 16 : 32), 2>;
-    }
-    return nullptr;
-  }
-  if constexpr (P == 0) {
-    if (method == METHOD_RK64 || fp32 || team == 16) return nullptr;
-    return minb == 1 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1>
-                     : (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2>;
-  }
-  return nullptr;
 }
 
 #define PPB_CAT2(a, b) a##b
@@ -308,6 +331,7 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
   const DevMech& M = *m.dm;
   if (b.ncells <= 0) return 0;
   if (lc.engine == ENGINE_PLAIN) {
+    if constexpr (qss_only<NS>()) return (int)cudaErrorNotSupported;
     PPB_CAT4(launch_plain_, PPB_NS, _p, 3)(M, o, method, b, dt, st);
     return (int)cudaGetLastError();
   }
@@ -315,10 +339,11 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
   const int team = (lc.team == 16 || lc.team > 32) ? lc.team : 32;
   // a multi-warp team is one block
   const int wpb = team > 32 ? team / 32 : (lc.warps_per_block > 0 ? lc.warps_per_block : 4);
-  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.srk, wpb);
+  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.rhsv, wpb);
   if (!kern) return (int)cudaErrorInvalidConfiguration;
   const int tpb = team > 32 ? 1 : wpb * (32 / team); // cells per block
-  const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
+  const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn, M.nqss, M.nrq)
+                         : team_bytes<double>(M.nsp, M.nrxn, M.nqss, M.nrq);
   const size_t shm = cb * tpb;
   cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   if (e != cudaSuccess) return (int)e;
@@ -349,10 +374,11 @@ static int occupancy_ns(const DevMech& M, int method, const LaunchConfig& lc)
   const bool fp32 = lc.lu_fp32 && method == METHOD_BDF;
   const int team = (lc.team == 16 || lc.team > 32) ? lc.team : 32;
   const int wpb = team > 32 ? team / 32 : (lc.warps_per_block > 0 ? lc.warps_per_block : 4);
-  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.srk, wpb);
+  TeamKernel kern = team_kernel<NS>(method, fp32, team, lc.minb, lc.rhsv, wpb);
   if (!kern) return 0;
   const int tpb = team > 32 ? 1 : wpb * (32 / team);
-  const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn) : team_bytes<double>(M.nsp, M.nrxn);
+  const size_t cb = fp32 ? team_bytes<float>(M.nsp, M.nrxn, M.nqss, M.nrq)
+                         : team_bytes<double>(M.nsp, M.nrxn, M.nqss, M.nrq);
   const size_t shm = cb * tpb;
   int dev = 0, smem_max = 0, per_sm = 0;
   cudaGetDevice(&dev);
@@ -427,7 +453,9 @@ int PPB_CAT(react_occupancy_, PPB_NS)(const DevMech& M, int method, const Launch
 int PPB_CAT(launch_ajacobian_, PPB_NS)(const DevMech& M, const double* sc, const double* T, int consP, double* J,
                                        int ncells, int team, cudaStream_t st)
 {
-  return launch_ajac_ns<PPB_NS>(M, sc, T, consP, J, ncells, team, st);
+  // a QSS mechanism has no analytical Jacobian here
+  if constexpr (qss_only<PPB_NS>()) return (int)cudaErrorNotSupported;
+  else return launch_ajac_ns<PPB_NS>(M, sc, T, consP, J, ncells, team, st);
 }
 #endif // PPB_PART == 0
 
@@ -435,12 +463,14 @@ int PPB_CAT(launch_ajacobian_, PPB_NS)(const DevMech& M, const double* sc, const
 void PPB_CAT4(launch_plain_, PPB_NS, _p, 3)(const DevMech& M, const Options& o, int method, Batch b, double dt,
                                             cudaStream_t st)
 {
-  const int threads = 128;
-  const int blocks = (b.ncells + threads - 1) / threads;
-  if (method == METHOD_BDF)
-    k_react_plain<PPB_NS, METHOD_BDF><<<blocks, threads, 0, st>>>(M, o, b, dt);
-  else
-    k_react_plain<PPB_NS, METHOD_RK64><<<blocks, threads, 0, st>>>(M, o, b, dt);
+  if constexpr (!qss_only<PPB_NS>()) {
+    const int threads = 128;
+    const int blocks = (b.ncells + threads - 1) / threads;
+    if (method == METHOD_BDF)
+      k_react_plain<PPB_NS, METHOD_BDF><<<blocks, threads, 0, st>>>(M, o, b, dt);
+    else
+      k_react_plain<PPB_NS, METHOD_RK64><<<blocks, threads, 0, st>>>(M, o, b, dt);
+  }
 }
 #endif
 

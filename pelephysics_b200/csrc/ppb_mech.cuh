@@ -36,6 +36,7 @@ constexpr double RU = 8.31446261815324e7; // erg/(mol K), PhysicsConstants.H:11
 // lists used to sum reaction rates into species rates without atomics.
 struct DevMech {
   int nsp, nrxn;
+  int nqss, nrq; // QSS species and reactions with one (PPBMechTables)
   const double *mw, *imw, *tmid;
   const double *th_cv, *th_cp, *th_dcp, *th_u, *th_h, *th_g;
   const int *rx_kind, *rx_rev, *rx_kcpow;
@@ -84,6 +85,9 @@ struct DevMech {
   const double* jg_c;
   // SRK equation of state: [sqrt(1/Tc) | sqrt(a*) | B | F(omega)], N each
   const double* srk;
+  // QSS balance (PPBMechTables: q_rx, q_off, q_term, q_role); the thermo
+  // arrays then have an entry per concentration slot
+  const int *q_rx, *q_off, *q_term, *q_role;
 };
 
 // One reaction in 80 bytes (5 x 16-byte loads).  Species lists are expanded
@@ -613,10 +617,11 @@ __device__ __forceinline__ bool slots_has(const unsigned char (&sp)[K], int k)
   return h;
 }
 
-// Net rate of progress from a packed record (same formulas as rxn_qdot).
-__device__ __forceinline__ double rx_qdot_packed(
+// Rates of progress q_f, q_r from a packed record (same formulas as
+// rxn_qdot).
+__device__ __forceinline__ void rx_rates_packed(
   const DevMech& M, const RxPack& p, double T, double invT, double logT, double refC, double refCinv, double mixture,
-  const double* sc, const double* g)
+  const double* sc, const double* g, double& qf_out, double& qr_out)
 {
   const int kind = p.kind;
   const double k_f = p.A * ppb_exp(p.beta * logT - p.EaR * invT);
@@ -659,15 +664,109 @@ __device__ __forceinline__ double rx_qdot_packed(
     const double phr = slots_product(p.rsp, sc);
     qr = (corr ? Corr * k_f : k_f) * ppb_exp(-arg) * refc_pow(p.kcpow, refC, refCinv) * phr;
   }
+  qf_out = qf;
+  qr_out = qr;
+}
+
+// Net rate of progress from a packed record.
+__device__ __forceinline__ double rx_qdot_packed(
+  const DevMech& M, const RxPack& p, double T, double invT, double logT, double refC, double refCinv, double mixture,
+  const double* sc, const double* g)
+{
+  double qf, qr;
+  rx_rates_packed(M, p, T, invT, logT, refC, refCinv, mixture, sc, g, qf, qr);
   return qf - qr;
+}
+
+// Scratch doubles of the QSS solve: the coefficients q_f,k, q_r,k (2 nrq)
+// and the balance matrix with its right-hand side (nqss (nqss + 1)).
+__host__ __device__ inline size_t qss_scratch_doubles(int nqss, int nrq)
+{
+  return nqss > 0 ? 2 * (size_t)nrq + (size_t)nqss * (nqss + 1) : 0;
+}
+
+// The QSS concentrations of a QSS mechanism into the slots sc[nsp + 1 + q]
+// (comp_qss_coeff and comp_sc_qss of the reference's generated QSS
+// mechanism.H), given sc[0..nsp] (sc[nsp] = 1) and g[0..nsp] (g[nsp] = 0);
+// it writes g/RT of the QSS slots too.  With the QSS slots at 1 the QSS
+// reactions' rates are their coefficients q_f,k, q_r,k; per QSS species i,
+// in reaction order, the production P_i = eps + sum, the loss D_i = eps -
+// sum and the couplings C_ij = (eps + sum) / D_i (eps = 1e-12, where the
+// generated code adds it); then x_i + sum_j C_ij x_j = -P_i / D_i is solved
+// by elimination in species order without pivoting (the loss of a species
+// includes its conversions into the others, so the matrix is
+// column-diagonally dominant), one lane per row, and back substitution.
+template <int TEAM>
+__device__ void qss_solve(const Team<TEAM>& tm, const DevMech& M, double* sc, double* g, double T, double invT,
+                          double logT, double refC, double refCinv, double mixture, double* co, double* A)
+{
+  const int N = M.nsp, Q = M.nqss, K = M.nrq, W = Q + 1;
+  constexpr double eps = 1e-12;
+  for (int q = tm.lane; q < Q; q += TEAM) {
+    g[N + 1 + q] = g_RT(M, N + 1 + q, T, invT, logT);
+    sc[N + 1 + q] = 1.0;
+  }
+  tm.sync();
+  for (int k = tm.lane; k < K; k += TEAM) {
+    const RxPack p = load_rx(M, __ldg(M.q_rx + k));
+    double qf, qr;
+    rx_rates_packed(M, p, T, invT, logT, refC, refCinv, mixture, sc, g, qf, qr);
+    co[2 * k] = qf;
+    co[2 * k + 1] = qr;
+  }
+  tm.sync();
+  for (int i = tm.lane; i < Q; i += TEAM) {
+    double* row = A + i * W;
+    for (int j = 0; j < Q; j++) row[j] = 0.0;
+    unsigned has = 0u; // couplings present (at most 32 QSS species)
+    double P = eps, D = eps;
+    const int t1 = __ldg(M.q_off + i + 1);
+    for (int t = __ldg(M.q_off + i); t < t1; t++) {
+      const double v = co[__ldg(M.q_term + t)];
+      const int role = __ldg(M.q_role + t);
+      if (role == -1) {
+        P += v;
+      } else if (role == -2) {
+        D -= v;
+      } else {
+        if (!((has >> role) & 1u)) {
+          row[role] = eps;
+          has |= 1u << role;
+        }
+        row[role] += v;
+      }
+    }
+    for (int j = 0; j < Q; j++)
+      if ((has >> j) & 1u) row[j] = row[j] / D;
+    row[i] = 1.0;
+    row[Q] = -P / D;
+  }
+  tm.sync();
+  for (int c = 0; c < Q; c++) {
+    for (int i = c + 1 + tm.lane; i < Q; i += TEAM) {
+      const double f = A[i * W + c] / A[c * W + c];
+      if (f != 0.0)
+        for (int j = c; j <= Q; j++) A[i * W + j] -= f * A[c * W + j];
+    }
+    tm.sync();
+  }
+  if (tm.lane == 0) {
+    for (int i = Q - 1; i >= 0; i--) {
+      double x = A[i * W + Q];
+      for (int j = i + 1; j < Q; j++) x -= A[i * W + j] * sc[N + 1 + j];
+      sc[N + 1 + i] = x / A[i * W + i];
+    }
+  }
+  tm.sync();
 }
 
 // Per-cell scratch for the rate evaluation (team-shared).
 struct RateScratch {
-  double* sc;           // [nsp + 1] SI concentrations (+ the padding slot)
-  double* g;            // [nsp + 1] g/RT (+ the padding slot)
+  double* sc;           // [nsp + 1 (+ nqss)] SI concentrations (+ the unit slot, the QSS slots)
+  double* g;            // [nsp + 1 (+ nqss)] g/RT (+ the unit slot, the QSS slots)
   double* qd;           // [nrxn] net rates (TEAM > 1)
   double* jx = nullptr; // [4 nrxn] per-reaction Jacobian factors (TEAM > 1)
+  double* qco = nullptr; // QSS scratch (qss_scratch_doubles), for a QSS mechanism
 };
 
 // The reactions and the species gather of productionRate for a team of
@@ -693,9 +792,11 @@ __device__ __forceinline__ void production_rate_core(const Team<TEAM>& tm, const
 }
 
 // productionRate (SI): wdot[s] for s owned by the lane (team-shared wdot).
+// sc_in[nsp] holds 1 (the unit slot); for a QSS mechanism the QSS slots of
+// sc_in are solved first (qss_solve, with rs.qco as scratch).
 template <int TEAM>
 __device__ void production_rate(
-  const Team<TEAM>& tm, const DevMech& M, double* wdot, const double* sc_in, double T, RateScratch& rs)
+  const Team<TEAM>& tm, const DevMech& M, double* wdot, double* sc_in, double T, RateScratch& rs)
 {
   const double invT = 1.0 / T;
   const double logT = ppb_log(T);
@@ -708,6 +809,11 @@ __device__ void production_rate(
   }
   const double mixture = tm.sum(mix);
   tm.sync();
+  if (M.nqss > 0) {
+    if (tm.lane == 0) rs.g[M.nsp] = 0.0;
+    tm.sync();
+    qss_solve<TEAM>(tm, M, sc_in, rs.g, T, invT, logT, refC, refCinv, mixture, rs.qco, rs.qco + 2 * M.nrq);
+  }
   if (TEAM == 1) {
     for (int s = 0; s < M.nsp; s++) wdot[s] = 0.0;
     for (int r = 0; r < M.nrxn; r++) {

@@ -152,6 +152,7 @@ extern "C" int ppb_react_flat_device_noalloc(const char* mechanism, const char* 
     return nf(PPB_E_ARG, "invalid integrator options");
   if (o.engine != PPB_ENGINE_TUNED)
     return nf(PPB_E_ARG, "the allocation-free path runs the tuned engine only (engine = PPB_ENGINE_TUNED)");
+  if (t->nqss > 0) return nf(PPB_E_ARG, "the allocation-free path does not take QSS mechanisms");
   // options this path cannot honour are rejected, never silently dropped
   if (o.eos != PPB_EOS_IDEAL && o.eos != PPB_EOS_SRK) return nf(PPB_E_ARG, "eos must be 0 or 1");
   if (o.eos == PPB_EOS_SRK &&
@@ -216,7 +217,7 @@ extern "C" int ppb_react_flat_device_noalloc(const char* mechanism, const char* 
   lc.engine = o.engine;
   lc.lu_fp32 = o.lu_fp32;
   lc.persistent = 1;
-  lc.srk = o.eos == PPB_EOS_SRK ? 1 : 0;
+  lc.rhsv = o.eos == PPB_EOS_SRK ? 1 : 0;
   lc.warps_per_block = o.warps_per_block;
   lc.team = (o.team_lanes == 16 || o.team_lanes == 64 || o.team_lanes == 128) ? o.team_lanes : 32;
   lc.minb = o.register_budget == 1 ? 1 : 2;

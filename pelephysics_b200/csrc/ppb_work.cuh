@@ -45,20 +45,25 @@ __host__ __device__ inline size_t j_region_bytes(int N)
   return (n * n * sizeof(LT) + 15) & ~size_t(15);
 }
 
-// pivots and row permutation (2n ints), then the coefficient arrays
+// pivots and row permutation (2n ints), then the coefficient arrays; for a
+// QSS mechanism (Q QSS species, K reactions with one) a tail with the
+// concentrations and g/RT over all n + Q slots (in place of the n-long
+// ones) and the QSS solve's scratch
 template <typename LT>
-__host__ __device__ inline size_t team_bytes(int N, int R)
+__host__ __device__ inline size_t team_bytes(int N, int R, int Q = 0, int K = 0)
 {
   const int n = N + 1;
   const size_t d = 22 * (size_t)n + (size_t)R;
   size_t b = d * 8 + j_region_bytes<LT>(N) + jx_region_bytes<LT>(R) + a_region_bytes<LT>(N, R) +
              ((8 * (size_t)n + 7) & ~size_t(7)) + sizeof(BdfArrays);
-  return (b + 15) & ~size_t(15);
+  b = (b + 15) & ~size_t(15);
+  if (Q > 0) b += ((2 * ((size_t)n + Q) + qss_scratch_doubles(Q, K)) * 8 + 15) & ~size_t(15);
+  return b;
 }
 
 
 template <typename LT>
-__device__ inline void carve(Work<LT>& w, char* base, int N, int R)
+__device__ inline void carve(Work<LT>& w, char* base, int N, int R, int Q = 0, int K = 0)
 {
   const int n = N + 1;
   double* p = (double*)base;
@@ -101,6 +106,14 @@ __device__ inline void carve(Work<LT>& w, char* base, int N, int R)
   w.piv = (int*)((char*)w.A + a_region_bytes<LT>(N, R));
   w.perm = w.piv + n;
   w.ba = (BdfArrays*)((char*)w.piv + ((8 * (size_t)n + 7) & ~size_t(7)));
+  if (Q > 0) {
+    double* t = (double*)(base + team_bytes<LT>(N, R));
+    w.sc = t;
+    t += n + Q;
+    w.g = t;
+    t += n + Q;
+    w.qco = t;
+  }
 }
 
 
@@ -111,5 +124,12 @@ __host__ __device__ inline size_t point_doubles(int N, int R, bool jac)
 {
   const int n = N + 1;
   return (size_t)8 * n + R + (jac ? 4 * (size_t)R + (size_t)n * n : 0);
+}
+
+// the pointwise rate kernels' QSS tail: sc and g/RT over all n + Q slots,
+// then the QSS solve's scratch
+__host__ __device__ inline size_t point_qss_doubles(int N, int Q, int K)
+{
+  return Q > 0 ? 2 * ((size_t)N + 1 + Q) + qss_scratch_doubles(Q, K) : 0;
 }
 } // namespace ppb
