@@ -393,7 +393,7 @@ def our_arm(args):
     if rank == 0 and ws == 1 and not args.no_configs:
         from oracle import pyoracle as po
 
-        configs = {"lidryer_16cubed": measure_lidryer(po, dev)}
+        configs = {"lidryer_16cubed": measure_lidryer(po, dev), "ch4_lean_qss": measure_qss(po, dev)}
         for cfg in ("dodecane", "heptane"):
             configs[cfg] = measure_config(cfg, 1, 256)
 
@@ -652,6 +652,59 @@ def measure_lidryer(po, dev):
         out[name] = {"cells_per_s": n / (ms / 1e3), "ms_per_react": ms, "accuracy_vs_fp64_oracle": acc}
         r.close()
     out["tuned_vs_plain"] = out["tuned"]["cells_per_s"] / out["plain"]["cells_per_s"]
+    return out
+
+
+def measure_qss(po, dev, sample=1024):
+    """A QSS mechanism: CH4_lean_qss, 65536 e-reactors (T 1100 + 1000 U,
+    phi 0.5 + 0.5 U, 1 atm), dt 1e-5 s, rtol = atol = 1e-10, BDF orders <= 5
+    with a difference-quotient Jacobian (the reference's dense_direct
+    solve); one timed react after a warm-up react, and a seeded sample of
+    cells against the oracle over the reference's compiled kernels (the
+    oracle's time on the sample is the CPU baseline)."""
+    import torch
+
+    from pelephysics_b200 import workloads as wl
+    from pelephysics_b200.reactor import Reactor
+
+    mech = "CH4_lean_qss"
+    cells = wl.ch4_lean_qss(device=dev)
+    n = cells.ncells
+    opts = dict(rtol=1e-10, atol=1e-10, max_order=5)
+    idx = np.sort(np.random.default_rng(7).permutation(n)[:sample])
+    yc = np.ascontiguousarray(cells.rY[idx])
+    t0 = time.perf_counter()
+    flag, _, _ = po.react_flat(mech, 1, yc, np.ascontiguousarray(cells.rYsrc[idx]), cells.rX[idx].copy(),
+                               cells.rX_src[idx].copy(), cells.dt, use_ref_kernels=1, **opts)
+    cpu_s = time.perf_counter() - t0
+    out = {"workload": f"{mech} {n} e-reactors, 1 atm, T 1100+1000 U, phi 0.5+0.5 U, dt 1e-5 s, rtol=atol=1e-10, "
+                       "BDF q<=5, difference-quotient Jacobian", "cells": n,
+           "oracle_sample": {"cells": int(sample), "cells_per_s": sample / cpu_s, "cores": os.cpu_count(),
+                             "flag": int(flag)}}
+    y0 = torch.as_tensor(cells.rY.T.copy(), device=dev)
+    s0 = torch.as_tensor(cells.rYsrc.T.copy(), device=dev)
+    x0 = torch.as_tensor(cells.rX, device=dev)
+    xs = torch.as_tensor(cells.rX_src, device=dev)
+    r = Reactor(mech)
+    r.init(1, n, **opts)
+    y, x = y0.clone(), x0.clone()
+    r.react_soa(y, s0, x, xs, cells.dt)
+    y.copy_(y0)
+    x.copy_(x0)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    r.react_soa(y, s0, x, xs, cells.dt)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    yg = y.cpu().numpy().T.copy()[idx]
+    acc = po.compare_to_reference(mech, 1, cells.rY[idx], cells.rYsrc[idx], cells.rX[idx], cells.rX_src[idx],
+                                  cells.dt, yg, yc, use_ref_kernels=1, **opts)
+    wpb, team, regs, _ = r.launch_config()
+    out["tuned"] = {"cells_per_s": n / (ms / 1e3), "ms_per_react": ms, "accuracy_vs_fp64_oracle": acc,
+                    "launch": {"warps_per_block": wpb, "lanes_per_cell": team}}
+    out["tuned_vs_oracle_sample"] = out["tuned"]["cells_per_s"] / out["oracle_sample"]["cells_per_s"]
+    r.close()
     return out
 
 

@@ -116,8 +116,11 @@ void ppb_default_options(ppb_options* opt);
 /* Last error message of the calling thread. */
 const char* ppb_last_error(void);
 
-/* Mechanisms compiled into the library: returns the number of species and
- * reactions of `mechanism`, or PPB_E_MECH. */
+/* Mechanisms compiled into the library (LiDryer, drm19, dodecane_lu,
+ * heptane_lu_88sk, and the QSS mechanism CH4_lean_qss, whose species in
+ * quasi-steady state are not counted: its productionRate solves them first,
+ * as its mechanism.H does): returns the number of species and reactions of
+ * `mechanism`, or PPB_E_MECH. */
 int ppb_mechanism_info(const char* mechanism, int* nspecies, int* nreactions);
 /* Name of species k of `mechanism` (NULL when out of range). */
 const char* ppb_species_name(const char* mechanism, int k);
@@ -222,7 +225,8 @@ int ppb_probe_fp64_peak(double* gflops, void* stream);
 int ppb_production_rate(const char* mechanism, const double* sc, const double* T, double* wdot, int ncells, int team,
                         void* stream);
 /* mechanism.H aJacobian (SI), J[ncells*(N+1)^2] with
- * J[k*(N+1)+m] = d wdot_m / d sc_k */
+ * J[k*(N+1)+m] = d wdot_m / d sc_k (not for a QSS mechanism: PPB_E_CUDA,
+ * "operation not supported"; its reactor forms the Jacobian by differences) */
 int ppb_ajacobian(const char* mechanism, const double* sc, const double* T, int consP, double* J, int ncells,
                   int team, void* stream);
 /* mechanism.H GET_T_GIVEN_EY (eh = 0) / GET_T_GIVEN_HY (eh = 1): e[ncells],

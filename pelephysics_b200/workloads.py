@@ -50,6 +50,7 @@ FUELS = {
     "drm19": ("CH4", 2.0),
     "dodecane_lu": ("NC12H26", 18.5),
     "heptane_lu_88sk": ("nc7h16", 11.0),
+    "CH4_lean_qss": ("CH4", 2.0),
 }
 
 
@@ -142,6 +143,13 @@ def premix_cells(mech, ncells, seed, T0, dT, phi0, dphi, P=P_ATM, reactor_type=1
     rY[:, N] = T
     return Cells(mech, rY, np.zeros((ncells, N)), rhoE, np.zeros(ncells), reactor_type, dt,
                  {"T": T, "phi": phi, "P": P})
+
+
+def ch4_lean_qss(ncells=65536, device="cuda"):
+    """The QSS workload: CH4_lean_qss (13 transported species, 4 in steady
+    state) homogeneous e-reactors, T 1100-2100 K, phi 0.5-1.0 (seed 6),
+    1 atm, dt 1e-5 s."""
+    return premix_cells("CH4_lean_qss", ncells, 6, 1100.0, 1000.0, 0.5, 0.5, reactor_type=1, dt=1e-5, device=device)
 
 
 def lidryer_16(device="cuda"):
