@@ -480,15 +480,31 @@ struct CellIn {
 // of a QSS mechanism.  The last two have no analytical Jacobian.
 enum : int { RHS_IDEAL = 0, RHS_SRK = 1, RHS_QSS = 2 };
 
+// The difference-quotient variants (SRK, QSS) evaluate the right-hand
+// side from two call sites, the integrator and the Jacobian's n + 1
+// columns: one out-of-line copy of it (drm19 SRK at 50 atm 39k -> 60k
+// cells/s, CH4_lean_qss 294k -> 672k against the copy inlined at both).
 template <int TEAM, int RHSV>
-__device__ PPB_RHS_ATTR void bdf_rhs(Team<TEAM> tm, const DevMech& M, int rtype, double t, const double* y,
-                                     double* fy, double rhoe, double rhoesrc, const double* src, double* Y,
-                                     double* sc, double* g, double* qd, double* wdot, double* ei, double* qco)
+__device__ __noinline__ void bdf_rhs_dq(Team<TEAM> tm, const DevMech& M, int rtype, double t, const double* y,
+                                        double* fy, double rhoe, double rhoesrc, const double* src, double* Y,
+                                        double* sc, double* g, double* qd, double* wdot, double* ei, double* qco)
 {
   if constexpr (RHSV == RHS_SRK) {
     reactor_rhs_srk<TEAM>(tm, M, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei);
   } else {
     reactor_rhs<TEAM, RHSV == RHS_QSS>(tm, M, rtype, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei, qco);
+  }
+}
+
+template <int TEAM, int RHSV>
+__device__ PPB_RHS_ATTR void bdf_rhs(Team<TEAM> tm, const DevMech& M, int rtype, double t, const double* y,
+                                     double* fy, double rhoe, double rhoesrc, const double* src, double* Y,
+                                     double* sc, double* g, double* qd, double* wdot, double* ei, double* qco)
+{
+  if constexpr (RHSV == RHS_IDEAL) {
+    reactor_rhs<TEAM, false>(tm, M, rtype, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei, qco);
+  } else {
+    bdf_rhs_dq<TEAM, RHSV>(tm, M, rtype, t, y, fy, rhoe, rhoesrc, src, Y, sc, g, qd, wdot, ei, qco);
   }
 }
 
