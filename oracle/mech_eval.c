@@ -12,6 +12,8 @@
 #include "../pelephysics_b200/csrc/mech/mech_dodecane_lu.h"
 #include "../pelephysics_b200/csrc/mech/mech_heptane_lu_88sk.h"
 #include "../pelephysics_b200/csrc/mech/mech_CH4_lean_qss.h"
+#include "../pelephysics_b200/csrc/mech/mech_C1-C2-NO_qss.h"
+#include "../pelephysics_b200/csrc/mech/mech_LuEthylene_qss.h"
 
 const PPBMechTables* ppo_mech(const char* name)
 {
@@ -20,6 +22,8 @@ const PPBMechTables* ppo_mech(const char* name)
   if (!strcmp(name, "dodecane_lu")) return &ppbm_dodecane_lu;
   if (!strcmp(name, "heptane_lu_88sk")) return &ppbm_heptane_lu_88sk;
   if (!strcmp(name, "CH4_lean_qss")) return &ppbm_CH4_lean_qss;
+  if (!strcmp(name, "C1-C2-NO_qss")) return &ppbm_C1_C2_NO_qss;
+  if (!strcmp(name, "LuEthylene_qss")) return &ppbm_LuEthylene_qss;
   return 0;
 }
 
@@ -328,7 +332,8 @@ static void rxn_rates(const PPBMechTables* M, int r, double T, double invT, doub
       const double conv = refc_pow(M->rx_kcpow[r], refC, refCinv);
       qr = (corr ? Corr * k_f : k_f) * exp(-arg) * conv * phr;
     }
-    *qf_out = qf;
+    // a forward rate the QSS reduction removed counts 0 (qdot = -q_r)
+    *qf_out = (M->nqss > 0 && M->rx_rmfwd[r]) ? 0.0 : qf;
     *qr_out = qr;
   }
 }
@@ -348,7 +353,7 @@ static void rxn_rates(const PPBMechTables* M, int r, double T, double invT, doub
 // stable, while a row swap can mix a species of concentration 1e-17 with one
 // of 1e-2 and lose the small one to cancellation.
 static void qss_concentrations(const PPBMechTables* M, double T, double invT, double logT, double refC,
-                               double refCinv, double mixture, double* sc, const double* g_RT)
+                               double refCinv, double mixture, double* sc, const double* g_RT, double* sys_out)
 {
   const int N = M->nsp, Q = M->nqss, K = M->nrq;
   const double eps = 1e-12;
@@ -365,7 +370,8 @@ static void qss_concentrations(const PPBMechTables* M, double T, double invT, do
     }
     double P = eps, D = eps;
     for (int t = M->q_off[i]; t < M->q_off[i + 1]; t++) {
-      const double v = co[M->q_term[t]];
+      const double c = M->q_coef[t];
+      const double v = c == 1.0 ? co[M->q_term[t]] : c * co[M->q_term[t]];
       const int role = M->q_role[t];
       if (role == -1) {
         P += v;
@@ -384,6 +390,10 @@ static void qss_concentrations(const PPBMechTables* M, double T, double invT, do
     row[i] = 1.0;
     row[Q] = -P / D;
   }
+  if (sys_out) {
+    for (int i = 0; i < Q * (Q + 1); i++) sys_out[i] = A[i];
+    return;
+  }
   // forward elimination, then back substitution
   for (int c = 0; c < Q; c++) {
     for (int i = c + 1; i < Q; i++) {
@@ -400,7 +410,21 @@ static void qss_concentrations(const PPBMechTables* M, double T, double invT, do
 }
 
 // The QSS concentrations (SI) productionRate uses at (sc, T): out[nqss].
+static void qss_eval(const PPBMechTables* M, const double* sc_in, double T, double* out, double* sys_out);
+
 void ppo_qss_concentrations(const PPBMechTables* M, const double* sc_in, double T, double* out)
+{
+  qss_eval(M, sc_in, T, out, 0);
+}
+
+// The QSS balance system [C + I | -P/D] (nqss rows of nqss + 1) at (sc, T),
+// for checks of the solve against exact arithmetic.
+void ppo_qss_system(const PPBMechTables* M, const double* sc_in, double T, double* sys_out)
+{
+  qss_eval(M, sc_in, T, 0, sys_out);
+}
+
+static void qss_eval(const PPBMechTables* M, const double* sc_in, double T, double* out, double* sys_out)
 {
   const int N = M->nsp, Q = M->nqss;
   const double invT = 1.0 / T, logT = log(T);
@@ -413,8 +437,9 @@ void ppo_qss_concentrations(const PPBMechTables* M, const double* sc_in, double 
   sc[N] = 1.0;
   g_RT[N] = 0.0;
   for (int q = 0; q < Q; q++) g_RT[N + 1 + q] = gibbs_one(M, N + 1 + q, T, invT, logT);
-  qss_concentrations(M, T, invT, logT, refC, refCinv, mixture, sc, g_RT);
-  for (int q = 0; q < Q; q++) out[q] = sc[N + 1 + q];
+  qss_concentrations(M, T, invT, logT, refC, refCinv, mixture, sc, g_RT, sys_out);
+  if (out)
+    for (int q = 0; q < Q; q++) out[q] = sc[N + 1 + q];
 }
 
 // production.py:991-1435 (productionRate, SI units).  When absterm is not
@@ -440,7 +465,7 @@ static void production_rate_impl(const PPBMechTables* M, double* wdot, const dou
   g_RT[N] = 0.0;
   if (Q > 0) {
     for (int q = 0; q < Q; q++) g_RT[N + 1 + q] = gibbs_one(M, N + 1 + q, T, invT, logT);
-    qss_concentrations(M, T, invT, logT, refC, refCinv, mixture, sc, g_RT);
+    qss_concentrations(M, T, invT, logT, refC, refCinv, mixture, sc, g_RT, 0);
   }
   for (int r = 0; r < M->nrxn; r++) {
     double qf, qr;

@@ -45,6 +45,7 @@ int ppo_get_t_given_hy(const PPBMechTables* M, double h, const double* y, double
 // rates and Jacobian (mechanism.H productionRate / aJacobian / DWDOT / CKWC)
 void ppo_production_rate(const PPBMechTables* M, double* wdot, const double* sc, double T);
 void ppo_qss_concentrations(const PPBMechTables* M, const double* sc, double T, double* out);
+void ppo_qss_system(const PPBMechTables* M, const double* sc, double T, double* sys_out);
 // per species sum |nu| (|q_f| + |q_r|): the scale of wdot's rounding error
 void ppo_production_rate_abs(const PPBMechTables* M, double* absterm, const double* sc, double T);
 void ppo_ckwc(const PPBMechTables* M, double T, const double* C, double* wdot);

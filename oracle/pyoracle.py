@@ -82,6 +82,7 @@ def lib():
         L.ppo_nsp.argtypes = [C.c_char_p]
         L.ppo_nqss.argtypes = [C.c_char_p]
         L.ppo_qss_concentrations.argtypes = [C.c_void_p, _DP, C.c_double, _DP]
+        L.ppo_qss_system.argtypes = [C.c_void_p, _DP, C.c_double, _DP]
         for fn in ("ppo_cv_R", "ppo_cp_R", "ppo_dcvpRdT", "ppo_species_internal_energy",
                    "ppo_species_enthalpy", "ppo_gibbs", "ppo_ckums", "ppo_ckhms"):
             getattr(L, fn).argtypes = [C.c_void_p, C.c_double, _DP]
@@ -164,6 +165,12 @@ class Mech:
         out = np.zeros(self.nqss)
         self.L.ppo_qss_concentrations(self.M, _p(np.ascontiguousarray(sc, float)), float(T), _p(out))
         return out
+
+    def qss_system(self, sc, T):
+        """The QSS balance system [I + C | -P/D], nqss x (nqss + 1)."""
+        out = np.zeros(self.nqss * (self.nqss + 1))
+        self.L.ppo_qss_system(self.M, _p(np.ascontiguousarray(sc, float)), float(T), _p(out))
+        return out.reshape(self.nqss, self.nqss + 1)
 
     def species(self):
         return [self.L.ppo_species_name(self.name.encode(), k).decode() for k in range(self.nsp)]

@@ -20,10 +20,10 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libppb200.so")
 NVCC = os.environ.get("NVCC", "nvcc")
-SPECIES_COUNTS = (9, 13, 21, 53, 88)
+SPECIES_COUNTS = (9, 13, 21, 22, 39, 53, 88)
 # species counts of the QSS mechanisms, compiled for their QSS kernel only
 # (no adjoint, no ReactorArkode)
-QSS_ONLY_COUNTS = (13,)
+QSS_ONLY_COUNTS = (13, 22, 39)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-diag-suppress", "177,550"]
 

@@ -125,6 +125,8 @@ typedef struct PPBMechTables {
   const int* q_off;                 // [nqss + 1] each QSS species' balance terms, in k order:
   const int* q_term;                //   2 k + 0 (forward coefficient of k) or 2 k + 1 (reverse)
   const int* q_role;                //   -1 production, -2 loss, j >= 0 production from QSS species j
+  const double* q_coef;             //   molecules of the species the term makes or uses (1 or 2)
+  const int* rx_rmfwd;              // [nrxn] 1: forward rate removed by the QSS reduction (qdot = -q_r)
 } PPBMechTables;
 
 #ifdef __cplusplus

@@ -22,6 +22,8 @@
 #include "mech/mech_dodecane_lu.h"
 #include "mech/mech_heptane_lu_88sk.h"
 #include "mech/mech_CH4_lean_qss.h"
+#include "mech/mech_C1-C2-NO_qss.h"
+#include "mech/mech_LuEthylene_qss.h"
 
 namespace ppb {
 
@@ -32,6 +34,8 @@ const PPBMechTables* find_mechanism(const char* name)
   if (!strcmp(name, "dodecane_lu")) return &ppbm_dodecane_lu;
   if (!strcmp(name, "heptane_lu_88sk")) return &ppbm_heptane_lu_88sk;
   if (!strcmp(name, "CH4_lean_qss")) return &ppbm_CH4_lean_qss;
+  if (!strcmp(name, "C1-C2-NO_qss")) return &ppbm_C1_C2_NO_qss;
+  if (!strcmp(name, "LuEthylene_qss")) return &ppbm_LuEthylene_qss;
   return nullptr;
 }
 
@@ -138,6 +142,8 @@ static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
     PPB_ADD(q_off, t->q_off, t->nqss + 1);
     PPB_ADD(q_term, t->q_term, t->q_off[t->nqss]);
     PPB_ADD(q_role, t->q_role, t->q_off[t->nqss]);
+    PPB_ADD(q_coef, t->q_coef, t->q_off[t->nqss]);
+    PPB_ADD(rx_rmfwd, t->rx_rmfwd, R);
     // the balance solve keeps a 32-bit coupling mask; slots are bytes
     if (t->nqss > 32 || N + 1 + t->nqss > 255) pk.overflow = true;
   } else {
@@ -145,6 +151,8 @@ static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
     PPB_ADD(q_off, t->rx_kind, 0);
     PPB_ADD(q_term, t->rx_kind, 0);
     PPB_ADD(q_role, t->rx_kind, 0);
+    PPB_ADD(q_coef, t->rx_A, 0);
+    PPB_ADD(rx_rmfwd, t->rx_kind, 0);
   }
 #undef PPB_ADD
   // gather lists, written entry by entry at exact offsets (no temporary
@@ -274,6 +282,7 @@ static size_t pack_all(const PPBMechTables* t, Packer& pk, DevMech& dm)
     p.eff0 = (unsigned short)t->eff_off[r];
     p.effn = (unsigned short)(t->eff_off[r + 1] - t->eff_off[r]);
     p.fo = 255;
+    p.rmf = (unsigned char)(t->nqss > 0 && t->rx_rmfwd[r] ? 1 : 0);
     if (t->rx_kind[r] == PPB_RX_TROE || t->rx_kind[r] == PPB_RX_LINDEMANN) {
       const double* d = t->fo_d + r * PPB_NFOD;
       const int* fi = t->fo_i + r * PPB_NFOI;
@@ -481,6 +490,8 @@ size_t team_cell_bytes(const PPBMechTables* t, int lu_fp32)
   int react_occupancy_##NS(const DevMech&, int, const LaunchConfig&);
 PPB_DECL(9)
 PPB_DECL(13)
+PPB_DECL(22)
+PPB_DECL(39)
 PPB_DECL(21)
 PPB_DECL(53)
 PPB_DECL(88)
@@ -510,6 +521,10 @@ int launch_react(const DeviceMechanism& m, const Options& o, int method, const L
     return launch_react_9(m, o, method, lc, b, dt, queue, st);
   case 13:
     return launch_react_13(m, o, method, lc, b, dt, queue, st);
+  case 22:
+    return launch_react_22(m, o, method, lc, b, dt, queue, st);
+  case 39:
+    return launch_react_39(m, o, method, lc, b, dt, queue, st);
   case 21:
     return launch_react_21(m, o, method, lc, b, dt, queue, st);
   case 53:
@@ -527,6 +542,8 @@ int react_occupancy(const DeviceMechanism& m, int method, const LaunchConfig& lc
   switch (M.nsp) {
   case 9: return react_occupancy_9(M, method, lc);
   case 13: return react_occupancy_13(M, method, lc);
+  case 22: return react_occupancy_22(M, method, lc);
+  case 39: return react_occupancy_39(M, method, lc);
   case 21: return react_occupancy_21(M, method, lc);
   case 53: return react_occupancy_53(M, method, lc);
   case 88: return react_occupancy_88(M, method, lc);
@@ -820,6 +837,10 @@ int launch_ajacobian(const DeviceMechanism& m, const double* sc, const double* T
     return launch_ajacobian_9(M, sc, T, consP, J, ncells, team, st);
   case 13:
     return launch_ajacobian_13(M, sc, T, consP, J, ncells, team, st);
+  case 22:
+    return launch_ajacobian_22(M, sc, T, consP, J, ncells, team, st);
+  case 39:
+    return launch_ajacobian_39(M, sc, T, consP, J, ncells, team, st);
   case 21:
     return launch_ajacobian_21(M, sc, T, consP, J, ncells, team, st);
   case 53:

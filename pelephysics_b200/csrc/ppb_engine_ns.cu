@@ -210,12 +210,13 @@ constexpr int big_team()
 //   2: the multi-warp teams (FP64 and FP32 BDF, RK64)
 //   3: FP32 BDF and RK64 with 32 lanes, the 16-lane variants, the SRK kernel
 //   4: FP32 BDF, 32 lanes, 12 and 16 warps per block
-// Species counts compiled for a QSS mechanism only (CH4_lean_qss: 13
-// transported species): the one QSS kernel, no other variant.
+// Species counts compiled for a QSS mechanism only (transported species of
+// CH4_lean_qss 13, LuEthylene_qss 22, C1-C2-NO_qss 39): the one QSS
+// kernel, no other variant.
 template <int NS>
 constexpr bool qss_only()
 {
-  return NS == 13;
+  return NS == 13 || NS == 22 || NS == 39;
 }
 
 template <int NS>

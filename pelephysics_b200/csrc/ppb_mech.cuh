@@ -85,9 +85,11 @@ struct DevMech {
   const double* jg_c;
   // SRK equation of state: [sqrt(1/Tc) | sqrt(a*) | B | F(omega)], N each
   const double* srk;
-  // QSS balance (PPBMechTables: q_rx, q_off, q_term, q_role); the thermo
-  // arrays then have an entry per concentration slot
+  // QSS balance (PPBMechTables: q_rx, q_off, q_term, q_role, q_coef,
+  // rx_rmfwd); the thermo arrays then have an entry per concentration slot
   const int *q_rx, *q_off, *q_term, *q_role;
+  const double* q_coef;
+  const int* rx_rmfwd;
 };
 
 // One reaction in 80 bytes (5 x 16-byte loads).  Species lists are expanded
@@ -108,7 +110,8 @@ struct alignas(16) RxPack {
   unsigned char nf, nr, njn;
   unsigned short eff0, effn; // efficiency list
   unsigned short aslot;      // row of the dense efficiency table (effd)
-  unsigned char pad[2];
+  unsigned char rmf;         // forward rate removed by the QSS reduction (qdot = -q_r)
+  unsigned char pad;
 };
 static_assert(sizeof(RxPack) == 80, "RxPack is five 16-byte words");
 
@@ -508,9 +511,11 @@ __device__ __forceinline__ double rxn_qdot(
     const double phr = phase_space(M.rps_sp + r * PPB_MAXPS, M.rps_c + r * PPB_MAXPS, __ldg(M.rps_n + r), sc);
     qr = (corr ? Corr * k_f : k_f) * ppb_exp(-arg) * refc_pow(__ldg(M.rx_kcpow + r), refC, refCinv) * phr;
   }
-  if (qf_out) *qf_out = qf;
+  // a forward rate the QSS reduction removed counts 0 (qdot = -q_r)
+  const double qfe = (M.nqss > 0 && __ldg(M.rx_rmfwd + r)) ? 0.0 : qf;
+  if (qf_out) *qf_out = qfe;
   if (qr_out) *qr_out = qr;
-  return qf - qr;
+  return qfe - qr;
 }
 
 __device__ __forceinline__ RxPack load_rx(const DevMech& M, int r)
@@ -664,7 +669,7 @@ __device__ __forceinline__ void rx_rates_packed(
     const double phr = slots_product(p.rsp, sc);
     qr = (corr ? Corr * k_f : k_f) * ppb_exp(-arg) * refc_pow(p.kcpow, refC, refCinv) * phr;
   }
-  qf_out = qf;
+  qf_out = p.rmf ? 0.0 : qf;
   qr_out = qr;
 }
 
@@ -722,7 +727,8 @@ __device__ void qss_solve(const Team<TEAM>& tm, const DevMech& M, double* sc, do
     double P = eps, D = eps;
     const int t1 = __ldg(M.q_off + i + 1);
     for (int t = __ldg(M.q_off + i); t < t1; t++) {
-      const double v = co[__ldg(M.q_term + t)];
+      const double cf = __ldg(M.q_coef + t);
+      const double v = cf == 1.0 ? co[__ldg(M.q_term + t)] : cf * co[__ldg(M.q_term + t)];
       const int role = __ldg(M.q_role + t);
       if (role == -1) {
         P += v;

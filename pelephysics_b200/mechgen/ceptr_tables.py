@@ -46,7 +46,7 @@ from collections import Counter, OrderedDict
 import numpy as np
 import yaml
 
-MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "CH4_lean_qss"]
+MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "CH4_lean_qss", "C1-C2-NO_qss", "LuEthylene_qss"]
 
 RC = 1.98721558317399615845  # cal/mol/K
 ATOMIC_WEIGHTS = {
@@ -65,6 +65,23 @@ MAXKC = 10  # Gibbs terms of the equilibrium exponent
 MAXJN = 8  # Jacobian net-stoichiometry entries
 
 K_SIMPLE, K_THIRD, K_COLLIDER, K_TROE, K_LINDEMANN, K_SRI = range(6)
+
+
+class _Yaml12Loader(yaml.SafeLoader):
+    """PyYAML's safe loader with YAML 1.2 booleans (true / false only), as
+    Cantera reads its files: a species named NO (nitric oxide) stays a
+    string instead of YAML 1.1's False."""
+
+
+for _ch, _res in list(_Yaml12Loader.yaml_implicit_resolvers.items()):
+    _Yaml12Loader.yaml_implicit_resolvers[_ch] = [(t, r) for t, r in _res if t != "tag:yaml.org,2002:bool"]
+_Yaml12Loader.add_implicit_resolver("tag:yaml.org,2002:bool", re.compile(r"^(?:true|True|TRUE|false|False|FALSE)$"),
+                                    list("tTfF"))
+
+
+def load_yaml(path):
+    with open(path) as fh:
+        return yaml.load(fh, Loader=_Yaml12Loader)
 
 
 def fmt(x: float, f: str) -> float:
@@ -255,7 +272,7 @@ def mechanism_file(mech_dir):
 
 
 def build(mech_dir, name):
-    y = yaml.safe_load(open(mechanism_file(mech_dir)))
+    y = load_yaml(mechanism_file(mech_dir))
     # rate units: the Chemkin-converted mechanisms declare cm / mol / cal/mol;
     # a file without a units entry (Cantera's writer, e.g. qssa.yaml) is in
     # Cantera's own m / kmol / J/kmol, the units CEPTR converts from
@@ -277,9 +294,12 @@ def build(mech_dir, name):
     idx = {s: i for i, s in enumerate(species)}
     idx.update({s: nsp + 1 + q for q, s in enumerate(qss)})
     spdata = {s["name"]: s for s in y["species"]}
+    # reactions whose forward rate the QSS reduction removes (their forward
+    # would be quadratic in QSS species): productionRate uses qdot = -q_r
+    rm_fwd = set(int(i) for i in phase.get("forward_to_remove_idx", []))
     nonq = os.path.join(mech_dir, "non_qssa_list.yaml")
     if qss and os.path.exists(nonq):
-        listed = yaml.safe_load(open(nonq))["species"]
+        listed = load_yaml(nonq)["species"]
         assert listed == species, (listed, species)
 
     # --- species data (mw, imw: transported species; thermo: transported,
@@ -327,7 +347,7 @@ def build(mech_dir, name):
     order = ceptr_sort(rxns)
     R = []
     for r in order:
-        rec = {"orig": r.orig, "eq": r.eq, "kind": r.kind, "rev": int(r.reversible)}
+        rec = {"orig": r.orig, "eq": r.eq, "kind": r.kind, "rev": int(r.reversible), "rmf": int(r.orig in rm_fwd)}
         # forward / reverse phase space (utilities.py:23-157): reactants plus
         # the explicit collider, sorted by species index
         fwd = Counter(r.reactants)
@@ -457,7 +477,7 @@ def build(mech_dir, name):
         rec["hp"] = [(idx[s], float(v)) for s, v in sorted_by_species(pro, idx)]
         R.append(rec)
 
-    qss_info = qss_structure(order, qss, qss_set) if qss else None
+    qss_info = qss_structure(order, qss, qss_set, rm_fwd) if qss else None
     return {
         "name": name,
         "qss": qss,
@@ -474,52 +494,68 @@ def build(mech_dir, name):
     }
 
 
-def qss_structure(order, qss, qss_set):
+def qss_structure(order, qss, qss_set, rm_fwd=()):
     """The steady-state balance of each QSS species, as the reference's
     generated comp_qss_coeff / comp_sc_qss form it
     (Support/ceptr/ceptr/qssa_converter.py: qssa_coeff_functions,
     qssa_component_functions): the reactions that involve a QSS species
     (in evaluation order, k = 0 ..) give coefficients q_f,k and q_r,k, the
-    rates with the QSS concentration left out.  For QSS species i, in k order:
-    a reaction consuming i adds its coefficient to the loss (role -2); one
-    producing i from transported species only adds to the production
-    (role -1); one producing i from QSS species j adds to the coupling
-    with j (role j).  A reaction with more than one QSS species on a side,
-    or a QSS species of order above one, would make the balance nonlinear:
-    rejected, as the reference's converter rejects it."""
+    rates with the QSS concentrations left out.  For QSS species i, in k
+    order, each direction of a reaction adds nu times its coefficient: to
+    the loss (role -2) when it consumes i, to the production (role -1) when
+    it makes i from transported species only, to the coupling with QSS
+    species j (role j) when it makes i from j.  A direction that consumes
+    more than one QSS molecule would make the balance nonlinear: the
+    reference's reduction removes such a forward rate (forward_to_remove_idx
+    of the mechanism's phase; its q_f is 0 in productionRate too, qdot = -q_r)
+    and rejects any other, and so does this generator."""
     q_rx, terms = [], [[] for _ in qss]
     qi = {s: q for q, s in enumerate(qss)}
     for pos, r in enumerate(order):
-        rq = [s for s in r.reactants if s in qss_set]
-        pq = [s for s in r.products if s in qss_set]
+        rq = [(s, float(v)) for s, v in r.reactants.items() if s in qss_set]
+        pq = [(s, float(v)) for s, v in r.products.items() if s in qss_set]
         if not rq and not pq:
             continue
-        if len(rq) > 1 or len(pq) > 1 or any(r.reactants[s] != 1 for s in rq) or any(r.products[s] != 1 for s in pq):
-            raise NotImplementedError(f"nonlinear QSS reaction {r.eq}")
-        if rq and pq and rq[0] == pq[0]:
-            raise NotImplementedError(f"QSS species on both sides of {r.eq}")
         k = len(q_rx)
         q_rx.append(pos)
-        if rq:
-            i = qi[rq[0]]
-            terms[i].append((2 * k, -2))  # forward consumes i
-            if r.reversible:
-                terms[i].append((2 * k + 1, qi[pq[0]] if pq else -1))  # reverse produces i
-        if pq:
-            i = qi[pq[0]]
-            terms[i].append((2 * k, qi[rq[0]] if rq else -1))  # forward produces i
-            if r.reversible:
-                terms[i].append((2 * k + 1, -2))  # reverse consumes i
-    off, term, role = [0], [], []
+        dirs = []
+        if r.orig not in rm_fwd:
+            dirs.append((2 * k, rq, pq))  # forward: consumes rq, makes pq
+        if r.reversible:
+            dirs.append((2 * k + 1, pq, rq))  # reverse: consumes pq, makes rq
+        for term, cons, made in dirs:
+            if len(cons) > 1 or any(v != 1.0 for _, v in cons):
+                raise NotImplementedError(f"nonlinear QSS reaction {r.eq}")
+            if cons and any(s == cons[0][0] for s, _ in made):
+                raise NotImplementedError(f"QSS species on both sides of {r.eq}")
+            if len(made) > 1:
+                # a direction making two QSS species: the reverse of a
+                # reaction whose forward is removed counts for each; an
+                # irreversible forward the reference's converter leaves out
+                # of every balance ("does not contribute to any QSSA
+                # coefficients and is thus ignored"); from a QSS species, it
+                # handles neither
+                if cons:
+                    raise NotImplementedError(f"QSS reaction {r.eq} turns a QSS species into two")
+                if term % 2 == 0 and not r.reversible:
+                    continue
+            for s, v in cons:
+                terms[qi[s]].append((term, -2, v))
+            for s, v in made:
+                terms[qi[s]].append((term, qi[cons[0][0]] if cons else -1, v))
+    for q, lst in enumerate(terms):
+        lst.sort(key=lambda t: t[0] // 2)  # k order (stable: a reaction's terms keep their order)
+    off, term, role, coef = [0], [], [], []
     for lst in terms:
-        for t, ro in lst:
+        for t, ro, v in lst:
             term.append(t)
             role.append(ro)
+            coef.append(v)
         off.append(len(term))
     for q, lst in enumerate(terms):
-        if not any(ro == -2 for _, ro in lst) or not any(ro != -2 for _, ro in lst):
+        if not any(ro == -2 for _, ro, _ in lst) or not any(ro != -2 for _, ro, _ in lst):
             raise ValueError(f"QSS species {qss[q]} is not both produced and consumed")
-    return {"q_rx": q_rx, "q_off": off, "q_term": term, "q_role": role}
+    return {"q_rx": q_rx, "q_off": off, "q_term": term, "q_role": role, "q_coef": coef}
 
 
 def _carr(ctype, name, vals, per_line=4):
@@ -538,9 +574,10 @@ def _carr(ctype, name, vals, per_line=4):
 
 def emit_header(M, path):
     name = M["name"]
+    cid = re.sub(r"[^A-Za-z0-9_]", "_", name)  # C identifier (C1-C2-NO_qss -> C1_C2_NO_qss)
     nsp = len(M["species"])
     nr = len(M["rxns"])
-    P = f"ppbm_{name}_"
+    P = f"ppbm_{cid}_"
     out = []
     out.append(f"// Generated by pelephysics_b200/mechgen/ceptr_tables.py from\n")
     src = "qssa.yaml" if M["qss"] else "mechanism.yaml"
@@ -633,7 +670,9 @@ def emit_header(M, path):
         out.append(_carr("int", P + "q_off", qi["q_off"], 16))
         out.append(_carr("int", P + "q_term", qi["q_term"], 16))
         out.append(_carr("int", P + "q_role", qi["q_role"], 16))
-    out.append(f"\nstatic const PPBMechTables ppbm_{name} = {{\n")
+        out.append(_carr("double", P + "q_coef", qi["q_coef"]))
+        out.append(_carr("int", P + "rx_rmfwd", [r["rmf"] for r in M["rxns"]], 16))
+    out.append(f"\nstatic const PPBMechTables ppbm_{cid} = {{\n")
     out.append(f'  "{name}", {nsp}, {nr},\n')
     fields = [
         "species", "mw", "imw", "tmid", "th_cv", "th_cp", "th_dcp", "th_u", "th_h", "th_g",
@@ -646,7 +685,8 @@ def emit_header(M, path):
     if M["qss"]:
         qi = M["qss_info"]
         out.append(f"  {len(M['qss'])}, {len(qi['q_rx'])},\n")
-        out.append("".join(f"  {P}{f},\n" for f in ("qss_species", "q_rx", "q_off", "q_term", "q_role")))
+        out.append("".join(f"  {P}{f},\n" for f in ("qss_species", "q_rx", "q_off", "q_term", "q_role", "q_coef",
+                                                      "rx_rmfwd")))
     out.append("};\n")
     with open(path, "w") as fh:
         fh.write("".join(out))

@@ -51,6 +51,8 @@ FUELS = {
     "dodecane_lu": ("NC12H26", 18.5),
     "heptane_lu_88sk": ("nc7h16", 11.0),
     "CH4_lean_qss": ("CH4", 2.0),
+    "C1-C2-NO_qss": ("CH4", 2.0),
+    "LuEthylene_qss": ("C2H4", 3.0),
 }
 
 

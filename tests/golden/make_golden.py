@@ -95,7 +95,7 @@ def srk_main():
         print(mech, npts, os.path.getsize(path), "bytes")
 
 
-QSS_POINTS = {"CH4_lean_qss": 32}
+QSS_POINTS = {"CH4_lean_qss": 32, "C1-C2-NO_qss": 24, "LuEthylene_qss": 24}
 
 
 def qss_main():

@@ -1,15 +1,28 @@
 """QSS mechanisms on the CPU (no GPU): the oracle's table-driven QSS
-chemistry (CH4_lean_qss: 13 transported species, 4 in quasi-steady state,
-73 reactions, 41 of them with a QSS species) against the golden vectors of
-the reference's own compiled Mechanisms/CH4_lean_qss/mechanism.H
-(tests/golden/make_golden.py qss): the QSS concentrations comp_sc_qss
-solves, productionRate, thermo, the temperature solves and the reactor
-right-hand side of both reactor types; the generated tables' balance
-structure; and BDF over the table kernels against BDF over the reference's
-compiled kernels (difference-quotient Jacobian in both, as the reference's
-dense_direct solve forms it)."""
+chemistry against the reference's own compiled Mechanisms/<mech>/mechanism.H
+(golden vectors of tests/golden/make_golden.py qss): the QSS concentrations
+comp_sc_qss solves, productionRate, thermo, the temperature solves and the
+reactor right-hand side of both reactor types; the generated tables' balance
+structure against the reference's generated comp_sc_qss, term for term; and
+BDF over the table kernels against BDF over the reference's compiled kernels
+(difference-quotient Jacobian in both, as the reference's dense_direct solve
+forms it).
+
+Mechanisms: CH4_lean_qss (13 transported species, 4 QSS) and C1-C2-NO_qss
+(39, 5; two forward rates removed by the reduction) are pinned to the
+reference at rounding level.  LuEthylene_qss (22, 10) is pinned in
+structure, and its solve against exact rational elimination of the same
+linear system: the reference's generated symbolic elimination for its
+10-species coupled group loses accuracy on some states (measured on a
+random state with a balance matrix of condition number 2: the reference's
+CH2* off by 100 %, this solve within 2e-16 of the exact solution; on states
+along ignition trajectories its error reaches 5.5e-6 relative, median
+5.5e-16), so its rates are compared with the reference only where the
+reference's own solve is accurate."""
 
 import os
+import re
+from fractions import Fraction
 
 import numpy as np
 import pytest
@@ -18,10 +31,29 @@ from tests.helpers import premix_oracle
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 MECH = "CH4_lean_qss"
+PINNED = ["CH4_lean_qss", "C1-C2-NO_qss"]
+ALL = PINNED + ["LuEthylene_qss"]
 
 
-def load():
-    return dict(np.load(os.path.join(GOLD, f"point_{MECH}.npz")))
+def load(mech=MECH):
+    return dict(np.load(os.path.join(GOLD, f"point_{mech}.npz")))
+
+
+def exact_solve(system):
+    """Gaussian elimination in rational arithmetic of [A | b]."""
+    A = [[Fraction(float(v)) for v in row] for row in system]
+    Q = len(A)
+    for c in range(Q):
+        p = max(range(c, Q), key=lambda i: abs(A[i][c]))
+        A[c], A[p] = A[p], A[c]
+        for i in range(c + 1, Q):
+            f = A[i][c] / A[c][c]
+            for j in range(c, Q + 1):
+                A[i][j] -= f * A[c][j]
+    x = [Fraction(0)] * Q
+    for i in reversed(range(Q)):
+        x[i] = (A[i][Q] - sum(A[i][j] * x[j] for j in range(i + 1, Q))) / A[i][i]
+    return np.array([float(v) for v in x])
 
 
 def test_qss_tables(oracle):
@@ -31,32 +63,55 @@ def test_qss_tables(oracle):
     assert oracle.Mech("drm19").nqss == 0
 
 
-def test_qss_concentrations_match_reference(oracle):
+@pytest.mark.parametrize("mech", PINNED)
+def test_qss_concentrations_match_reference(oracle, mech):
     """comp_sc_qss eliminates symbolically in an order of its own; the
     oracle solves the same linear balance in species order: equal to a few
     ulps of the solution."""
-    g = load()
-    M = oracle.Mech(MECH)
+    g = load(mech)
+    M = oracle.Mech(mech)
     for i, T in enumerate(g["T"]):
         x = M.qss_concentrations(g["sc"][i], T)
         ref = g["sc_qss"][i]
         assert np.all(np.abs(x - ref) <= 1e-12 * np.abs(ref) + 1e-300), (i, x, ref)
 
 
-def test_qss_production_rate_matches_reference(oracle):
-    """|wdot - wdot_ref| <= 1e-12 * sum_r |nu| (|qf| + |qr|) per species."""
-    g = load()
-    M = oracle.Mech(MECH)
+@pytest.mark.parametrize("mech", ALL)
+def test_qss_solve_matches_exact_arithmetic(oracle, mech):
+    """The species-order elimination against rational elimination of the
+    same system, on the golden states."""
+    g = load(mech)
+    M = oracle.Mech(mech)
     for i, T in enumerate(g["T"]):
+        x = M.qss_concentrations(g["sc"][i], T)
+        ex = exact_solve(M.qss_system(g["sc"][i], T))
+        assert np.all(np.abs(x - ex) <= 1e-13 * np.abs(ex) + 1e-300), (i, x, ex)
+
+
+@pytest.mark.parametrize("mech", ALL)
+def test_qss_production_rate_matches_reference(oracle, mech):
+    """|wdot - wdot_ref| <= tol * sum_r |nu| (|qf| + |qr|) per species, tol =
+    1e-12; for LuEthylene_qss tol = max(1e-12, 2 e_ref) with e_ref the
+    largest relative error of the reference's own QSS concentrations against
+    the exact solution of the balance system (its rates differ from these by
+    what its solve lost, no more)."""
+    g = load(mech)
+    M = oracle.Mech(mech)
+    for i, T in enumerate(g["T"]):
+        tol = 1e-12
+        if mech not in PINNED:
+            ex = exact_solve(M.qss_system(g["sc"][i], T))
+            tol = max(tol, 2.0 * np.max(np.abs(g["sc_qss"][i] - ex) / np.abs(ex)))
         w = M.production_rate(g["sc"][i], T)
         scale = M.production_rate_abs(g["sc"][i], T)
         err = np.abs(w - g["wdot"][i])
-        assert np.all(err <= 1e-12 * scale + 1e-300), (i, np.max(err / (scale + 1e-300)))
+        assert np.all(err <= tol * scale + 1e-300), (i, tol, np.max(err / (scale + 1e-300)))
 
 
-def test_qss_thermo_matches_reference(oracle):
-    g = load()
-    M = oracle.Mech(MECH)
+@pytest.mark.parametrize("mech", ALL)
+def test_qss_thermo_matches_reference(oracle, mech):
+    g = load(mech)
+    M = oracle.Mech(mech)
     np.testing.assert_array_equal(M.mw(), g["mw"])
     for i, T in enumerate(g["T"]):
         np.testing.assert_allclose(M.gibbs(T), g["gibbs"][i], rtol=1e-13, atol=1e-13)
@@ -71,11 +126,12 @@ def test_qss_thermo_matches_reference(oracle):
 
 
 @pytest.mark.parametrize("rtype", [1, 2])
-def test_qss_reactor_rhs_matches_reference(oracle, rtype):
-    """fKernelSpec over the QSS productionRate: species rates within 1e-12
-    of their gross rates, the T row within 1e-10 of its scale."""
-    g = load()
-    M = oracle.Mech(MECH)
+@pytest.mark.parametrize("mech", PINNED)
+def test_qss_reactor_rhs_matches_reference(oracle, rtype, mech):
+    """fKernelSpec over the QSS productionRate: species rates within 1e-10
+    of their gross rates, the T row within 1e-9 of its scale."""
+    g = load(mech)
+    M = oracle.Mech(mech)
     N = M.nsp
     mw = M.mw()
     for i in range(len(g["T"])):
@@ -121,3 +177,62 @@ def test_mechanism_tables_regenerate_identically(oracle, tmp_path):
         ship = os.path.join(os.path.dirname(os.path.dirname(__file__)), "pelephysics_b200", "csrc", "mech",
                             f"mech_{mech}.h")
         assert out.read_text() == open(ship).read(), mech
+
+
+def _reference_balances(path):
+    """Per QSS species of a generated comp_sc_qss: the (term, coefficient)
+    lists of its production, loss and each coupling, term = 2 k (+1 for q_r)."""
+    text = open(path).read()
+    a = text.index("comp_sc_qss(amrex::Real* sc_qss")
+    b = text.index("// Putting it all together", a)
+    blocks = re.split(r"QSSA species (\d+): (\S+)", text[a:b])[1:]
+    out = {}
+    for i in range(0, len(blocks), 3):
+        d = {"num": [], "den": [], "cpl": []}
+        for st in blocks[i + 2].split(";"):
+            if "amrex::Real" not in st:
+                continue
+            lhs, rhs = st.split("=", 1)
+            lhs = lhs.replace("amrex::Real", "").strip()
+            terms = [(2 * int(k) + (1 if w == "qr" else 0), float(c) if c else 1.0)
+                     for c, w, k in re.findall(r"(?:(\d+\.\d+)\s*\*\s*)?(q[fr])_co\[(\d+)\]", rhs)]
+            if lhs.endswith("_num"):
+                d["num"] = terms
+            elif lhs.endswith("_denom"):
+                d["den"] = terms
+            elif not lhs.endswith("_rhs"):
+                d["cpl"].append(sorted(terms))
+        out[int(blocks[i])] = d
+    return out
+
+
+@pytest.mark.parametrize("mech", ALL)
+def test_qss_balance_structure_matches_reference(oracle, mech):
+    """The generated tables' balance terms are those of the reference's
+    generated comp_sc_qss, term for term and in order (a removed forward
+    rate, 0 there, is left out here)."""
+    from pelephysics_b200.mechgen import ceptr_tables as ct
+
+    root = oracle.reference_root()
+    if root is None or not os.path.isdir(os.path.join(root, "Mechanisms")):
+        pytest.skip("needs the reference tree")
+    M = ct.build(os.path.join(root, "Mechanisms", mech), mech)
+    qi = M["qss_info"]
+    removed = {k for k, pos in enumerate(qi["q_rx"]) if M["rxns"][pos]["rmf"]}
+    ref = _reference_balances(os.path.join(root, "Mechanisms", mech, "mechanism.H"))
+    assert sorted(ref) == list(range(len(M["qss"])))
+    keep = lambda lst: [(t, c) for t, c in lst if not (t % 2 == 0 and t // 2 in removed)]
+    for q in range(len(M["qss"])):
+        mine = {"num": [], "den": [], "cpl": {}}
+        for t in range(qi["q_off"][q], qi["q_off"][q + 1]):
+            term, role, c = qi["q_term"][t], qi["q_role"][t], qi["q_coef"][t]
+            if role == -1:
+                mine["num"].append((term, c))
+            elif role == -2:
+                mine["den"].append((term, c))
+            else:
+                mine["cpl"].setdefault(role, []).append((term, c))
+        assert keep(ref[q]["num"]) == mine["num"], q
+        assert [t for t, _ in keep(ref[q]["den"])] == [t for t, _ in mine["den"]], q
+        assert sorted(keep(c) for c in ref[q]["cpl"]) == sorted(sorted(v) for v in mine["cpl"].values()), q
+
