@@ -117,10 +117,10 @@ void ppb_default_options(ppb_options* opt);
 const char* ppb_last_error(void);
 
 /* Mechanisms compiled into the library (LiDryer, drm19, dodecane_lu,
- * heptane_lu_88sk, and the QSS mechanism CH4_lean_qss, whose species in
- * quasi-steady state are not counted: its productionRate solves them first,
- * as its mechanism.H does): returns the number of species and reactions of
- * `mechanism`, or PPB_E_MECH. */
+ * heptane_lu_88sk, and the QSS mechanisms CH4_lean_qss, C1-C2-NO_qss and
+ * LuEthylene_qss, whose species in quasi-steady state are not counted: their
+ * productionRate solves them first, as their mechanism.H does): returns the
+ * number of species and reactions of `mechanism`, or PPB_E_MECH. */
 int ppb_mechanism_info(const char* mechanism, int* nspecies, int* nreactions);
 /* Name of species k of `mechanism` (NULL when out of range). */
 const char* ppb_species_name(const char* mechanism, int k);
