@@ -79,7 +79,8 @@ typedef struct ppb_options {
   int rendezvous_cycles;    /* tuned engine, one warp per cell: before each right-hand side a cell's warp waits
                                up to this many SM clock cycles for the other warps of its block, so that they
                                run the right-hand side's instruction stream together (0: off; at most 1e7;
-                               results are unchanged either way), 1000000 */
+                               -1: 300000 for blocks of more than 8 warps, 1000000 for smaller ones; results
+                               are unchanged either way), -1 */
   int arkode_barrier_us;    /* ReactorArkode: longest wait of a block at the grid barrier of its one cooperative
                                launch, in microseconds (0..60000000; 0: a block that would have to wait gives up
                                at once); a wait that runs out ends the call with PPB_E_CUDA and the message

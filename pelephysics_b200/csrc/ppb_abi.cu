@@ -645,7 +645,7 @@ void ppb_default_options(ppb_options* o)
   o->arkode_max_steps = 500;
   o->eos = PPB_EOS_IDEAL;
   o->cost_order = 1;
-  o->rendezvous_cycles = 1000000;
+  o->rendezvous_cycles = -1;
   o->arkode_barrier_us = 20000000;
   o->adjoint_keep_segments = 1;
 }
@@ -717,8 +717,8 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
   if (r->opt.engine == PPB_ENGINE_PLAIN && r->opt.lu_fp32)
     return fail(PPB_E_ARG, "the plain engine is FP64 only");
   if (r->opt.eos != PPB_EOS_IDEAL && r->opt.eos != PPB_EOS_SRK) return fail(PPB_E_ARG, "eos must be 0 or 1");
-  if (r->opt.rendezvous_cycles < 0 || r->opt.rendezvous_cycles > 10000000)
-    return fail(PPB_E_ARG, "rendezvous_cycles must be in 0..10000000");
+  if (r->opt.rendezvous_cycles < -1 || r->opt.rendezvous_cycles > 10000000)
+    return fail(PPB_E_ARG, "rendezvous_cycles must be -1 or in 0..10000000");
   if (r->opt.warps_per_block > 16) return fail(PPB_E_ARG, "warps_per_block must be at most 16");
   if (r->opt.arkode_barrier_us < 0 || r->opt.arkode_barrier_us > 60000000)
     return fail(PPB_E_ARG, "arkode_barrier_us must be in 0..60000000");

@@ -663,12 +663,14 @@ static int batched_ns_t(const DevMech& M, const Options& o, const AdjBatch& b, A
   const size_t sw_wb = ((8 * (9 * (size_t)n + 1 + (size_t)n * n) + 4 * n) + 15) & ~size_t(15);
   if ((err = best_blocks((const void*)k_adj_sweep<NS>, sw_wb, 8, &sw_w, &sw_b))) return err;
   const int seg_grid = std::min(nsm * seg_b, (nc + seg_w - 1) / seg_w);
+  Options os = o;
+  os.rendezvous = rendezvous_bound(o.rendezvous, seg_w);
   const ItemLayout IL(NS, R);
   // forward with checkpoints
   if ((e = cudaMemsetAsync(C.pool_next, 0, sizeof(int), st)) || (e = cudaMemsetAsync(queue, 0, sizeof(int), st)))
     return (int)e;
   if (C.tpool && (e = cudaMemsetAsync(C.tpool_next, 0, sizeof(unsigned long long), st))) return (int)e;
-  k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, o, b, C, dt, queue, 0, SEG_FORWARD, seg_wb);
+  k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, os, b, C, dt, queue, 0, SEG_FORWARD, seg_wb);
   if ((e = cudaGetLastError())) return (int)e;
   std::vector<int> nseg(nc), ny(nc), off(nc + 1);
   if ((e = cudaMemcpyAsync(nseg.data(), C.nseg, nc * sizeof(int), cudaMemcpyDeviceToHost, st)) ||
@@ -678,7 +680,7 @@ static int batched_ns_t(const DevMech& M, const Options& o, const AdjBatch& b, A
   for (int c = 0; c < nc; c++) maxseg = std::max(maxseg, nseg[c]);
   for (int s = maxseg - 1; s >= 0; s--) {
     if ((e = cudaMemsetAsync(queue, 0, sizeof(int), st))) return (int)e;
-    k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, o, b, C, dt, queue, s, SEG_REPLAY, seg_wb);
+    k_adj_seg<NS, LT><<<seg_grid, seg_w * 32, seg_wb * seg_w, st>>>(M, os, b, C, dt, queue, s, SEG_REPLAY, seg_wb);
     if ((e = cudaGetLastError())) return (int)e;
     if ((e = cudaMemcpyAsync(nseg.data(), C.nseg, nc * sizeof(int), cudaMemcpyDeviceToHost, st)) ||
         (e = cudaMemcpyAsync(ny.data(), C.ny, nc * sizeof(int), cudaMemcpyDeviceToHost, st)) ||

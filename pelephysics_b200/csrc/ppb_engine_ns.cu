@@ -364,7 +364,9 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
   } else {
     blocks = (b.ncells + tpb - 1) / tpb;
   }
-  kern<<<blocks, wpb * 32, shm, st>>>(M, o, b, dt, queue, cb, lc.persistent);
+  Options ob = o;
+  ob.rendezvous = rendezvous_bound(o.rendezvous, wpb);
+  kern<<<blocks, wpb * 32, shm, st>>>(M, ob, b, dt, queue, cb, lc.persistent);
   return (int)cudaGetLastError();
 }
 

@@ -208,8 +208,8 @@ extern "C" int ppb_react_flat_device_noalloc(const char* mechanism, const char* 
   eo.rk_min = o.rk64_nsubsteps_min;
   eo.rk_max = o.rk64_nsubsteps_max;
   eo.use_typ_vals = 0;
-  if (o.rendezvous_cycles < 0 || o.rendezvous_cycles > 10000000)
-    return nf(PPB_E_ARG, "rendezvous_cycles must be in 0..10000000");
+  if (o.rendezvous_cycles < -1 || o.rendezvous_cycles > 10000000)
+    return nf(PPB_E_ARG, "rendezvous_cycles must be -1 or in 0..10000000");
   eo.rendezvous = o.rendezvous_cycles;
   // the launch the allocating path makes for the same options with a fixed
   // block size (no autotuner here: it would need scratch of its own)

@@ -31,8 +31,9 @@ def test_default_options_match_reference_defaults():
     o = _lib.default_options()
     assert (o.rtol, o.atol, o.max_order, o.max_steps, o.max_nls_iters) == (1e-6, 1e-10, 2, 10000, 3)
     assert (o.rk64_nsubsteps_guess, o.rk64_nsubsteps_min, o.rk64_nsubsteps_max) == (10, 5, 500)
-    # engine tuning: the block rendezvous before each right-hand side is on
-    assert o.rendezvous_cycles == 1000000 and o.cost_order == 1
+    # engine tuning: the block rendezvous before each right-hand side is on,
+    # its bound picked by block size
+    assert o.rendezvous_cycles == -1 and o.cost_order == 1
     assert o.arkode_barrier_us == 20000000
 
 
@@ -40,7 +41,7 @@ def test_rendezvous_and_block_size_bounds_checked_without_device():
     L = _lib.lib()
     h = C.c_void_p()
     assert L.ppb_create(b"drm19", b"ReactorCvode", C.byref(h)) == 0
-    for field, bad, msg in (("rendezvous_cycles", -1, b"rendezvous_cycles"),
+    for field, bad, msg in (("rendezvous_cycles", -2, b"rendezvous_cycles"),
                             ("rendezvous_cycles", 10000001, b"rendezvous_cycles"),
                             ("warps_per_block", 17, b"warps_per_block"),
                             ("arkode_barrier_us", -1, b"arkode_barrier_us"),

@@ -406,13 +406,13 @@ def test_cost_ordered_queue_changes_no_bits(cuda, oracle):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("wpb,cyc", [(8, 1000000), (12, 1000000), (16, 1000000), (16, 2000)])
+@pytest.mark.parametrize("wpb,cyc", [(8, -1), (12, -1), (16, -1), (16, 1000000), (16, 2000)])
 def test_block_rendezvous_changes_no_bits(cuda, oracle, wpb, cyc):
     """The rendezvous before each right-hand side only changes when a cell's
     warp runs, never what it computes: every cell gives the same bits with
-    rendezvous_cycles = 0 and with a bound (the default, and a bound short
-    enough that most waits time out), at 8, 12 and 16 warps per block, and
-    the cells still match the CPU oracle."""
+    rendezvous_cycles = 0 and with a bound (the default, picked by block
+    size; 1e6; and a bound short enough that most waits time out), at 8, 12
+    and 16 warps per block, and the cells still match the CPU oracle."""
     torch = cuda
     mech, dt, nc = "drm19", 1e-5, 3000
     rY, src, rX, rXs = premix_oracle(oracle, mech, nc, 8, 1000.0, 1000.0, 0.5, 1.5)
