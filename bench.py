@@ -275,6 +275,7 @@ def our_arm(args):
     y_gpu = y.cpu().numpy().T.copy()
     stats = r.cell_stats(n)
     wpb, team, regs, tune_ms = r.launch_config()
+    rv_cycles = r.rendezvous_cycles()
     status, _ = r.cell_status(n)
 
     # end to end through the public flat API on pinned host buffers
@@ -349,12 +350,14 @@ def our_arm(args):
         fp32_value = n * len(ms_f) / (sum(ms_f) / 1e3)
         y_fp32 = yf.cpu().numpy().T.copy()
         fw, ft, fr, _ = rf.launch_config()
+        frv = rf.rendezvous_cycles()
         rf.close()
         if not args.no_adjoint:
             out["adjoint"] = adjoint_measure(dev, args.adjoint_cells)
         peak = probe_fp64_peak()
         out.update(plain_value=plain_value, dT_plain=dT_plain, fp64_peak_gflops=peak, fp32_value=fp32_value,
-                   fp32_launch={"warps_per_block": fw, "lanes_per_cell": ft, "register_budget": fr})
+                   fp32_launch={"warps_per_block": fw, "lanes_per_cell": ft, "register_budget": fr,
+                                "rendezvous_cycles": frv})
 
     cpu = None
     acc = None
@@ -428,7 +431,7 @@ def our_arm(args):
                        "engine": "tuned: team of lanes per cell, persistent work queue, CUDA graph, FP64 LU",
                        "autotuned_launch": {"warps_per_block": wpb, "lanes_per_cell": team,
                                             "register_budget": "<=128 regs" if regs == 2 else "<=255 regs",
-                                            "sample_ms": tune_ms}},
+                                            "rendezvous_cycles": rv_cycles, "sample_ms": tune_ms}},
             "e2e": {"value": e2e, "unit": "cells/s", "h2d_bytes_per_step": h2d * ws, "d2h_bytes_per_step": d2h * ws},
             "gpu_launches": 2 * args.steps,
             "roofline": roof,
@@ -489,6 +492,9 @@ def adjoint_measure(dev, ncells):
     torch.cuda.synchronize()
     t_fwd = a.elapsed_time(b) / 1e3
     fwd_stats = r.cell_stats(n)
+    fw, ft, fr, _ = r.launch_config()
+    fwd_launch = {"warps_per_block": fw, "lanes_per_cell": ft, "register_budget": fr,
+                  "rendezvous_cycles": r.rendezvous_cycles()}
     w = g(cells.meta["w"])
     L, lam = adj.loss_T_OH(y, ioh, w[0], w[1])
     t_adjs = []
@@ -506,7 +512,7 @@ def adjoint_measure(dev, ncells):
     r.close()
     return {"workload": f"drm19 {n} h/cp reactors, T 1100+500U, phi 0.5+1.5U, 1 atm, t_end 5e-4 s, "
                         "rtol=atol=1e-10; L = sum(w_T T + w_OH Y_OH), w ~ N(0,1) seed 4",
-            "cells": n, "forward_ms": 1e3 * t_fwd, "adjoint_ms": 1e3 * t_adj,
+            "cells": n, "forward_ms": 1e3 * t_fwd, "forward_launch": fwd_launch, "adjoint_ms": 1e3 * t_adj,
             "adjoint_ms_runs": [1e3 * v for v in t_adjs], "ratio": t_adj / t_fwd,
             "target_ratio": 5.0, "checkpoint_interval": 16, "loss": float(L),
             "grad_norm": {"lnA": float(np.linalg.norm(gr[:R])), "beta": float(np.linalg.norm(gr[R:2 * R])),

@@ -60,7 +60,8 @@ typedef struct ppb_options {
   int refine_sweeps;        /* refinement sweeps with lu_fp32, 1 */
   int warps_per_block;      /* tuned engine block size in warps (1, 2, 4, 8; 12 or 16 for the BDF, either LU
                                precision, with 32 lanes per cell and budget 2: one block per SM); 0 = autotune the block
-                               size, lanes per cell and register budget on the first call */
+                               size, lanes per cell and register budget on the first call (the SRK EOS and QSS
+                               mechanisms, not autotuned: 16 warps where 16 cells fit one SM, else <= 8) */
   int use_graph;            /* replay react() as a captured CUDA graph, 1 */
   int adjoint_checkpoint_interval; /* accepted BDF steps between adjoint checkpoints, 16 */
   int adjoint_memory_mb;    /* device memory for adjoint checkpoints, tapes and points, 16384 */
@@ -79,8 +80,9 @@ typedef struct ppb_options {
   int rendezvous_cycles;    /* tuned engine, one warp per cell: before each right-hand side a cell's warp waits
                                up to this many SM clock cycles for the other warps of its block, so that they
                                run the right-hand side's instruction stream together (0: off; at most 1e7;
-                               -1: 300000 for blocks of more than 8 warps, 1000000 for smaller ones; results
-                               are unchanged either way), -1 */
+                               -1: for blocks of more than 8 warps the autotuner picks 300000 or 1000000, a
+                               fixed launch takes 300000; 1000000 for smaller blocks and in the adjoint;
+                               results are unchanged either way), -1 */
   int arkode_barrier_us;    /* ReactorArkode: longest wait of a block at the grid barrier of its one cooperative
                                launch, in microseconds (0..60000000; 0: a block that would have to wait gives up
                                at once); a wait that runs out ends the call with PPB_E_CUDA and the message
@@ -305,6 +307,13 @@ int ppb_react_flat_device_noalloc(const char* mechanism, const char* integrator,
  * reference. */
 int ppb_get_launch_config(ppb_reactor* r, int* warps_per_block, int* team_lanes, int* register_budget,
                           double* tuned_ms);
+
+/* The block rendezvous bound (SM clocks) the reactor's tuned BDF launches use:
+ * rendezvous_cycles when set, else the autotuner's pick or the block-size
+ * default; 0 when its launches have no rendezvous (rendezvous_cycles = 0,
+ * RK64, the plain engine, teams of other than 32 lanes).  No counterpart in
+ * the reference. */
+int ppb_get_rendezvous_cycles(ppb_reactor* r, int* cycles);
 
 /* ---- Differentiation (no counterpart in the reference; the ReactorBase
  * interface has no derivative entry points).

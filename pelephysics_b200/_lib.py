@@ -127,6 +127,7 @@ def lib():
     L.ppb_molecular_weights.argtypes = [C.c_char_p, dpp]
     L.ppb_pyt2re.argtypes = [C.c_char_p, C.c_int, dp, dp, dp, dp, dp, C.c_int, vp]
     L.ppb_get_launch_config.argtypes = [vp, ip, ip, ip, dpp]
+    L.ppb_get_rendezvous_cycles.argtypes = [vp, ip]
     L.ppb_get_arrhenius.argtypes = [vp, dpp, dpp, dpp]
     L.ppb_set_arrhenius.argtypes = [vp, dpp, dpp, dpp]
     L.ppb_adjoint_flat_device.argtypes = [vp, dp, dp, dp, dp, C.c_double, C.c_int, dp, dp, dp, dp, dp, vp]

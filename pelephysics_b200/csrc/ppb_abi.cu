@@ -18,6 +18,7 @@
 #include <atomic>
 #include <map>
 #include <memory>
+#include <numeric>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -130,6 +131,8 @@ struct ppb_reactor {
   ppb_options opt{};
   std::vector<double> typ_vals;
   double* atolv = nullptr;
+  // SRK / QSS kernels: a 16-warp block is compiled and fits one SM
+  bool dq16 = false;
   // bumped whenever something a captured graph holds changes (typical
   // values, Arrhenius tables, options): graphs of older generations are
   // captured again
@@ -382,7 +385,7 @@ struct TuneEntry {
   int dev, method, rtype, lu_fp32, typ;
   LaunchConfig lc;
   double ms;
-  int sample, target; // cells timed, and the sample size wanted (four resident waves)
+  int sample, target; // cells timed, and the sample size wanted (32 resident waves)
 };
 static std::mutex g_tune_mu;
 static std::vector<TuneEntry> g_tune;
@@ -419,13 +422,16 @@ static LaunchConfig launch_config(const ppb_reactor* r)
   lc.lu_fp32 = r->opt.lu_fp32;
   lc.persistent = 1;
   if (r->opt.eos == PPB_EOS_SRK || r->t->nqss > 0) {
-    // one compiled SRK or QSS kernel: warp teams, <= 128 registers; the
-    // block size the caller gives, else the largest (<= 8 warps) that fits
+    // the SRK or QSS kernel: warp teams, <= 128 registers; the block size
+    // the caller gives, else 16 warps (one block per SM, one rendezvous)
+    // where that kernel is compiled and fits, else the largest <= 8 that fits
     lc.rhsv = r->opt.eos == PPB_EOS_SRK ? 1 : 2;
     lc.team = 32;
     lc.minb = 2;
     if (r->opt.warps_per_block > 0) {
       lc.warps_per_block = r->opt.warps_per_block;
+    } else if (r->dq16) {
+      lc.warps_per_block = 16;
     } else {
       const size_t cb = team_cell_bytes(r->t, 0);
       int w = 8;
@@ -458,8 +464,8 @@ static LaunchConfig launch_config(const ppb_reactor* r)
   return lc;
 }
 
-// Time the candidate configurations on a copy of (up to) four resident
-// waves of the batch's first cells and cache the fastest; a batch that gives
+// Time the candidate configurations on copies of the batch's first cells
+// (up to 4, then 32 resident waves) and cache the fastest; a batch that gives
 // at least twice the cells of an earlier, smaller-than-wanted sample tunes
 // again.  Not during a stream capture (the caller checks).
 static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
@@ -489,7 +495,17 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
         const int res = react_occupancy(*r->dm, r->method, lc);
         if (res <= 0) continue;
         max_res = std::max(max_res, res);
-        cand.push_back(lc);
+        if (wpb > 8 && r->opt.rendezvous_cycles < 0) {
+          // one block per SM: the rendezvous bound is tuned too (drm19, 16
+          // warps: the 64^3 field runs faster at 3e5 SM clocks, long
+          // integrations of h/cp reactors at 1e6)
+          for (int rv : {300000, 1000000}) {
+            lc.rv = rv;
+            cand.push_back(lc);
+          }
+        } else {
+          cand.push_back(lc);
+        }
       }
     }
   }
@@ -497,10 +513,19 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const int m = (int)std::min<long>(b.ncells, 4L * max_res * nsm);
-  const size_t nm = (size_t)m;
+  // Two samples of the batch's first cells: a short one (4 resident waves of
+  // the largest candidate) times every candidate, then a long one (32 waves,
+  // or the whole batch) times those within 1.5x of the fastest.  On a short
+  // sample the few longest cells decide the time, and with them the
+  // configurations that finish one cell soonest; the long one weighs
+  // throughput as a full call does (drm19, 65,536 h/cp reactors over 5e-4 s:
+  // the short sample picked 8 warps per block, 188 ms a call, against 131 ms
+  // for 16).
+  const int m1 = (int)std::min<long>(b.ncells, 4L * max_res * nsm);
+  const int m2 = (int)std::min<long>(b.ncells, 32L * max_res * nsm);
+  const size_t nm = (size_t)m2;
   double *y0 = nullptr, *y = nullptr, *sr = nullptr, *re = nullptr, *rs = nullptr;
-  int *stt = nullptr, *nfe = nullptr, *q = nullptr;
+  int *stt = nullptr, *nfe = nullptr, *q = nullptr, *ord = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int err = 0;
   auto cleanup = [&]() {
@@ -512,12 +537,14 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
     cudaFree(stt);
     cudaFree(nfe);
     cudaFree(q);
+    cudaFree(ord);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
   };
   if ((err = cudaMalloc(&y0, n * nm * 8)) || (err = cudaMalloc(&y, n * nm * 8)) || (err = cudaMalloc(&sr, n * nm * 8)) ||
       (err = cudaMalloc(&re, nm * 8)) || (err = cudaMalloc(&rs, nm * 8)) || (err = cudaMalloc(&stt, nm * 4)) ||
-      (err = cudaMalloc(&nfe, nm * 4)) || (err = cudaMalloc(&q, 16)) || (err = cudaEventCreate(&e0)) ||
+      (err = cudaMalloc(&nfe, nm * 4)) || (err = cudaMalloc(&q, 16)) || (err = cudaMalloc(&ord, nm * 4)) ||
+      (err = cudaEventCreate(&e0)) ||
       (err = cudaEventCreate(&e1))) {
     cleanup();
     return cuda_fail(err, "autotune scratch");
@@ -527,14 +554,9 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
   if (!err) err = cudaMemcpyAsync(re, b.rhoe, nm * 8, cudaMemcpyDeviceToDevice, st);
   if (!err) err = cudaMemcpyAsync(rs, b.rhoesrc, nm * 8, cudaMemcpyDeviceToDevice, st);
   const Options o = engine_options(r);
-  // Two interleaved passes over the candidates after one warm-up launch;
-  // each candidate keeps its faster time, so a clock ramp or a neighbour's
-  // burst during one pass does not decide the pick.
-  const size_t nc = cand.size();
-  std::vector<double> tbest(nc, 1e300);
-  for (size_t k = 0; k < 2 * nc + 1 && !err; k++) {
-    const size_t ci = k == 0 ? 0 : (k - 1) % nc;
-    const LaunchConfig& lc = cand[ci];
+  bool use_ord = false;
+  // one launch of candidate lc on the first m cells of the sample (device time)
+  auto timed = [&](const LaunchConfig& lc, int m, float* ms) -> int {
     Batch tb{};
     tb.y = y;
     tb.src = sr;
@@ -544,29 +566,74 @@ static int autotune(ppb_reactor* r, const Batch& b, double dt, cudaStream_t st)
     tb.status = stt;
     tb.nfe = nfe;
     tb.ncells = m;
-    tb.ld = m;
-    err = cudaMemcpyAsync(y, y0, n * nm * 8, cudaMemcpyDeviceToDevice, st);
-    if (!err) err = cudaEventRecord(e0, st);
-    if (!err) err = launch_react(*r->dm, o, r->method, lc, tb, dt, q, st);
-    if (!err) err = cudaEventRecord(e1, st);
-    if (!err) err = cudaEventSynchronize(e1);
+    tb.ld = m2;
+    tb.order = use_ord ? ord : nullptr;
+    int e = cudaMemcpyAsync(y, y0, n * nm * 8, cudaMemcpyDeviceToDevice, st);
+    if (!e) e = cudaEventRecord(e0, st);
+    if (!e) e = launch_react(*r->dm, o, r->method, lc, tb, dt, q, st);
+    if (!e) e = cudaEventRecord(e1, st);
+    if (!e) e = cudaEventSynchronize(e1);
+    if (!e) e = cudaEventElapsedTime(ms, e0, e1);
+    return e;
+  };
+  // One warm-up launch, then two interleaved passes over the candidates
+  // `which`; each keeps its faster time, so a clock ramp or a neighbour's
+  // burst during one pass does not decide the pick.  With cost_order the
+  // timed launches take the cells in the order the calls after the first one
+  // use: by descending cost (right-hand sides) in the warm-up launch, ties in
+  // index order.
+  auto stage = [&](int m, const std::vector<size_t>& which, std::vector<double>& t) -> int {
     float ms = 0.f;
-    if (!err) err = cudaEventElapsedTime(&ms, e0, e1);
-    if (!err && k > 0) tbest[ci] = std::min(tbest[ci], (double)ms);
-  }
-  double best = 1e300;
-  LaunchConfig pick = cand[0];
-  for (size_t ci = 0; ci < nc; ci++) {
-    if (tbest[ci] < best) {
-      best = tbest[ci];
-      pick = cand[ci];
+    use_ord = false;
+    int e = timed(cand[which[0]], m, &ms);
+    if (!e && r->opt.cost_order && m > 1) {
+      std::vector<int> cost((size_t)m), idx((size_t)m);
+      e = cudaMemcpyAsync(cost.data(), nfe, (size_t)m * 4, cudaMemcpyDeviceToHost, st);
+      if (!e) e = cudaStreamSynchronize(st);
+      if (e) return e;
+      std::iota(idx.begin(), idx.end(), 0);
+      std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+      e = cudaMemcpyAsync(ord, idx.data(), (size_t)m * 4, cudaMemcpyHostToDevice, st);
+      if (!e) e = cudaStreamSynchronize(st);
+      use_ord = true;
+    }
+    for (size_t k = 0; k < 2 * which.size() && !e; k++) {
+      const size_t ci = which[k % which.size()];
+      e = timed(cand[ci], m, &ms);
+      if (!e) t[ci] = std::min(t[ci], (double)ms);
+    }
+    return e;
+  };
+  const size_t nc = cand.size();
+  std::vector<size_t> all(nc);
+  std::iota(all.begin(), all.end(), 0);
+  std::vector<double> t1(nc, 1e300), t2(nc, 1e300);
+  err = stage(m1, all, t1);
+  size_t bi = 0;
+  for (size_t ci = 0; ci < nc; ci++)
+    if (t1[ci] < t1[bi]) bi = ci;
+  double best = t1[bi];
+  int sample = m1;
+  if (!err && m2 > m1) {
+    std::vector<size_t> keep;
+    for (size_t ci : all)
+      if (t1[ci] <= 1.5 * t1[bi]) keep.push_back(ci);
+    std::stable_sort(keep.begin(), keep.end(), [&](size_t a, size_t c) { return t1[a] < t1[c]; });
+    err = stage(m2, keep, t2);
+    if (!err) {
+      bi = keep[0];
+      for (size_t ci : keep)
+        if (t2[ci] < t2[bi]) bi = ci;
+      best = t2[bi];
+      sample = m2;
     }
   }
+  const LaunchConfig pick = cand[bi];
   cleanup();
   if (err) return cuda_fail(err, "autotune");
-  const int target = (int)std::min<long>(1L << 30, 4L * max_res * nsm);
+  const int target = (int)std::min<long>(1L << 30, 32L * max_res * nsm);
   TuneEntry te{r->dm->host, dev, r->method, r->reactor_type, r->opt.lu_fp32, (int)!r->typ_vals.empty(), pick, best,
-               m, target};
+               sample, target};
   std::lock_guard<std::mutex> lk(g_tune_mu);
   if (TuneEntry* e = find_tune(r)) {
     *e = te;
@@ -731,6 +798,8 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
         r->opt.lu_fp32)
       return fail(PPB_E_ARG, "the SRK EOS needs ReactorCvode, reactor type 1, the tuned engine and the FP64 LU");
     if (!find_srk(r->t->name)) return fail(PPB_E_MECH, "the mechanism has no SRK parameters");
+    if (r->opt.warps_per_block > 8 && r->opt.warps_per_block != 16)
+      return fail(PPB_E_ARG, "the SRK EOS runs 1 to 8 or 16 warps per block");
   }
   if (r->t->nqss > 0) {
     // a QSS mechanism: the QSS species solved in every right-hand side, the
@@ -740,7 +809,8 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
     if (r->method != METHOD_BDF || r->opt.engine != PPB_ENGINE_TUNED || r->opt.lu_fp32 ||
         r->opt.eos != PPB_EOS_IDEAL)
       return fail(PPB_E_ARG, "a QSS mechanism needs ReactorCvode, the tuned engine, the FP64 LU and the ideal-gas EOS");
-    if (r->opt.warps_per_block > 8) return fail(PPB_E_ARG, "a QSS mechanism runs at most 8 warps per block");
+    if (r->opt.warps_per_block > 8 && r->opt.warps_per_block != 16)
+      return fail(PPB_E_ARG, "a QSS mechanism runs 1 to 8 or 16 warps per block");
   }
   r->reactor_type = reactor_type;
   int e = 0;
@@ -753,6 +823,12 @@ int ppb_init(ppb_reactor* r, int reactor_type, int ncells, const ppb_options* op
   if (ncells > 0) {
     e = ensure_scratch(r, ctx_of(r), ncells);
     if (e) return e;
+  }
+  r->dq16 = false;
+  if (r->opt.eos == PPB_EOS_SRK || r->t->nqss > 0) {
+    LaunchConfig l16 = launch_config(r);
+    l16.warps_per_block = 16;
+    r->dq16 = react_occupancy(*r->dm, r->method, l16) >= 16;
   }
   r->gen++;
   r->inited = true;
@@ -1313,6 +1389,21 @@ int ppb_get_launch_config(ppb_reactor* r, int* warps_per_block, int* team_lanes,
   if (team_lanes) *team_lanes = lc.team;
   if (register_budget) *register_budget = lc.minb;
   if (tuned_ms) *tuned_ms = ms;
+  return 0;
+}
+
+int ppb_get_rendezvous_cycles(ppb_reactor* r, int* cycles)
+{
+  if (!r || !r->inited) return fail(PPB_E_STATE, "ppb_get_rendezvous_cycles before init");
+  if (!cycles) return fail(PPB_E_ARG, "ppb_get_rendezvous_cycles: null argument");
+  const LaunchConfig lc = launch_config(r);
+  // the rendezvous runs in the tuned BDF kernels of one warp per cell
+  if (r->method != METHOD_BDF || lc.engine != ENGINE_TUNED || lc.team != 32) {
+    *cycles = 0;
+    return 0;
+  }
+  const int o = r->opt.rendezvous_cycles;
+  *cycles = (o < 0 && lc.rv > 0) ? lc.rv : rendezvous_bound(o, lc.warps_per_block);
   return 0;
 }
 

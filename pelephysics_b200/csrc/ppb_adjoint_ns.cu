@@ -663,8 +663,11 @@ static int batched_ns_t(const DevMech& M, const Options& o, const AdjBatch& b, A
   const size_t sw_wb = ((8 * (9 * (size_t)n + 1 + (size_t)n * n) + 4 * n) + 15) & ~size_t(15);
   if ((err = best_blocks((const void*)k_adj_sweep<NS>, sw_wb, 8, &sw_w, &sw_b))) return err;
   const int seg_grid = std::min(nsm * seg_b, (nc + seg_w - 1) / seg_w);
+  // the recording kernel waits up to 1e6 SM clocks unless the caller set a
+  // bound (drm19, 65536 cells, 16 warps: adjoint 519 ms at 1e6 against 579
+  // at 3e5)
   Options os = o;
-  os.rendezvous = rendezvous_bound(o.rendezvous, seg_w);
+  if (o.rendezvous < 0) os.rendezvous = 1000000;
   const ItemLayout IL(NS, R);
   // forward with checkpoints
   if ((e = cudaMemsetAsync(C.pool_next, 0, sizeof(int), st)) || (e = cudaMemsetAsync(queue, 0, sizeof(int), st)))

@@ -46,10 +46,11 @@ struct Options {
   int rendezvous;        // cycles a warp waits at a right-hand side for its block's other warps (0: off)
 };
 
-// The rendezvous bound a launch of `warps` warps per block runs with; -1
-// picks it by block size: 300,000 SM clocks above 8 warps, 1,000,000 up to 8
-// (drm19 64^3 field: 16 warps 947k-959k cells/s at 300k against 894k-898k at
-// 1M; 8 warps 425k-432k against 450k-454k).
+// The rendezvous bound a launch of `warps` warps per block runs with when
+// the autotuner picked none; -1 picks it by block size: 300,000 SM clocks
+// above 8 warps, 1,000,000 up to 8 (drm19 64^3 field: 16 warps 947k-959k
+// cells/s at 300k against 894k-898k at 1M; 8 warps 425k-432k against
+// 450k-454k).
 inline int rendezvous_bound(int cycles, int warps)
 {
   return cycles >= 0 ? cycles : (warps > 8 ? 300000 : 1000000);

@@ -56,6 +56,7 @@ struct LaunchConfig {
   int minb = 2;       // register budget: >= minb blocks of 256 threads per SM
   int rhsv = 0;       // right-hand side: 0 ideal gas, 1 the SRK e-reactor, 2 a QSS mechanism (the last two:
                       // warp teams, <= 128 registers, difference-quotient Jacobian)
+  int rv = -1;        // rendezvous bound the autotuner picked, used when the option is -1 (-1: by block size)
 };
 // Resident cells per SM of the tuned kernel in configuration lc (0: the
 // configuration does not fit or is not compiled).

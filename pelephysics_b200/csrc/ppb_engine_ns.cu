@@ -207,12 +207,15 @@ constexpr int big_team()
 // and nullptr for the others:
 //   0: FP64 BDF, 32 lanes, 8 warps (<= 128 and <= 255 registers)
 //   1: FP64 BDF, 32 lanes, 12 and 16 warps per block (one block per SM)
-//   2: the multi-warp teams (FP64 and FP32 BDF, RK64)
+//   2: the multi-warp teams (FP64 and FP32 BDF, RK64); the SRK kernel at 16
+//      warps per block (<= 21 species)
 //   3: FP32 BDF and RK64 with 32 lanes, the 16-lane variants, the SRK kernel
+//      (<= 8 warps per block)
 //   4: FP32 BDF, 32 lanes, 12 and 16 warps per block
 // Species counts compiled for a QSS mechanism only (transported species of
-// CH4_lean_qss 13, LuEthylene_qss 22, C1-C2-NO_qss 39): the one QSS
-// kernel, no other variant.
+// CH4_lean_qss 13, LuEthylene_qss 22, C1-C2-NO_qss 39): the QSS kernel at
+// <= 8 warps per block (part 3) and, for <= 21 species, at 16 (part 1); no
+// other variant.
 template <int NS>
 constexpr bool qss_only()
 {
@@ -227,17 +230,26 @@ static TeamKernel team_kernel_part(int method, bool fp32, int team, int minb, in
   // the QSS reactor (srk == RHS_QSS): FP64 BDF, one warp per cell, <= 128
   // registers, difference-quotient Jacobian
   if constexpr (qss_only<NS>()) {
+    if (srk != RHS_QSS || method != METHOD_BDF || fp32 || team != 32 || minb != 2) return nullptr;
     if constexpr (P == 3)
-      return (srk == RHS_QSS && method == METHOD_BDF && !fp32 && team == 32 && minb == 2 && wpb <= 8)
-               ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, RHS_QSS>
-               : nullptr;
+      return wpb <= 8 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 2, RHS_QSS> : nullptr;
+    // 16 warps per block, one block per SM (<= 21 species: sixteen cell
+    // workspaces fit one SM's shared memory), all under one rendezvous
+    if constexpr (P == 1 && small)
+      return wpb == 16 ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, RHS_QSS, 512> : nullptr;
     return nullptr;
   } else {
     if (srk == RHS_QSS) return nullptr;
     // 12 or 16 warps per block (one block per SM: <= 168 or <= 128 registers):
-    // the FP64 BDF warp-per-cell kernel
+    // the FP64 BDF warp-per-cell kernel; the SRK e-reactor at 16
     if (wpb > 8) {
-      if (method != METHOD_BDF || team != 32 || minb != 2 || srk) return nullptr;
+      if (method != METHOD_BDF || team != 32 || minb != 2) return nullptr;
+      if (srk) {
+        if constexpr (P == 2 && small)
+          return (!fp32 && wpb == 16) ? (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, RHS_SRK, 512>
+                                      : nullptr;
+        return nullptr;
+      }
       if constexpr (P == 1) {
         if (fp32) return nullptr;
         if (wpb == 16) return (TeamKernel)k_react_team<NS, double, METHOD_BDF, 32, 1, RHS_IDEAL, 512>;
@@ -365,7 +377,7 @@ static int launch_react_ns(const DeviceMechanism& m, const Options& o, int metho
     blocks = (b.ncells + tpb - 1) / tpb;
   }
   Options ob = o;
-  ob.rendezvous = rendezvous_bound(o.rendezvous, wpb);
+  ob.rendezvous = (o.rendezvous < 0 && lc.rv > 0) ? lc.rv : rendezvous_bound(o.rendezvous, wpb);
   kern<<<blocks, wpb * 32, shm, st>>>(M, ob, b, dt, queue, cb, lc.persistent);
   return (int)cudaGetLastError();
 }

@@ -109,6 +109,14 @@ class Reactor:
         check(lib().ppb_get_launch_config(self._h, C.byref(w), C.byref(t), C.byref(rb), C.byref(ms)))
         return w.value, t.value, rb.value, ms.value
 
+    def rendezvous_cycles(self):
+        """The block rendezvous bound (SM clocks) of the tuned BDF launches:
+        the option when set, else the autotuner's pick or the block-size
+        default; 0 without a rendezvous."""
+        v = C.c_int()
+        check(lib().ppb_get_rendezvous_cycles(self._h, C.byref(v)))
+        return v.value
+
     # ---- differentiation (no counterpart in the reference)
     def get_arrhenius(self):
         """Forward Arrhenius parameters (A in SI units, beta, Ea/R in K)."""

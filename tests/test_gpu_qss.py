@@ -15,6 +15,8 @@ forward rates removed by the reduction), LuEthylene_qss (22, 10).
   reference's compiled kernels (over the table kernels for LuEthylene_qss),
   with the replica criterion (T 1e-6 relative, Y 1e-8 absolute,
   compare_to_reference) for cells whose step sequence parts in the last bit;
+* block size: CH4_lean_qss runs 16 warps per block by default (sixteen
+  cell workspaces fit one SM) and gives the same bits at 8;
 * the option checks: a QSS mechanism runs on the tuned FP64 BDF only, and
   has no analytical Jacobian here."""
 
@@ -126,9 +128,32 @@ def test_qss_react_vs_reference_kernels(cuda, oracle, mech, rtype, nc, dt):
     assert res["max_rel_T"] <= 1e-5 and res["max_abs_Y"] <= 1e-7, res
 
 
+def test_qss_block_size_changes_no_bits(cuda, oracle):
+    """The default launch of CH4_lean_qss is one 16-warp block per SM (one
+    rendezvous for all its warps); 8-warp blocks give the same bits and the
+    same per-cell counters, as block size only changes when a cell's warp
+    runs."""
+    nc, dt = 600, 1e-3
+    rY, src, rX, rXs = premix_oracle(oracle, MECH, nc, 7, 1700.0, 400.0, 0.5, 0.5, reactor_type=1)
+    outs, stats, picks = [], [], []
+    for wpb in (0, 8):
+        r = Reactor(MECH)
+        r.init(1, nc, rtol=1e-10, atol=1e-10, max_order=5, warps_per_block=wpb)
+        y = rY.copy()
+        _, _, _, code = r.react(y, src.copy(), rX.copy(), rXs.copy(), dt)
+        assert code == 0
+        outs.append(y)
+        stats.append(r.cell_stats(nc))
+        picks.append(r.launch_config()[0])
+    assert picks == [16, 8]
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(stats[0], stats[1])
+
+
 def test_qss_option_checks(cuda):
     for integ, extra in (("ReactorRK64", {}), ("ReactorCvode", {"lu_fp32": 1}), ("ReactorCvode", {"engine": 0}),
-                         ("ReactorArkode", {}), ("ReactorCvode", {"eos": 1})):
+                         ("ReactorArkode", {}), ("ReactorCvode", {"eos": 1}),
+                         ("ReactorCvode", {"warps_per_block": 12})):
         r = Reactor(MECH, integ)
         with pytest.raises(_lib.EngineError):
             r.init(1, 4, **extra)

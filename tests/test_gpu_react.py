@@ -328,6 +328,9 @@ def test_autotuner_choice_is_reproducible(cuda, oracle, mech):
     ra.react(y, s, x, xs, dt)
     wpb, team, regs, ms = ra.launch_config()
     assert ms > 0 and wpb in (1, 2, 4, 8, 12, 16) and team in (16, 32) and regs in (1, 2)
+    # one block per SM: the autotuner picks the rendezvous bound as well
+    rv = ra.rendezvous_cycles()
+    assert rv == 0 if team != 32 else (rv in (300000, 1000000) if wpb > 8 else rv == 1000000)
     rb = Reactor(mech)
     rb.init(rtype, nc, **opts, warps_per_block=wpb, team_lanes=team, register_budget=regs)
     assert rb.launch_config()[:3] == (wpb, team, regs)
@@ -426,6 +429,8 @@ def test_block_rendezvous_changes_no_bits(cuda, oracle, wpb, cyc):
         outs.append(y.cpu().numpy())
         stats.append(r.cell_stats(nc))
         assert r.launch_config()[0] == wpb
+        # the bound the launches ran with: the option, or by block size
+        assert r.rendezvous_cycles() == (bound if bound >= 0 else (300000 if wpb > 8 else 1000000))
     np.testing.assert_array_equal(outs[0], outs[1])
     np.testing.assert_array_equal(stats[0], stats[1])
     idx = np.arange(0, nc, 97)

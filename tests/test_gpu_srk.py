@@ -1,7 +1,8 @@
 """The SRK real-gas e-reactor (eos = PPB_EOS_SRK) on the GPU against the
 oracle's BDF with the same SRK right-hand side and difference-quotient
-Jacobian, at the integration bar (T 1e-6 relative, Y 1e-8 absolute), and
-the option checks."""
+Jacobian, at the integration bar (T 1e-6 relative, Y 1e-8 absolute); the
+block size (16 warps by default for drm19, the same bits at 8); and the
+option checks."""
 
 import numpy as np
 import pytest
@@ -60,9 +61,30 @@ def test_srk_reactor_matches_oracle(cuda, oracle, mech, nc, dt, P, tol):
     assert np.max(np.abs(yi[:, -1] - y[:, -1])) > 1e-4
 
 
+def test_srk_block_size_changes_no_bits(cuda, oracle):
+    """drm19's SRK reactor runs one 16-warp block per SM by default and gives
+    the same bits and per-cell counters in 8-warp blocks."""
+    nc, dt = 600, 1e-5
+    rY, src, rX, rXs = srk_cells(oracle, "drm19", nc, 5, 1100.0, 500.0, 50 * 1013250.0)
+    outs, stats, picks = [], [], []
+    for wpb in (0, 8):
+        r = Reactor("drm19")
+        r.init(1, nc, rtol=1e-10, atol=1e-10, max_order=5, eos=1, warps_per_block=wpb)
+        y = rY.copy()
+        _, _, _, code = r.react(y, src.copy(), rX.copy(), rXs.copy(), dt)
+        assert code == 0
+        outs.append(y)
+        stats.append(r.cell_stats(nc))
+        picks.append(r.launch_config()[0])
+    assert picks == [16, 8]
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(stats[0], stats[1])
+
+
 def test_srk_option_checks(cuda):
     for integ, rtype, extra in (("ReactorRK64", 1, {}), ("ReactorCvode", 2, {}), ("ReactorCvode", 1, {"lu_fp32": 1}),
-                                ("ReactorCvode", 1, {"engine": 0}), ("ReactorArkode", 1, {})):
+                                ("ReactorCvode", 1, {"engine": 0}), ("ReactorArkode", 1, {}),
+                                ("ReactorCvode", 1, {"warps_per_block": 12})):
         r = Reactor("drm19", integ)
         with pytest.raises(_lib.EngineError):
             r.init(rtype, 4, eos=1, **extra)
