@@ -999,15 +999,29 @@ __global__ void k_energy_update(double* rX, const double* rXs, double dt, int n)
 }
 
 #ifdef PPB_PHASE_TIMERS
-int phase_cycles_9(unsigned long long*, int);
-int phase_cycles_21(unsigned long long*, int);
-int phase_cycles_53(unsigned long long*, int);
-int phase_cycles_88(unsigned long long*, int);
+// the counters of every kernel object (one per species count and part)
+#define PPB_PHASE_DECL(NS)                                                                                        \
+  int phase_cycles_##NS##_p0(unsigned long long*, int);                                                           \
+  int phase_cycles_##NS##_p1(unsigned long long*, int);                                                           \
+  int phase_cycles_##NS##_p2(unsigned long long*, int);                                                           \
+  int phase_cycles_##NS##_p3(unsigned long long*, int);                                                           \
+  int phase_cycles_##NS##_p4(unsigned long long*, int);
+#define PPB_PHASE_FNS(NS) phase_cycles_##NS##_p0, phase_cycles_##NS##_p1, phase_cycles_##NS##_p2, \
+                          phase_cycles_##NS##_p3, phase_cycles_##NS##_p4
+PPB_PHASE_DECL(9)
+PPB_PHASE_DECL(13)
+PPB_PHASE_DECL(21)
+PPB_PHASE_DECL(22)
+PPB_PHASE_DECL(39)
+PPB_PHASE_DECL(53)
+PPB_PHASE_DECL(88)
 
 int phase_cycles(unsigned long long* out, int reset)
 {
   for (int q = 0; q < PH_COUNT; q++) out[q] = 0;
-  int (*fns[4])(unsigned long long*, int) = {phase_cycles_9, phase_cycles_21, phase_cycles_53, phase_cycles_88};
+  int (*fns[])(unsigned long long*, int) = {PPB_PHASE_FNS(9),  PPB_PHASE_FNS(13), PPB_PHASE_FNS(21),
+                                            PPB_PHASE_FNS(22), PPB_PHASE_FNS(39), PPB_PHASE_FNS(53),
+                                            PPB_PHASE_FNS(88)};
   for (auto fn : fns) {
     unsigned long long part[PH_COUNT];
     const int e = fn(part, reset);

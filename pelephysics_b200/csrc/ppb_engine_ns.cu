@@ -489,8 +489,9 @@ void PPB_CAT4(launch_plain_, PPB_NS, _p, 3)(const DevMech& M, const Options& o, 
 }
 #endif
 
-#if defined(PPB_PHASE_TIMERS) && PPB_PART == 0
-int PPB_CAT(phase_cycles_, PPB_NS)(unsigned long long* out, int reset)
+#if defined(PPB_PHASE_TIMERS)
+// this object's copy of the phase counters (each part has its own)
+int PPB_CAT4(phase_cycles_, PPB_NS, _p, PPB_PART)(unsigned long long* out, int reset)
 {
   cudaError_t e = cudaMemcpyFromSymbol(out, g_phase_cycles, sizeof(unsigned long long) * PH_COUNT);
   if (e == cudaSuccess && reset) {
