@@ -315,6 +315,51 @@ __device__ int lu_factor(const Team<TEAM>& tm, LT* A, int n, int* piv)
 {
   for (int k = 0; k < n; k++) {
     LT* colk = A + k * n;
+    if constexpr (TEAM == 32) {
+      if (n - k <= 32) {
+        // one row per lane (row k + lane): the largest magnitude by a max
+        // reduction, the first row holding it by a ballot (rows in lane
+        // order), its value by one shuffle, so the reciprocal overlaps the
+        // row swap; a NaN entry never wins (its lane stays at -1)
+        const int i = k + tm.lane;
+        const LT a = i < n ? colk[i] : (LT)0;
+        const double v = fabs((double)a);
+        const double mine = (i < n && v > -1.0) ? v : -1.0;
+        double mx = mine;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        const unsigned hit = __ballot_sync(0xffffffffu, i < n && mine == mx);
+        const int src = hit ? __ffs(hit) - 1 : 0;
+        const LT pv = __shfl_sync(0xffffffffu, a, src);
+        const int l = k + src;
+        if (!(mx > 0.0) || !hit) {
+          tm.sync();
+          return k + 1;
+        }
+        if (tm.lane == 0) piv[k] = l;
+        const LT mult = (LT)1.0 / pv;
+        if (l != k) {
+          for (int j = tm.lane; j < n; j += TEAM) {
+            const LT t = A[j * n + l];
+            A[j * n + l] = A[j * n + k];
+            A[j * n + k] = t;
+          }
+        }
+        tm.sync();
+        if (i > k && i < n) {
+          // the lane scales its own row's multiplier and keeps it
+          const LT lik = colk[i] * mult;
+          colk[i] = lik;
+#pragma unroll 4
+          for (int j = k + 1; j < n; j++) {
+            const LT akj = A[j * n + k];
+            if (akj != (LT)0) A[j * n + i] -= akj * lik;
+          }
+        }
+        tm.sync();
+        continue;
+      }
+    }
     double best = -1.0;
     int bi = n;
     for (int i = k + tm.lane; i < n; i += TEAM) {
