@@ -107,7 +107,13 @@ __device__ __forceinline__ void rendezvous(int* rv, int cycles)
     const unsigned g = (unsigned)atomicAdd(&rv[0], 1) >> 16;
     rendezvous_try_release(rv);
     const long long t0 = clock64();
-    while (((unsigned)v[0] >> 16) == g && clock64() - t0 < cycles) __nanosleep(32);
+    // polls back off from 32 to 256 ns: a waiting warp's polls take issue
+    // slots from the warps still working
+    unsigned ns = 32;
+    while (((unsigned)v[0] >> 16) == g && clock64() - t0 < cycles) {
+      __nanosleep(ns);
+      if (ns < 256) ns <<= 1;
+    }
   }
   __syncwarp();
 }
