@@ -46,10 +46,10 @@ FLOPS_JAC = {"drm19": 22908.0}
 CPU_SAMPLE = 8192  # cells of the field integrated by the CPU baseline
 # DRAM bytes (read + write) per cell of one launch of the tuned kernel,
 # from an ncu capture of the same kernel (16 warps per block, rendezvous on)
-# on the 16^3 field (4096 cells: 2.198 MB + 0.631 MB);
+# on the 16^3 field (4096 cells: 1.890 MB + 0.462 MB);
 # profiles/k_react_team_drm19_16cubed.md has the command.  Scaled by the
 # cells of a launch (the traffic grows with them).
-TRAFFIC_PER_CELL = (2.197760e6 + 0.630784e6) / 4096
+TRAFFIC_PER_CELL = (1.889536e6 + 0.462336e6) / 4096
 
 
 def log(*a):
