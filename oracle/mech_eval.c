@@ -14,6 +14,7 @@
 #include "../pelephysics_b200/csrc/mech/mech_CH4_lean_qss.h"
 #include "../pelephysics_b200/csrc/mech/mech_C1-C2-NO_qss.h"
 #include "../pelephysics_b200/csrc/mech/mech_LuEthylene_qss.h"
+#include "../pelephysics_b200/csrc/mech/mech_grimech30.h"
 
 const PPBMechTables* ppo_mech(const char* name)
 {
@@ -24,6 +25,7 @@ const PPBMechTables* ppo_mech(const char* name)
   if (!strcmp(name, "CH4_lean_qss")) return &ppbm_CH4_lean_qss;
   if (!strcmp(name, "C1-C2-NO_qss")) return &ppbm_C1_C2_NO_qss;
   if (!strcmp(name, "LuEthylene_qss")) return &ppbm_LuEthylene_qss;
+  if (!strcmp(name, "grimech30")) return &ppbm_grimech30;
   return 0;
 }
 

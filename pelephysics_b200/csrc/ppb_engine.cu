@@ -24,6 +24,7 @@
 #include "mech/mech_CH4_lean_qss.h"
 #include "mech/mech_C1-C2-NO_qss.h"
 #include "mech/mech_LuEthylene_qss.h"
+#include "mech/mech_grimech30.h"
 
 namespace ppb {
 
@@ -36,6 +37,7 @@ const PPBMechTables* find_mechanism(const char* name)
   if (!strcmp(name, "CH4_lean_qss")) return &ppbm_CH4_lean_qss;
   if (!strcmp(name, "C1-C2-NO_qss")) return &ppbm_C1_C2_NO_qss;
   if (!strcmp(name, "LuEthylene_qss")) return &ppbm_LuEthylene_qss;
+  if (!strcmp(name, "grimech30")) return &ppbm_grimech30;
   return nullptr;
 }
 

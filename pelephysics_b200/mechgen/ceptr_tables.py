@@ -46,7 +46,8 @@ from collections import Counter, OrderedDict
 import numpy as np
 import yaml
 
-MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "CH4_lean_qss", "C1-C2-NO_qss", "LuEthylene_qss"]
+MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "CH4_lean_qss", "C1-C2-NO_qss", "LuEthylene_qss",
+         "grimech30"]
 
 RC = 1.98721558317399615845  # cal/mol/K
 ATOMIC_WEIGHTS = {

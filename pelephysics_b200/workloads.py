@@ -53,6 +53,7 @@ FUELS = {
     "CH4_lean_qss": ("CH4", 2.0),
     "C1-C2-NO_qss": ("CH4", 2.0),
     "LuEthylene_qss": ("C2H4", 3.0),
+    "grimech30": ("CH4", 2.0),
 }
 
 

@@ -12,7 +12,7 @@ mechanism's productionRate with the QSS concentrations it solves.  The .npz file
 are the committed fixtures the tests compare the CPU oracle and the CUDA
 kernels against.
 
-Usage: python tests/golden/make_golden.py [point|transport|srk|qss]   (default all)
+Usage: python tests/golden/make_golden.py [point|transport|srk|qss|<mech>]   (default all)
 """
 
 import os
@@ -25,7 +25,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import pyoracle as po  # noqa: E402
 
-POINTS = {"LiDryer": 16, "drm19": 16, "dodecane_lu": 6, "heptane_lu_88sk": 4}
+POINTS = {"LiDryer": 16, "drm19": 16, "dodecane_lu": 6, "heptane_lu_88sk": 4, "grimech30": 8}
 
 
 def states(nsp, npts, seed):
@@ -152,7 +152,10 @@ def main():
         qss_main()
     if what in ("transport", "srk", "qss"):
         return
+    # `python make_golden.py <mech>` writes that mechanism's point file only
     for seed, (mech, npts) in enumerate(POINTS.items()):
+        if what not in ("all", "point") and what != mech:
+            continue
         R = po.Ref(mech)
         N = R.nsp
         T, sc, Y = states(N, npts, 1000 + seed)

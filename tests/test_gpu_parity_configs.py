@@ -116,3 +116,20 @@ def test_lidryer_16cubed_vs_reference_kernels(cuda, oracle, engine, max_order):
     y_ref = _oracle(oracle, cells, idx, opts)
     y = _gpu_react(cells, dict(engine=engine, **opts))
     _check(oracle, cells, idx, y, y_ref, opts)
+
+
+@pytest.mark.parametrize("engine", ["tuned", "tuned_fp32", "plain"])
+def test_grimech30_premixed_vs_reference_kernels(cuda, oracle, engine):
+    """GRI-Mech 3.0 (53 species, 325 reactions: Lindemann and Troe fall-off,
+    explicit third bodies; Mechanisms/grimech30) as one more mechanism on
+    the 53-species kernels: 256 premixed CH4-air e-reactors, T 1100-2100 K,
+    phi 0.5-1.5, 1 atm, dt 1e-5 s, rtol = atol = 1e-10, against the oracle
+    integrator over the reference's compiled grimech30 kernels."""
+    cells = wl.premix_cells("grimech30", 256, 8, 1100.0, 1000.0, 0.5, 1.0, reactor_type=1, dt=1e-5)
+    idx = np.arange(256)
+    opts = dict(OPTS, engine=0 if engine == "plain" else 1)
+    if engine == "tuned_fp32":
+        opts["lu_fp32"] = 1
+    y_gpu = _gpu_react(cells, opts)
+    y_ref = _oracle(oracle, cells, idx, OPTS)
+    _check(oracle, cells, idx, y_gpu, y_ref, OPTS)

@@ -18,7 +18,7 @@ from tests.helpers import premix_oracle
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk"]
+MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "grimech30"]
 
 
 def load(mech):
@@ -85,7 +85,7 @@ def test_t_from_energy(cuda, mech, team):
         np.testing.assert_allclose(T.cpu().numpy(), g[key], rtol=1e-12)
 
 
-@pytest.mark.parametrize("mech", ["LiDryer", "drm19", "dodecane_lu"])
+@pytest.mark.parametrize("mech", ["LiDryer", "drm19", "dodecane_lu", "grimech30"])
 @pytest.mark.parametrize("team", [1, 32])
 @pytest.mark.parametrize("rtype", [1, 2])
 def test_reactor_rhs(cuda, oracle, mech, team, rtype):
