@@ -120,7 +120,7 @@ void ppb_default_options(ppb_options* opt);
 const char* ppb_last_error(void);
 
 /* Mechanisms compiled into the library (LiDryer, drm19, dodecane_lu,
- * heptane_lu_88sk, grimech30, and the QSS mechanisms CH4_lean_qss, C1-C2-NO_qss and
+ * heptane_lu_88sk, grimech30, FFCM1_Red, chem-H, and the QSS mechanisms CH4_lean_qss, C1-C2-NO_qss and
  * LuEthylene_qss, whose species in quasi-steady state are not counted: their
  * productionRate solves them first, as their mechanism.H does): returns the
  * number of species and reactions of `mechanism`, or PPB_E_MECH. */

@@ -16,7 +16,7 @@ if [ ! -d "$REF/Mechanisms" ]; then
   exit 0
 fi
 printf '%s\n' "$REF" > "$OUT/reference_root"
-for mech in LiDryer drm19 dodecane_lu heptane_lu_88sk CH4_lean_qss C1-C2-NO_qss LuEthylene_qss grimech30; do
+for mech in LiDryer drm19 dodecane_lu heptane_lu_88sk CH4_lean_qss C1-C2-NO_qss LuEthylene_qss grimech30 FFCM1_Red chem-H; do
   src="$REF/Mechanisms/$mech/mechanism.H"
   lib="$OUT/libref_${mech}.so"
   if [ -f "$lib" ] && [ "$lib" -nt "$src" ] && [ "$lib" -nt "$HERE/ref_wrap.cpp" ]; then

@@ -15,6 +15,8 @@
 #include "../pelephysics_b200/csrc/mech/mech_C1-C2-NO_qss.h"
 #include "../pelephysics_b200/csrc/mech/mech_LuEthylene_qss.h"
 #include "../pelephysics_b200/csrc/mech/mech_grimech30.h"
+#include "../pelephysics_b200/csrc/mech/mech_FFCM1_Red.h"
+#include "../pelephysics_b200/csrc/mech/mech_chem-H.h"
 
 const PPBMechTables* ppo_mech(const char* name)
 {
@@ -26,6 +28,8 @@ const PPBMechTables* ppo_mech(const char* name)
   if (!strcmp(name, "C1-C2-NO_qss")) return &ppbm_C1_C2_NO_qss;
   if (!strcmp(name, "LuEthylene_qss")) return &ppbm_LuEthylene_qss;
   if (!strcmp(name, "grimech30")) return &ppbm_grimech30;
+  if (!strcmp(name, "FFCM1_Red")) return &ppbm_FFCM1_Red;
+  if (!strcmp(name, "chem-H")) return &ppbm_chem_H;
   return 0;
 }
 

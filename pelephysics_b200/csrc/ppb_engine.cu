@@ -25,6 +25,8 @@
 #include "mech/mech_C1-C2-NO_qss.h"
 #include "mech/mech_LuEthylene_qss.h"
 #include "mech/mech_grimech30.h"
+#include "mech/mech_FFCM1_Red.h"
+#include "mech/mech_chem-H.h"
 
 namespace ppb {
 
@@ -38,6 +40,8 @@ const PPBMechTables* find_mechanism(const char* name)
   if (!strcmp(name, "C1-C2-NO_qss")) return &ppbm_C1_C2_NO_qss;
   if (!strcmp(name, "LuEthylene_qss")) return &ppbm_LuEthylene_qss;
   if (!strcmp(name, "grimech30")) return &ppbm_grimech30;
+  if (!strcmp(name, "FFCM1_Red")) return &ppbm_FFCM1_Red;
+  if (!strcmp(name, "chem-H")) return &ppbm_chem_H;
   return nullptr;
 }
 

@@ -47,7 +47,7 @@ import numpy as np
 import yaml
 
 MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "CH4_lean_qss", "C1-C2-NO_qss", "LuEthylene_qss",
-         "grimech30"]
+         "grimech30", "FFCM1_Red", "chem-H"]
 
 RC = 1.98721558317399615845  # cal/mol/K
 ATOMIC_WEIGHTS = {

@@ -54,6 +54,8 @@ FUELS = {
     "C1-C2-NO_qss": ("CH4", 2.0),
     "LuEthylene_qss": ("C2H4", 3.0),
     "grimech30": ("CH4", 2.0),
+    "FFCM1_Red": ("CH4", 2.0),
+    "chem-H": ("H2", 0.5),
 }
 
 

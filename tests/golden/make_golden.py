@@ -25,7 +25,8 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import pyoracle as po  # noqa: E402
 
-POINTS = {"LiDryer": 16, "drm19": 16, "dodecane_lu": 6, "heptane_lu_88sk": 4, "grimech30": 8}
+POINTS = {"LiDryer": 16, "drm19": 16, "dodecane_lu": 6, "heptane_lu_88sk": 4, "grimech30": 8,
+          "FFCM1_Red": 12, "chem-H": 12}
 
 
 def states(nsp, npts, seed):

@@ -4,7 +4,8 @@ import numpy as np
 
 FUELS = {"LiDryer": ("H2", 0.5), "drm19": ("CH4", 2.0), "dodecane_lu": ("NC12H26", 18.5),
          "heptane_lu_88sk": ("nc7h16", 11.0), "CH4_lean_qss": ("CH4", 2.0), "C1-C2-NO_qss": ("CH4", 2.0),
-         "LuEthylene_qss": ("C2H4", 3.0), "grimech30": ("CH4", 2.0)}
+         "LuEthylene_qss": ("C2H4", 3.0), "grimech30": ("CH4", 2.0),
+         "FFCM1_Red": ("CH4", 2.0), "chem-H": ("H2", 0.5)}
 P_ATM = 1013250.0
 
 

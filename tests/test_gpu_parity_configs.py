@@ -118,15 +118,28 @@ def test_lidryer_16cubed_vs_reference_kernels(cuda, oracle, engine, max_order):
     _check(oracle, cells, idx, y, y_ref, opts)
 
 
+
+# Mechanisms of the reference that run on kernels compiled for another
+# mechanism of the same species count: (mechanism, cells, T0, dT, phi0, dphi)
+# of premixed e-reactors at 1 atm, dt 1e-5 s.
+MORE_MECHS = {
+    "grimech30": (256, 1100.0, 1000.0, 0.5, 1.0),  # GRI-Mech 3.0, 53 species, 325 reactions
+    "FFCM1_Red": (256, 1100.0, 1000.0, 0.5, 1.0),  # 21 species, 124 reactions
+    "chem-H": (256, 1000.0, 400.0, 0.5, 1.5),  # 9 species, 27 reactions
+}
+
+
 @pytest.mark.parametrize("engine", ["tuned", "tuned_fp32", "plain"])
-def test_grimech30_premixed_vs_reference_kernels(cuda, oracle, engine):
-    """GRI-Mech 3.0 (53 species, 325 reactions: Lindemann and Troe fall-off,
-    explicit third bodies; Mechanisms/grimech30) as one more mechanism on
-    the 53-species kernels: 256 premixed CH4-air e-reactors, T 1100-2100 K,
-    phi 0.5-1.5, 1 atm, dt 1e-5 s, rtol = atol = 1e-10, against the oracle
-    integrator over the reference's compiled grimech30 kernels."""
-    cells = wl.premix_cells("grimech30", 256, 8, 1100.0, 1000.0, 0.5, 1.0, reactor_type=1, dt=1e-5)
-    idx = np.arange(256)
+@pytest.mark.parametrize("mech", list(MORE_MECHS))
+def test_more_mechanisms_premixed_vs_reference_kernels(cuda, oracle, mech, engine):
+    """A mechanism with its own tables on the kernels of its species count
+    (Lindemann and Troe fall-off and explicit third bodies among its
+    reactions): premixed e-reactors at rtol = atol = 1e-10 against the
+    oracle integrator over the reference's compiled kernels of that
+    mechanism (Mechanisms/<mech>/mechanism.H)."""
+    n, T0, dT, phi0, dphi = MORE_MECHS[mech]
+    cells = wl.premix_cells(mech, n, 8, T0, dT, phi0, dphi, reactor_type=1, dt=1e-5)
+    idx = np.arange(n)
     opts = dict(OPTS, engine=0 if engine == "plain" else 1)
     if engine == "tuned_fp32":
         opts["lu_fp32"] = 1

@@ -18,7 +18,7 @@ from tests.helpers import premix_oracle
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "grimech30"]
+MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "grimech30", "FFCM1_Red", "chem-H"]
 
 
 def load(mech):

@@ -11,7 +11,7 @@ import pytest
 from tests.helpers import premix_oracle
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "grimech30"]
+MECHS = ["LiDryer", "drm19", "dodecane_lu", "heptane_lu_88sk", "grimech30", "FFCM1_Red", "chem-H"]
 
 
 def load(mech):
